@@ -1,0 +1,85 @@
+// Shared definitions for the bbhx_b200 CUDA kernels (sm_100a).
+//
+// Constants are the reference's (src/bbhx/cutils/constants.h:6-60); they must match
+// bit-for-bit for parity.  Complex numbers are a plain {re, im} pair of doubles (or
+// floats) laid out like numpy complex128 / complex64, so caller buffers can be
+// reinterpreted without copies.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace bbhx {
+
+constexpr double MSUN_SI = 1.98848e+30;
+constexpr double YRSID_SI = 31558149.763545603;
+constexpr double AU_SI = 149597870700.0;
+constexpr double C_SI = 299792458.;
+constexpr double MTSUN_SI = 4.925491025873693e-06;
+constexpr double MRSUN_SI = 1476.6250615036158;
+constexpr double PC_SI = 3.0856775814913674e+16;
+constexpr double PI = 3.141592653589793238462643383279502884;
+constexpr double PI_2 = 1.570796326794896619231321691639751442;
+constexpr double PI_4 = 0.785398163397448309615660845819875721;
+constexpr double TWO_PI = 6.283185307179586476925286766559005768;
+constexpr double GAMMA_E = 0.577215664901532860606512090082402431;
+constexpr double SQRT2 = 1.414213562373095048801688724209698079;
+constexpr double INVSQRT3 = 0.577350269189625764509148780501957455;
+constexpr double INVSQRT6 = 0.408248290463863016366214012450981898;
+constexpr double Omega0 = 1.9909865927683788e-07;
+
+// status codes returned by every C-ABI entry point
+enum Status : int {
+  OK = 0,
+  ERR_BAD_ARG = 1,
+  ERR_CUDA = 2,
+  ERR_TIMEOUT = 3,
+  ERR_NONFINITE = 4,
+  ERR_NO_ORBITS = 5,
+  ERR_TOO_LARGE = 6,
+};
+
+struct cplx {
+  double re, im;
+};
+struct cplxf {
+  float re, im;
+};
+
+__host__ __device__ __forceinline__ cplx mk(double r, double i) { return cplx{r, i}; }
+__host__ __device__ __forceinline__ cplx operator+(cplx a, cplx b) { return {a.re + b.re, a.im + b.im}; }
+__host__ __device__ __forceinline__ cplx operator-(cplx a, cplx b) { return {a.re - b.re, a.im - b.im}; }
+__host__ __device__ __forceinline__ cplx operator*(cplx a, cplx b) {
+  return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+__host__ __device__ __forceinline__ cplx operator*(double s, cplx a) { return {s * a.re, s * a.im}; }
+__host__ __device__ __forceinline__ cplx operator*(cplx a, double s) { return {s * a.re, s * a.im}; }
+__host__ __device__ __forceinline__ cplx conj(cplx a) { return {a.re, -a.im}; }
+__host__ __device__ __forceinline__ cplx times_i(cplx a) { return {-a.im, a.re}; }
+__device__ __forceinline__ cplx expi(double x) {
+  double s, c;
+  sincos(x, &s, &c);
+  return {c, s};
+}
+__device__ __forceinline__ double cabs(cplx a) { return hypot(a.re, a.im); }
+
+__host__ __device__ __forceinline__ cplxf operator+(cplxf a, cplxf b) { return {a.re + b.re, a.im + b.im}; }
+__host__ __device__ __forceinline__ cplxf operator*(cplxf a, cplxf b) {
+  return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+
+// Phase reduction to [-pi, pi]: k = rint(x / 2pi), then x - k*2pi with 2pi split into a
+// double (hi) and its residual (lo); each FMA forms k*part exactly before its single
+// rounding, so the reduced angle is good to a few ulp of pi for |x| far beyond the
+// 1e7 rad that waveform phases reach.
+__device__ __forceinline__ double reduce_2pi(double x) {
+  const double INV2PI = 0.15915494309189533577;
+  const double TWO_PI_HI = 6.28318530717958623200e+00;   // 2*pi rounded to double
+  const double TWO_PI_LO = 2.44929359829470635446e-16;   // 2*pi - TWO_PI_HI
+  double k = rint(x * INV2PI);
+  double r = fma(-k, TWO_PI_HI, x);
+  r = fma(-k, TWO_PI_LO, r);
+  return r;
+}
+
+}  // namespace bbhx

@@ -1,0 +1,50 @@
+// Host-side helpers shared by the C-ABI translation units: error capture and status codes.
+#pragma once
+
+#include <cstdarg>
+#include <cstdio>
+#include <cuda_runtime.h>
+
+#include "bbhx_common.cuh"
+
+namespace bbhx {
+
+// Last error message of the calling host thread (bbhx_last_error_string()).
+void set_error(const char* fmt, ...);
+const char* get_error();
+
+inline int cuda_status(cudaError_t e, const char* where) {
+  if (e == cudaSuccess) return OK;
+  set_error("%s: %s", where, cudaGetErrorString(e));
+  return ERR_CUDA;
+}
+
+#define BBHX_CHECK_CUDA(expr)                                   \
+  do {                                                          \
+    cudaError_t _e = (expr);                                    \
+    if (_e != cudaSuccess) return ::bbhx::cuda_status(_e, #expr); \
+  } while (0)
+
+#define BBHX_REQUIRE(cond, ...)          \
+  do {                                   \
+    if (!(cond)) {                       \
+      ::bbhx::set_error(__VA_ARGS__);    \
+      return ::bbhx::ERR_BAD_ARG;        \
+    }                                    \
+  } while (0)
+
+inline int launch_status(const char* kernel) {
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) return OK;
+  set_error("launch of %s failed: %s", kernel, cudaGetErrorString(e));
+  return ERR_CUDA;
+}
+
+inline unsigned int grid_for(long long n, int threads, int max_blocks = 148 * 32) {
+  long long b = (n + threads - 1) / threads;
+  if (b < 1) b = 1;
+  if (b > max_blocks) b = max_blocks;
+  return (unsigned int)b;
+}
+
+}  // namespace bbhx

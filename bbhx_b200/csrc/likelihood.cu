@@ -1,0 +1,489 @@
+// Likelihood kernels.
+//
+// Reference interfaces replaced (src/bbhx/cutils/Likelihood.hh:6-13):
+//   direct_like (Likelihood.cu:356-471): noise-weight each stored template in place, then
+//               6 cuBLAS Zdotc per binary, each followed by a stream sync; results
+//               accumulated into HOST d_h / h_h.
+//   hdyn        (Likelihood.cu:20-120 GPU form): relative-binning sums, one thread per binary.
+// New (no reference counterpart, same result as InterpTDI + direct_like):
+//   bbhx_direct_like_fused: evaluates the splines on the data grid, sums the modes,
+//   noise-weights and reduces <d|h>, <h|h> without ever storing a template.
+//
+// Reductions are deterministic: per-(tile, binary) partials in FP64, then a fixed-order sum.
+#include <vector>
+
+#include "capi_internal.cuh"
+#include "spline_eval.cuh"
+
+namespace bbhx {
+
+// ---------------------------------------------------------------------------- direct_like
+struct DirectJob {
+  cplx* tmpl;
+  int start, len;
+  long long part0;  // first partial slot of this binary
+  int nparts;
+};
+
+constexpr int DL_CHUNK = 2048;
+
+__global__ void k_direct_like_partials(const DirectJob* jobs, const cplx* __restrict__ data,
+                                       const double* __restrict__ noise, int N, double* partials) {
+  const int b = blockIdx.y;
+  const DirectJob J = jobs[b];
+  __shared__ double red[3][32];
+  for (int part = blockIdx.x; part < J.nparts; part += gridDim.x) {
+    int i0 = part * DL_CHUNK;
+    int i1 = min(i0 + DL_CHUNK, J.len);
+    double dr = 0, di = 0, hh = 0;
+    for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+      for (int ch = 0; ch < 3; ++ch) {
+        long long gi = (long long)ch * N + J.start + i;
+        double w = noise[gi];
+        cplx h = J.tmpl[(long long)ch * J.len + i] * w;  // weighted in place (reference side effect)
+        J.tmpl[(long long)ch * J.len + i] = h;
+        cplx d = data[gi];
+        dr += d.re * h.re + d.im * h.im;  // conj(d) * h
+        di += d.re * h.im - d.im * h.re;
+        hh += h.re * h.re + h.im * h.im;
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      dr += __shfl_xor_sync(0xffffffffu, dr, o);
+      di += __shfl_xor_sync(0xffffffffu, di, o);
+      hh += __shfl_xor_sync(0xffffffffu, hh, o);
+    }
+    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) {
+      red[0][w] = dr;
+      red[1][w] = di;
+      red[2][w] = hh;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double a = 0, bb = 0, c = 0;
+      for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+        a += red[0][k];
+        bb += red[1][k];
+        c += red[2][k];
+      }
+      double* P = partials + 3 * (J.part0 + part);
+      P[0] = a;
+      P[1] = bb;
+      P[2] = c;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void k_sum_partials(const DirectJob* jobs, const double* partials, double* out, int B) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < B; b += gridDim.x * blockDim.x) {
+    double a = 0, c = 0, h = 0;
+    for (int p = 0; p < jobs[b].nparts; ++p) {
+      const double* P = partials + 3 * (jobs[b].part0 + p);
+      a += P[0];
+      c += P[1];
+      h += P[2];
+    }
+    out[4 * b + 0] = 4.0 * a;
+    out[4 * b + 1] = 4.0 * c;
+    out[4 * b + 2] = 4.0 * h;
+    out[4 * b + 3] = 0.0;
+  }
+}
+
+// ---------------------------------------------------------------------------- hdyn
+// residuals r[(j*3 + ch)*B + b], constants [(k*3 + ch)*L + j] (k = A0, A1, B0, B1)
+__global__ void k_hdyn(cplx* d_h, cplx* h_h, const cplx* __restrict__ r,
+                       const cplx* __restrict__ K, const double* __restrict__ f, int B, int L,
+                       int nch) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < B; b += gridDim.x * blockDim.x) {
+    cplx dh = mk(0, 0);
+    double hh_re = 0.0, hh_im = 0.0;
+    for (int ch = 0; ch < nch; ++ch) {
+      cplx prev = r[((long long)0 * nch + ch) * B + b];
+      double fprev = f[0];
+      for (int j = 1; j < L; ++j) {
+        cplx cur = r[((long long)j * nch + ch) * B + b];
+        double fj = f[j];
+        if (fprev != 0.0) {
+          double df = fj - fprev;
+          cplx r1 = mk((cur.re - prev.re) / df, (cur.im - prev.im) / df);
+          double fmid = (fj + fprev) / 2.0;
+          cplx r0 = cur - r1 * (fj - fmid);
+          cplx A0 = K[((long long)0 * nch + ch) * L + j];
+          cplx A1 = K[((long long)1 * nch + ch) * L + j];
+          cplx B0 = K[((long long)2 * nch + ch) * L + j];
+          cplx B1 = K[((long long)3 * nch + ch) * L + j];
+          dh = dh + A0 * conj(r0) + A1 * conj(r1);
+          double mag2 = r0.re * r0.re + r0.im * r0.im;
+          double re01 = r0.re * r1.re + r0.im * r1.im;  // Re(r0 conj(r1))
+          hh_re += B0.re * mag2 + 2.0 * B1.re * re01;
+          hh_im += B0.im * mag2 + 2.0 * B1.im * re01;
+        }
+        prev = cur;
+        fprev = fj;
+      }
+    }
+    d_h[b] = dh;
+    h_h[b] = mk(hh_re, hh_im);
+  }
+}
+
+// ---------------------------------------------------------------------------- fused direct
+// Support of each binary on the data grid (waveformbuild.py:136-177): [start, start+len) with
+// start = searchsorted(f, min x, 'right'), end = searchsorted(f, max x, 'right').
+__global__ void k_support(const double* __restrict__ x, int M, int L, int B,
+                          const double* __restrict__ data_freqs, int N, int* start, int* len) {
+  int b = blockIdx.x;
+  double lo = 1e300, hi = -1e300;
+  for (int t = threadIdx.x; t < M * L; t += blockDim.x) {
+    double v = x[(long long)b * M * L + t];
+    lo = fmin(lo, v);
+    hi = fmax(hi, v);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+  __shared__ double slo[32], shi[32];
+  int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    slo[w] = lo;
+    shi[w] = hi;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < (int)(blockDim.x >> 5); ++k) {
+      lo = fmin(lo, slo[k]);
+      hi = fmax(hi, shi[k]);
+    }
+    // searchsorted right: number of entries <= v
+    int a = 0, c = N;
+    while (a < c) {
+      int mid = (a + c) >> 1;
+      if (data_freqs[mid] <= lo) a = mid + 1; else c = mid;
+    }
+    int s = a;
+    a = s;
+    c = N;
+    while (a < c) {
+      int mid = (a + c) >> 1;
+      if (data_freqs[mid] <= hi) a = mid + 1; else c = mid;
+    }
+    start[b] = s;
+    len[b] = a - s;
+  }
+}
+
+constexpr int FD_WARPS = 4;
+constexpr int FD_K = 4;                          // bins per lane per warp chunk
+constexpr int FD_WARP_BINS = 32 * FD_K;          // 128
+constexpr int FD_TILE = FD_WARPS * FD_WARP_BINS;  // 512
+
+struct FusedArgs {
+  const double* data_freqs;
+  const cplx* data;     // [3, N] noise-weighted data
+  const double* noise;  // [3, N] sqrt(df / S)
+  int N;
+  const double* x;  // [B, M, L]
+  const double* y;  // [9, B, M, L]
+  const double* c1;
+  const double* c2;
+  const double* c3;
+  const double* t_start;
+  const double* t_end;
+  const int* sup_start;
+  const int* sup_len;
+  int B, M, L;
+  int ntiles;
+  double* partials;  // [ntiles * B][3]
+};
+
+__global__ void __launch_bounds__(FD_WARPS * 32) k_direct_fused(FusedArgs A) {
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  __shared__ double red[3][FD_WARPS];
+  const long long nitems = (long long)A.ntiles * A.B;
+  const long long BML = (long long)A.B * A.M * A.L;
+  for (long long q = blockIdx.x; q < nitems; q += gridDim.x) {
+    const int tile = (int)(q / A.B);
+    const int b = (int)(q % A.B);
+    const int s0 = A.sup_start[b];
+    const int s1 = s0 + A.sup_len[b];
+    const int t0 = tile * FD_TILE;
+    if (t0 >= s1 || t0 + FD_TILE <= s0) {
+      if (threadIdx.x == 0) {
+        double* P = A.partials + 3 * q;
+        P[0] = 0.0; P[1] = 0.0; P[2] = 0.0;
+      }
+      continue;
+    }
+    const int c0 = t0 + warp * FD_WARP_BINS;  // warp chunk start
+    const double ts = A.t_start[b], te = A.t_end[b];
+    double fbin[FD_K];
+    bool valid[FD_K];
+#pragma unroll
+    for (int j = 0; j < FD_K; ++j) {
+      int i = c0 + 32 * j + lane;
+      valid[j] = (i >= s0) && (i < s1);
+      fbin[j] = valid[j] ? A.data_freqs[i] : 0.0;
+    }
+    cplx acc[FD_K][3];
+#pragma unroll
+    for (int j = 0; j < FD_K; ++j)
+      for (int c = 0; c < 3; ++c) acc[j][c] = mk(0.0, 0.0);
+
+    // first valid bin of this warp chunk (all lanes agree)
+    int first = max(c0, s0);
+    bool warp_active = first < min(c0 + FD_WARP_BINS, s1);
+    if (warp_active) {
+      double ffirst = A.data_freqs[first];
+      for (int m = 0; m < A.M; ++m) {
+        const long long rowi = (long long)b * A.M + m;
+        const double* xrow = A.x + rowi * A.L;
+        int k = warp_segment_search(xrow, A.L, ffirst);
+        int kc = -2;  // cached segment
+        double cx = 0.0, cy[9], cc1[9], cc2[9], cc3[9];
+#pragma unroll
+        for (int j = 0; j < FD_K; ++j) {
+          if (!valid[j]) continue;
+          double f = fbin[j];
+          while (k + 1 < A.L && __ldg(xrow + k + 1) <= f) ++k;
+          if (k < 0 || k >= A.L - 1) continue;
+          if (k != kc) {
+            kc = k;
+            cx = __ldg(xrow + k);
+#pragma unroll
+            for (int p = 0; p < 9; ++p) {
+              long long o = p * BML + rowi * A.L + k;
+              cy[p] = __ldg(A.y + o);
+              cc1[p] = __ldg(A.c1 + o);
+              cc2[p] = __ldg(A.c2 + o);
+              cc3[p] = __ldg(A.c3 + o);
+            }
+          }
+          double u = f - cx;
+          double u2 = u * u, u3 = u2 * u;
+          double v[9];
+#pragma unroll
+          for (int p = 0; p < 9; ++p) v[p] = cy[p] + cc1[p] * u + cc2[p] * u2 + cc3[p] * u3;
+          if (!tf_gate(v[2], ts, te)) continue;
+          cplx h1, h2, h3;
+          combine_channels(v[0], v[1], mk(v[3], v[4]), mk(v[5], v[6]), mk(v[7], v[8]), h1, h2, h3);
+          acc[j][0] = acc[j][0] + h1;
+          acc[j][1] = acc[j][1] + h2;
+          acc[j][2] = acc[j][2] + h3;
+        }
+      }
+    }
+    double dr = 0.0, di = 0.0, hh = 0.0;
+#pragma unroll
+    for (int j = 0; j < FD_K; ++j) {
+      if (!valid[j]) continue;
+      int i = c0 + 32 * j + lane;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        long long gi = (long long)c * A.N + i;
+        double w = __ldg(A.noise + gi);
+        cplx h = acc[j][c] * w;
+        cplx d = A.data[gi];
+        dr += d.re * h.re + d.im * h.im;
+        di += d.re * h.im - d.im * h.re;
+        hh += h.re * h.re + h.im * h.im;
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      dr += __shfl_xor_sync(0xffffffffu, dr, o);
+      di += __shfl_xor_sync(0xffffffffu, di, o);
+      hh += __shfl_xor_sync(0xffffffffu, hh, o);
+    }
+    if (lane == 0) {
+      red[0][warp] = dr;
+      red[1][warp] = di;
+      red[2][warp] = hh;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double a = 0, c = 0, h = 0;
+#pragma unroll
+      for (int w = 0; w < FD_WARPS; ++w) {
+        a += red[0][w];
+        c += red[1][w];
+        h += red[2][w];
+      }
+      double* P = A.partials + 3 * q;
+      P[0] = a;
+      P[1] = c;
+      P[2] = h;
+    }
+    __syncthreads();
+  }
+}
+
+// out: d_h[b], h_h[b] complex (device); fixed-order sum over the binary's tiles
+__global__ void k_fused_reduce(const double* partials, const int* sup_start, const int* sup_len,
+                               int B, double* d_h, double* h_h) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < B; b += gridDim.x * blockDim.x) {
+    double a = 0, c = 0, h = 0;
+    int s0 = sup_start[b], n = sup_len[b];
+    if (n > 0) {
+      int tlo = s0 / FD_TILE, thi = (s0 + n - 1) / FD_TILE;
+      for (int t = tlo; t <= thi; ++t) {
+        const double* P = partials + 3 * ((long long)t * B + b);
+        a += P[0];
+        c += P[1];
+        h += P[2];
+      }
+    }
+    d_h[2 * b] = 4.0 * a;
+    d_h[2 * b + 1] = 4.0 * c;
+    h_h[2 * b] = 4.0 * h;
+    h_h[2 * b + 1] = 0.0;
+  }
+}
+
+}  // namespace bbhx
+
+using namespace bbhx;
+
+extern "C" {
+
+// Likelihood.hh:11.  d_h, h_h: HOST complex128 arrays, accumulated (+=) like the reference;
+// template_ptrs / inds_start / ind_lengths: HOST arrays.  Templates are noise-weighted in
+// place, as the reference does.
+int bbhx_direct_like(double* d_h, double* h_h, const double* data, const double* noise,
+                     const int64_t* template_ptrs, const int* inds_start, const int* ind_lengths,
+                     int data_stream_length, int num_bin_all, void* stream) {
+  BBHX_REQUIRE(num_bin_all <= 65535, "direct_like handles at most 65535 binaries per call");
+  if (num_bin_all == 0) return OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  std::vector<DirectJob> jobs(num_bin_all);
+  long long nparts = 0;
+  int maxparts = 0;
+  for (int b = 0; b < num_bin_all; ++b) {
+    BBHX_REQUIRE(ind_lengths[b] >= 0 && inds_start[b] >= 0 &&
+                     (long long)inds_start[b] + ind_lengths[b] <= data_stream_length,
+                 "binary %d: data range outside the data grid", b);
+    jobs[b].tmpl = (cplx*)template_ptrs[b];
+    jobs[b].start = inds_start[b];
+    jobs[b].len = ind_lengths[b];
+    jobs[b].part0 = nparts;
+    jobs[b].nparts = (ind_lengths[b] + DL_CHUNK - 1) / DL_CHUNK;
+    nparts += jobs[b].nparts;
+    if (jobs[b].nparts > maxparts) maxparts = jobs[b].nparts;
+  }
+  DirectJob* d_jobs = nullptr;
+  double* d_part = nullptr;
+  double* d_out = nullptr;
+  BBHX_CHECK_CUDA(cudaMallocAsync((void**)&d_jobs, sizeof(DirectJob) * num_bin_all, s));
+  BBHX_CHECK_CUDA(cudaMallocAsync((void**)&d_part, sizeof(double) * 3 * (nparts + 1), s));
+  BBHX_CHECK_CUDA(cudaMallocAsync((void**)&d_out, sizeof(double) * 4 * num_bin_all, s));
+  BBHX_CHECK_CUDA(cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(DirectJob) * num_bin_all,
+                                  cudaMemcpyHostToDevice, s));
+  int st = OK;
+  if (maxparts > 0) {
+    unsigned gx = maxparts > 1024 ? 1024 : maxparts;
+    k_direct_like_partials<<<dim3(gx, num_bin_all), 256, 0, s>>>(d_jobs, (const cplx*)data, noise,
+                                                                 data_stream_length, d_part);
+    st = launch_status("k_direct_like_partials");
+  }
+  if (!st) {
+    k_sum_partials<<<grid_for(num_bin_all, 128), 128, 0, s>>>(d_jobs, d_part, d_out, num_bin_all);
+    st = launch_status("k_sum_partials");
+  }
+  std::vector<double> host(4 * (size_t)num_bin_all);
+  if (!st) {
+    cudaError_t e = cudaMemcpyAsync(host.data(), d_out, sizeof(double) * 4 * num_bin_all,
+                                    cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) st = cuda_status(e, "direct_like result copy");
+  }
+  cudaFreeAsync(d_jobs, s);
+  cudaFreeAsync(d_part, s);
+  cudaFreeAsync(d_out, s);
+  if (st) return st;
+  for (int b = 0; b < num_bin_all; ++b) {
+    d_h[2 * b] += host[4 * b];
+    d_h[2 * b + 1] += host[4 * b + 1];
+    h_h[2 * b] += host[4 * b + 2];
+    h_h[2 * b + 1] += host[4 * b + 3];
+  }
+  return OK;
+}
+
+// Likelihood.hh:6-9 (GPU semantics: every bin j = 1..L-1 contributes)
+int bbhx_hdyn(double* d_h, double* h_h, const double* residuals, const double* constants,
+              const double* freqs, int num_bin_all, int length, int n_channels, void* stream) {
+  BBHX_REQUIRE(length >= 1 && n_channels >= 1, "bad sizes");
+  if (num_bin_all == 0) return OK;
+  k_hdyn<<<grid_for(num_bin_all, 128), 128, 0, (cudaStream_t)stream>>>(
+      (cplx*)d_h, (cplx*)h_h, (const cplx*)residuals, (const cplx*)constants, freqs, num_bin_all,
+      length, n_channels);
+  return launch_status("k_hdyn");
+}
+
+// Support [start, start+len) of each binary on the data grid (device int arrays).
+int bbhx_template_support(int* start, int* len, const double* x, int num_modes, int length,
+                          int num_bin_all, const double* data_freqs, int data_length,
+                          void* stream) {
+  if (num_bin_all == 0) return OK;
+  k_support<<<num_bin_all, 128, 0, (cudaStream_t)stream>>>(x, num_modes, length, num_bin_all,
+                                                           data_freqs, data_length, start, len);
+  return launch_status("k_support");
+}
+
+// Fused direct likelihood: d_h, h_h device complex128 [B] (overwritten, scaled by 4 like the
+// reference), data [3, N] noise-weighted complex128, noise [3, N] = sqrt(df / S).
+int bbhx_direct_like_fused(double* d_h, double* h_h, const double* data_freqs, const double* data,
+                           const double* noise, int data_length, const double* x, const double* y,
+                           const double* c1, const double* c2, const double* c3,
+                           const double* t_start, const double* t_end, int num_modes, int length,
+                           int num_bin_all, void* stream) {
+  BBHX_REQUIRE(length >= 2 && num_modes >= 1 && data_length >= 1, "bad sizes");
+  if (num_bin_all == 0) return OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  int ntiles = (data_length + FD_TILE - 1) / FD_TILE;
+  long long nitems = (long long)ntiles * num_bin_all;
+  int* sup = nullptr;
+  double* part = nullptr;
+  BBHX_CHECK_CUDA(cudaMallocAsync((void**)&sup, sizeof(int) * 2 * num_bin_all, s));
+  BBHX_CHECK_CUDA(cudaMallocAsync((void**)&part, sizeof(double) * 3 * nitems, s));
+  k_support<<<num_bin_all, 128, 0, s>>>(x, num_modes, length, num_bin_all, data_freqs, data_length,
+                                        sup, sup + num_bin_all);
+  int st = launch_status("k_support");
+  if (!st) {
+    FusedArgs A;
+    A.data_freqs = data_freqs;
+    A.data = (const cplx*)data;
+    A.noise = noise;
+    A.N = data_length;
+    A.x = x;
+    A.y = y;
+    A.c1 = c1;
+    A.c2 = c2;
+    A.c3 = c3;
+    A.t_start = t_start;
+    A.t_end = t_end;
+    A.sup_start = sup;
+    A.sup_len = sup + num_bin_all;
+    A.B = num_bin_all;
+    A.M = num_modes;
+    A.L = length;
+    A.ntiles = ntiles;
+    A.partials = part;
+    unsigned grid = (unsigned)(nitems < 148LL * 16 ? nitems : 148LL * 16);
+    k_direct_fused<<<grid, FD_WARPS * 32, 0, s>>>(A);
+    st = launch_status("k_direct_fused");
+  }
+  if (!st) {
+    k_fused_reduce<<<grid_for(num_bin_all, 128), 128, 0, s>>>(part, sup, sup + num_bin_all,
+                                                              num_bin_all, d_h, h_h);
+    st = launch_status("k_fused_reduce");
+  }
+  cudaFreeAsync(sup, s);
+  cudaFreeAsync(part, s);
+  return st;
+}
+
+}  // extern "C"

@@ -1,0 +1,385 @@
+// PhenomHM kernels and their C-ABI entry points.
+//
+// Reference interfaces replaced (src/bbhx/cutils/PhenomHMWaveform.hh:322-371):
+//   get_phenomhm_ringdown_frequencies_wrap, get_phenomd_ringdown_frequencies_wrap,
+//   waveform_amp_phase.
+// Layout of the waveform buffer (phenomhm.py:201-249): flat [nparams, B, M, L] with
+// slot 0 = amplitude, 1 = phase, 2 = t(f); freqs flat [B, M, L].
+#include "capi_internal.cuh"
+#include "phenomhm_model.cuh"
+
+namespace bbhx {
+
+// ------------------------------------------------------------------ ringdown frequencies
+// thread per (binary, mode); output index b*M + mode (PhenomHMWaveform.cu:1816-1877)
+__global__ void k_ringdown_hm(double* fring, double* fdamp, const double* m1, const double* m2,
+                              const double* chi1, const double* chi2, const int* ells,
+                              const int* mms, int M, int B, int out_stride) {
+  long long n = (long long)B * M;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    int b = (int)(t / M), i = (int)(t % M);
+    double fm, fs;
+    final_mass_spin(m1[b], m2[b], chi1[b], chi2[b], &fm, &fs);
+    cplx z = qnm_cw(fs, ells[i], mms[i]);
+    long long o = (long long)b * out_stride + i;
+    fring[o] = (0.5 / PI) * z.re / fm;
+    fdamp[o] = (0.5 / PI) * z.im / fm;
+  }
+}
+
+// PhenomD 22 ringdown/damping frequency from the tabulated QNM spline of the final spin
+// (PhenomHMWaveform.cu:1930-1993): index int((a + 1) / dspin), local cubic in (a - a_k).
+__device__ __forceinline__ void phenomd_qnm_lookup(double fs, double fm, const double* y_rd,
+                                                   const double* c1_rd, const double* c2_rd,
+                                                   const double* c3_rd, const double* y_dm,
+                                                   const double* c1_dm, const double* c2_dm,
+                                                   const double* c3_dm, double dspin,
+                                                   double* fr, double* fd) {
+  int ind = int((fs - (-1.0)) / dspin);
+  double x = fs - (dspin * ind + (-1.0));
+  double x2 = x * x, x3 = x2 * x;
+  double r = y_rd[ind] + c1_rd[ind] * x + c2_rd[ind] * x2 + c3_rd[ind] * x3;
+  double d = y_dm[ind] + c1_dm[ind] * x + c2_dm[ind] * x2 + c3_dm[ind] * x3;
+  *fr = r / fm;
+  *fd = d / fm;
+}
+
+__global__ void k_ringdown_d(double* fring, double* fdamp, const double* m1, const double* m2,
+                             const double* chi1, const double* chi2, int B, const double* y_rd,
+                             const double* c1_rd, const double* c2_rd, const double* c3_rd,
+                             const double* y_dm, const double* c1_dm, const double* c2_dm,
+                             const double* c3_dm, double dspin, int out_stride, int out_offset) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < B; b += gridDim.x * blockDim.x) {
+    double fm, fs;
+    final_mass_spin(m1[b], m2[b], chi1[b], chi2[b], &fm, &fs);
+    double fr, fd;
+    phenomd_qnm_lookup(fs, fm, y_rd, c1_rd, c2_rd, c3_rd, y_dm, c1_dm, c2_dm, c3_dm, dspin, &fr,
+                       &fd);
+    fring[(long long)b * out_stride + out_offset] = fr;
+    fdamp[(long long)b * out_stride + out_offset] = fd;
+  }
+}
+
+// ------------------------------------------------------------------ per-mode setup
+__global__ void k_phm_setup(ModeCoeffs* coeffs, const int* ells, const int* mms,
+                            const double* m1_SI, const double* m2_SI, const double* chi1,
+                            const double* chi2, const double* dist, const double* Mf_RD_lm,
+                            const double* Mf_DM_lm, int M, int B, int run_phenomd) {
+  long long n = (long long)B * M;
+  int add = run_phenomd ? 0 : 1;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    int b = (int)(t / M), i = (int)(t % M);
+    const double* rd = Mf_RD_lm + (long long)b * (M + add);
+    const double* dm = Mf_DM_lm + (long long)b * (M + add);
+    double rd22 = run_phenomd ? rd[0] : rd[M];
+    double dm22 = run_phenomd ? dm[0] : dm[M];
+    int ell = run_phenomd ? 2 : ells[i];
+    int mm = run_phenomd ? 2 : mms[i];
+    ModeCoeffs c;
+    phm_setup_mode(c, m1_SI[b], m2_SI[b], chi1[b], chi2[b], dist[b], ell, mm, rd[i], dm[i], rd22,
+                   dm22, run_phenomd);
+    coeffs[t] = c;
+  }
+}
+
+// ------------------------------------------------------------------ per-point evaluation
+// thread per (binary, mode, frequency).  t_ref (optional) adds 2 pi f (t_ref - t_init) to the
+// phase and t_ref to t(f), the driver-side shift of phenomhm.py:485-507.
+__global__ void k_phm_points(double* out, const double* freqs, const ModeCoeffs* coeffs, int M,
+                             int L, int B, const double* t_ref, double t_init) {
+  long long n = (long long)B * M * L;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    long long bm = t / L;
+    const ModeCoeffs& c = coeffs[bm];
+    double f = freqs[t];
+    PointOut o = phm_eval_point(c, f);
+    if (t_ref) {
+      int b = (int)(bm / M);
+      double tr = t_ref[b];
+      o.phase += f * (tr - t_init) * 2 * PI;
+      o.tf += tr;
+    }
+    out[t] = o.amp;
+    out[n + t] = o.phase;
+    out[2 * n + t] = o.tf;
+  }
+}
+
+// t(f) only (first pass of the observation-window regrid)
+__global__ void k_phm_tf(double* tf_out, const double* freqs, const ModeCoeffs* coeffs, int M,
+                         int L, int B, const double* t_ref) {
+  long long n = (long long)B * M * L;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    long long bm = t / L;
+    const ModeCoeffs& c = coeffs[bm];
+    double Mf = freqs[t] * c.M_sec;
+    double Mfp;
+    if (c.phenomd_only)
+      Mfp = Mf;
+    else if (!(Mf > c.ph_fi))
+      Mfp = c.ph_ai * Mf;
+    else if (!(Mf > c.ph_fr))
+      Mfp = c.ph_am * Mf + c.ph_bm;
+    else
+      Mfp = c.ph_ar * Mf;
+    double tf;
+    if (c.phenomd_only)
+      tf = c.M_sec * phenomd_dphase(c.d, Mfp) / (2 * PI) - (c.t0 / (2. * PI) * c.M_sec);
+    else
+      tf = c.M_sec * (phenomd_dphase(c.d, Mfp) / (2. * PI)) - (c.t0 / (2. * PI) * c.M_sec);
+    tf_out[t] = tf + (t_ref ? t_ref[bm / M] : 0.0);
+  }
+}
+
+// ------------------------------------------------------------------ observation window
+// One thread per (binary, mode): the linear-interpolation crossing search of
+// phenomhm.py:520-606 followed by the log-spaced regrid of :608-610.
+//   freqs_in/tf: [BM, L]; Tobs [BM]; writes freqs_out [BM, L] and fminmax [BM, 2].
+// err[0] is set to 1 (lower edge) or 2 (upper edge) when a row that needs clipping does not
+// have exactly one crossing (the reference raises ValueError there).
+__global__ void k_tf_window(double* freqs_out, double* fminmax, const double* freqs_in,
+                            const double* tf, const double* Tobs, int L, long long BM, int* err) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < BM;
+       r += (long long)gridDim.x * blockDim.x) {
+    const double* f = freqs_in + r * L;
+    const double* x = tf + r * L;
+    double tmin = x[0], tmax = x[0], flo = f[0], fhi = f[0];
+    for (int i = 1; i < L; ++i) {
+      tmin = fmin(tmin, x[i]);
+      tmax = fmax(tmax, x[i]);
+      flo = fmin(flo, f[i]);
+      fhi = fmax(fhi, f[i]);
+    }
+    if (tmin < 0.0) {
+      int cnt = 0, seg = -1;
+      for (int i = 0; i < L - 1; ++i)
+        if ((0.0 < x[i + 1]) && (0.0 > x[i])) {
+          if (cnt == 0) seg = i;
+          ++cnt;
+        }
+      if (cnt != 1) {
+        atomicCAS(err, 0, 1);
+      } else {
+        double m = (f[seg + 1] - f[seg]) / (x[seg + 1] - x[seg]);
+        flo = m * (0.0 - x[seg]) + f[seg];
+      }
+    }
+    double To = Tobs[r];
+    if (tmax > To) {
+      int cnt = 0, seg = -1;
+      for (int i = 0; i < L - 1; ++i)
+        if ((To < x[i + 1]) && (To > x[i])) {
+          if (cnt == 0) seg = i;
+          ++cnt;
+        }
+      if (cnt != 1) {
+        atomicCAS(err, 0, 2);
+      } else {
+        double m = (f[seg + 1] - f[seg]) / (x[seg + 1] - x[seg]);
+        fhi = m * (To - x[seg]) + f[seg];
+      }
+    }
+    fminmax[2 * r] = flo;
+    fminmax[2 * r + 1] = fhi;
+    // numpy.logspace: y_k = k * step + start (two roundings), last y = stop, f = 10**y
+    double start = log10(flo), stop = log10(fhi);
+    double step = (stop - start) / (double)(L - 1);
+    double* o = freqs_out + r * L;
+    for (int k = 0; k < L; ++k) {
+      double y = (k == L - 1) ? stop : __dadd_rn(__dmul_rn((double)k, step), start);
+      o[k] = pow(10.0, y);
+    }
+  }
+}
+
+// default sparse grid (phenomhm.py:208-224): logspace(mf_min, mf_max, L) / M_sec * m / 2
+__global__ void k_default_freqs(double* freqs, const double* m1, const double* m2, const int* mms,
+                                double mf_min, double mf_max, int M, int L, int B) {
+  long long n = (long long)B * M * L;
+  double start = log10(mf_min), stop = log10(mf_max);
+  double step = (stop - start) / (double)(L - 1);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    int k = (int)(t % L);
+    int i = (int)((t / L) % M);
+    int b = (int)(t / ((long long)L * M));
+    double y = (k == L - 1) ? stop : __dadd_rn(__dmul_rn((double)k, step), start);
+    double base = pow(10.0, y);
+    double Msec = (m1[b] + m2[b]) * MTSUN_SI;
+    freqs[t] = base / Msec * (double)mms[i] / 2;
+  }
+}
+
+}  // namespace bbhx
+
+using namespace bbhx;
+
+namespace {
+constexpr int kThreads = 256;
+
+int alloc_coeffs(ModeCoeffs** p, long long n, cudaStream_t s) {
+  BBHX_CHECK_CUDA(cudaMallocAsync((void**)p, sizeof(ModeCoeffs) * (size_t)n, s));
+  return OK;
+}
+}  // namespace
+
+extern "C" {
+
+size_t bbhx_mode_coeffs_bytes(void) { return sizeof(ModeCoeffs); }
+
+// PhenomHMWaveform.hh:322-333
+int bbhx_get_phenomhm_ringdown_frequencies(double* fringdown, double* fdamp, const double* m1,
+                                           const double* m2, const double* chi1z,
+                                           const double* chi2z, const int* ells, const int* mms,
+                                           int num_modes, int num_bin_all, void* stream) {
+  BBHX_REQUIRE(num_modes > 0 && num_modes <= MAX_MODES, "num_modes must be 1..6");
+  BBHX_REQUIRE(num_bin_all >= 0, "num_bin_all < 0");
+  if (num_bin_all == 0) return OK;
+  long long n = (long long)num_bin_all * num_modes;
+  k_ringdown_hm<<<grid_for(n, kThreads), kThreads, 0, (cudaStream_t)stream>>>(
+      fringdown, fdamp, m1, m2, chi1z, chi2z, ells, mms, num_modes, num_bin_all, num_modes);
+  return launch_status("k_ringdown_hm");
+}
+
+// PhenomHMWaveform.hh:335-352
+int bbhx_get_phenomd_ringdown_frequencies(double* fringdown, double* fdamp, const double* m1,
+                                          const double* m2, const double* chi1z,
+                                          const double* chi2z, int num_bin_all,
+                                          const double* y_rd, const double* c1_rd,
+                                          const double* c2_rd, const double* c3_rd,
+                                          const double* y_dm, const double* c1_dm,
+                                          const double* c2_dm, const double* c3_dm, double dspin,
+                                          void* stream) {
+  BBHX_REQUIRE(num_bin_all >= 0, "num_bin_all < 0");
+  BBHX_REQUIRE(dspin > 0.0, "dspin must be positive");
+  if (num_bin_all == 0) return OK;
+  k_ringdown_d<<<grid_for(num_bin_all, kThreads), kThreads, 0, (cudaStream_t)stream>>>(
+      fringdown, fdamp, m1, m2, chi1z, chi2z, num_bin_all, y_rd, c1_rd, c2_rd, c3_rd, y_dm, c1_dm,
+      c2_dm, c3_dm, dspin, 1, 0);
+  return launch_status("k_ringdown_d");
+}
+
+// Both ringdown sets in the [B, M+1] layout that waveform_amp_phase consumes
+// (phenomhm.py:397-463 builds it with two calls and a concatenation).  With run_phenomd the
+// layout is [B, 1] holding the PhenomD values.
+int bbhx_ringdown_frequencies_all(double* fringdown, double* fdamp, const double* m1,
+                                  const double* m2, const double* chi1z, const double* chi2z,
+                                  const int* ells, const int* mms, int num_modes, int num_bin_all,
+                                  const double* qnm_table /* 8 x 1001: y,c1,c2,c3 rd; y,c1,c2,c3 dm */,
+                                  int table_len, double dspin, int run_phenomd, void* stream) {
+  BBHX_REQUIRE(num_modes > 0 && num_modes <= MAX_MODES, "num_modes must be 1..6");
+  BBHX_REQUIRE(table_len > 0 && dspin > 0.0, "bad QNM table");
+  if (num_bin_all == 0) return OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  const double* T = qnm_table;
+  int stride = run_phenomd ? 1 : num_modes + 1;
+  int off = run_phenomd ? 0 : num_modes;
+  if (!run_phenomd) {
+    long long n = (long long)num_bin_all * num_modes;
+    k_ringdown_hm<<<grid_for(n, kThreads), kThreads, 0, s>>>(
+        fringdown, fdamp, m1, m2, chi1z, chi2z, ells, mms, num_modes, num_bin_all, num_modes + 1);
+    int st = launch_status("k_ringdown_hm");
+    if (st) return st;
+  }
+  k_ringdown_d<<<grid_for(num_bin_all, kThreads), kThreads, 0, s>>>(
+      fringdown, fdamp, m1, m2, chi1z, chi2z, num_bin_all, T, T + table_len, T + 2 * table_len,
+      T + 3 * table_len, T + 4 * table_len, T + 5 * table_len, T + 6 * table_len,
+      T + 7 * table_len, dspin, stride, off);
+  return launch_status("k_ringdown_d");
+}
+
+// PhenomHMWaveform.hh:354-371.  waveform_out [3 or more, B, M, L] (amp, phase, tf slots).
+int bbhx_waveform_amp_phase(double* waveform_out, const int* ells, const int* mms,
+                            const double* freqs, const double* m1_SI, const double* m2_SI,
+                            const double* chi1z, const double* chi2z, const double* distance,
+                            const double* f_ref, int num_modes, int length, int num_bin_all,
+                            const double* Mf_RD_lm, const double* Mf_DM_lm, int run_phenomd,
+                            void* stream) {
+  (void)f_ref;  // the reference always sets f_ref to the 22 amplitude peak (PhenomHMWaveform.cu:2767)
+  BBHX_REQUIRE(num_modes > 0 && num_modes <= MAX_MODES, "num_modes must be 1..6");
+  BBHX_REQUIRE(length >= 1 && num_bin_all >= 0, "bad length / num_bin_all");
+  if (run_phenomd) BBHX_REQUIRE(num_modes == 1, "run_phenomd requires one mode");
+  if (num_bin_all == 0) return OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  long long nbm = (long long)num_bin_all * num_modes;
+  ModeCoeffs* c = nullptr;
+  int st = alloc_coeffs(&c, nbm, s);
+  if (st) return st;
+  k_phm_setup<<<grid_for(nbm, 128), 128, 0, s>>>(c, ells, mms, m1_SI, m2_SI, chi1z, chi2z,
+                                                  distance, Mf_RD_lm, Mf_DM_lm, num_modes,
+                                                  num_bin_all, run_phenomd);
+  st = launch_status("k_phm_setup");
+  if (!st) {
+    long long n = nbm * length;
+    k_phm_points<<<grid_for(n, kThreads), kThreads, 0, s>>>(waveform_out, freqs, c, num_modes,
+                                                            length, num_bin_all, nullptr, 0.0);
+    st = launch_status("k_phm_points");
+  }
+  cudaFreeAsync(c, s);
+  return st;
+}
+
+// Setup records for later fused kernels (caller owns `coeffs`, B*M records of
+// bbhx_mode_coeffs_bytes() bytes each).
+int bbhx_phenomhm_setup(void* coeffs, const int* ells, const int* mms, const double* m1_SI,
+                        const double* m2_SI, const double* chi1z, const double* chi2z,
+                        const double* distance, const double* Mf_RD_lm, const double* Mf_DM_lm,
+                        int num_modes, int num_bin_all, int run_phenomd, void* stream) {
+  BBHX_REQUIRE(num_modes > 0 && num_modes <= MAX_MODES, "num_modes must be 1..6");
+  if (num_bin_all == 0) return OK;
+  long long nbm = (long long)num_bin_all * num_modes;
+  k_phm_setup<<<grid_for(nbm, 128), 128, 0, (cudaStream_t)stream>>>(
+      (ModeCoeffs*)coeffs, ells, mms, m1_SI, m2_SI, chi1z, chi2z, distance, Mf_RD_lm, Mf_DM_lm,
+      num_modes, num_bin_all, run_phenomd);
+  return launch_status("k_phm_setup");
+}
+
+// amplitude/phase/t(f) from prepared records, with the t_ref shift fused (t_ref may be null)
+int bbhx_phenomhm_points(double* waveform_out, const double* freqs, const void* coeffs,
+                         const double* t_ref, double t_init, int num_modes, int length,
+                         int num_bin_all, void* stream) {
+  if (num_bin_all == 0) return OK;
+  long long n = (long long)num_bin_all * num_modes * length;
+  k_phm_points<<<grid_for(n, kThreads), kThreads, 0, (cudaStream_t)stream>>>(
+      waveform_out, freqs, (const ModeCoeffs*)coeffs, num_modes, length, num_bin_all, t_ref,
+      t_init);
+  return launch_status("k_phm_points");
+}
+
+int bbhx_phenomhm_tf(double* tf_out, const double* freqs, const void* coeffs, const double* t_ref,
+                     int num_modes, int length, int num_bin_all, void* stream) {
+  if (num_bin_all == 0) return OK;
+  long long n = (long long)num_bin_all * num_modes * length;
+  k_phm_tf<<<grid_for(n, kThreads), kThreads, 0, (cudaStream_t)stream>>>(
+      tf_out, freqs, (const ModeCoeffs*)coeffs, num_modes, length, num_bin_all, t_ref);
+  return launch_status("k_phm_tf");
+}
+
+int bbhx_default_freqs(double* freqs, const double* m1, const double* m2, const int* mms,
+                       double mf_min, double mf_max, int num_modes, int length, int num_bin_all,
+                       void* stream) {
+  BBHX_REQUIRE(length >= 2, "length must be >= 2");
+  if (num_bin_all == 0) return OK;
+  long long n = (long long)num_bin_all * num_modes * length;
+  k_default_freqs<<<grid_for(n, kThreads), kThreads, 0, (cudaStream_t)stream>>>(
+      freqs, m1, m2, mms, mf_min, mf_max, num_modes, length, num_bin_all);
+  return launch_status("k_default_freqs");
+}
+
+// Observation-window regrid.  `err_dev` is a device int (zeroed by the caller); after the
+// stream completes it holds 0, 1 (lower crossing search failed) or 2 (upper).
+int bbhx_tf_window_regrid(double* freqs_out, double* fminmax, const double* freqs_in,
+                          const double* tf, const double* Tobs, int length, long long num_rows,
+                          int* err_dev, void* stream) {
+  BBHX_REQUIRE(length >= 2, "length must be >= 2");
+  if (num_rows == 0) return OK;
+  k_tf_window<<<grid_for(num_rows, 128), 128, 0, (cudaStream_t)stream>>>(
+      freqs_out, fminmax, freqs_in, tf, Tobs, length, num_rows, err_dev);
+  return launch_status("k_tf_window");
+}
+
+}  // extern "C"

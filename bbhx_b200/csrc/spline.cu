@@ -1,0 +1,190 @@
+// Batched not-a-knot cubic splines.
+//
+// Reference interface replaced: interpolate() (src/bbhx/cutils/Interpolate.hh:4-6,
+// Interpolate.cu:320-359) which fills the tridiagonal system for every (param, binary,
+// mode) (fill_B, :14-182), solves it with cusparseDgtsv2StridedBatch / LAPACKE_dgtsv
+// (:201-241) and converts slopes to cubic coefficients (:245-318).
+//
+// Here one CTA owns one (binary, mode) system: the P interpolated quantities share the
+// same knots x and therefore the same matrix, so the CTA builds the matrix once, carries
+// all P right-hand sides through one cyclic reduction in shared memory (log2 L levels
+// down, log2 L levels back up), and writes the slopes and coefficients coalesced.
+//
+// System for the slopes s_i (scipy CubicSpline "not-a-knot"):
+//   row 0:     (x2-x1) s0 + (x2-x0) s1 = ((dx1 + 2 d) dx2 m1 + dx1^2 m2) / d
+//   row i:     dx2 s_{i-1} + 2 (dx1 + dx2) s_i + dx1 s_{i+1} = 3 (dx2 m1 + dx1 m2)
+//   row L-1:   d s_{L-2} + dx1 s_{L-1} = (dx2^2 m1 + (2 d + dx2) dx1 m2) / d
+// (dx1, dx2 the two intervals around the row, d = dx1 + dx2, m1, m2 their secant slopes).
+// Coefficients on segment i: y(x) = y_i + c1 u + c2 u^2 + c3 u^3, u = x - x_i, with
+//   c1 = s_i,  t = (s_i + s_{i+1} - 2 m) / h,  c2 = (m - s_i) / h - t,  c3 = t / h.
+// Entry L-1 of c1/c2/c3 (no segment) holds the last row's (upper, diagonal, lower)
+// coefficients, as the reference GPU path leaves them.
+#include "capi_internal.cuh"
+
+namespace bbhx {
+
+// In-place cyclic reduction on a[n], b[n], c[n] and P right-hand sides d[p*ld + i];
+// solution returned in d.  All threads of the block participate.
+__device__ void cr_solve(double* a, double* b, double* c, double* d, int ld, int P, int n) {
+  for (int s = 1; s < n; s <<= 1) {
+    int cnt = n / (2 * s);
+    for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
+      int i = 2 * s * k + 2 * s - 1;
+      int im = i - s, ip = i + s;
+      bool hp = ip < n;
+      double al = -a[i] / b[im];
+      double ga = hp ? -c[i] / b[ip] : 0.0;
+      double an = al * a[im];
+      double bn = b[i] + al * c[im] + (hp ? ga * a[ip] : 0.0);
+      double cn = hp ? ga * c[ip] : 0.0;
+      for (int p = 0; p < P; ++p) {
+        double* dp = d + (size_t)p * ld;
+        dp[i] = dp[i] + al * dp[im] + (hp ? ga * dp[ip] : 0.0);
+      }
+      a[i] = an;
+      b[i] = bn;
+      c[i] = cn;
+    }
+    __syncthreads();
+  }
+  int top = 1;
+  while (top < n) top <<= 1;
+  for (int s = top; s >= 1; s >>= 1) {
+    int cnt = (n >= s) ? (n - s) / (2 * s) + 1 : 0;
+    for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
+      int i = s - 1 + 2 * s * k;
+      int im = i - s, ip = i + s;
+      for (int p = 0; p < P; ++p) {
+        double* dp = d + (size_t)p * ld;
+        double xm = (im >= 0) ? dp[im] : 0.0;
+        double xp = (ip < n) ? dp[ip] : 0.0;
+        dp[i] = (dp[i] - a[i] * xm - c[i] * xp) / b[i];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// x: [S, L]; y: [P, S, L]; outputs slopes / c1 / c2 / c3 in y's layout (any may alias the
+// reference's B / upper / diag / lower buffers).  `scratch` (used only when the system does
+// not fit in shared memory) holds gridDim.x * (4 + P) * L doubles.
+__global__ void k_spline(const double* __restrict__ x, const double* __restrict__ y,
+                         double* slopes, double* c1, double* c2, double* c3, int L, int P,
+                         long long S, bool use_smem, double* scratch) {
+  extern __shared__ double smem[];
+  double* base = use_smem ? smem : scratch + (size_t)blockIdx.x * (4 + P) * L;
+  double* xs = base;
+  double* a = xs + L;
+  double* b = a + L;
+  double* c = b + L;
+  double* d = c + L;
+  for (long long sys = blockIdx.x; sys < S; sys += gridDim.x) {
+    const double* xg = x + sys * L;
+    for (int i = threadIdx.x; i < L; i += blockDim.x) xs[i] = xg[i];
+    __syncthreads();
+    for (int i = threadIdx.x; i < L; i += blockDim.x) {
+      double dx1, dx2, dd;
+      int i0, i1, i2;
+      if (i == 0) {
+        i0 = 0; i1 = 1; i2 = 2;
+      } else if (i == L - 1) {
+        i0 = L - 3; i1 = L - 2; i2 = L - 1;
+      } else {
+        i0 = i - 1; i1 = i; i2 = i + 1;
+      }
+      dx1 = xs[i1] - xs[i0];
+      dx2 = xs[i2] - xs[i1];
+      dd = xs[i2] - xs[i0];
+      if (i == 0) {
+        a[i] = 0.0; b[i] = dx2; c[i] = dd;
+      } else if (i == L - 1) {
+        a[i] = dd; b[i] = dx1; c[i] = 0.0;
+      } else {
+        a[i] = dx2; b[i] = 2 * (dx1 + dx2); c[i] = dx1;
+      }
+      for (int p = 0; p < P; ++p) {
+        const double* yg = y + ((long long)p * S + sys) * L;
+        double y1 = yg[i1];
+        double m1 = (y1 - yg[i0]) / dx1;
+        double m2 = (yg[i2] - y1) / dx2;
+        double r;
+        if (i == 0)
+          r = ((dx1 + 2 * dd) * dx2 * m1 + dx1 * dx1 * m2) / dd;
+        else if (i == L - 1)
+          r = (dx2 * dx2 * m1 + (2 * dd + dx2) * dx1 * m2) / dd;
+        else
+          r = 3.0 * (dx2 * m1 + dx1 * m2);
+        d[(size_t)p * L + i] = r;
+      }
+    }
+    __syncthreads();
+    // keep the last row's matrix entries for the c1/c2/c3[L-1] convention
+    double last_a = a[L - 1], last_b = b[L - 1];
+    __syncthreads();
+    cr_solve(a, b, c, d, L, P, L);
+    for (int p = 0; p < P; ++p) {
+      const double* yg = y + ((long long)p * S + sys) * L;
+      long long o = ((long long)p * S + sys) * L;
+      const double* sp = d + (size_t)p * L;
+      for (int i = threadIdx.x; i < L; i += blockDim.x) {
+        double si = sp[i];
+        if (slopes) slopes[o + i] = si;
+        if (i < L - 1) {
+          double h = xs[i + 1] - xs[i];
+          double m = (yg[i + 1] - yg[i]) / h;
+          double t = (si + sp[i + 1] - 2 * m) / h;
+          c1[o + i] = si;
+          c2[o + i] = (m - si) / h - t;
+          c3[o + i] = t / h;
+        } else {
+          c1[o + i] = 0.0;
+          c2[o + i] = last_b;
+          c3[o + i] = last_a;
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace bbhx
+
+using namespace bbhx;
+
+namespace {
+constexpr size_t kMaxSplineSmem = 200 * 1024;
+}
+
+extern "C" {
+
+// Interpolate.hh:4-6: freqs [B*M, L], y [P, B, M, L]; B_ receives the slopes, upper_diag /
+// diag / lower_diag receive c1 / c2 / c3 (the reference reuses those buffers the same way).
+int bbhx_interpolate(const double* freqs, const double* y, double* B_, double* upper_diag,
+                     double* diag, double* lower_diag, int length, int num_interp_params,
+                     int num_modes, int num_bin_all, void* stream) {
+  BBHX_REQUIRE(length >= 3, "spline length must be >= 3 (not-a-knot)");
+  BBHX_REQUIRE(num_interp_params >= 1 && num_modes >= 1 && num_bin_all >= 0, "bad sizes");
+  long long S = (long long)num_modes * num_bin_all;
+  if (S == 0) return OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  size_t smem = sizeof(double) * (size_t)(4 + num_interp_params) * length;
+  bool use_smem = smem <= kMaxSplineSmem;
+  int threads = 256;
+  unsigned int grid = (unsigned int)(S < 148 * 16 ? S : 148 * 16);
+  double* scratch = nullptr;
+  if (use_smem) {
+    BBHX_CHECK_CUDA(cudaFuncSetAttribute(k_spline, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kMaxSplineSmem));
+  } else {
+    grid = (unsigned int)(S < 148 * 2 ? S : 148 * 2);
+    BBHX_CHECK_CUDA(cudaMallocAsync((void**)&scratch, sizeof(double) * grid * (4 + num_interp_params) * (size_t)length, s));
+  }
+  k_spline<<<grid, threads, use_smem ? smem : 0, s>>>(freqs, y, B_, upper_diag, diag, lower_diag,
+                                                      length, num_interp_params, S, use_smem,
+                                                      scratch);
+  int st = launch_status("k_spline");
+  if (scratch) cudaFreeAsync(scratch, s);
+  return st;
+}
+
+}  // extern "C"

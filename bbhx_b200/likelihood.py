@@ -1,0 +1,199 @@
+"""Direct and heterodyned log-likelihoods on the GPU.
+
+Drop-ins for the reference's ``Likelihood`` and ``HeterodynedLikelihood``
+(src/bbhx/likelihood.py:26-648): same constructors, attributes (``d_d``, ``noise_factors``,
+``data_channels``, ``reference_d_d``, ``data_constants``, ``freqs``, ...) and ``get_ll``
+keywords (``return_extracted_snr``, ``phase_marginalize``, waveform keywords); results come
+back as numpy arrays, as in the reference.
+
+``Likelihood.get_ll`` runs the fused device path (``BBHWaveformFD.inner_products``): no
+per-binary templates are materialised and the single host synchronisation is the copy of
+the results (together with the deferred error flags).
+"""
+import numpy as np
+
+from . import _lib
+from .sensitivity import AET1SensitivityMatrix, SensitivityMatrix
+from .utils.arrays import device, to_dev, to_np, torch
+
+
+class Likelihood:
+    def __init__(self, template_gen, data_freqs, data_channels, psd, force_backend=None):
+        t = torch()
+        self.data_freqs = to_dev(data_freqs)
+        data_freqs_cpu = to_np(data_freqs).astype(np.float64)
+        self.psd = np.asarray(to_np(psd), dtype=np.float64)
+        self.delta_f = np.zeros_like(self.psd)
+        self.delta_f[:, 1:] = np.diff(data_freqs_cpu)
+        self.delta_f[:, 0] = self.delta_f[:, 1]
+        self.noise_factors = to_dev(np.sqrt(1.0 / self.psd * self.delta_f).flatten())
+        self.data_channels = (self.noise_factors * to_dev(data_channels, t.complex128).flatten()).contiguous()
+        self.waveform_gen = template_gen
+        self.data_stream_length = len(data_freqs_cpu)
+        self.d_d = float((4 * (self.data_channels.conj() * self.data_channels).sum()).real.item())
+
+    @property
+    def xp(self):
+        return torch()
+
+    def get_ll(self, params, return_extracted_snr=False, phase_marginalize=False,
+               **waveform_kwargs):
+        """log-likelihood for params of shape (12,) or (12, B) (likelihood.py:140-225)."""
+        t = torch()
+        self.phase_marginalize = phase_marginalize
+        self.return_extracted_snr = return_extracted_snr
+        params = np.atleast_2d(np.asarray(to_np(params) if isinstance(params, t.Tensor) else params,
+                                          dtype=np.float64))
+        if params.shape[0] != 12 and params.shape[1] == 12:
+            params = params.T
+        kw = dict(waveform_kwargs)
+        for k in ("freqs", "fill", "direct", "compress", "squeeze", "combine"):
+            kw.pop(k, None)
+        flags = t.zeros(2, dtype=t.int32, device=device())
+        d_h, h_h = self.waveform_gen.inner_products(tuple(params), self.data_freqs,
+                                                    self.data_channels, self.noise_factors,
+                                                    flags=flags, **kw)
+        self.d_h, self.h_h = d_h, h_h
+        d_h_temp = d_h if not phase_marginalize else d_h.abs().to(t.complex128)
+        out = -1.0 / 2.0 * (self.d_d + h_h - 2 * d_h_temp).real
+        packed = t.cat([out, d_h_temp.real, h_h.real, flags.to(t.float64)]).cpu().numpy()
+        B = out.numel()
+        fl = packed[3 * B:]
+        if fl[0] == 1:
+            raise ValueError("The search for a window at x_min did not run correctly. If t_ref is "
+                             "close to zero, the time-frequency correspondence may be crossing zero twice.")
+        if fl[0] == 2:
+            raise ValueError("The search for a window at x_max did not run correctly. If t_ref is "
+                             "close to the observation time, the time-frequency correspondence may be "
+                             "crossing zero twice.")
+        if fl[1] != 0:
+            raise ValueError("Orbital information does not cover the t(f) range of the templates.")
+        ll = packed[:B]
+        if return_extracted_snr:
+            return np.array([ll, packed[B:2 * B] / np.sqrt(packed[2 * B:3 * B])]).T
+        return ll
+
+
+class HeterodynedLikelihood:
+    def __init__(self, template_gen, data_freqs, data_channels, reference_template_params,
+                 length_f_het, template_gen_kwargs=None, reference_gen_kwargs=None, sens_mat=None,
+                 force_backend=None):
+        template_gen_kwargs = {} if template_gen_kwargs is None else template_gen_kwargs
+        reference_gen_kwargs = {} if reference_gen_kwargs is None else reference_gen_kwargs
+        self.template_gen = template_gen
+        self.f_dense = to_dev(data_freqs)
+        self.d = to_dev(data_channels, torch().complex128)
+        self.length_f_het = length_f_het
+        self.sens_mat = sens_mat
+        self.init_heterodyne_info(reference_template_params,
+                                  template_gen_kwargs=template_gen_kwargs,
+                                  reference_gen_kwargs=reference_gen_kwargs)
+
+    @property
+    def xp(self):
+        return torch()
+
+    @property
+    def sens_mat(self):
+        return self._sens_mat
+
+    @sens_mat.setter
+    def sens_mat(self, sens_mat):
+        if sens_mat is None:
+            sens_mat = AET1SensitivityMatrix(np.logspace(-5, -1, 1000))
+        assert isinstance(sens_mat, SensitivityMatrix)
+        self._sens_mat = sens_mat
+
+    def init_heterodyne_info(self, reference_template_params, template_gen_kwargs=None,
+                             reference_gen_kwargs=None):
+        """Reference template, sparse grid and relative-binning constants
+        (likelihood.py:380-548)."""
+        t = torch()
+        template_gen_kwargs = dict(template_gen_kwargs or {})
+        reference_gen_kwargs = dict(reference_gen_kwargs or {})
+        template_gen_kwargs["squeeze"] = True
+        template_gen_kwargs["compress"] = True
+        template_gen_kwargs["direct"] = True
+        fd = to_np(self.f_dense)
+        minF = fd.min() * 0.999999999999
+        maxF = fd.max() * 1.000000000001
+        if minF == 0.0:
+            minF = 1e-6
+        reference_gen_kwargs["squeeze"] = True
+        reference_gen_kwargs["compress"] = True
+        reference_gen_kwargs["fill"] = True
+        if not ("direct" in reference_gen_kwargs and reference_gen_kwargs["direct"] is True):
+            reference_gen_kwargs["direct"] = False
+            if "length" not in reference_gen_kwargs:
+                reference_gen_kwargs["length"] = 8096
+        freqs = np.logspace(np.log10(minF), np.log10(maxF), self.length_f_het)
+        p = [np.atleast_1d(v) for v in reference_template_params]
+        h0 = self.template_gen(*p, freqs=self.f_dense, **reference_gen_kwargs)[0]
+        h0_temp = self.template_gen(*p, freqs=freqs, **template_gen_kwargs)[0]
+        keep = to_np(~(h0_temp.abs() == 0.0))
+        freqs_keep = freqs[keep]
+        freqs = np.logspace(np.log10(freqs_keep[0]), np.log10(freqs_keep[-1]), self.length_f_het)
+        self.h0_sparse = self.template_gen(*p, freqs=freqs, **template_gen_kwargs)[None, :, :]
+        fd_all = to_np(self.f_dense)
+        inds = (fd_all >= freqs[0]) & (fd_all <= freqs[-1])
+        inds_d = to_dev(inds, t.bool)
+        self.f_dense = self.f_dense[inds_d]
+        self.d = self.d[:, inds_d]
+        h0 = h0[:, inds_d]
+        f_dense_h = fd_all[inds]
+        bins = np.searchsorted(freqs, f_dense_h, "right") - 1
+        f_m = (freqs[1:] + freqs[:-1]) / 2
+        df = f_dense_h[1] - f_dense_h[0]
+        self.sens_mat.update_frequency_arr(f_dense_h)
+        S_n = to_dev(np.asarray([self.sens_mat[0], self.sens_mat[1], self.sens_mat[2]]))
+        bins_d = to_dev(bins, t.int64)
+        fmb = to_dev(f_dense_h - f_m[np.clip(bins, 0, len(f_m) - 1)])
+        A0_flat = 4 * (h0.conj() * self.d) / S_n * df
+        A1_flat = A0_flat * fmb
+        B0_flat = 4 * (h0.conj() * h0) / S_n * df
+        B1_flat = B0_flat * fmb
+        # per-bin sums into slot ind + 1, the last dense point excluded (likelihood.py:512-522)
+        L = self.length_f_het
+        consts = []
+        for arr in (A0_flat, A1_flat, B0_flat, B1_flat):
+            acc = t.zeros((3, L), dtype=t.complex128, device=device())
+            acc.index_add_(1, (bins_d[:-1] + 1), arr[:, :-1])
+            consts.append(acc)
+        self.data_constants = t.cat([c.flatten() for c in consts]).contiguous()
+        self.reference_d_d = float((4 * (self.d.conj() * self.d) / S_n * df).sum().real.item())
+        self.reference_h_h = float(B0_flat.sum().real.item())
+        self.reference_d_h = float(A0_flat.sum().real.item())
+        self.reference_ll = -1 / 2 * (self.reference_d_d + self.reference_h_h - 2 * self.reference_d_h)
+        self.freqs = to_dev(freqs)
+        self.f_m = f_m
+        template_gen_kwargs["squeeze"] = False
+        self.template_gen_kwargs = template_gen_kwargs
+
+    def get_ll(self, params, return_extracted_snr=False, phase_marginalize=False,
+               **waveform_kwargs):
+        """Heterodyned log-likelihood (likelihood.py:550-648)."""
+        t = torch()
+        self.phase_marginalize = phase_marginalize
+        self.return_extracted_snr = return_extracted_snr
+        keys = set(waveform_kwargs) | set(self.template_gen_kwargs)
+        for key in keys:
+            if key in ["direct", "compress", "squeeze"]:
+                waveform_kwargs[key] = self.template_gen_kwargs[key]
+            elif key in self.template_gen_kwargs:
+                waveform_kwargs[key] = waveform_kwargs.get(key, self.template_gen_kwargs[key])
+        waveform_kwargs["freqs"] = self.freqs
+        params = np.atleast_2d(np.asarray(params, dtype=np.float64))
+        self.h_sparse = self.template_gen(*params, **waveform_kwargs)
+        r = self.h_sparse / self.h0_sparse
+        B = r.shape[0]
+        residuals = r.permute(2, 1, 0).contiguous().flatten()
+        self.hdyn_d_h = t.zeros(B, dtype=t.complex128, device=device())
+        self.hdyn_h_h = t.zeros(B, dtype=t.complex128, device=device())
+        _lib.call("bbhx_hdyn", _lib.dptr(self.hdyn_d_h), _lib.dptr(self.hdyn_h_h), _lib.dptr(residuals),
+                  _lib.dptr(self.data_constants), _lib.dptr(self.freqs), B, len(self.freqs), 3,
+                  _lib.stream())
+        d_h_temp = self.hdyn_d_h if not phase_marginalize else self.hdyn_d_h.abs().to(t.complex128)
+        out = (-1 / 2.0 * (self.reference_d_d + self.hdyn_h_h - 2 * d_h_temp).real).cpu().numpy()
+        if return_extracted_snr:
+            return np.array([out, to_np(d_h_temp.real) / np.sqrt(to_np(self.hdyn_h_h.real))]).T
+        return out

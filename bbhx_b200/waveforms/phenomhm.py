@@ -1,0 +1,260 @@
+"""PhenomHM / PhenomD in the amplitude-phase representation on the GPU.
+
+Drop-in for the reference's ``PhenomHMAmpPhase`` (src/bbhx/waveforms/phenomhm.py:32-614):
+same constructor keywords, ``run_wave`` / ``__call__`` arguments, flat
+``waveform_carrier`` layout ``[3, B, M, L]`` (amp, phase, t(f)) and the ``amp`` /
+``phase`` / ``tf`` / ``freqs`` / ``freqs_shaped`` views.  Arrays are torch CUDA tensors.
+
+Differences in mechanism (not in results): the per-(binary, mode) model setup runs once
+and is shared by the two evaluations of ``__call__`` (the reference re-runs the whole
+model on the regridded frequencies), the first pass evaluates t(f) only, the t_ref shift
+is fused into the evaluation kernel, and the observation-window regrid runs on the GPU.
+"""
+import numpy as np
+
+from .. import _lib
+from ..utils.arrays import atleast_1d, device, to_dev, torch
+from ..utils.constants import MSUN_SI
+from .ringdownphenomd import QNMData_a, QNMData_fdamp, QNMData_fring, dspin
+
+ALLOWABLE_MODES = [(2, 2), (3, 3), (4, 4), (2, 1), (3, 2), (4, 3)]
+
+
+def qnm_spline_table():
+    """(8, 1001) device table: y, c1, c2, c3 of the not-a-knot spline of the ringdown and of
+    the damping frequency over final spin (phenomhm.py:148-163), built with the library's
+    spline kernel."""
+    t = torch()
+    x = to_dev(QNMData_a).reshape(1, -1)
+    y = to_dev(np.stack([QNMData_fring, QNMData_fdamp])).reshape(2, 1, -1).contiguous()
+    n = x.shape[1]
+    c1 = t.empty((2, 1, n), dtype=t.float64, device=device())
+    c2 = t.empty_like(c1)
+    c3 = t.empty_like(c1)
+    _lib.call("bbhx_interpolate", _lib.dptr(x), _lib.dptr(y), _lib._VP(0), _lib.dptr(c1),
+              _lib.dptr(c2), _lib.dptr(c3), n, 2, 1, 1, _lib.stream())
+    tab = t.stack([y[0, 0], c1[0, 0], c2[0, 0], c3[0, 0], y[1, 0], c1[1, 0], c2[1, 0], c3[1, 0]])
+    return tab.contiguous()
+
+
+class PhenomHMAmpPhase:
+    """PhenomHM amplitude, phase and t(f) for batches of binaries.
+
+    Args:
+        force_backend: accepted for call compatibility; only the CUDA backend exists.
+        run_phenomd (bool): run PhenomD (only the (2,2) mode).
+        mf_min, mf_max (float): dimensionless frequency range of the default grid.
+        initial_t_val (float): start of the time window; shifts the phase only.
+    """
+
+    def __init__(self, force_backend=None, run_phenomd=False, mf_min=1e-4, mf_max=0.6,
+                 initial_t_val=0.0):
+        t = torch()
+        self.run_phenomd = run_phenomd
+        self.allowable_modes = [(2, 2)] if run_phenomd else list(ALLOWABLE_MODES)
+        self.ells_default = to_dev([ell for ell, _ in self.allowable_modes], t.int32)
+        self.mms_default = to_dev([mm for _, mm in self.allowable_modes], t.int32)
+        self.mf_min = mf_min
+        self.mf_max = mf_max
+        self.initial_t_val = initial_t_val
+        self._init_phenomd_fring_spline()
+        self._coeffs = None
+
+    @property
+    def xp(self):
+        return torch()
+
+    def _init_phenomd_fring_spline(self):
+        self.qnm_table = qnm_spline_table()
+        (self.y_rd, self.c1_rd, self.c2_rd, self.c3_rd,
+         self.y_dm, self.c1_dm, self.c2_dm, self.c3_dm) = self.qnm_table
+
+    # ------------------------------------------------------------------ checks
+    def _sanity_check_modes(self, ells, mms):
+        for ell, mm in zip(ells, mms):
+            if (int(ell), int(mm)) not in self.allowable_modes:
+                raise ValueError(
+                    "Requested mode [(l,m) = ({},{})] is not available. Allowable modes include {}"
+                    .format(ell, mm, self.allowable_modes))
+
+    @staticmethod
+    def _sanity_check_params(m1, m2, chi1z, chi2z):
+        t = torch()
+        if bool((chi1z.abs() > 1.0).any()):
+            raise ValueError("chi1z array contains values with abs(chi1z) > 1.0 which is not allowed.")
+        if bool((chi2z.abs() > 1.0).any()):
+            raise ValueError("chi2z array contains values with abs(chi2z) > 1.0 which is not allowed.")
+        switch = m1 < m2
+        return (t.where(switch, m2, m1), t.where(switch, m1, m2), t.where(switch, chi2z, chi1z),
+                t.where(switch, chi1z, chi2z))
+
+    # ------------------------------------------------------------------ views
+    @property
+    def amp(self):
+        return self.waveform_carrier[0: self.num_per_param].reshape(
+            self.num_bin_all, self.num_modes, self.length)
+
+    @property
+    def phase(self):
+        return self.waveform_carrier[self.num_per_param: 2 * self.num_per_param].reshape(
+            self.num_bin_all, self.num_modes, self.length)
+
+    @property
+    def tf(self):
+        return self.waveform_carrier[2 * self.num_per_param: 3 * self.num_per_param].reshape(
+            self.num_bin_all, self.num_modes, self.length)
+
+    @property
+    def freqs_shaped(self):
+        return self._freqs.reshape(self.num_bin_all, self.num_modes, self.length)
+
+    @property
+    def freqs(self):
+        return self._freqs
+
+    @freqs.setter
+    def freqs(self, f):
+        self._freqs = f.flatten() if f.ndim > 1 else f
+
+    # ------------------------------------------------------------------ core
+    def _prepare(self, m1, m2, chi1z, chi2z, distance, phi_ref, f_ref, t_ref, length, freqs,
+                 out_buffer, modes):
+        """Shared front half of run_wave: parameter checks, modes, buffers, ringdown
+        frequencies and the per-(binary, mode) model records."""
+        t = torch()
+        m1 = to_dev(atleast_1d(m1)).clone()
+        m2 = to_dev(atleast_1d(m2)).clone()
+        chi1z = to_dev(atleast_1d(chi1z)).clone()
+        chi2z = to_dev(atleast_1d(chi2z)).clone()
+        m1, m2, chi1z, chi2z = self._sanity_check_params(m1, m2, chi1z, chi2z)
+        if modes is not None:
+            ells = to_dev([ell for ell, mm in modes], t.int32)
+            mms = to_dev([mm for ell, mm in modes], t.int32)
+            self.modes = modes
+            self._sanity_check_modes([e for e, _ in modes], [m for _, m in modes])
+        else:
+            self.modes = self.allowable_modes
+            ells, mms = self.ells_default, self.mms_default
+        if self.run_phenomd:
+            ells = to_dev([2], t.int32)
+            mms = to_dev([2], t.int32)
+            self.modes = self.allowable_modes
+        self.ells, self.mms = ells, mms
+        num_modes = len(ells)
+        num_bin_all = len(m1)
+        self.length = length
+        self.num_modes = num_modes
+        self.num_bin_all = num_bin_all
+        self.nparams = 3
+        self.num_per_param = length * num_modes * num_bin_all
+        self.num_per_bin = length * num_modes
+        distance = to_dev(atleast_1d(distance))
+        self.t_ref_dev = to_dev(atleast_1d(t_ref))
+        if distance.numel() != num_bin_all or self.t_ref_dev.numel() != num_bin_all:
+            raise ValueError("all parameter arrays must have the same length")
+        if out_buffer is None:
+            self.waveform_carrier = t.zeros(self.nparams * self.num_per_param, dtype=t.float64,
+                                            device=device())
+        else:
+            self.waveform_carrier = out_buffer
+        if freqs is None:
+            f = t.empty(self.num_per_param, dtype=t.float64, device=device())
+            _lib.call("bbhx_default_freqs", _lib.dptr(f), _lib.dptr(m1), _lib.dptr(m2),
+                      _lib.dptr(mms), float(self.mf_min), float(self.mf_max), num_modes, length,
+                      num_bin_all, _lib.stream())
+            self.freqs = f
+        else:
+            freqs = to_dev(freqs)
+            if freqs.ndim == 1:
+                self.freqs = freqs.reshape(1, 1, -1).expand(num_bin_all, num_modes, -1).flatten()
+            elif freqs.ndim == 3:
+                self.freqs = freqs.flatten().clone()
+            else:
+                raise ValueError(
+                    "If providing freqs, must be 1D array (length,) or 3D array (length, num_modes, length).")
+        m1_SI = (m1 * MSUN_SI).contiguous()
+        m2_SI = (m2 * MSUN_SI).contiguous()
+        ncol = 1 if self.run_phenomd else num_modes + 1
+        self.fringdown = t.zeros(num_bin_all * ncol, dtype=t.float64, device=device())
+        self.fdamp = t.zeros_like(self.fringdown)
+        tab = self.qnm_table
+        _lib.call("bbhx_ringdown_frequencies_all", _lib.dptr(self.fringdown), _lib.dptr(self.fdamp),
+                  _lib.dptr(m1), _lib.dptr(m2), _lib.dptr(chi1z), _lib.dptr(chi2z), _lib.dptr(ells),
+                  _lib.dptr(mms), num_modes, num_bin_all, _lib.dptr(tab), tab.shape[1],
+                  float(dspin), int(self.run_phenomd), _lib.stream())
+        nbytes = int(_lib.lib().bbhx_mode_coeffs_bytes())
+        self._coeffs = t.empty(num_bin_all * num_modes * nbytes, dtype=t.uint8, device=device())
+        _lib.call("bbhx_phenomhm_setup", _lib.dptr(self._coeffs), _lib.dptr(ells), _lib.dptr(mms),
+                  _lib.dptr(m1_SI), _lib.dptr(m2_SI), _lib.dptr(chi1z), _lib.dptr(chi2z),
+                  _lib.dptr(distance), _lib.dptr(self.fringdown), _lib.dptr(self.fdamp), num_modes,
+                  num_bin_all, int(self.run_phenomd), _lib.stream())
+        self._m1, self._m2 = m1, m2
+
+    def _evaluate(self):
+        _lib.call("bbhx_phenomhm_points", _lib.dptr(self.waveform_carrier), _lib.dptr(self._freqs),
+                  _lib.dptr(self._coeffs), _lib.dptr(self.t_ref_dev), float(self.initial_t_val),
+                  self.num_modes, self.length, self.num_bin_all, _lib.stream())
+
+    def run_wave(self, m1, m2, chi1z, chi2z, distance, phi_ref, f_ref, t_ref, length, freqs=None,
+                 out_buffer=None, modes=None):
+        """Generate amplitude, phase and t(f) (phenomhm.py:270-507 semantics)."""
+        self._prepare(m1, m2, chi1z, chi2z, distance, phi_ref, f_ref, t_ref, length, freqs,
+                      out_buffer, modes)
+        self._evaluate()
+
+    def _tobs_rows(self, Tobs):
+        t = torch()
+        B, M = self.num_bin_all, self.num_modes
+        if Tobs is None:
+            return t.full((B * M,), 1e300, dtype=t.float64, device=device())
+        if isinstance(Tobs, float):
+            return t.full((B * M,), Tobs, dtype=t.float64, device=device())
+        Tobs_np = Tobs
+        if isinstance(Tobs, np.ndarray) or isinstance(Tobs, t.Tensor):
+            To = to_dev(Tobs)
+            if To.ndim == 1:
+                assert To.shape[0] == B
+                return To.reshape(B, 1).expand(B, M).flatten().contiguous()
+            if To.ndim == 2:
+                assert tuple(To.shape) == (B, M)
+                return To.flatten().contiguous()
+        raise ValueError(f"Tobs entered incorrectly: {type(Tobs_np)}")
+
+    def __call__(self, *args, Tobs=None, direct=False, **kwargs):
+        """``run_wave`` plus, unless ``direct``, the regrid onto the frequency band where
+        0 <= t(f) <= Tobs (phenomhm.py:509-614)."""
+        t = torch()
+        names = ["m1", "m2", "chi1z", "chi2z", "distance", "phi_ref", "f_ref", "t_ref", "length"]
+        kw = dict(zip(names, args))
+        kw.update(kwargs)
+        kw.setdefault("freqs", None)
+        kw.setdefault("out_buffer", None)
+        kw.setdefault("modes", None)
+        self._prepare(**kw)
+        if direct:
+            self._evaluate()
+            return
+        n = self.num_per_param
+        tf0 = t.empty(n, dtype=t.float64, device=device())
+        _lib.call("bbhx_phenomhm_tf", _lib.dptr(tf0), _lib.dptr(self._freqs), _lib.dptr(self._coeffs),
+                  _lib.dptr(self.t_ref_dev), self.num_modes, self.length, self.num_bin_all,
+                  _lib.stream())
+        rows = self.num_bin_all * self.num_modes
+        new_f = t.empty(n, dtype=t.float64, device=device())
+        fminmax = t.empty(2 * rows, dtype=t.float64, device=device())
+        err = t.zeros(1, dtype=t.int32, device=device())
+        tobs_rows = self._tobs_rows(Tobs)
+        _lib.call("bbhx_tf_window_regrid", _lib.dptr(new_f), _lib.dptr(fminmax), _lib.dptr(self._freqs),
+                  _lib.dptr(tf0), _lib.dptr(tobs_rows), self.length, rows,
+                  _lib.dptr(err), _lib.stream())
+        e = int(err.item())
+        if e == 1:
+            raise ValueError(
+                "The search for a window at x_min did not run correctly. If t_ref is close to zero, "
+                "the time-frequency correspondence may be crossing zero twice.")
+        if e == 2:
+            raise ValueError(
+                "The search for a window at x_max did not run correctly. If t_ref is close to the "
+                "observation time, the time-frequency correspondence may be crossing zero twice.")
+        self._freqs = new_f
+        self._evaluate()

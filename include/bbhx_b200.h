@@ -1,0 +1,169 @@
+/*
+ * bbhx_b200 -- C ABI of the B200 (sm_100a) implementation of the BBHx batched
+ * waveform -> likelihood path.
+ *
+ * Conventions (all entry points):
+ *   - return int status: 0 ok, 1 bad argument, 2 CUDA error, 3 timeout, 4 non-finite,
+ *     5 missing orbit tables, 6 size above a fixed limit;
+ *     bbhx_last_error_string() describes the last failure of the calling thread;
+ *   - the last argument is a cudaStream_t passed as void* (NULL = legacy default stream);
+ *     work is stream-ordered, nothing synchronises unless stated;
+ *   - pointers are DEVICE pointers unless marked [host]; complex arrays are interleaved
+ *     (re, im) doubles, layout-compatible with numpy/torch complex128;
+ *   - array layouts are the reference's flat layouts: B = binaries, M = modes,
+ *     L = sparse length, N = data length, P = interpolated quantities (9).
+ *
+ * Each entry point names the reference interface it replaces (paths inside the BBHx
+ * source tree).  Python binds these with ctypes (bbhx_b200/_lib.py).
+ */
+#ifndef BBHX_B200_H
+#define BBHX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ library */
+const char *bbhx_last_error_string(void);
+int bbhx_version(void);
+int bbhx_stream_synchronize(void *stream);
+int bbhx_pointer_is_device(const void *ptr);
+size_t bbhx_mode_coeffs_bytes(void);
+size_t bbhx_response_mode_bytes(void);
+
+/* ------------------------------------------------------------------ PhenomHM */
+/* replaces get_phenomhm_ringdown_frequencies_wrap (src/bbhx/cutils/PhenomHMWaveform.hh:322-333);
+ * masses in solar masses; outputs [B, M] */
+int bbhx_get_phenomhm_ringdown_frequencies(double *fringdown, double *fdamp, const double *m1,
+                                           const double *m2, const double *chi1z,
+                                           const double *chi2z, const int *ells, const int *mms,
+                                           int num_modes, int num_bin_all, void *stream);
+
+/* replaces get_phenomd_ringdown_frequencies_wrap (PhenomHMWaveform.hh:335-352); outputs [B] */
+int bbhx_get_phenomd_ringdown_frequencies(double *fringdown, double *fdamp, const double *m1,
+                                          const double *m2, const double *chi1z,
+                                          const double *chi2z, int num_bin_all,
+                                          const double *y_rd, const double *c1_rd,
+                                          const double *c2_rd, const double *c3_rd,
+                                          const double *y_dm, const double *c1_dm,
+                                          const double *c2_dm, const double *c3_dm, double dspin,
+                                          void *stream);
+
+/* both ringdown sets in the [B, M+1] layout the waveform kernel reads
+ * (replaces the two calls + concatenation of src/bbhx/waveforms/phenomhm.py:397-463);
+ * qnm_table = 8 rows of table_len: y, c1, c2, c3 (ringdown), y, c1, c2, c3 (damping) */
+int bbhx_ringdown_frequencies_all(double *fringdown, double *fdamp, const double *m1,
+                                  const double *m2, const double *chi1z, const double *chi2z,
+                                  const int *ells, const int *mms, int num_modes, int num_bin_all,
+                                  const double *qnm_table, int table_len, double dspin,
+                                  int run_phenomd, void *stream);
+
+/* replaces waveform_amp_phase (PhenomHMWaveform.hh:354-371): waveform_out [>=3, B, M, L] */
+int bbhx_waveform_amp_phase(double *waveform_out, const int *ells, const int *mms,
+                            const double *freqs, const double *m1_SI, const double *m2_SI,
+                            const double *chi1z, const double *chi2z, const double *distance,
+                            const double *f_ref, int num_modes, int length, int num_bin_all,
+                            const double *Mf_RD_lm, const double *Mf_DM_lm, int run_phenomd,
+                            void *stream);
+
+/* split form of waveform_amp_phase: per-(binary, mode) records (B*M * bbhx_mode_coeffs_bytes()),
+ * then per-frequency evaluation with the t_ref shift of phenomhm.py:485-507 fused (t_ref may
+ * be NULL), or t(f) alone */
+int bbhx_phenomhm_setup(void *coeffs, const int *ells, const int *mms, const double *m1_SI,
+                        const double *m2_SI, const double *chi1z, const double *chi2z,
+                        const double *distance, const double *Mf_RD_lm, const double *Mf_DM_lm,
+                        int num_modes, int num_bin_all, int run_phenomd, void *stream);
+int bbhx_phenomhm_points(double *waveform_out, const double *freqs, const void *coeffs,
+                         const double *t_ref, double t_init, int num_modes, int length,
+                         int num_bin_all, void *stream);
+int bbhx_phenomhm_tf(double *tf_out, const double *freqs, const void *coeffs, const double *t_ref,
+                     int num_modes, int length, int num_bin_all, void *stream);
+
+/* default sparse grid of phenomhm.py:208-224 */
+int bbhx_default_freqs(double *freqs, const double *m1, const double *m2, const int *mms,
+                       double mf_min, double mf_max, int num_modes, int length, int num_bin_all,
+                       void *stream);
+
+/* observation-window regrid of phenomhm.py:513-614 (t(f) crossing of 0 and Tobs, then
+ * logspace); err_dev: device int, zeroed by the caller, 1/2 on a failed crossing search */
+int bbhx_tf_window_regrid(double *freqs_out, double *fminmax, const double *freqs_in,
+                          const double *tf, const double *Tobs, int length, long long num_rows,
+                          int *err_dev, void *stream);
+
+/* ------------------------------------------------------------------ response */
+/* replaces pyFastLISAResponse / AddOrbits (src/bbhx/cutils/lisaresponse.pyx:12-13,34-76) */
+int bbhx_orbits_create(void **handle);
+/* n_arr, L_arr, x_arr, links, sc_r, sc_e are [host] arrays (copied to the device) */
+int bbhx_orbits_add_orbit_information(void *handle, double dt, int N, const double *n_arr,
+                                      const double *L_arr, const double *x_arr, const int *links,
+                                      const int *sc_r, const int *sc_e, double armlength);
+int bbhx_orbits_destroy(void *handle);
+
+/* replaces FastLISAResponse::LISA_response (src/bbhx/cutils/Response.hh:27-41) */
+int bbhx_LISA_response(void *orbits, double *response_out, const int *ells, const int *mms,
+                       const double *freqs, const double *phi_ref, const double *inc,
+                       const double *lam, const double *beta, const double *psi, int TDItag,
+                       int rescaled, int tdi2, int order_fresnel_stencil, int num_modes,
+                       int length, int num_bin_all, int includes_amps, void *stream);
+
+/* fused PhenomHM + response into a [9, B, M, L] buffer (waveformbuild.py:516-560 in one pass) */
+int bbhx_waveform_response_fused(void *orbits, double *buf, const double *freqs,
+                                 const void *coeffs, const int *ells, const int *mms,
+                                 const double *phi_ref, const double *inc, const double *lam,
+                                 const double *beta, const double *psi, const double *t_ref,
+                                 double t_init, int TDItag, int rescaled, int tdi2, int num_modes,
+                                 int length, int num_bin_all, void *stream);
+
+/* ------------------------------------------------------------------ spline */
+/* replaces interpolate (src/bbhx/cutils/Interpolate.hh:4-6) */
+int bbhx_interpolate(const double *freqs, const double *y, double *B_, double *upper_diag,
+                     double *diag, double *lower_diag, int length, int num_interp_params,
+                     int num_modes, int num_bin_all, void *stream);
+
+/* ------------------------------------------------------------------ templates */
+/* replaces InterpTDI (src/bbhx/cutils/WaveformBuild.hh:6); template_ptrs, t_start, t_end,
+ * inds_ptrs, inds_start, ind_lengths are [host] arrays (pointer arrays hold device addresses) */
+int bbhx_InterpTDI(const int64_t *template_ptrs, const double *data_freqs, const double *freqs,
+                   const double *y, const double *c1, const double *c2, const double *c3,
+                   const double *t_start, const double *t_end, int length, int data_length,
+                   int num_bin_all, int num_modes, const int64_t *inds_ptrs,
+                   const int *inds_start, const int *ind_lengths, void *stream);
+
+/* replaces direct_sum (WaveformBuild.hh:8-10) */
+int bbhx_direct_sum(double *templates, const double *buffer, int num_bin_all, int length,
+                    int n_channels, int num_modes, const double *t_start, const double *t_end,
+                    void *stream);
+
+/* ------------------------------------------------------------------ likelihood */
+/* replaces direct_like (src/bbhx/cutils/Likelihood.hh:11); d_h, h_h [host] complex, += ;
+ * template_ptrs, inds_start, ind_lengths [host]; blocks until the results are on the host */
+int bbhx_direct_like(double *d_h, double *h_h, const double *data, const double *noise,
+                     const int64_t *template_ptrs, const int *inds_start, const int *ind_lengths,
+                     int data_stream_length, int num_bin_all, void *stream);
+
+/* replaces hdyn (Likelihood.hh:6-9) */
+int bbhx_hdyn(double *d_h, double *h_h, const double *residuals, const double *constants,
+              const double *freqs, int num_bin_all, int length, int n_channels, void *stream);
+
+/* support [start, start+len) of each binary on the data grid (waveformbuild.py:136-177) */
+int bbhx_template_support(int *start, int *len, const double *x, int num_modes, int length,
+                          int num_bin_all, const double *data_freqs, int data_length,
+                          void *stream);
+
+/* fused interpolate + mode sum + noise weighting + <d|h>, <h|h> reduction; no templates are
+ * stored (equivalent to InterpTDI followed by direct_like, waveformbuild.py:641-660 +
+ * likelihood.py:177-214); d_h, h_h device complex [B], overwritten */
+int bbhx_direct_like_fused(double *d_h, double *h_h, const double *data_freqs, const double *data,
+                           const double *noise, int data_length, const double *x, const double *y,
+                           const double *c1, const double *c2, const double *c3,
+                           const double *t_start, const double *t_end, int num_modes, int length,
+                           int num_bin_all, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BBHX_B200_H */
