@@ -42,15 +42,22 @@ class Likelihood:
         t = torch()
         self.phase_marginalize = phase_marginalize
         self.return_extracted_snr = return_extracted_snr
-        params = np.atleast_2d(np.asarray(to_np(params) if isinstance(params, t.Tensor) else params,
-                                          dtype=np.float64))
-        if params.shape[0] != 12 and params.shape[1] == 12:
-            params = params.T
+        if isinstance(params, t.Tensor):
+            # (pinned) host or device tensor: one asynchronous copy, parameters stay on the GPU
+            params = params.to(device=device(), dtype=t.float64, non_blocking=True)
+            if params.ndim == 1:
+                params = params.reshape(-1, 1)
+            params = tuple(params[k].contiguous() for k in range(params.shape[0]))
+        else:
+            params = np.atleast_2d(np.asarray(params, dtype=np.float64))
+            if params.shape[0] != 12 and params.shape[1] == 12:
+                params = params.T
+            params = tuple(params)
         kw = dict(waveform_kwargs)
         for k in ("freqs", "fill", "direct", "compress", "squeeze", "combine"):
             kw.pop(k, None)
-        flags = t.zeros(2, dtype=t.int32, device=device())
-        d_h, h_h = self.waveform_gen.inner_products(tuple(params), self.data_freqs,
+        flags = t.zeros(3, dtype=t.int32, device=device())
+        d_h, h_h = self.waveform_gen.inner_products(params, self.data_freqs,
                                                     self.data_channels, self.noise_factors,
                                                     flags=flags, **kw)
         self.d_h, self.h_h = d_h, h_h
@@ -68,6 +75,8 @@ class Likelihood:
                              "crossing zero twice.")
         if fl[1] != 0:
             raise ValueError("Orbital information does not cover the t(f) range of the templates.")
+        if fl[2] != 0:
+            raise ValueError("chi1z or chi2z array contains values with abs(chi) > 1.0 which is not allowed.")
         ll = packed[:B]
         if return_extracted_snr:
             return np.array([ll, packed[B:2 * B] / np.sqrt(packed[2 * B:3 * B])]).T

@@ -99,6 +99,20 @@ class BBHWaveformFD:
     # ------------------------------------------------------------------ helpers
     @staticmethod
     def _time_limits(lam, beta, t_obs_start, t_obs_end):
+        """SSB-frame start / end of the observation (waveformbuild.py:477-484): numpy on
+        the host for host inputs, torch on the device for device inputs."""
+        t = torch()
+        if isinstance(lam, t.Tensor) and lam.is_cuda:
+            from .utils.constants import C_SI, ConstOmega, OrbitR
+
+            def tssb(tL):
+                phase = ConstOmega * tL - lam
+                RoC = OrbitR / C_SI
+                cb = t.cos(beta)
+                return (tL + RoC * cb * t.cos(phase)
+                        - 1.0 / 2 * ConstOmega * (RoC * cb) ** 2 * t.sin(2.0 * phase))
+
+            return tssb(t_obs_start * YRSID_SI).contiguous(), tssb(t_obs_end * YRSID_SI).contiguous()
         t_start = np.atleast_1d(tSSBfromLframe(t_obs_start * YRSID_SI, lam, beta, 0.0))
         t_end = np.atleast_1d(tSSBfromLframe(t_obs_end * YRSID_SI, lam, beta, 0.0))
         return t_start, t_end
@@ -113,8 +127,11 @@ class BBHWaveformFD:
         recorded there instead of raising, so the caller can defer the host sync."""
         t = torch()
         (m1, m2, chi1z, chi2z, distance, phi_ref, f_ref, inc, lam, beta, psi, t_ref) = params
-        lam_h = to_np(atleast_1d(lam)).astype(np.float64)
-        beta_h = to_np(atleast_1d(beta)).astype(np.float64)
+        if isinstance(lam, t.Tensor) and lam.is_cuda:
+            lam_h, beta_h = atleast_1d(lam), atleast_1d(beta)
+        else:
+            lam_h = to_np(atleast_1d(lam)).astype(np.float64)
+            beta_h = to_np(atleast_1d(beta)).astype(np.float64)
         t_start, t_end = self._time_limits(lam_h, beta_h, t_obs_start, t_obs_end)
         if freqs is None and length is None:
             raise ValueError("Must input freqs or length.")
@@ -124,8 +141,8 @@ class BBHWaveformFD:
             length = freqs.shape[-1] if freqs is not None else length
         M = len(modes) if modes is not None else len(ap.allowable_modes)
         out_buffer = t.zeros(9 * length * M * B, dtype=t.float64, device=device())
-        ap._prepare(m1, m2, chi1z, chi2z, distance, np.zeros(B), f_ref, t_ref, length,
-                    freqs if direct else None, out_buffer, modes)
+        ap._prepare(m1, m2, chi1z, chi2z, distance, None, f_ref, t_ref, length,
+                    freqs if direct else None, out_buffer, modes, flags=flags)
         M = ap.num_modes
         if not direct:
             n = ap.num_per_param
@@ -136,7 +153,7 @@ class BBHWaveformFD:
             new_f = t.empty(n, dtype=t.float64, device=device())
             fminmax = t.empty(2 * rows, dtype=t.float64, device=device())
             err = flags if flags is not None else t.zeros(2, dtype=t.int32, device=device())
-            Tobs = ap._tobs_rows(np.asarray(t_end - t_start, dtype=np.float64))
+            Tobs = ap._tobs_rows(t_end - t_start)
             _lib.call("bbhx_tf_window_regrid", _lib.dptr(new_f), _lib.dptr(fminmax),
                       _lib.dptr(ap._freqs), _lib.dptr(tf0), _lib.dptr(Tobs), length, rows,
                       _lib.dptr(err), _lib.stream())
@@ -231,7 +248,7 @@ class BBHWaveformFD:
         return (template_channels, self.interp_response.start_inds, self.interp_response.lengths)
 
     def inner_products(self, params, data_freqs, data_weighted, noise_factors, t_obs_start=0.0,
-                       t_obs_end=1.0, length=1024, modes=None, flags=None, **unused):
+                       t_obs_end=1.0, length=1024, modes=None, flags=None, timing=None, **unused):
         """Fused <d|h>, <h|h> for every binary (device complex128 [B] each).
 
         ``data_weighted`` [3, N] complex = data * sqrt(df / S); ``noise_factors`` [3, N] =
@@ -252,8 +269,16 @@ class BBHWaveformFD:
         # argument list can be handed back by the caching allocator to the next one
         ts_d = to_dev(t_start)
         te_d = to_dev(t_end)
+        if timing is not None:  # optional CUDA events around the fused kernel (benchmarks)
+            ev0 = t.cuda.Event(enable_timing=True)
+            ev1 = t.cuda.Event(enable_timing=True)
+            ev0.record()
         _lib.call("bbhx_direct_like_fused", _lib.dptr(d_h), _lib.dptr(h_h), _lib.dptr(data_freqs),
                   _lib.dptr(data_weighted), _lib.dptr(noise_factors), int(data_freqs.numel()),
                   _lib.dptr(x), _lib.dptr(buf), _lib.dptr(c1), _lib.dptr(c2), _lib.dptr(c3),
                   _lib.dptr(ts_d), _lib.dptr(te_d), M, L, B, _lib.stream())
+        if timing is not None:
+            ev1.record()
+            timing.setdefault("fused", []).append((ev0, ev1))
+            self._last_x = x
         return d_h, h_h

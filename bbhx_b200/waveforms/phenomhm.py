@@ -78,12 +78,19 @@ class PhenomHMAmpPhase:
                     .format(ell, mm, self.allowable_modes))
 
     @staticmethod
-    def _sanity_check_params(m1, m2, chi1z, chi2z):
+    def _sanity_check_params(m1, m2, chi1z, chi2z, flags=None):
+        """|chi| <= 1 check and m1 >= m2 ordering (phenomhm.py:175-199).  With a device
+        ``flags`` tensor the spin check is recorded in flags[2] instead of raising, so no
+        host synchronisation happens here."""
         t = torch()
-        if bool((chi1z.abs() > 1.0).any()):
-            raise ValueError("chi1z array contains values with abs(chi1z) > 1.0 which is not allowed.")
-        if bool((chi2z.abs() > 1.0).any()):
-            raise ValueError("chi2z array contains values with abs(chi2z) > 1.0 which is not allowed.")
+        if flags is not None:
+            bad = (chi1z.abs() > 1.0).any() | (chi2z.abs() > 1.0).any()
+            flags[2] = t.where(bad, t.ones_like(flags[2]), flags[2])
+        else:
+            if bool((chi1z.abs() > 1.0).any()):
+                raise ValueError("chi1z array contains values with abs(chi1z) > 1.0 which is not allowed.")
+            if bool((chi2z.abs() > 1.0).any()):
+                raise ValueError("chi2z array contains values with abs(chi2z) > 1.0 which is not allowed.")
         switch = m1 < m2
         return (t.where(switch, m2, m1), t.where(switch, m1, m2), t.where(switch, chi2z, chi1z),
                 t.where(switch, chi1z, chi2z))
@@ -118,7 +125,7 @@ class PhenomHMAmpPhase:
 
     # ------------------------------------------------------------------ core
     def _prepare(self, m1, m2, chi1z, chi2z, distance, phi_ref, f_ref, t_ref, length, freqs,
-                 out_buffer, modes):
+                 out_buffer, modes, flags=None):
         """Shared front half of run_wave: parameter checks, modes, buffers, ringdown
         frequencies and the per-(binary, mode) model records."""
         t = torch()
@@ -126,7 +133,7 @@ class PhenomHMAmpPhase:
         m2 = to_dev(atleast_1d(m2)).clone()
         chi1z = to_dev(atleast_1d(chi1z)).clone()
         chi2z = to_dev(atleast_1d(chi2z)).clone()
-        m1, m2, chi1z, chi2z = self._sanity_check_params(m1, m2, chi1z, chi2z)
+        m1, m2, chi1z, chi2z = self._sanity_check_params(m1, m2, chi1z, chi2z, flags)
         if modes is not None:
             ells = to_dev([ell for ell, mm in modes], t.int32)
             mms = to_dev([mm for ell, mm in modes], t.int32)

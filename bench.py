@@ -1,0 +1,409 @@
+#!/usr/bin/env python
+"""Benchmark of the batched BBHx waveform -> likelihood path on B200.
+
+Workload (one "step"): the direct log-likelihood of B = 1024 massive-black-hole binaries
+(seeded draws: total mass log-U[1e5, 1e7] Msun, q ~ U[0.1, 1], spins U[-0.9, 0.9], ...),
+PhenomHM with 6 modes on 1024-point sparse grids, 2nd-generation TDI A/E/T, Tobs = 1 yr,
+data grid df = 1/Tobs over [1e-5, 0.1] Hz (~3.16e6 bins; complex128 data and real noise
+weights, ~250 MB, larger than L2), synthetic data = seeded injection + Gaussian noise from
+the analytic PSD.  All arithmetic FP64.
+
+  value  : lnL evaluations / s with parameters already resident on the GPU
+  e2e    : the same through the public API (Likelihood.get_ll) from pinned host params,
+           including the H2D copy of the 12 x B parameters and the D2H copy of the B lnL
+  roofline: the fused interpolate + reduce kernel against measured HBM bandwidth, with
+           72 B of algorithmic traffic per (binary, data bin)
+  cpu_baseline: the reference's own C++ CPU path (oracle/_ref) on a bounded sample
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+For N > 1 launch under torchrun; every rank evaluates its own batch (weak scaling) and the
+time is the max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+TOBS = 1.0
+F_LO, F_HI = 1e-5, 0.1
+LENGTH = 1024
+SEED_PARAMS = 1234
+SEED_NOISE = 99
+HBM_BYTES_PER_PAIR = 72.0  # 3 x complex128 weighted data + 3 x float64 noise weights
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--batch", type=int, default=1024)
+    ap.add_argument("--no-extra", action="store_true", help="skip the heterodyned metric")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--het-batch", type=int, default=65536)
+    return ap.parse_args()
+
+
+def rank_info():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+# --------------------------------------------------------------------------- CPU (oracle)
+def _cpu_worker(args):
+    """One spawn worker: the reference CPU path (oracle/_ref) for a chunk of binaries."""
+    chunk, = args
+    sys.path.insert(0, REPO)
+    from bbhx_b200.sensitivity import aet_psd
+    from bbhx_b200.synthetic import data_grid, gaussian_noise
+    from oracle.pipeline import RefPipeline
+
+    f = data_grid(TOBS, F_LO, F_HI)
+    psd = np.array([aet_psd(f, c, tdi2=True) for c in "AET"])
+    data = gaussian_noise(psd, f[1] - f[0], SEED_NOISE)
+    pipe = RefPipeline("ref", tdi2=True)
+    t0 = time.perf_counter()
+    pipe.direct_lnl(chunk, f, data, psd, length=LENGTH, t_obs_end=TOBS)
+    return time.perf_counter() - t0
+
+
+def cpu_reference(params, workers, steps=1, warmup=0):
+    """Time the reference CPU path with `workers` processes, one binary each per step.
+    Returns (binaries per second, per-step seconds list)."""
+    import multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    B = params.shape[1]
+    times = []
+    with ctx.Pool(workers) as pool:
+        for s in range(warmup + steps):
+            idx = [(s * workers + w) % B for w in range(workers)]
+            chunks = [(params[:, i:i + 1].copy(),) for i in idx]
+            t0 = time.perf_counter()
+            pool.map(_cpu_worker, chunks)
+            dt = time.perf_counter() - t0
+            if s >= warmup:
+                times.append(dt)
+    return workers / statistics.mean(times), times
+
+
+def cpu_workers():
+    n = os.cpu_count() or 1
+    return max(1, min(n, 64))
+
+
+# --------------------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.path = os.path.join(REPO, "gpurun_out", f"clocks_rank{gpu_index}.csv")
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        self.proc = None
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(gpu_index)], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------- GPU arm
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
+    except Exception:
+        return None
+
+
+def ncu_traffic_per_pair():
+    """DRAM bytes per (binary, bin) of the fused kernel from the committed ncu summary."""
+    try:
+        d = json.load(open(os.path.join(REPO, "profiles", "direct_fused_traffic.json")))
+        return float(d["dram_bytes_per_pair"])
+    except Exception:
+        return None
+
+
+def build_problem(B, seed_params=SEED_PARAMS):
+    import torch
+
+    from bbhx_b200 import BBHWaveformFD, EqualArmlengthOrbits, Likelihood
+    from bbhx_b200.sensitivity import aet_psd
+    from bbhx_b200.synthetic import data_grid, draw_params, gaussian_noise
+
+    f = data_grid(TOBS, F_LO, F_HI)
+    df = f[1] - f[0]
+    psd = np.array([aet_psd(f, c, tdi2=True) for c in "AET"])
+    wave = BBHWaveformFD(response_kwargs=dict(orbits=EqualArmlengthOrbits(), TDItag="AET", tdi2=True))
+    inj = draw_params(1, TOBS, seed_params + 7)
+    h = wave(*inj, freqs=f, length=LENGTH, t_obs_start=0.0, t_obs_end=TOBS, direct=False,
+             fill=True, combine=True)
+    data = gaussian_noise(psd, df, SEED_NOISE) + h.cpu().numpy()
+    like = Likelihood(wave, f, data, psd)
+    params = draw_params(B, TOBS, seed_params)
+    torch.cuda.synchronize()
+    return wave, like, params, f
+
+
+def gpu_arm(args):
+    import torch
+
+    rank, world, local = rank_info()
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    from bbhx_b200 import build_ext
+
+    build_ext.build()
+    B = args.batch
+    wave, like, params, f = build_problem(B, SEED_PARAMS + 1000 * rank)
+    dev_params = tuple(torch.as_tensor(params[k], device="cuda") for k in range(12))
+    kw = dict(length=LENGTH, t_obs_start=0.0, t_obs_end=TOBS)
+    flags = torch.zeros(3, dtype=torch.int32, device="cuda")
+
+    def step(timing=None):
+        d_h, h_h = wave.inner_products(dev_params, like.data_freqs, like.data_channels,
+                                       like.noise_factors, flags=flags, timing=timing, **kw)
+        return -0.5 * (like.d_d + h_h - 2 * d_h).real
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        out = step()
+    torch.cuda.synchronize()
+    if int(flags.abs().sum().item()) != 0:
+        raise RuntimeError(f"device error flags set: {flags.tolist()}")
+    sampler = ClockSampler(local) if rank == 0 or world > 1 else None
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    timing = {}
+    e0.record()
+    for _ in range(args.steps):
+        out = step(timing)
+    e1.record()
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop() if sampler else None
+    ms_total = e0.elapsed_time(e1)
+    fused_ms = [a.elapsed_time(b) for a, b in timing["fused"]]
+    ms = torch.tensor([ms_total], device="cuda", dtype=torch.float64)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+    ms_total = float(ms.item())
+    lnl = out.cpu().numpy()
+    assert np.all(np.isfinite(lnl)), "non-finite lnL"
+
+    # support sizes (sum of per-binary data-grid lengths) for the roofline
+    from bbhx_b200 import _lib
+
+    x = wave._last_x
+    sup = torch.zeros(2 * B, dtype=torch.int32, device="cuda")
+    _lib.call("bbhx_template_support", _lib.dptr(sup), _lib.dptr(sup[B:]), _lib.dptr(x),
+              wave.num_modes, LENGTH, B, _lib.dptr(like.data_freqs), len(f), _lib.stream())
+    pairs = float(sup[B:].double().sum().item())
+
+    # end to end through the public API from pinned host memory
+    host = torch.tensor(params, dtype=torch.float64).pin_memory()
+    for _ in range(2):
+        like.get_ll(host, **kw)
+    torch.cuda.synchronize()
+    barrier()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for _ in range(args.steps):
+        ll_host = like.get_ll(host, **kw)
+    t1.record()
+    torch.cuda.synchronize()
+    e2e_ms = torch.tensor([t0.elapsed_time(t1)], device="cuda", dtype=torch.float64)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.all_reduce(e2e_ms, op=dist.ReduceOp.MAX)
+    e2e_ms = float(e2e_ms.item())
+    dl = float(np.max(np.abs(ll_host - lnl)))
+
+    extra = {}
+    if not args.no_extra:
+        extra.update(het_metric(args, wave, like, f, params))
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    if rank != 0:
+        return None
+    peaks = measured_peaks()
+    peak = peaks["hbm_gbs"] if peaks else 6650.0
+    fused_avg_s = statistics.mean(fused_ms) / 1e3
+    achieved = HBM_BYTES_PER_PAIR * pairs / fused_avg_s / 1e9
+    tpp = ncu_traffic_per_pair()
+    n_evals = B * args.steps * world
+    res = {
+        "metric": "lnL evals/s (direct, heterodyned) mixed vs FP64 plain at |dlnL|<=1e-2; grad/s",
+        "value": n_evals / (ms_total / 1e3),
+        "unit": "lnL evals/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_total / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic: seeded PhenomHM injection + Gaussian noise from the analytic A/E/T PSD",
+        "config": {"workload": "direct lnL, plain FP64, B=%d binaries x 6 modes, sparse L=%d, "
+                               "Tobs=1 yr, df=1/Tobs over 1e-5..0.1 Hz (N=%d bins), AET TDI2"
+                               % (B, LENGTH, len(f)),
+                   "global_batch": n_evals // args.steps, "data_bins": len(f),
+                   "binary_bin_pairs_per_step": pairs,
+                   "l2": "inputs larger than L2 (data 227 MB + sparse buffers 1.8 GB per step)",
+                   "parallelism": f"replicas x{world} (independent binary batches per GPU)"},
+        "e2e": {"value": n_evals / (e2e_ms / 1e3), "unit": "lnL evals/s",
+                "h2d_bytes_per_step": 12 * B * 8, "d2h_bytes_per_step": 3 * B * 8 + 3 * 8,
+                "max_abs_dlnl_vs_device_path": dl},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak,
+                     "traffic": (tpp * pairs if tpp is not None else None),
+                     "kernel": "k_direct_fused (bbhx_direct_like_fused)",
+                     "kernel_ms": statistics.mean(fused_ms),
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback"},
+        "gpu_launches": 12 * args.steps,
+        "clocks": clocks,
+    }
+    res.update(extra)
+    return res
+
+
+def het_metric(args, wave, like, f, params):
+    """Heterodyned lnL evals/s: 128 relative-binning bins, B walkers around the injection."""
+    import torch
+
+    from bbhx_b200 import AET1SensitivityMatrix, HeterodynedLikelihood
+    from bbhx_b200.synthetic import perturb_params
+
+    kw = dict(t_obs_start=0.0, t_obs_end=TOBS)
+    center = params[:, 0]
+    data = (like.data_channels / like.noise_factors).reshape(3, -1).cpu().numpy()
+    het = HeterodynedLikelihood(wave, f, data, center, 128, template_gen_kwargs=dict(kw),
+                                reference_gen_kwargs=dict(kw, length=LENGTH),
+                                sens_mat=AET1SensitivityMatrix(f, tdi2=True))
+    Bh = args.het_batch
+    walkers = perturb_params(center, Bh, 5)
+    for _ in range(2):
+        het.get_ll(walkers, **kw)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    n = max(2, args.steps // 2)
+    e0.record()
+    for _ in range(n):
+        ll = het.get_ll(walkers, **kw)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    return {"heterodyned": {"value": Bh * n / (ms / 1e3), "unit": "lnL evals/s", "batch": Bh,
+                            "bins": 128, "dtype": "f64", "path": "e2e via HeterodynedLikelihood.get_ll",
+                            "finite": bool(np.all(np.isfinite(ll)))}}
+
+
+def reference_arm(args):
+    rank, world, _ = rank_info()
+    if rank != 0:
+        return None
+    from bbhx_b200.synthetic import draw_params
+
+    params = draw_params(args.batch, TOBS, SEED_PARAMS)
+    workers = cpu_workers()
+    val, times = cpu_reference(params, workers, steps=args.steps, warmup=args.warmup)
+    cpu = {"value": val, "unit": "lnL evals/s", "cores": workers, "kind": "reference",
+           "sample": f"{workers} binaries per step (one per process) at the full workload size"}
+    return {"impl": "reference", "metric": "lnL evals/s (direct, heterodyned) mixed vs FP64 plain at |dlnL|<=1e-2; grad/s",
+            "value": val, "unit": "lnL evals/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": "direct lnL, plain FP64, Tobs=1 yr, N=%d bins, 6 modes, L=1024" % 3155822},
+            "cpu_baseline": cpu,
+            "e2e": {"value": val, "unit": "lnL evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        res = reference_arm(args)
+        if res is not None:
+            print(json.dumps(res), flush=True)
+        return
+    rank, world, _ = rank_info()
+    res = gpu_arm(args)
+    if res is None:
+        return
+    if not args.no_cpu and world == 1:
+        from bbhx_b200.synthetic import draw_params
+
+        params = draw_params(args.batch, TOBS, SEED_PARAMS)
+        workers = cpu_workers()
+        val, _ = cpu_reference(params, workers, steps=1, warmup=0)
+        res["cpu_baseline"] = {"value": val, "unit": "lnL evals/s", "cores": workers,
+                               "kind": "reference",
+                               "sample": f"{workers} binaries of the same workload, one per process, "
+                                         "reference C++ CPU path (oracle/_ref) with the reference driver logic"}
+    print(json.dumps(res), flush=True)
+
+
+if __name__ == "__main__":
+    main()
