@@ -28,6 +28,7 @@ _SIGS = {
     "bbhx_get_phenomd_ringdown_frequencies": [_VP] * 6 + [_I] + [_VP] * 8 + [_D, _VP],
     "bbhx_ringdown_frequencies_all": [_VP] * 8 + [_I, _I, _VP, _I, _D, _I, _VP],
     "bbhx_waveform_amp_phase": [_VP] * 10 + [_I, _I, _I, _VP, _VP, _I, _VP],
+    "bbhx_waveform_amp_phase_noalloc": [_VP] * 10 + [_I, _I, _I, _VP, _VP, _I, _VP],
     "bbhx_phenomhm_setup": [_VP] * 10 + [_I, _I, _I, _VP],
     "bbhx_phenomhm_points": [_VP, _VP, _VP, _VP, _D, _I, _I, _I, _VP],
     "bbhx_phenomhm_tf": [_VP, _VP, _VP, _VP, _I, _I, _I, _VP],

@@ -5,6 +5,8 @@
 //   waveform_amp_phase.
 // Layout of the waveform buffer (phenomhm.py:201-249): flat [nparams, B, M, L] with
 // slot 0 = amplitude, 1 = phase, 2 = t(f); freqs flat [B, M, L].
+#include <mutex>
+
 #include "capi_internal.cuh"
 #include "phenomhm_model.cuh"
 
@@ -214,12 +216,42 @@ __global__ void k_default_freqs(double* freqs, const double* m1, const double* m
   }
 }
 
+// ------------------------------------------------------------------ allocation-free variant
+// Scratch of bbhx_waveform_amp_phase_noalloc: the per-(binary, mode) model records live in
+// this file-scope device array instead of memory obtained with cudaMalloc / cudaMallocAsync.
+// It is part of the library's device image, so every GPU that loads the library holds it
+// (kNoAllocMaxRecords * sizeof(ModeCoeffs) = 8192 * 752 B, about 6.2 MB) until the process
+// exits.  All calls share it.
+constexpr long long kNoAllocMaxRecords = 8192;
+static __device__ __align__(256) ModeCoeffs g_noalloc_records[kNoAllocMaxRecords];
+
 }  // namespace bbhx
 
 using namespace bbhx;
 
 namespace {
 constexpr int kThreads = 256;
+
+// Device address of g_noalloc_records for the current device, looked up once per device.
+// In host code the array's name is only a host-side stand-in, not a device address, so the
+// kernels are given the address that cudaGetSymbolAddress returns.
+std::mutex g_noalloc_mutex;
+void* g_noalloc_addr[256] = {};
+
+int noalloc_records(ModeCoeffs** out) {
+  int dev = 0;
+  BBHX_CHECK_CUDA(cudaGetDevice(&dev));
+  BBHX_REQUIRE(dev >= 0 && dev < 256, "device ordinal %d out of range", dev);
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (g_noalloc_addr[dev] == nullptr) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_records);
+    if (e != cudaSuccess) return cuda_status(e, "cudaGetSymbolAddress(g_noalloc_records)");
+    g_noalloc_addr[dev] = p;
+  }
+  *out = (ModeCoeffs*)g_noalloc_addr[dev];
+  return OK;
+}
 
 int alloc_coeffs(ModeCoeffs** p, long long n, cudaStream_t s) {
   BBHX_CHECK_CUDA(cudaMallocAsync((void**)p, sizeof(ModeCoeffs) * (size_t)n, s));
@@ -321,6 +353,56 @@ int bbhx_waveform_amp_phase(double* waveform_out, const int* ells, const int* mm
   }
   cudaFreeAsync(c, s);
   return st;
+}
+
+// Allocation-free form of bbhx_waveform_amp_phase, for callers that must not allocate
+// device memory: hosts whose own memory pool owns the whole GPU and forbids allocations made
+// behind its back, latency-critical loops in which cudaMalloc's implicit device-wide
+// synchronisation would stall work on other streams, and deployments without the
+// stream-ordered allocator that cudaMallocAsync needs.  Same arguments, layout and results
+// as bbhx_waveform_amp_phase; the per-(binary, mode) records go to the library's static
+// device array (at most 8192 records, i.e. num_bin_all * num_modes <= 8192; larger requests
+// return status 6 without launching anything).
+//   * Nothing is allocated or freed: no cudaMalloc / cudaFree / cudaMallocAsync, no library
+//     routine that allocates.
+//   * The first call on a device looks up the array's device address once for that device
+//     (cudaGetSymbolAddress, which may also load the library's device code); make that first
+//     call before any stream capture.
+//   * Every call uses the same array and it keeps the last call's records.  Each call
+//     overwrites every record it reads before reading it, so nothing needs clearing, but calls
+//     that overlap on the GPU (different streams, or different host threads, without ordering
+//     between them) race on the array: serialise them.
+int bbhx_waveform_amp_phase_noalloc(double* waveform_out, const int* ells, const int* mms,
+                                    const double* freqs, const double* m1_SI, const double* m2_SI,
+                                    const double* chi1z, const double* chi2z,
+                                    const double* distance, const double* f_ref, int num_modes,
+                                    int length, int num_bin_all, const double* Mf_RD_lm,
+                                    const double* Mf_DM_lm, int run_phenomd, void* stream) {
+  (void)f_ref;
+  BBHX_REQUIRE(num_modes > 0 && num_modes <= MAX_MODES, "num_modes must be 1..6");
+  BBHX_REQUIRE(length >= 1 && num_bin_all >= 0, "bad length / num_bin_all");
+  if (run_phenomd) BBHX_REQUIRE(num_modes == 1, "run_phenomd requires one mode");
+  long long nbm = (long long)num_bin_all * num_modes;
+  if (nbm > kNoAllocMaxRecords) {
+    set_error("bbhx_waveform_amp_phase_noalloc: num_bin_all * num_modes = %lld exceeds the "
+              "static scratch capacity of %lld (binary, mode) records; split the batch or use "
+              "bbhx_waveform_amp_phase", nbm, kNoAllocMaxRecords);
+    return ERR_TOO_LARGE;
+  }
+  if (num_bin_all == 0) return OK;
+  ModeCoeffs* c = nullptr;
+  int st = noalloc_records(&c);
+  if (st) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  k_phm_setup<<<grid_for(nbm, 128), 128, 0, s>>>(c, ells, mms, m1_SI, m2_SI, chi1z, chi2z,
+                                                  distance, Mf_RD_lm, Mf_DM_lm, num_modes,
+                                                  num_bin_all, run_phenomd);
+  st = launch_status("k_phm_setup");
+  if (st) return st;
+  long long n = nbm * length;
+  k_phm_points<<<grid_for(n, kThreads), kThreads, 0, s>>>(waveform_out, freqs, c, num_modes,
+                                                          length, num_bin_all, nullptr, 0.0);
+  return launch_status("k_phm_points");
 }
 
 // Setup records for later fused kernels (caller owns `coeffs`, B*M records of

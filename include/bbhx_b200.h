@@ -69,6 +69,21 @@ int bbhx_waveform_amp_phase(double *waveform_out, const int *ells, const int *mm
                             const double *Mf_RD_lm, const double *Mf_DM_lm, int run_phenomd,
                             void *stream);
 
+/* No counterpart in the reference.  Allocation-free form of bbhx_waveform_amp_phase for
+ * callers that must not allocate device memory (a host whose own pool owns the GPU, loops
+ * where cudaMalloc's device-wide synchronisation would stall other streams, deployments
+ * without the stream-ordered allocator).  Its per-(binary, mode) scratch is a static device
+ * array inside the library (8192 records, ~6.2 MB held by every GPU that loads the library):
+ * num_bin_all * num_modes must be <= 8192 (else status 6, nothing launched).  The first call
+ * on a device looks up that array's address (make it before any stream capture); all calls
+ * share the array, so calls that overlap on the GPU race and must be serialised. */
+int bbhx_waveform_amp_phase_noalloc(double *waveform_out, const int *ells, const int *mms,
+                                    const double *freqs, const double *m1_SI,
+                                    const double *m2_SI, const double *chi1z, const double *chi2z,
+                                    const double *distance, const double *f_ref, int num_modes,
+                                    int length, int num_bin_all, const double *Mf_RD_lm,
+                                    const double *Mf_DM_lm, int run_phenomd, void *stream);
+
 /* split form of waveform_amp_phase: per-(binary, mode) records (B*M * bbhx_mode_coeffs_bytes()),
  * then per-frequency evaluation with the t_ref shift of phenomhm.py:485-507 fused (t_ref may
  * be NULL), or t(f) alone */
