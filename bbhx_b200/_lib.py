@@ -24,6 +24,7 @@ _SIGS = {
     "bbhx_pointer_is_device": [_VP],
     "bbhx_mode_coeffs_bytes": [],
     "bbhx_response_mode_bytes": [],
+    "bbhx_selftest_sincos": [_VP, _VP, _I, _VP],
     "bbhx_get_phenomhm_ringdown_frequencies": [_VP] * 8 + [_I, _I, _VP],
     "bbhx_get_phenomd_ringdown_frequencies": [_VP] * 6 + [_I] + [_VP] * 8 + [_D, _VP],
     "bbhx_ringdown_frequencies_all": [_VP] * 8 + [_I, _I, _VP, _I, _D, _I, _VP],
@@ -45,7 +46,7 @@ _SIGS = {
     "bbhx_direct_like": [_VP] * 7 + [_I, _I, _VP],
     "bbhx_hdyn": [_VP] * 5 + [_I, _I, _I, _VP],
     "bbhx_template_support": [_VP, _VP, _VP, _I, _I, _I, _VP, _I, _VP],
-    "bbhx_direct_like_fused": [_VP] * 5 + [_I] + [_VP] * 7 + [_I, _I, _I, _VP],
+    "bbhx_direct_like_fused": [_VP] * 5 + [_I] + [_VP] * 7 + [_I, _I, _I, _I, _VP],
 }
 _RESTYPES = {
     "bbhx_mode_coeffs_bytes": ctypes.c_size_t,

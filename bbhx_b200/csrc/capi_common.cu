@@ -16,9 +16,44 @@ void set_error(const char* fmt, ...) {
 
 const char* get_error() { return g_err; }
 
+int retain_pool_memory() {
+  static bool done[256] = {};
+  int dev = 0;
+  BBHX_CHECK_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 256 || done[dev]) return OK;
+  cudaMemPool_t pool;
+  BBHX_CHECK_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
+  unsigned long long thr = ~0ULL;
+  BBHX_CHECK_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+  done[dev] = true;
+  return OK;
+}
+
+}  // namespace bbhx
+
+namespace bbhx {
+// out[4 i .. 4 i + 3] = (sin, cos) from the hot-loop sincos_cw and (sin, cos) from CUDA's sincos
+__global__ void k_selftest_sincos(const double* x, double* out, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double s, c, s2, c2;
+    sincos_cw(x[i], &s, &c);
+    sincos(x[i], &s2, &c2);
+    out[4 * i] = s;
+    out[4 * i + 1] = c;
+    out[4 * i + 2] = s2;
+    out[4 * i + 3] = c2;
+  }
+}
 }  // namespace bbhx
 
 extern "C" {
+
+// Self-test of the hot-loop sine/cosine against CUDA's sincos (used by the kernel tests).
+int bbhx_selftest_sincos(const double* x, double* out, int n, void* stream) {
+  if (n <= 0) return bbhx::OK;
+  bbhx::k_selftest_sincos<<<bbhx::grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(x, out, n);
+  return bbhx::launch_status("k_selftest_sincos");
+}
 
 const char* bbhx_last_error_string(void) { return bbhx::get_error(); }
 

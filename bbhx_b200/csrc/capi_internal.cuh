@@ -40,6 +40,17 @@ inline int launch_status(const char* kernel) {
   return ERR_CUDA;
 }
 
+// Keep the stream-ordered pool's memory across synchronisations: the default release
+// threshold (0) hands freed pool memory back to the driver at every sync, so the next call's
+// cudaMallocAsync would re-map it.  Applied once per device to the device's default pool.
+int retain_pool_memory();
+
+// Stream-ordered scratch allocation used by the regular entry points.
+inline cudaError_t pool_alloc(void** p, size_t bytes, cudaStream_t s) {
+  retain_pool_memory();
+  return cudaMallocAsync(p, bytes, s);
+}
+
 inline unsigned int grid_for(long long n, int threads, int max_blocks = 148 * 32) {
   long long b = (n + threads - 1) / threads;
   if (b < 1) b = 1;

@@ -10,6 +10,7 @@
 //   noise-weights and reduces <d|h>, <h|h> without ever storing a template.
 //
 // Reductions are deterministic: per-(tile, binary) partials in FP64, then a fixed-order sum.
+#include <type_traits>
 #include <vector>
 
 #include "capi_internal.cuh"
@@ -200,17 +201,50 @@ struct FusedArgs {
   double* partials;  // [ntiles * B][3]
 };
 
-__global__ void __launch_bounds__(FD_WARPS * 32) k_direct_fused(FusedArgs A) {
+// sin / cos in FP32 of an FP64 angle: the quadrant reduction by pi/2 stays in FP64 (the
+// angle reaches ~1e7 rad), the reduced |y| <= pi/4 goes to FP32 Taylor polynomials
+// (through y^9 and y^10; truncation < 2e-9).
+__device__ __forceinline__ void sincos_mixed(double x, float* s, float* c) {
+  const double TWO_OVER_PI = 0.6366197723675814;
+  double k = rint(x * TWO_OVER_PI);
+  double yd = fma(-k, 1.5707963267948966, x);
+  yd = fma(-k, 6.123233995736766e-17, yd);
+  float y = (float)yd;
+  float y2 = y * y;
+  float ps = fmaf(fmaf(fmaf(2.7557319e-06f, y2, -1.9841270e-04f), y2, 8.3333333e-03f), y2,
+                  -1.6666667e-01f);
+  float sy = fmaf(ps * y2, y, y);
+  float pc = fmaf(fmaf(fmaf(fmaf(-2.7557319e-07f, y2, 2.4801587e-05f), y2, -1.3888889e-03f), y2,
+                       4.1666667e-02f), y2, -0.5f);
+  float cy = fmaf(pc, y2, 1.0f);
+  int q = (int)(__double2ll_rn(k) & 3);
+  float ss = (q & 1) ? cy : sy;
+  float cc = (q & 1) ? sy : cy;
+  *s = (q & 2) ? -ss : ss;
+  *c = ((q + 1) & 2) ? -cc : cc;
+}
+
+// One CTA item = (data tile of FD_TILE bins, binary); items are enumerated tile-major so the
+// CTAs in flight work on the same data tile for different binaries and share it through L2.
+// Warp w owns bins [tile + 128 w, +128); lane l owns bins tile + 128 w + l + 32 j, j < FD_K.
+// Per mode: one warp-cooperative search for the segment of the warp's first bin, then each
+// lane walks forward; the cubic coefficients of the current segment stay in registers.
+// MIXED: phase, t(f), the phase reduction and all accumulations in FP64; amplitude, transfer
+// functions, sin/cos of the reduced phase, the mode sum and the per-bin products in FP32.
+template <bool MIXED>
+__global__ void __launch_bounds__(FD_WARPS * 32, MIXED ? 4 : 3) k_direct_fused(FusedArgs A) {
+  using R = typename std::conditional<MIXED, float, double>::type;
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   __shared__ double red[3][FD_WARPS];
   const long long nitems = (long long)A.ntiles * A.B;
   const long long BML = (long long)A.B * A.M * A.L;
+  const int L = A.L;
   for (long long q = blockIdx.x; q < nitems; q += gridDim.x) {
     const int tile = (int)(q / A.B);
-    const int b = (int)(q % A.B);
-    const int s0 = A.sup_start[b];
-    const int s1 = s0 + A.sup_len[b];
+    const int b = (int)(q - (long long)tile * A.B);
+    const int s0 = __ldg(A.sup_start + b);
+    const int s1 = s0 + __ldg(A.sup_len + b);
     const int t0 = tile * FD_TILE;
     if (t0 >= s1 || t0 + FD_TILE <= s0) {
       if (threadIdx.x == 0) {
@@ -219,78 +253,103 @@ __global__ void __launch_bounds__(FD_WARPS * 32) k_direct_fused(FusedArgs A) {
       }
       continue;
     }
-    const int c0 = t0 + warp * FD_WARP_BINS;  // warp chunk start
-    const double ts = A.t_start[b], te = A.t_end[b];
+    const int c0 = t0 + warp * FD_WARP_BINS;
+    const double ts = __ldg(A.t_start + b), te = __ldg(A.t_end + b);
     double fbin[FD_K];
-    bool valid[FD_K];
+    R acc[FD_K][6];
 #pragma unroll
     for (int j = 0; j < FD_K; ++j) {
       int i = c0 + 32 * j + lane;
-      valid[j] = (i >= s0) && (i < s1);
-      fbin[j] = valid[j] ? A.data_freqs[i] : 0.0;
-    }
-    cplx acc[FD_K][3];
+      fbin[j] = (i >= s0 && i < s1) ? __ldg(A.data_freqs + i) : -1.0;
 #pragma unroll
-    for (int j = 0; j < FD_K; ++j)
-      for (int c = 0; c < 3; ++c) acc[j][c] = mk(0.0, 0.0);
-
-    // first valid bin of this warp chunk (all lanes agree)
-    int first = max(c0, s0);
-    bool warp_active = first < min(c0 + FD_WARP_BINS, s1);
-    if (warp_active) {
-      double ffirst = A.data_freqs[first];
+      for (int c = 0; c < 6; ++c) acc[j][c] = R(0);
+    }
+    const int first = max(c0, s0);
+    if (first < min(c0 + FD_WARP_BINS, s1)) {
+      const double ffirst = __ldg(A.data_freqs + first);
       for (int m = 0; m < A.M; ++m) {
         const long long rowi = (long long)b * A.M + m;
-        const double* xrow = A.x + rowi * A.L;
-        int k = warp_segment_search(xrow, A.L, ffirst);
-        int kc = -2;  // cached segment
-        double cx = 0.0, cy[9], cc1[9], cc2[9], cc3[9];
+        const double* xrow = A.x + rowi * L;
+        const double* yr = A.y + rowi * L;
+        const double* c1r = A.c1 + rowi * L;
+        const double* c2r = A.c2 + rowi * L;
+        const double* c3r = A.c3 + rowi * L;
+        int k = warp_segment_search(xrow, L, ffirst);
+        int kc = -2;
+        double xk = 0.0, xk1 = -1.0;
+        double py[2], p1[2], p2[2], p3[2];  // phase, t(f): always FP64
+        R ay[7], a1[7], a2[7], a3[7];       // amplitude and the six transfer components
 #pragma unroll
         for (int j = 0; j < FD_K; ++j) {
-          if (!valid[j]) continue;
-          double f = fbin[j];
-          while (k + 1 < A.L && __ldg(xrow + k + 1) <= f) ++k;
-          if (k < 0 || k >= A.L - 1) continue;
+          const double f = fbin[j];
+          if (f < 0.0) continue;
+          if (!(f < xk1) || k != kc) {
+            while (k + 1 < L && __ldg(xrow + k + 1) <= f) ++k;
+          }
+          if (k < 0 || k >= L - 1) continue;
           if (k != kc) {
             kc = k;
-            cx = __ldg(xrow + k);
+            xk = __ldg(xrow + k);
+            xk1 = __ldg(xrow + k + 1);
 #pragma unroll
             for (int p = 0; p < 9; ++p) {
-              long long o = p * BML + rowi * A.L + k;
-              cy[p] = __ldg(A.y + o);
-              cc1[p] = __ldg(A.c1 + o);
-              cc2[p] = __ldg(A.c2 + o);
-              cc3[p] = __ldg(A.c3 + o);
+              const long long o = p * BML + k;
+              const double vy = __ldg(yr + o), v1 = __ldg(c1r + o), v2 = __ldg(c2r + o),
+                           v3 = __ldg(c3r + o);
+              if (p == 1 || p == 2) {
+                py[p - 1] = vy; p1[p - 1] = v1; p2[p - 1] = v2; p3[p - 1] = v3;
+              } else {
+                const int a = (p == 0) ? 0 : p - 2;
+                ay[a] = (R)vy; a1[a] = (R)v1; a2[a] = (R)v2; a3[a] = (R)v3;
+              }
             }
           }
-          double u = f - cx;
-          double u2 = u * u, u3 = u2 * u;
-          double v[9];
+          const double u = f - xk;
+          const double tf = fma(fma(fma(p3[1], u, p2[1]), u, p1[1]), u, py[1]);
+          if (!tf_gate(tf, ts, te)) continue;
+          const double ph = fma(fma(fma(p3[0], u, p2[0]), u, p1[0]), u, py[0]);
+          const R ur = (R)u;
+          R v[7];
 #pragma unroll
-          for (int p = 0; p < 9; ++p) v[p] = cy[p] + cc1[p] * u + cc2[p] * u2 + cc3[p] * u3;
-          if (!tf_gate(v[2], ts, te)) continue;
-          cplx h1, h2, h3;
-          combine_channels(v[0], v[1], mk(v[3], v[4]), mk(v[5], v[6]), mk(v[7], v[8]), h1, h2, h3);
-          acc[j][0] = acc[j][0] + h1;
-          acc[j][1] = acc[j][1] + h2;
-          acc[j][2] = acc[j][2] + h3;
+          for (int a = 0; a < 7; ++a) v[a] = fma(fma(fma(a3[a], ur, a2[a]), ur, a1[a]), ur, ay[a]);
+          R sn, cs;
+          if (MIXED) {
+            float sf, cf;
+            sincos_mixed(ph, &sf, &cf);
+            sn = (R)sf;
+            cs = (R)cf;
+          } else {
+            double sd, cd;
+            sincos_cw(ph, &sd, &cd);
+            sn = (R)sd;
+            cs = (R)cd;
+          }
+          // conj(T_c * A e^{i phi})
+          const R apr = v[0] * cs, api = v[0] * sn;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const R tr = v[1 + 2 * c], ti = v[2 + 2 * c];
+            acc[j][2 * c] += tr * apr - ti * api;
+            acc[j][2 * c + 1] -= tr * api + ti * apr;
+          }
         }
       }
     }
     double dr = 0.0, di = 0.0, hh = 0.0;
 #pragma unroll
     for (int j = 0; j < FD_K; ++j) {
-      if (!valid[j]) continue;
-      int i = c0 + 32 * j + lane;
+      if (fbin[j] < 0.0) continue;
+      const int i = c0 + 32 * j + lane;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        long long gi = (long long)c * A.N + i;
-        double w = __ldg(A.noise + gi);
-        cplx h = acc[j][c] * w;
-        cplx d = A.data[gi];
-        dr += d.re * h.re + d.im * h.im;
-        di += d.re * h.im - d.im * h.re;
-        hh += h.re * h.re + h.im * h.im;
+        const long long gi = (long long)c * A.N + i;
+        const R w = (R)__ldg(A.noise + gi);
+        const double2 d = __ldg(reinterpret_cast<const double2*>(A.data) + gi);
+        const R hr = acc[j][2 * c] * w, hi = acc[j][2 * c + 1] * w;
+        const R dxr = (R)d.x, dyr = (R)d.y;
+        dr += (double)(dxr * hr + dyr * hi);
+        di += (double)(dxr * hi - dyr * hr);
+        hh += (double)(hr * hr + hi * hi);
       }
     }
     for (int o = 16; o > 0; o >>= 1) {
@@ -321,25 +380,35 @@ __global__ void __launch_bounds__(FD_WARPS * 32) k_direct_fused(FusedArgs A) {
   }
 }
 
-// out: d_h[b], h_h[b] complex (device); fixed-order sum over the binary's tiles
+// out: d_h[b], h_h[b] complex (device).  One warp per binary: lane l sums tiles l, l+32, ...
+// of the binary's support, then a fixed shuffle tree; the order is the same on every run.
 __global__ void k_fused_reduce(const double* partials, const int* sup_start, const int* sup_len,
                                int B, double* d_h, double* h_h) {
-  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < B; b += gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const int wpb = blockDim.x >> 5;
+  for (int b = blockIdx.x * wpb + (threadIdx.x >> 5); b < B; b += gridDim.x * wpb) {
     double a = 0, c = 0, h = 0;
     int s0 = sup_start[b], n = sup_len[b];
     if (n > 0) {
       int tlo = s0 / FD_TILE, thi = (s0 + n - 1) / FD_TILE;
-      for (int t = tlo; t <= thi; ++t) {
+      for (int t = tlo + lane; t <= thi; t += 32) {
         const double* P = partials + 3 * ((long long)t * B + b);
         a += P[0];
         c += P[1];
         h += P[2];
       }
     }
-    d_h[2 * b] = 4.0 * a;
-    d_h[2 * b + 1] = 4.0 * c;
-    h_h[2 * b] = 4.0 * h;
-    h_h[2 * b + 1] = 0.0;
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_xor_sync(0xffffffffu, a, o);
+      c += __shfl_xor_sync(0xffffffffu, c, o);
+      h += __shfl_xor_sync(0xffffffffu, h, o);
+    }
+    if (lane == 0) {
+      d_h[2 * b] = 4.0 * a;
+      d_h[2 * b + 1] = 4.0 * c;
+      h_h[2 * b] = 4.0 * h;
+      h_h[2 * b + 1] = 0.0;
+    }
   }
 }
 
@@ -376,9 +445,9 @@ int bbhx_direct_like(double* d_h, double* h_h, const double* data, const double*
   DirectJob* d_jobs = nullptr;
   double* d_part = nullptr;
   double* d_out = nullptr;
-  BBHX_CHECK_CUDA(cudaMallocAsync((void**)&d_jobs, sizeof(DirectJob) * num_bin_all, s));
-  BBHX_CHECK_CUDA(cudaMallocAsync((void**)&d_part, sizeof(double) * 3 * (nparts + 1), s));
-  BBHX_CHECK_CUDA(cudaMallocAsync((void**)&d_out, sizeof(double) * 4 * num_bin_all, s));
+  BBHX_CHECK_CUDA(pool_alloc((void**)&d_jobs, sizeof(DirectJob) * num_bin_all, s));
+  BBHX_CHECK_CUDA(pool_alloc((void**)&d_part, sizeof(double) * 3 * (nparts + 1), s));
+  BBHX_CHECK_CUDA(pool_alloc((void**)&d_out, sizeof(double) * 4 * num_bin_all, s));
   BBHX_CHECK_CUDA(cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(DirectJob) * num_bin_all,
                                   cudaMemcpyHostToDevice, s));
   int st = OK;
@@ -439,16 +508,17 @@ int bbhx_direct_like_fused(double* d_h, double* h_h, const double* data_freqs, c
                            const double* noise, int data_length, const double* x, const double* y,
                            const double* c1, const double* c2, const double* c3,
                            const double* t_start, const double* t_end, int num_modes, int length,
-                           int num_bin_all, void* stream) {
+                           int num_bin_all, int precision, void* stream) {
   BBHX_REQUIRE(length >= 2 && num_modes >= 1 && data_length >= 1, "bad sizes");
+  BBHX_REQUIRE(precision == 0 || precision == 1, "precision must be 0 (FP64) or 1 (mixed)");
   if (num_bin_all == 0) return OK;
   cudaStream_t s = (cudaStream_t)stream;
   int ntiles = (data_length + FD_TILE - 1) / FD_TILE;
   long long nitems = (long long)ntiles * num_bin_all;
   int* sup = nullptr;
   double* part = nullptr;
-  BBHX_CHECK_CUDA(cudaMallocAsync((void**)&sup, sizeof(int) * 2 * num_bin_all, s));
-  BBHX_CHECK_CUDA(cudaMallocAsync((void**)&part, sizeof(double) * 3 * nitems, s));
+  BBHX_CHECK_CUDA(pool_alloc((void**)&sup, sizeof(int) * 2 * num_bin_all, s));
+  BBHX_CHECK_CUDA(pool_alloc((void**)&part, sizeof(double) * 3 * nitems, s));
   k_support<<<num_bin_all, 128, 0, s>>>(x, num_modes, length, num_bin_all, data_freqs, data_length,
                                         sup, sup + num_bin_all);
   int st = launch_status("k_support");
@@ -473,11 +543,14 @@ int bbhx_direct_like_fused(double* d_h, double* h_h, const double* data_freqs, c
     A.ntiles = ntiles;
     A.partials = part;
     unsigned grid = (unsigned)(nitems < 148LL * 16 ? nitems : 148LL * 16);
-    k_direct_fused<<<grid, FD_WARPS * 32, 0, s>>>(A);
+    if (precision == 1)
+      k_direct_fused<true><<<grid, FD_WARPS * 32, 0, s>>>(A);
+    else
+      k_direct_fused<false><<<grid, FD_WARPS * 32, 0, s>>>(A);
     st = launch_status("k_direct_fused");
   }
   if (!st) {
-    k_fused_reduce<<<grid_for(num_bin_all, 128), 128, 0, s>>>(part, sup, sup + num_bin_all,
+    k_fused_reduce<<<grid_for(32LL * num_bin_all, 128), 128, 0, s>>>(part, sup, sup + num_bin_all,
                                                               num_bin_all, d_h, h_h);
     st = launch_status("k_fused_reduce");
   }

@@ -254,7 +254,7 @@ int noalloc_records(ModeCoeffs** out) {
 }
 
 int alloc_coeffs(ModeCoeffs** p, long long n, cudaStream_t s) {
-  BBHX_CHECK_CUDA(cudaMallocAsync((void**)p, sizeof(ModeCoeffs) * (size_t)n, s));
+  BBHX_CHECK_CUDA(pool_alloc((void**)p, sizeof(ModeCoeffs) * (size_t)n, s));
   return OK;
 }
 }  // namespace

@@ -172,7 +172,7 @@ int bbhx_LISA_response(void* orbits, double* response_out, const int* ells, cons
   cudaStream_t s = (cudaStream_t)stream;
   long long nbm = (long long)num_bin_all * num_modes;
   ResponseMode* rm = nullptr;
-  BBHX_CHECK_CUDA(cudaMallocAsync((void**)&rm, sizeof(ResponseMode) * nbm, s));
+  BBHX_CHECK_CUDA(pool_alloc((void**)&rm, sizeof(ResponseMode) * nbm, s));
   k_response_setup<<<grid_for(nbm, 128), 128, 0, s>>>(rm, ells, mms, phi_ref, inc, lam, beta, psi,
                                                       num_modes, num_bin_all);
   int st = launch_status("k_response_setup");
@@ -202,7 +202,7 @@ int bbhx_waveform_response_fused(void* orbits, double* buf, const double* freqs,
   cudaStream_t s = (cudaStream_t)stream;
   long long nbm = (long long)num_bin_all * num_modes;
   ResponseMode* rm = nullptr;
-  BBHX_CHECK_CUDA(cudaMallocAsync((void**)&rm, sizeof(ResponseMode) * nbm, s));
+  BBHX_CHECK_CUDA(pool_alloc((void**)&rm, sizeof(ResponseMode) * nbm, s));
   k_response_setup<<<grid_for(nbm, 128), 128, 0, s>>>(rm, ells, mms, phi_ref, inc, lam, beta, psi,
                                                       num_modes, num_bin_all);
   int st = launch_status("k_response_setup");

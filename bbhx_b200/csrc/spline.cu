@@ -177,7 +177,7 @@ int bbhx_interpolate(const double* freqs, const double* y, double* B_, double* u
                                          (int)kMaxSplineSmem));
   } else {
     grid = (unsigned int)(S < 148 * 2 ? S : 148 * 2);
-    BBHX_CHECK_CUDA(cudaMallocAsync((void**)&scratch, sizeof(double) * grid * (4 + num_interp_params) * (size_t)length, s));
+    BBHX_CHECK_CUDA(pool_alloc((void**)&scratch, sizeof(double) * grid * (4 + num_interp_params) * (size_t)length, s));
   }
   k_spline<<<grid, threads, use_smem ? smem : 0, s>>>(freqs, y, B_, upper_diag, diag, lower_diag,
                                                       length, num_interp_params, S, use_smem,

@@ -15,7 +15,7 @@ __device__ __forceinline__ bool tf_gate(double tf, double t_start, double t_end)
 __device__ __forceinline__ void combine_channels(double amp, double phase, cplx T1, cplx T2,
                                                  cplx T3, cplx& h1, cplx& h2, cplx& h3) {
   double s, c;
-  sincos(reduce_2pi(phase), &s, &c);
+  sincos_cw(phase, &s, &c);
   cplx ap = mk(amp * c, amp * s);
   h1 = conj(T1 * ap);
   h2 = conj(T2 * ap);

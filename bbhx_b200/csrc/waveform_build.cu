@@ -116,7 +116,7 @@ int bbhx_InterpTDI(const int64_t* template_ptrs, const double* data_freqs, const
   }
   if (maxlen == 0) return OK;
   InterpJob* d_jobs = nullptr;
-  BBHX_CHECK_CUDA(cudaMallocAsync((void**)&d_jobs, sizeof(InterpJob) * num_bin_all, s));
+  BBHX_CHECK_CUDA(pool_alloc((void**)&d_jobs, sizeof(InterpJob) * num_bin_all, s));
   BBHX_CHECK_CUDA(cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(InterpJob) * num_bin_all,
                                   cudaMemcpyHostToDevice, s));
   int threads = 256;

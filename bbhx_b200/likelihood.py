@@ -18,8 +18,14 @@ from .utils.arrays import device, to_dev, to_np, torch
 
 
 class Likelihood:
-    def __init__(self, template_gen, data_freqs, data_channels, psd, force_backend=None):
+    """Direct log-likelihood.  ``precision`` selects the arithmetic of the fused kernel:
+    "fp64" (default, the parity form) or "mixed" (FP64 phase / t(f) / accumulations, FP32
+    amplitudes, transfer functions and per-bin products)."""
+
+    def __init__(self, template_gen, data_freqs, data_channels, psd, force_backend=None,
+                 precision="fp64"):
         t = torch()
+        self.precision = precision
         self.data_freqs = to_dev(data_freqs)
         data_freqs_cpu = to_np(data_freqs).astype(np.float64)
         self.psd = np.asarray(to_np(psd), dtype=np.float64)
@@ -59,7 +65,7 @@ class Likelihood:
         flags = t.zeros(3, dtype=t.int32, device=device())
         d_h, h_h = self.waveform_gen.inner_products(params, self.data_freqs,
                                                     self.data_channels, self.noise_factors,
-                                                    flags=flags, **kw)
+                                                    flags=flags, precision=self.precision, **kw)
         self.d_h, self.h_h = d_h, h_h
         d_h_temp = d_h if not phase_marginalize else d_h.abs().to(t.complex128)
         out = -1.0 / 2.0 * (self.d_d + h_h - 2 * d_h_temp).real

@@ -14,8 +14,9 @@ A/E and T PSDs (x = 2 pi f L / c):
     S_A = S_E = 8 sin^2 x [ 2 S_acc (3 + 2 cos x + cos 2x) + S_oms (2 + cos x) ]
     S_T = 32 sin^2 x sin^2(x/2) [ 4 S_acc sin^2(x/2) + S_oms ]
 
-and, when ``tdi2`` is set, multiplied by |2 sin 4x|^2, the same factor the response
-applies to go from first- to second-generation TDI (``Response.cu:247-258``).
+and, when ``tdi2`` is set, multiplied by |2 sin 2x|^2 -- the response's first- to
+second-generation factor -2i sin(4x') e^{4ix'} with its x' = pi f L / c = x / 2
+(``Response.cu:205,247-258``), so that signal and noise vanish at the same frequencies.
 """
 import numpy as np
 
@@ -47,7 +48,7 @@ def aet_psd(f, channel, tdi2=False, armlength=L_SI, acc=3.0e-15, oms=15.0e-12):
     else:
         raise ValueError(f"unknown channel {channel!r}")
     if tdi2:
-        out = out * (2.0 * np.sin(4.0 * x)) ** 2
+        out = out * (2.0 * np.sin(2.0 * x)) ** 2
     return out
 
 
@@ -55,8 +56,9 @@ class AET1SensitivityMatrix:
     """A/E/T PSD container with the call pattern the heterodyne setup uses
     (``likelihood.py:361,493-496``: ``update_frequency_arr`` then ``[0]``, ``[1]``, ``[2]``)."""
 
-    def __init__(self, f, tdi2=False, **kwargs):
+    def __init__(self, f, tdi2=False, notch=False, **kwargs):
         self.tdi2 = tdi2
+        self.notch = notch
         self.kwargs = kwargs
         self.update_frequency_arr(f)
 
@@ -65,6 +67,10 @@ class AET1SensitivityMatrix:
         self.sens_mat = np.asarray(
             [aet_psd(self.frequency_arr, c, tdi2=self.tdi2, **self.kwargs) for c in "AET"]
         )
+        if self.notch:
+            from .synthetic import notch_tdi_zeros
+
+            self.sens_mat = notch_tdi_zeros(self.frequency_arr, self.sens_mat)
 
     def __getitem__(self, i):
         return self.sens_mat[i]

@@ -75,7 +75,31 @@ def data_grid(tobs_years, f_lo, f_hi):
 
 
 def gaussian_noise(psd, df, seed):
-    """Complex Gaussian noise with <|n|^2> = psd / (2 df) per bin, shape of ``psd``."""
+    """Complex Gaussian noise with <|n|^2> = psd / (2 df) per bin, shape of ``psd``; zero in
+    notched bins (psd = inf)."""
     rng = np.random.default_rng(seed)
-    sig = np.sqrt(np.asarray(psd) / (4.0 * df))
+    psd = np.asarray(psd)
+    sig = np.sqrt(np.where(np.isfinite(psd), psd, 0.0) / (4.0 * df))
     return sig * (rng.standard_normal(sig.shape) + 1j * rng.standard_normal(sig.shape))
+
+
+def notch_tdi_zeros(f, psd, half_width=16, armlength=None):
+    """Notch the bins around the zeros of the equal-arm A/E/T noise, f = k c / (4 L)
+    (the second-generation factor sin^2(2x) and, at even k, the first-generation sin^2(x),
+    x = 2 pi f L / c): psd = inf there, i.e. zero noise weight.
+
+    At those frequencies the idealised PSD goes to zero while a spline-interpolated template
+    cannot reproduce the transfer function's exact zero, so a single bin within ~1e-9 Hz of
+    a zero can dominate <h|h> by many orders of magnitude.  Returns a copy."""
+    from .utils.constants import C_SI, L_SI
+
+    L = L_SI if armlength is None else armlength
+    f = np.asarray(f, dtype=np.float64)
+    out = np.array(psd, dtype=np.float64, copy=True)
+    df = f[1] - f[0]
+    f0 = C_SI / (4.0 * L)
+    for k in range(1, int(f[-1] / f0) + 1):
+        fz = k * f0
+        m = np.abs(f - fz) <= half_width * df
+        out[..., m] = np.inf
+    return out

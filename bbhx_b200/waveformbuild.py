@@ -25,6 +25,11 @@ from .utils.transform import tSSBfromLframe
 from .waveforms.phenomhm import PhenomHMAmpPhase
 
 
+# arithmetic of the fused direct likelihood: "fp64" (parity form) or "mixed" (FP64 phase,
+# t(f) and accumulations; FP32 amplitude, transfer functions and per-bin products)
+PRECISIONS = {"fp64": 0, "mixed": 1}
+
+
 class TemplateInterpFD:
     """Interpolate the sparse (amp, phase, t(f), transfer) representation onto a data grid
     (waveformbuild.py:36-239)."""
@@ -248,7 +253,8 @@ class BBHWaveformFD:
         return (template_channels, self.interp_response.start_inds, self.interp_response.lengths)
 
     def inner_products(self, params, data_freqs, data_weighted, noise_factors, t_obs_start=0.0,
-                       t_obs_end=1.0, length=1024, modes=None, flags=None, timing=None, **unused):
+                       t_obs_end=1.0, length=1024, modes=None, flags=None, timing=None,
+                       precision="fp64", **unused):
         """Fused <d|h>, <h|h> for every binary (device complex128 [B] each).
 
         ``data_weighted`` [3, N] complex = data * sqrt(df / S); ``noise_factors`` [3, N] =
@@ -276,7 +282,7 @@ class BBHWaveformFD:
         _lib.call("bbhx_direct_like_fused", _lib.dptr(d_h), _lib.dptr(h_h), _lib.dptr(data_freqs),
                   _lib.dptr(data_weighted), _lib.dptr(noise_factors), int(data_freqs.numel()),
                   _lib.dptr(x), _lib.dptr(buf), _lib.dptr(c1), _lib.dptr(c2), _lib.dptr(c3),
-                  _lib.dptr(ts_d), _lib.dptr(te_d), M, L, B, _lib.stream())
+                  _lib.dptr(ts_d), _lib.dptr(te_d), M, L, B, PRECISIONS[precision], _lib.stream())
         if timing is not None:
             ev1.record()
             timing.setdefault("fused", []).append((ev0, ev1))

@@ -6,7 +6,9 @@ Workload (one "step"): the direct log-likelihood of B = 1024 massive-black-hole 
 PhenomHM with 6 modes on 1024-point sparse grids, 2nd-generation TDI A/E/T, Tobs = 1 yr,
 data grid df = 1/Tobs over [1e-5, 0.1] Hz (~3.16e6 bins; complex128 data and real noise
 weights, ~250 MB, larger than L2), synthetic data = seeded injection + Gaussian noise from
-the analytic PSD.  All arithmetic FP64.
+the analytic PSD with the equal-arm TDI noise zeros notched (f = k c / 4L, +-16 bins).
+Headline arithmetic: mixed (FP64 phase, t(f) and sums; FP32 amplitude, transfer and per-bin
+products); the plain-FP64 form is timed beside it.
 
   value  : lnL evaluations / s with parameters already resident on the GPU
   e2e    : the same through the public API (Likelihood.get_ll) from pinned host params,
@@ -64,11 +66,11 @@ def _cpu_worker(args):
     chunk, = args
     sys.path.insert(0, REPO)
     from bbhx_b200.sensitivity import aet_psd
-    from bbhx_b200.synthetic import data_grid, gaussian_noise
+    from bbhx_b200.synthetic import data_grid, gaussian_noise, notch_tdi_zeros
     from oracle.pipeline import RefPipeline
 
     f = data_grid(TOBS, F_LO, F_HI)
-    psd = np.array([aet_psd(f, c, tdi2=True) for c in "AET"])
+    psd = notch_tdi_zeros(f, np.array([aet_psd(f, c, tdi2=True) for c in "AET"]))
     data = gaussian_noise(psd, f[1] - f[0], SEED_NOISE)
     pipe = RefPipeline("ref", tdi2=True)
     t0 = time.perf_counter()
@@ -170,17 +172,19 @@ def build_problem(B, seed_params=SEED_PARAMS):
 
     from bbhx_b200 import BBHWaveformFD, EqualArmlengthOrbits, Likelihood
     from bbhx_b200.sensitivity import aet_psd
-    from bbhx_b200.synthetic import data_grid, draw_params, gaussian_noise
+    from bbhx_b200.synthetic import data_grid, draw_params, gaussian_noise, notch_tdi_zeros
 
     f = data_grid(TOBS, F_LO, F_HI)
     df = f[1] - f[0]
-    psd = np.array([aet_psd(f, c, tdi2=True) for c in "AET"])
+    psd = notch_tdi_zeros(f, np.array([aet_psd(f, c, tdi2=True) for c in "AET"]))
     wave = BBHWaveformFD(response_kwargs=dict(orbits=EqualArmlengthOrbits(), TDItag="AET", tdi2=True))
     inj = draw_params(1, TOBS, seed_params + 7)
     h = wave(*inj, freqs=f, length=LENGTH, t_obs_start=0.0, t_obs_end=TOBS, direct=False,
              fill=True, combine=True)
     data = gaussian_noise(psd, df, SEED_NOISE) + h.cpu().numpy()
     like = Likelihood(wave, f, data, psd)
+    like.raw_data = data
+    like.injection = inj[:, 0]
     params = draw_params(B, TOBS, seed_params)
     torch.cuda.synchronize()
     return wave, like, params, f
@@ -208,9 +212,10 @@ def gpu_arm(args):
     kw = dict(length=LENGTH, t_obs_start=0.0, t_obs_end=TOBS)
     flags = torch.zeros(3, dtype=torch.int32, device="cuda")
 
-    def step(timing=None):
+    def step(timing=None, precision="mixed"):
         d_h, h_h = wave.inner_products(dev_params, like.data_freqs, like.data_channels,
-                                       like.noise_factors, flags=flags, timing=timing, **kw)
+                                       like.noise_factors, flags=flags, timing=timing,
+                                       precision=precision, **kw)
         return -0.5 * (like.d_d + h_h - 2 * d_h).real
 
     def barrier():
@@ -219,6 +224,25 @@ def gpu_arm(args):
 
             dist.barrier()
 
+    def timed(precision, timing):
+        for _ in range(args.warmup):
+            step(precision=precision)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        z = torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(args.steps):
+            res = step(timing, precision=precision)
+        z.record()
+        torch.cuda.synchronize()
+        barrier()
+        return a.elapsed_time(z), res
+
+    # plain FP64 form first (the parity form; reported beside the mixed headline)
+    fp64_timing = {}
+    fp64_ms, out64 = timed("fp64", fp64_timing)
     for _ in range(args.warmup):
         out = step()
     torch.cuda.synchronize()
@@ -246,7 +270,15 @@ def gpu_arm(args):
         dist.all_reduce(ms, op=dist.ReduceOp.MAX)
     ms_total = float(ms.item())
     lnl = out.cpu().numpy()
-    assert np.all(np.isfinite(lnl)), "non-finite lnL"
+    lnl64 = out64.cpu().numpy()
+    assert np.all(np.isfinite(lnl)) and np.all(np.isfinite(lnl64)), "non-finite lnL"
+    dl_mixed = np.abs(lnl - lnl64)
+    fp64_ms_t = torch.tensor([fp64_ms], device="cuda", dtype=torch.float64)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.all_reduce(fp64_ms_t, op=dist.ReduceOp.MAX)
+    fp64_ms = float(fp64_ms_t.item())
 
     # support sizes (sum of per-binary data-grid lengths) for the roofline
     from bbhx_b200 import _lib
@@ -258,6 +290,7 @@ def gpu_arm(args):
     pairs = float(sup[B:].double().sum().item())
 
     # end to end through the public API from pinned host memory
+    like.precision = "mixed"
     host = torch.tensor(params, dtype=torch.float64).pin_memory()
     for _ in range(2):
         like.get_ll(host, **kw)
@@ -304,9 +337,15 @@ def gpu_arm(args):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f64",
+        "dtype": "mixed: f64 phase/t(f)/accumulation, f32 amplitude/transfer/products",
         "data": "synthetic: seeded PhenomHM injection + Gaussian noise from the analytic A/E/T PSD",
-        "config": {"workload": "direct lnL, plain FP64, B=%d binaries x 6 modes, sparse L=%d, "
+        "fp64_plain": {"value": n_evals / (fp64_ms / 1e3), "unit": "lnL evals/s",
+                       "ms_per_step": fp64_ms / args.steps,
+                       "kernel_ms": statistics.mean(a.elapsed_time(b) for a, b in fp64_timing["fused"])},
+        "dlnl_mixed_vs_fp64": {"max": float(dl_mixed.max()), "p99": float(np.percentile(dl_mixed, 99)),
+                               "median": float(np.median(dl_mixed)),
+                               "max_relative_to_hh": float(np.max(dl_mixed / np.maximum(1.0, np.abs(lnl64))))},
+        "config": {"workload": "direct lnL, mixed precision (FP64 plain beside), B=%d binaries x 6 modes, sparse L=%d, "
                                "Tobs=1 yr, df=1/Tobs over 1e-5..0.1 Hz (N=%d bins), AET TDI2"
                                % (B, LENGTH, len(f)),
                    "global_batch": n_evals // args.steps, "data_bins": len(f),
@@ -337,11 +376,11 @@ def het_metric(args, wave, like, f, params):
     from bbhx_b200.synthetic import perturb_params
 
     kw = dict(t_obs_start=0.0, t_obs_end=TOBS)
-    center = params[:, 0]
-    data = (like.data_channels / like.noise_factors).reshape(3, -1).cpu().numpy()
+    center = like.injection
+    data = like.raw_data
     het = HeterodynedLikelihood(wave, f, data, center, 128, template_gen_kwargs=dict(kw),
                                 reference_gen_kwargs=dict(kw, length=LENGTH),
-                                sens_mat=AET1SensitivityMatrix(f, tdi2=True))
+                                sens_mat=AET1SensitivityMatrix(f, tdi2=True, notch=True))
     Bh = args.het_batch
     walkers = perturb_params(center, Bh, 5)
     for _ in range(2):

@@ -33,6 +33,9 @@ int bbhx_stream_synchronize(void *stream);
 int bbhx_pointer_is_device(const void *ptr);
 size_t bbhx_mode_coeffs_bytes(void);
 size_t bbhx_response_mode_bytes(void);
+/* self-test (no reference counterpart): out[4i..4i+3] = sin, cos of x[i] from the hot-loop
+ * Cody-Waite + Taylor routine and from CUDA's sincos */
+int bbhx_selftest_sincos(const double *x, double *out, int n, void *stream);
 
 /* ------------------------------------------------------------------ PhenomHM */
 /* replaces get_phenomhm_ringdown_frequencies_wrap (src/bbhx/cutils/PhenomHMWaveform.hh:322-333);
@@ -170,12 +173,14 @@ int bbhx_template_support(int *start, int *len, const double *x, int num_modes, 
 
 /* fused interpolate + mode sum + noise weighting + <d|h>, <h|h> reduction; no templates are
  * stored (equivalent to InterpTDI followed by direct_like, waveformbuild.py:641-660 +
- * likelihood.py:177-214); d_h, h_h device complex [B], overwritten */
+ * likelihood.py:177-214); d_h, h_h device complex [B], overwritten.
+ * precision 0: FP64 throughout (the parity form); 1: mixed -- phase, t(f) and all
+ * accumulations in FP64, amplitude / transfer / per-bin products in FP32 */
 int bbhx_direct_like_fused(double *d_h, double *h_h, const double *data_freqs, const double *data,
                            const double *noise, int data_length, const double *x, const double *y,
                            const double *c1, const double *c2, const double *c3,
                            const double *t_start, const double *t_end, int num_modes, int length,
-                           int num_bin_all, void *stream);
+                           int num_bin_all, int precision, void *stream);
 
 #ifdef __cplusplus
 }

@@ -199,3 +199,21 @@ def test_heterodyned_likelihood_matches_reference(golden, golden_data):
     ll_adj = -0.5 * (het.reference_d_d + h_h - 2 * d_h).real
     lnl_close(ll_adj, golden["het_lnl"])
     assert np.all(np.isfinite(ll))
+
+
+def test_direct_likelihood_mixed_precision_error(golden, golden_data):
+    """Mixed precision (FP32 amplitude / transfer / products, FP64 phase, t(f), sums) against
+    the FP64 form on the golden case: |dlnL| <= 2e-6 * <h|h> (the FP32 relative error times
+    the template norm squared; these pure-noise golden data have <h|h> up to 2.6e10)."""
+    from bbhx_b200 import Likelihood
+
+    wave = _waveform_gen()
+    kw = dict(length=1024, t_obs_start=0.0, t_obs_end=golden_data["tobs"])
+    like = Likelihood(wave, golden_data["f"], golden_data["data"], golden_data["psd"])
+    ll64 = like.get_ll(golden["params"], **kw)
+    hh = like.h_h.cpu().numpy().real
+    like.precision = "mixed"
+    llm = like.get_ll(golden["params"], **kw)
+    d = np.abs(llm - ll64)
+    print("mixed |dlnL|", d, "relative to h_h", d / hh)
+    assert np.all(d <= 2e-6 * np.maximum(hh, 1.0))
