@@ -181,6 +181,9 @@ constexpr int FD_WARPS = 4;
 constexpr int FD_K = 4;                          // bins per lane per warp chunk
 constexpr int FD_WARP_BINS = 32 * FD_K;          // 128
 constexpr int FD_TILE = FD_WARPS * FD_WARP_BINS;  // 512
+constexpr int FD_NSEG = 8;    // spline segments per (tile, mode) staged in shared memory
+constexpr int FD_MAXM = 6;    // modes per binary
+constexpr int FD_NC = 36;     // 9 quantities x (y, c1, c2, c3) per segment
 
 struct FusedArgs {
   const double* data_freqs;
@@ -198,8 +201,45 @@ struct FusedArgs {
   const int* sup_len;
   int B, M, L;
   int ntiles;
-  double* partials;  // [ntiles * B][3]
+  double* partials;    // [ntiles * B][3]
+  const int2* segtab;  // [ntiles][B][M]: segments of the tile's first and last bin
 };
+
+// Segment table: for every (tile, binary, mode) the spline segments holding the first and the
+// last data bin of the binary's support inside the tile (searchsorted(side='right') - 1 of
+// their frequencies), or (1, 0) when the tile misses the support.  One thread per entry.
+__global__ void k_tile_segments(int2* tab, const double* __restrict__ x,
+                                const double* __restrict__ data_freqs, const int* sup_start,
+                                const int* sup_len, int B, int M, int L, int ntiles) {
+  const long long n = (long long)ntiles * B * M;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int m = (int)(t % M);
+    const long long tb = t / M;
+    const int b = (int)(tb % B);
+    const int tile = (int)(tb / B);
+    const int s0 = sup_start[b], s1 = s0 + sup_len[b];
+    const int i0 = max(tile * FD_TILE, s0), i1 = min((tile + 1) * FD_TILE, s1) - 1;
+    if (i0 > i1) {
+      tab[t] = make_int2(1, 0);
+      continue;
+    }
+    const double* xr = x + ((long long)b * M + m) * L;
+    const double f0 = data_freqs[i0], f1 = data_freqs[i1];
+    int lo = 0, hi = L;  // count of knots <= f0
+    while (lo < hi) {
+      int mid = (lo + hi) >> 1;
+      if (xr[mid] <= f0) lo = mid + 1; else hi = mid;
+    }
+    const int ka = lo - 1;
+    hi = L;
+    while (lo < hi) {
+      int mid = (lo + hi) >> 1;
+      if (xr[mid] <= f1) lo = mid + 1; else hi = mid;
+    }
+    tab[t] = make_int2(ka, lo - 1);
+  }
+}
 
 // sin / cos in FP32 of an FP64 angle: the quadrant reduction by pi/2 stays in FP64 (the
 // angle reaches ~1e7 rad), the reduced |y| <= pi/4 goes to FP32 Taylor polynomials
@@ -224,132 +264,233 @@ __device__ __forceinline__ void sincos_mixed(double x, float* s, float* c) {
   *c = ((q + 1) & 2) ? -cc : cc;
 }
 
-// One CTA item = (data tile of FD_TILE bins, binary); items are enumerated tile-major so the
-// CTAs in flight work on the same data tile for different binaries and share it through L2.
-// Warp w owns bins [tile + 128 w, +128); lane l owns bins tile + 128 w + l + 32 j, j < FD_K.
-// Per mode: one warp-cooperative search for the segment of the warp's first bin, then each
-// lane walks forward; the cubic coefficients of the current segment stay in registers.
+// Cubic coefficients of one spline segment held by a lane: phase and t(f) always in FP64,
+// amplitude and the six transfer components in R (FP32 when mixed).
+template <typename R>
+struct SegCoef {
+  double xk;
+  double py[2], p1[2], p2[2], p3[2];
+  R ay[7], a1[7], a2[7], a3[7];
+  // v(p, c) = coefficient c (y, c1, c2, c3) of quantity p (amp, phase, tf, T1re .. T3im)
+  __device__ __forceinline__ void set(int p, double vy, double v1, double v2, double v3) {
+    if (p == 1 || p == 2) {
+      py[p - 1] = vy; p1[p - 1] = v1; p2[p - 1] = v2; p3[p - 1] = v3;
+    } else {
+      const int a = (p == 0) ? 0 : p - 2;
+      ay[a] = (R)vy; a1[a] = (R)v1; a2[a] = (R)v2; a3[a] = (R)v3;
+    }
+  }
+};
+
+// Add conj(T_c A e^{i phi}) of one (bin, mode) to acc (6 reals: 3 complex channels), behind the
+// t(f) gate.
+template <bool MIXED, typename R>
+__device__ __forceinline__ void accumulate_bin(const SegCoef<R>& c, double f, double ts, double te,
+                                               R* acc) {
+  const double u = f - c.xk;
+  const double tf = fma(fma(fma(c.p3[1], u, c.p2[1]), u, c.p1[1]), u, c.py[1]);
+  if (!tf_gate(tf, ts, te)) return;
+  const double ph = fma(fma(fma(c.p3[0], u, c.p2[0]), u, c.p1[0]), u, c.py[0]);
+  const R ur = (R)u;
+  R v[7];
+#pragma unroll
+  for (int a = 0; a < 7; ++a) v[a] = fma(fma(fma(c.a3[a], ur, c.a2[a]), ur, c.a1[a]), ur, c.ay[a]);
+  R sn, cs;
+  if (MIXED) {
+    float sf, cf;
+    sincos_mixed(ph, &sf, &cf);
+    sn = (R)sf;
+    cs = (R)cf;
+  } else {
+    double sd, cd;
+    sincos_cw(ph, &sd, &cd);
+    sn = (R)sd;
+    cs = (R)cd;
+  }
+  const R apr = v[0] * cs, api = v[0] * sn;
+#pragma unroll
+  for (int ch = 0; ch < 3; ++ch) {
+    const R tr = v[1 + 2 * ch], ti = v[2 + 2 * ch];
+    acc[2 * ch] += tr * apr - ti * api;
+    acc[2 * ch + 1] -= tr * api + ti * apr;
+  }
+}
+
+// Per-warp shared-memory copy of the spline segments one (tile, binary) item needs, for every
+// mode: x of the segments' knots, the FP64 cubic coefficients of phase and t(f), and those of
+// the amplitude and six transfer components in R (FP32 when mixed), each quantity's
+// (y, c1, c2, c3) contiguous so a lane reloads a segment with vector loads.
+template <typename R>
+struct alignas(16) WarpStage {
+  double x[FD_MAXM][FD_NSEG + 1];
+  double pc[FD_MAXM][FD_NSEG][2][4];
+  R ac[FD_MAXM][FD_NSEG][7][4];
+  int klo[FD_MAXM];
+  int nseg[FD_MAXM];
+};
+
+template <typename R>
+__device__ __forceinline__ void load_seg(SegCoef<R>& cf, const WarpStage<R>& S, int m, int kl) {
+  cf.xk = S.x[m][kl];
+#pragma unroll
+  for (int a = 0; a < 2; ++a) {
+    const double2 lo = *reinterpret_cast<const double2*>(&S.pc[m][kl][a][0]);
+    const double2 hi = *reinterpret_cast<const double2*>(&S.pc[m][kl][a][2]);
+    cf.py[a] = lo.x; cf.p1[a] = lo.y; cf.p2[a] = hi.x; cf.p3[a] = hi.y;
+  }
+#pragma unroll
+  for (int a = 0; a < 7; ++a) {
+    if (sizeof(R) == 4) {
+      const float4 v = *reinterpret_cast<const float4*>(&S.ac[m][kl][a][0]);
+      cf.ay[a] = (R)v.x; cf.a1[a] = (R)v.y; cf.a2[a] = (R)v.z; cf.a3[a] = (R)v.w;
+    } else {
+      const double2 lo = *reinterpret_cast<const double2*>(&S.ac[m][kl][a][0]);
+      const double2 hi = *reinterpret_cast<const double2*>(&S.ac[m][kl][a][2]);
+      cf.ay[a] = (R)lo.x; cf.a1[a] = (R)lo.y; cf.a2[a] = (R)hi.x; cf.a3[a] = (R)hi.y;
+    }
+  }
+}
+
+// One WARP item = (data tile of FD_TILE bins, binary).  Items are enumerated tile-major, so the
+// warps in flight work on the same data tile for different binaries and share it through L2.
+// The warp stages the tile's segments of every mode (from the segment table) into its slice of
+// shared memory, then walks the tile in FD_TILE / FD_WARP_BINS chunks of 128 bins (lane l owns
+// bins chunk + l + 32 j, j < FD_K) and keeps the <d|h>, <h|h> partial sums in registers; no
+// block-wide barrier is involved.  Tiles whose modes span more than FD_NSEG segments (only the
+// lowest frequencies) take a per-lane walk over global memory instead.
 // MIXED: phase, t(f), the phase reduction and all accumulations in FP64; amplitude, transfer
 // functions, sin/cos of the reduced phase, the mode sum and the per-bin products in FP32.
 template <bool MIXED>
 __global__ void __launch_bounds__(FD_WARPS * 32, MIXED ? 4 : 3) k_direct_fused(FusedArgs A) {
   using R = typename std::conditional<MIXED, float, double>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
-  __shared__ double red[3][FD_WARPS];
+  WarpStage<R>& S = reinterpret_cast<WarpStage<R>*>(smem_raw)[warp];
   const long long nitems = (long long)A.ntiles * A.B;
   const long long BML = (long long)A.B * A.M * A.L;
   const int L = A.L;
-  for (long long q = blockIdx.x; q < nitems; q += gridDim.x) {
+  const long long gw = (long long)blockIdx.x * FD_WARPS + warp;
+  const long long nw = (long long)gridDim.x * FD_WARPS;
+  for (long long q = gw; q < nitems; q += nw) {
     const int tile = (int)(q / A.B);
     const int b = (int)(q - (long long)tile * A.B);
     const int s0 = __ldg(A.sup_start + b);
     const int s1 = s0 + __ldg(A.sup_len + b);
     const int t0 = tile * FD_TILE;
     if (t0 >= s1 || t0 + FD_TILE <= s0) {
-      if (threadIdx.x == 0) {
+      if (lane == 0) {
         double* P = A.partials + 3 * q;
         P[0] = 0.0; P[1] = 0.0; P[2] = 0.0;
       }
       continue;
     }
-    const int c0 = t0 + warp * FD_WARP_BINS;
-    const double ts = __ldg(A.t_start + b), te = __ldg(A.t_end + b);
-    double fbin[FD_K];
-    R acc[FD_K][6];
-#pragma unroll
-    for (int j = 0; j < FD_K; ++j) {
-      int i = c0 + 32 * j + lane;
-      fbin[j] = (i >= s0 && i < s1) ? __ldg(A.data_freqs + i) : -1.0;
-#pragma unroll
-      for (int c = 0; c < 6; ++c) acc[j][c] = R(0);
+    // ---- stage this tile's segments for every mode
+    if (lane < A.M) {
+      const int2 kk = A.segtab[q * A.M + lane];
+      const int klo = max(kk.x, 0), khi = min(kk.y, L - 2);
+      const int n = (kk.x > kk.y || khi < klo) ? 0 : khi - klo + 1;
+      S.klo[lane] = klo;
+      S.nseg[lane] = (n > FD_NSEG) ? -1 : n;
     }
-    const int first = max(c0, s0);
-    if (first < min(c0 + FD_WARP_BINS, s1)) {
-      const double ffirst = __ldg(A.data_freqs + first);
-      for (int m = 0; m < A.M; ++m) {
-        const long long rowi = (long long)b * A.M + m;
-        const double* xrow = A.x + rowi * L;
-        const double* yr = A.y + rowi * L;
-        const double* c1r = A.c1 + rowi * L;
-        const double* c2r = A.c2 + rowi * L;
-        const double* c3r = A.c3 + rowi * L;
-        int k = warp_segment_search(xrow, L, ffirst);
-        int kc = -2;
-        double xk = 0.0, xk1 = -1.0;
-        double py[2], p1[2], p2[2], p3[2];  // phase, t(f): always FP64
-        R ay[7], a1[7], a2[7], a3[7];       // amplitude and the six transfer components
-#pragma unroll
-        for (int j = 0; j < FD_K; ++j) {
-          const double f = fbin[j];
-          if (f < 0.0) continue;
-          if (!(f < xk1) || k != kc) {
-            while (k + 1 < L && __ldg(xrow + k + 1) <= f) ++k;
-          }
-          if (k < 0 || k >= L - 1) continue;
-          if (k != kc) {
-            kc = k;
-            xk = __ldg(xrow + k);
-            xk1 = __ldg(xrow + k + 1);
-#pragma unroll
-            for (int p = 0; p < 9; ++p) {
-              const long long o = p * BML + k;
-              const double vy = __ldg(yr + o), v1 = __ldg(c1r + o), v2 = __ldg(c2r + o),
-                           v3 = __ldg(c3r + o);
-              if (p == 1 || p == 2) {
-                py[p - 1] = vy; p1[p - 1] = v1; p2[p - 1] = v2; p3[p - 1] = v3;
-              } else {
-                const int a = (p == 0) ? 0 : p - 2;
-                ay[a] = (R)vy; a1[a] = (R)v1; a2[a] = (R)v2; a3[a] = (R)v3;
-              }
-            }
-          }
-          const double u = f - xk;
-          const double tf = fma(fma(fma(p3[1], u, p2[1]), u, p1[1]), u, py[1]);
-          if (!tf_gate(tf, ts, te)) continue;
-          const double ph = fma(fma(fma(p3[0], u, p2[0]), u, p1[0]), u, py[0]);
-          const R ur = (R)u;
-          R v[7];
-#pragma unroll
-          for (int a = 0; a < 7; ++a) v[a] = fma(fma(fma(a3[a], ur, a2[a]), ur, a1[a]), ur, ay[a]);
-          R sn, cs;
-          if (MIXED) {
-            float sf, cf;
-            sincos_mixed(ph, &sf, &cf);
-            sn = (R)sf;
-            cs = (R)cf;
-          } else {
-            double sd, cd;
-            sincos_cw(ph, &sd, &cd);
-            sn = (R)sd;
-            cs = (R)cd;
-          }
-          // conj(T_c * A e^{i phi})
-          const R apr = v[0] * cs, api = v[0] * sn;
-#pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            const R tr = v[1 + 2 * c], ti = v[2 + 2 * c];
-            acc[j][2 * c] += tr * apr - ti * api;
-            acc[j][2 * c + 1] -= tr * api + ti * apr;
-          }
+    __syncwarp();
+    for (int m = 0; m < A.M; ++m) {
+      const int n = S.nseg[m];
+      if (n <= 0) continue;
+      const long long rowo = ((long long)b * A.M + m) * L + S.klo[m];
+      const int total = n * FD_NC + n + 1;
+      for (int idx = lane; idx < total; idx += 32) {
+        if (idx < n * FD_NC) {
+          const int sg = idx / FD_NC, r = idx - sg * FD_NC, p = r >> 2, cc = r & 3;
+          const double* src = (cc == 0) ? A.y : (cc == 1) ? A.c1 : (cc == 2) ? A.c2 : A.c3;
+          const double v = __ldg(src + p * BML + rowo + sg);
+          if (p == 1 || p == 2)
+            S.pc[m][sg][p - 1][cc] = v;
+          else
+            S.ac[m][sg][(p == 0) ? 0 : p - 2][cc] = (R)v;
+        } else {
+          const int j = idx - n * FD_NC;
+          S.x[m][j] = __ldg(A.x + rowo + j);
         }
       }
     }
+    __syncwarp();
+    const double ts = __ldg(A.t_start + b), te = __ldg(A.t_end + b);
     double dr = 0.0, di = 0.0, hh = 0.0;
+    for (int ch0 = 0; ch0 < FD_TILE; ch0 += FD_WARP_BINS) {
+      const int c0 = t0 + ch0;
+      if (c0 >= s1 || c0 + FD_WARP_BINS <= s0) continue;
+      double fbin[FD_K];
+      R acc[FD_K][6];
 #pragma unroll
-    for (int j = 0; j < FD_K; ++j) {
-      if (fbin[j] < 0.0) continue;
-      const int i = c0 + 32 * j + lane;
+      for (int j = 0; j < FD_K; ++j) {
+        const int i = c0 + 32 * j + lane;
+        fbin[j] = (i >= s0 && i < s1) ? __ldg(A.data_freqs + i) : -1.0;
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const long long gi = (long long)c * A.N + i;
-        const R w = (R)__ldg(A.noise + gi);
-        const double2 d = __ldg(reinterpret_cast<const double2*>(A.data) + gi);
-        const R hr = acc[j][2 * c] * w, hi = acc[j][2 * c + 1] * w;
-        const R dxr = (R)d.x, dyr = (R)d.y;
-        dr += (double)(dxr * hr + dyr * hi);
-        di += (double)(dxr * hi - dyr * hr);
-        hh += (double)(hr * hr + hi * hi);
+        for (int c = 0; c < 6; ++c) acc[j][c] = R(0);
+      }
+      for (int m = 0; m < A.M; ++m) {
+        const int n = S.nseg[m];
+        if (n == 0) continue;
+        SegCoef<R> cf;
+        if (n > 0) {
+          int kl = 0, kc = -1;
+#pragma unroll
+          for (int j = 0; j < FD_K; ++j) {
+            const double f = fbin[j];
+            if (f < S.x[m][0]) continue;  // also skips bins outside the support (f = -1)
+            while (kl < n && f >= S.x[m][kl + 1]) ++kl;
+            if (kl >= n) continue;
+            if (kl != kc) {
+              kc = kl;
+              load_seg<R>(cf, S, m, kl);
+            }
+            accumulate_bin<MIXED, R>(cf, f, ts, te, acc[j]);
+          }
+        } else {
+          const long long rowi = (long long)b * A.M + m;
+          const double* xrow = A.x + rowi * L;
+          const double ffirst = __ldg(A.data_freqs + max(c0, s0));
+          int k = warp_segment_search(xrow, L, ffirst);
+          int kc = -2;
+          double xk1 = -1.0;
+#pragma unroll
+          for (int j = 0; j < FD_K; ++j) {
+            const double f = fbin[j];
+            if (f < 0.0) continue;
+            if (!(f < xk1) || k != kc) {
+              while (k + 1 < L && __ldg(xrow + k + 1) <= f) ++k;
+            }
+            if (k < 0 || k >= L - 1) continue;
+            if (k != kc) {
+              kc = k;
+              cf.xk = __ldg(xrow + k);
+              xk1 = __ldg(xrow + k + 1);
+              const long long o = rowi * L + k;
+#pragma unroll
+              for (int p = 0; p < 9; ++p)
+                cf.set(p, __ldg(A.y + p * BML + o), __ldg(A.c1 + p * BML + o),
+                       __ldg(A.c2 + p * BML + o), __ldg(A.c3 + p * BML + o));
+            }
+            accumulate_bin<MIXED, R>(cf, f, ts, te, acc[j]);
+          }
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < FD_K; ++j) {
+        if (fbin[j] < 0.0) continue;
+        const int i = c0 + 32 * j + lane;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const long long gi = (long long)c * A.N + i;
+          const R w = (R)__ldg(A.noise + gi);
+          const double2 d = __ldg(reinterpret_cast<const double2*>(A.data) + gi);
+          const R hr = acc[j][2 * c] * w, hi = acc[j][2 * c + 1] * w;
+          const R dxr = (R)d.x, dyr = (R)d.y;
+          dr += (double)(dxr * hr + dyr * hi);
+          di += (double)(dxr * hi - dyr * hr);
+          hh += (double)(hr * hr + hi * hi);
+        }
       }
     }
     for (int o = 16; o > 0; o >>= 1) {
@@ -358,25 +499,12 @@ __global__ void __launch_bounds__(FD_WARPS * 32, MIXED ? 4 : 3) k_direct_fused(F
       hh += __shfl_xor_sync(0xffffffffu, hh, o);
     }
     if (lane == 0) {
-      red[0][warp] = dr;
-      red[1][warp] = di;
-      red[2][warp] = hh;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double a = 0, c = 0, h = 0;
-#pragma unroll
-      for (int w = 0; w < FD_WARPS; ++w) {
-        a += red[0][w];
-        c += red[1][w];
-        h += red[2][w];
-      }
       double* P = A.partials + 3 * q;
-      P[0] = a;
-      P[1] = c;
-      P[2] = h;
+      P[0] = dr;
+      P[1] = di;
+      P[2] = hh;
     }
-    __syncthreads();
+    __syncwarp();
   }
 }
 
@@ -515,13 +643,21 @@ int bbhx_direct_like_fused(double* d_h, double* h_h, const double* data_freqs, c
   cudaStream_t s = (cudaStream_t)stream;
   int ntiles = (data_length + FD_TILE - 1) / FD_TILE;
   long long nitems = (long long)ntiles * num_bin_all;
+  BBHX_REQUIRE(num_modes <= FD_MAXM, "num_modes must be <= 6");
   int* sup = nullptr;
   double* part = nullptr;
+  int2* segtab = nullptr;
   BBHX_CHECK_CUDA(pool_alloc((void**)&sup, sizeof(int) * 2 * num_bin_all, s));
   BBHX_CHECK_CUDA(pool_alloc((void**)&part, sizeof(double) * 3 * nitems, s));
+  BBHX_CHECK_CUDA(pool_alloc((void**)&segtab, sizeof(int2) * nitems * num_modes, s));
   k_support<<<num_bin_all, 128, 0, s>>>(x, num_modes, length, num_bin_all, data_freqs, data_length,
                                         sup, sup + num_bin_all);
   int st = launch_status("k_support");
+  if (!st) {
+    k_tile_segments<<<grid_for(nitems * num_modes, 256, 148 * 64), 256, 0, s>>>(
+        segtab, x, data_freqs, sup, sup + num_bin_all, num_bin_all, num_modes, length, ntiles);
+    st = launch_status("k_tile_segments");
+  }
   if (!st) {
     FusedArgs A;
     A.data_freqs = data_freqs;
@@ -542,11 +678,21 @@ int bbhx_direct_like_fused(double* d_h, double* h_h, const double* data_freqs, c
     A.L = length;
     A.ntiles = ntiles;
     A.partials = part;
-    unsigned grid = (unsigned)(nitems < 148LL * 16 ? nitems : 148LL * 16);
-    if (precision == 1)
-      k_direct_fused<true><<<grid, FD_WARPS * 32, 0, s>>>(A);
-    else
-      k_direct_fused<false><<<grid, FD_WARPS * 32, 0, s>>>(A);
+    A.segtab = segtab;
+    const long long warps_needed = (nitems + 0);
+    long long g = (warps_needed + FD_WARPS - 1) / FD_WARPS;
+    unsigned grid = (unsigned)(g < 148LL * 16 ? g : 148LL * 16);
+    if (precision == 1) {
+      const size_t sm = sizeof(WarpStage<float>) * FD_WARPS;
+      BBHX_CHECK_CUDA(cudaFuncSetAttribute(k_direct_fused<true>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      k_direct_fused<true><<<grid, FD_WARPS * 32, sm, s>>>(A);
+    } else {
+      const size_t sm = sizeof(WarpStage<double>) * FD_WARPS;
+      BBHX_CHECK_CUDA(cudaFuncSetAttribute(k_direct_fused<false>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      k_direct_fused<false><<<grid, FD_WARPS * 32, sm, s>>>(A);
+    }
     st = launch_status("k_direct_fused");
   }
   if (!st) {
@@ -556,6 +702,7 @@ int bbhx_direct_like_fused(double* d_h, double* h_h, const double* data_freqs, c
   }
   cudaFreeAsync(sup, s);
   cudaFreeAsync(part, s);
+  cudaFreeAsync(segtab, s);
   return st;
 }
 
