@@ -316,6 +316,51 @@ __device__ __forceinline__ void accumulate_bin(const SegCoef<R>& c, double f, do
   }
 }
 
+// G bins of one lane that lie in the same spline segment: the same arithmetic as
+// accumulate_bin, written branch-free (invalid or gated-off bins are dropped by selects) so the
+// G independent evaluation chains interleave.
+template <bool MIXED, typename R, int G>
+__device__ __forceinline__ void accumulate_group(const SegCoef<R>& c, const double* f,
+                                                 const bool* ok, double ts, double te,
+                                                 R (*acc)[6]) {
+  double u[G], ph[G];
+  bool g[G];
+#pragma unroll
+  for (int j = 0; j < G; ++j) {
+    u[j] = f[j] - c.xk;
+    const double tf = fma(fma(fma(c.p3[1], u[j], c.p2[1]), u[j], c.p1[1]), u[j], c.py[1]);
+    g[j] = ok[j] && tf_gate(tf, ts, te);
+    ph[j] = fma(fma(fma(c.p3[0], u[j], c.p2[0]), u[j], c.p1[0]), u[j], c.py[0]);
+  }
+#pragma unroll
+  for (int j = 0; j < G; ++j) {
+    const R ur = (R)u[j];
+    R v[7];
+#pragma unroll
+    for (int a = 0; a < 7; ++a) v[a] = fma(fma(fma(c.a3[a], ur, c.a2[a]), ur, c.a1[a]), ur, c.ay[a]);
+    R sn, cs;
+    if (MIXED) {
+      float sf, cf;
+      sincos_mixed(ph[j], &sf, &cf);
+      sn = (R)sf;
+      cs = (R)cf;
+    } else {
+      double sd, cd;
+      sincos_cw(ph[j], &sd, &cd);
+      sn = (R)sd;
+      cs = (R)cd;
+    }
+    const R amp = g[j] ? v[0] : R(0);
+    const R apr = amp * cs, api = amp * sn;
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch) {
+      const R tr = v[1 + 2 * ch], ti = v[2 + 2 * ch];
+      acc[j][2 * ch] += tr * apr - ti * api;
+      acc[j][2 * ch + 1] -= tr * api + ti * apr;
+    }
+  }
+}
+
 // Per-warp shared-memory copy of the spline segments one (tile, binary) item needs, for every
 // mode: x of the segments' knots, the FP64 cubic coefficients of phase and t(f), and those of
 // the amplitude and six transfer components in R (FP32 when mixed), each quantity's
@@ -434,18 +479,50 @@ __global__ void __launch_bounds__(FD_WARPS * 32, MIXED ? 4 : 3) k_direct_fused(F
         if (n == 0) continue;
         SegCoef<R> cf;
         if (n > 0) {
-          int kl = 0, kc = -1;
+          // segment of every bin (local index; n = past the last staged segment)
+          int kb[FD_K];
+          bool ok[FD_K];
+          int kl = 0;
 #pragma unroll
           for (int j = 0; j < FD_K; ++j) {
             const double f = fbin[j];
-            if (f < S.x[m][0]) continue;  // also skips bins outside the support (f = -1)
-            while (kl < n && f >= S.x[m][kl + 1]) ++kl;
-            if (kl >= n) continue;
-            if (kl != kc) {
-              kc = kl;
-              load_seg<R>(cf, S, m, kl);
+            ok[j] = f >= S.x[m][0];  // also false for bins outside the support (f = -1)
+            while (ok[j] && kl < n && f >= S.x[m][kl + 1]) ++kl;
+            ok[j] = ok[j] && kl < n;
+            kb[j] = kl;
+          }
+          constexpr int G = MIXED ? 1 : 2;  // FP64 gains from 2 interleaved chains; mixed keeps occupancy
+          int kc = -1;
+#pragma unroll
+          for (int j0 = 0; j0 < FD_K; j0 += G) {
+            // group path when every valid bin of the group sits in one segment
+            int kg = -1;
+            bool same = true, any = false;
+#pragma unroll
+            for (int j = j0; j < j0 + G; ++j) {
+              if (!ok[j]) continue;
+              if (kg < 0) kg = kb[j];
+              same = same && (kb[j] == kg);
+              any = true;
             }
-            accumulate_bin<MIXED, R>(cf, f, ts, te, acc[j]);
+            if (!any) continue;
+            if (same) {
+              if (kg != kc) {
+                kc = kg;
+                load_seg<R>(cf, S, m, kg);
+              }
+              accumulate_group<MIXED, R, G>(cf, fbin + j0, ok + j0, ts, te, acc + j0);
+            } else {
+#pragma unroll
+              for (int j = j0; j < j0 + G; ++j) {
+                if (!ok[j]) continue;
+                if (kb[j] != kc) {
+                  kc = kb[j];
+                  load_seg<R>(cf, S, m, kc);
+                }
+                accumulate_bin<MIXED, R>(cf, fbin[j], ts, te, acc[j]);
+              }
+            }
           }
         } else {
           const long long rowi = (long long)b * A.M + m;
