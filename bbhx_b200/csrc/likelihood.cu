@@ -241,28 +241,6 @@ __global__ void k_tile_segments(int2* tab, const double* __restrict__ x,
   }
 }
 
-// sin / cos in FP32 of an FP64 angle: the quadrant reduction by pi/2 stays in FP64 (the
-// angle reaches ~1e7 rad), the reduced |y| <= pi/4 goes to FP32 Taylor polynomials
-// (through y^9 and y^10; truncation < 2e-9).
-__device__ __forceinline__ void sincos_mixed(double x, float* s, float* c) {
-  const double TWO_OVER_PI = 0.6366197723675814;
-  double k = rint(x * TWO_OVER_PI);
-  double yd = fma(-k, 1.5707963267948966, x);
-  yd = fma(-k, 6.123233995736766e-17, yd);
-  float y = (float)yd;
-  float y2 = y * y;
-  float ps = fmaf(fmaf(fmaf(2.7557319e-06f, y2, -1.9841270e-04f), y2, 8.3333333e-03f), y2,
-                  -1.6666667e-01f);
-  float sy = fmaf(ps * y2, y, y);
-  float pc = fmaf(fmaf(fmaf(fmaf(-2.7557319e-07f, y2, 2.4801587e-05f), y2, -1.3888889e-03f), y2,
-                       4.1666667e-02f), y2, -0.5f);
-  float cy = fmaf(pc, y2, 1.0f);
-  int q = (int)(__double2ll_rn(k) & 3);
-  float ss = (q & 1) ? cy : sy;
-  float cc = (q & 1) ? sy : cy;
-  *s = (q & 2) ? -ss : ss;
-  *c = ((q + 1) & 2) ? -cc : cc;
-}
 
 // Cubic coefficients of one spline segment held by a lane: phase and t(f) always in FP64,
 // amplitude and the six transfer components in R (FP32 when mixed).

@@ -211,6 +211,7 @@ struct PhenomD {
       pins_m53, pins_1, pins_43, pins_53, pins_2;
   double C1Int, C2Int, C1MRD, C2MRD, fMRDJoin;
   double Rholm, Taulm;
+  double inv_atan_scale;  // 1 / (Rholm fDM Taulm)
 };
 
 struct Powers {  // PhenomHMWaveform.cu:348-362 (same derivation of the fractional powers)
@@ -219,8 +220,8 @@ struct Powers {  // PhenomHMWaveform.cu:348-362 (same derivation of the fraction
 
 __device__ __forceinline__ Powers make_powers(double x) {
   Powers p;
-  p.sixth = pow(x, 1.0 / 6.0);
-  p.third = p.sixth * p.sixth;
+  p.third = cbrt(x);
+  p.sixth = sqrt(p.third);
   p.two_thirds = x / p.third;
   p.four_thirds = x * p.third;
   p.five_thirds = p.four_thirds * p.third;
@@ -347,6 +348,68 @@ __device__ __forceinline__ double phenomd_dphase(const PhenomD& d, double Mf) {
   return dphi_int(d, Mf) + d.C2Int;
 }
 
+// Phase and d(phase)/dMf at one frequency together (the two branches of phenomd_phase and
+// phenomd_dphase), sharing the fractional powers, the logarithm and the reciprocals.
+__device__ __forceinline__ void phenomd_phase_dphase(const PhenomD& d, double Mf, double* ph,
+                                                     double* dph) {
+  const double PI_THIRD = 1.4645918875615231;  // pi^(1/3)
+  if (Mf < PHI_FJOIN_INS) {
+    const double t = cbrt(Mf);  // Mf^(1/3)
+    const double it = 1.0 / t;
+    const double t2 = t * t, it2 = it * it;
+    const double v = t * PI_THIRD;
+    const double logv = log(v);
+    double p = d.pins_init;
+    p += d.pins_23 * t2;
+    p += d.pins_13 * t;
+    p += d.pins_13log * logv * t;
+    p += d.pins_log * logv;
+    p += d.pins_m13 * it;
+    p += d.pins_m23 * it2;
+    p += d.pins_m1 * (it2 * it);
+    p += d.pins_m53 * (it2 * it2 * it);
+    p += (d.pins_1 * Mf + d.pins_43 * (Mf * t) + d.pins_53 * (Mf * t2) + d.pins_2 * (Mf * Mf)) *
+         d.etaInv;
+    *ph = p;
+    const double v2 = v * v, v3 = v2 * v, v4 = v3 * v, v5 = v4 * v, v6 = v5 * v, v7 = v6 * v;
+    double s = 2.0 * d.pn_v[7] * v7;
+    s += (d.pn_v[6] + d.pn_vlogv6 * (1.0 + logv)) * v6;
+    s += d.pn_vlogv5 * v5;
+    s -= d.pn_v[4] * v4;
+    s -= 2.0 * d.pn_v[3] * v3;
+    s -= 3.0 * d.pn_v[2] * v2;
+    s -= 4.0 * d.pn_v[1] * v;
+    s -= 5.0 * d.pn_v[0];
+    const double iv = it * (1.0 / PI_THIRD);
+    const double iv2 = iv * iv, iv4 = iv2 * iv2;
+    s *= (PI / 3.0) * (iv4 * iv4);
+    s += (d.sig1 + d.sig2 * t + d.sig3 * t2 + d.sig4 * Mf) * d.etaInv;
+    *dph = s;
+    return;
+  }
+  if (Mf >= d.fMRDJoin) {
+    const double sq = sqrt(Mf);
+    const double q = sqrt(sq);  // Mf^(1/4)
+    const double f075 = sq * q;
+    const double iF = 1.0 / Mf;
+    const double x = Mf - d.alp5 * d.fRD;
+    const double y = x * d.inv_atan_scale;
+    *ph = d.etaInv * (-(d.alp2 * iF) + (4.0 / 3.0) * (d.alp3 * f075) + d.alp1 * Mf +
+                      d.alp4 * d.Rholm * atan(y)) +
+          d.C1MRD + d.C2MRD * Mf;
+    *dph = (d.alp1 + d.alp2 * (iF * iF) + d.alp3 * (f075 * iF) +
+            d.alp4 / (d.fDM * d.Taulm * (1.0 + y * y))) *
+               d.etaInv +
+           d.C2MRD;
+    return;
+  }
+  const double iF = 1.0 / Mf;
+  const double iF2 = iF * iF;
+  *ph = d.etaInv * (d.bet1 * Mf - d.bet3 * (1.0 / 3.0) * (iF2 * iF) + d.bet2 * log(Mf)) + d.C1Int +
+        d.C2Int * Mf;
+  *dph = (d.bet1 + d.bet3 * (iF2 * iF2) + d.bet2 * iF) * d.etaInv + d.C2Int;
+}
+
 // Build the PhenomD coefficient set.  m1, m2 in solar masses with m1 >= m2 already
 // enforced; fring/fdamp dimensionless; Rholm/Taulm mode ratios (1, 1 for PhenomD).
 __device__ inline void phenomd_setup(PhenomD& d, double m1, double m2, double chi1, double chi2,
@@ -363,6 +426,7 @@ __device__ inline void phenomd_setup(PhenomD& d, double m1, double m2, double ch
   d.fDM = fdamp;
   d.Rholm = Rholm;
   d.Taulm = Taulm;
+  d.inv_atan_scale = 1.0 / (Rholm * fdamp * Taulm);
 
   // ---------------- amplitude ----------------
   const double pi16 = pow(PI, 1.0 / 6.0);
@@ -543,6 +607,11 @@ struct ModeCoeffs {
   double am_fi, am_fr, am_ai, am_am, am_bm, am_br;
   // PN amplitude ratio inputs (PhenomHMWaveform.cu:2375-2455)
   double pn_m1, pn_m2, pn_chi1, pn_chi2;
+  // |H_lm(v)| constants: leading factor, eta, delta, chi_s, chi_a; case 0 = 22 / PhenomD,
+  // 1..5 = 21, 33, 32, 44, 43, 6 = no PN amplitude
+  double pn_k, pn_eta, pn_delta, pn_Xs, pn_Xa, pn_2pi_m, pn_4pi_m2;
+  int pn_case, pad2;
+  double ph_inv_ai, ph_inv_am, ph_inv_ar;
   // overall shifts / scales
   double t0, phi0, Mf_ref, amp_scale, M_sec, cshift;
 };
@@ -556,43 +625,6 @@ __device__ __forceinline__ double cshift_of(int mm) {
     case 5: return PI_2;
     default: return 0.0;
   }
-}
-
-// |H_lm| v^-3.5 scaled, the FD PN amplitude of a multipole (London 2017)
-__device__ inline double pn_mode_amp(double fM, int l, int m, double M1, double M2, double X1, double X2) {
-  double Min = M1 + M2;
-  M1 = M1 / Min;
-  M2 = M2 / Min;
-  double M = M1 + M2;
-  double eta = M1 * M2 / (M * M);
-  double delta = sqrt(1.0 - 4 * eta);
-  double Xs = 0.5 * (X1 + X2);
-  double Xa = 0.5 * (X1 - X2);
-  double v = cbrt(M * 2.0 * PI * fM / m);
-  double v2 = v * v, v3 = v * v2;
-  double hre = 0.0, him = 0.0;
-  if (l == 2 && m == 2) {
-    hre = 1.0;
-  } else if (l == 2 && m == 1) {
-    double v4 = v * v3;
-    double k = sqrt(2.0) / 3.0;
-    hre = k * (v * delta - v2 * 1.5 * (Xa + delta * Xs) +
-               v3 * delta * ((335.0 / 672.0) + (eta * 117.0 / 56.0)) +
-               v4 * (Xa * (3427.0 / 1344 - eta * 2101.0 / 336) +
-                     delta * Xs * (3427.0 / 1344 - eta * 965 / 336) + delta * (-PI)));
-    him = k * v4 * delta * (-0.5 - 2.0 * 0.69314718056);
-  } else if (l == 3 && m == 3) {
-    hre = 0.75 * sqrt(5.0 / 7.0) * (v * delta);
-  } else if (l == 3 && m == 2) {
-    hre = (1.0 / 3.0) * sqrt(5.0 / 7.0) * (v2 * (1.0 - 3.0 * eta));
-  } else if (l == 4 && m == 4) {
-    hre = (4.0 / 9.0) * sqrt(10.0 / 7.0) * v2 * (1.0 - 3.0 * eta);
-  } else if (l == 4 && m == 3) {
-    hre = 0.75 * sqrt(3.0 / 35.0) * v3 * delta * (1.0 - 2.0 * eta);
-  }
-  double habs = hypot(hre, him);
-  double vm35 = 1.0 / (v3 * sqrt(v));
-  return M * M * PI * sqrt(eta * 2.0 / 3) * vm35 * habs;
 }
 
 // Set up one (binary, mode) record.  Inputs as the reference's IMRPhenomHM kernel:
@@ -636,6 +668,24 @@ __device__ inline void phm_setup_mode(ModeCoeffs& c, double m1_SI, double m2_SI,
   c.pn_m2 = m2;
   c.pn_chi1 = chi1;
   c.pn_chi2 = chi2;
+  {
+    const double M1 = m1 / (m1 + m2), M2 = m2 / (m1 + m2);
+    const double eta = M1 * M2 / ((M1 + M2) * (M1 + M2));
+    c.pn_eta = eta;
+    c.pn_delta = sqrt(1.0 - 4 * eta);
+    c.pn_Xs = 0.5 * (chi1 + chi2);
+    c.pn_Xa = 0.5 * (chi1 - chi2);
+    c.pn_2pi_m = 2.0 * PI / mm;
+    c.pn_4pi_m2 = 4.0 * PI / ((double)mm * mm);
+    if (run_phenomd || (ell == 2 && mm == 2)) { c.pn_case = 0; c.pn_k = 1.0; }
+    else if (ell == 2 && mm == 1) { c.pn_case = 1; c.pn_k = sqrt(2.0) / 3.0; }
+    else if (ell == 3 && mm == 3) { c.pn_case = 2; c.pn_k = 0.75 * sqrt(5.0 / 7.0); }
+    else if (ell == 3 && mm == 2) { c.pn_case = 3; c.pn_k = (1.0 / 3.0) * sqrt(5.0 / 7.0); }
+    else if (ell == 4 && mm == 4) { c.pn_case = 4; c.pn_k = (4.0 / 9.0) * sqrt(10.0 / 7.0); }
+    else if (ell == 4 && mm == 3) { c.pn_case = 5; c.pn_k = 0.75 * sqrt(3.0 / 35.0); }
+    else { c.pn_case = 6; c.pn_k = 0.0; }
+    c.pad2 = 0;
+  }
   if (run_phenomd) {
     c.d = d22;
     c.cshift = cshift_of(2);
@@ -661,6 +711,9 @@ __device__ inline void phm_setup_mode(ModeCoeffs& c, double m1_SI, double m2_SI,
     c.ph_am = am;
     c.ph_bm = bm;
     c.ph_ar = ar;
+    c.ph_inv_ai = 1.0 / ai;
+    c.ph_inv_am = 1.0 / am;
+    c.ph_inv_ar = 1.0 / ar;
     const double PhDBconst = phenomd_phase(c.d, am * fi + bm) / am;
     const double PhDCconst = phenomd_phase(c.d, ar * fr) / ar;
     const double PhDBAterm = phenomd_phase(c.d, ai * fi) / ai;
@@ -684,6 +737,84 @@ __device__ inline void phm_setup_mode(ModeCoeffs& c, double m1_SI, double m2_SI,
   }
 }
 
+// |H_lm(v)| of the 1.5PN spinning amplitude (IMRPhenomHMOnePointFiveSpinPN,
+// PhenomHMWaveform.cu:2375-2455) for the non-22 cases.
+__device__ __forceinline__ double pn_habs(const ModeCoeffs& c, double v) {
+  const double v2 = v * v, v3 = v2 * v;
+  switch (c.pn_case) {
+    case 1: {
+      const double v4 = v3 * v;
+      const double re = c.pn_k * (v * c.pn_delta - v2 * 1.5 * (c.pn_Xa + c.pn_delta * c.pn_Xs) +
+                                  v3 * c.pn_delta * ((335.0 / 672.0) + (c.pn_eta * 117.0 / 56.0)) +
+                                  v4 * (c.pn_Xa * (3427.0 / 1344 - c.pn_eta * 2101.0 / 336) +
+                                        c.pn_delta * c.pn_Xs * (3427.0 / 1344 - c.pn_eta * 965 / 336) +
+                                        c.pn_delta * (-PI)));
+      const double im = c.pn_k * v4 * c.pn_delta * (-0.5 - 2.0 * 0.69314718056);
+      return hypot(re, im);
+    }
+    case 2: return fabs(c.pn_k * (v * c.pn_delta));
+    case 3: return fabs(c.pn_k * (v2 * (1.0 - 3.0 * c.pn_eta)));
+    case 4: return fabs(c.pn_k * v2 * (1.0 - 3.0 * c.pn_eta));
+    case 5: return fabs(c.pn_k * v3 * c.pn_delta * (1.0 - 2.0 * c.pn_eta));
+    default: return 0.0;
+  }
+}
+
+// HM amplitude factor of get_amp (PhenomHMWaveform.cu:2461-2514): beta * HMamp1 / HMamp2 =
+// [P(Mf) / P(2Mf/m)] * [P_lm(Mfa) / P_22(Mfa)] with P = v^-3.5 |H(v)|, v = (2 pi x / m)^(1/3).
+// The v^-3.5 factors cancel exactly (v(2Mf/m) / v(Mf) = (2/m)^(1/3), v_22(Mfa) / v_lm(Mfa)
+// = (m/2)^(1/3)), leaving |H(v(Mf))| |H(v(Mfa))| / |H(v(2Mf/m))|; zero where |H(v(Mf))| = 0
+// (the reference's equal-mass guard).
+__device__ __forceinline__ double hm_amp_factor(const ModeCoeffs& c, double Mf, double Mfa) {
+  if (c.pn_case == 0) return 1.0;
+  const double t1 = pn_habs(c, cbrt(c.pn_2pi_m * Mf));
+  if (t1 == 0.0) return 0.0;
+  const double t2 = pn_habs(c, cbrt(c.pn_4pi_m2 * Mf));
+  const double h1 = pn_habs(c, cbrt(c.pn_2pi_m * Mfa));
+  return (t1 / t2) * h1;
+}
+
+// Mapped PhenomD frequency and phase constants of the HM phase map (get_phase,
+// PhenomHMWaveform.cu:2517-2565): ph = phase(Mfp) * inv + add.
+__device__ __forceinline__ void hm_phase_map(const ModeCoeffs& c, double Mf, double* Mfp,
+                                             double* inv, double* add) {
+  if (!(Mf > c.ph_fi)) {
+    *Mfp = c.ph_ai * Mf;
+    *inv = c.ph_inv_ai;
+    *add = 0.0;
+  } else if (!(Mf > c.ph_fr)) {
+    *Mfp = c.ph_am * Mf + c.ph_bm;
+    *inv = c.ph_inv_am;
+    *add = c.ph_constB;
+  } else {
+    *Mfp = c.ph_ar * Mf;
+    *inv = c.ph_inv_ar;
+    *add = c.ph_constC;
+  }
+}
+
+// Phase and t(f) of one mode at Mf (no t_ref shift).
+__device__ __forceinline__ void mode_phase_tf(const ModeCoeffs& c, double Mf, double* phase,
+                                              double* tf) {
+  double ph, dph;
+  if (c.phenomd_only) {
+    phenomd_phase_dphase(c.d, Mf, &ph, &dph);
+    *phase = -c.t0 * (Mf - c.Mf_ref) + ((c.cshift + ph) - 2 * c.phi0);
+  } else {
+    double Mfp, inv, add;
+    hm_phase_map(c, Mf, &Mfp, &inv, &add);
+    phenomd_phase_dphase(c.d, Mfp, &ph, &dph);
+    *phase = -c.t0 * (Mf - c.Mf_ref) + ((c.cshift + (ph * inv + add)) - c.mm * c.phi0);
+  }
+  *tf = c.M_sec * (dph / (2. * PI)) - (c.t0 / (2. * PI) * c.M_sec);
+}
+
+// Mapped amplitude frequency (IMRPhenomHMFreqDomainMap with AmpFlag, :2295-2315).
+__device__ __forceinline__ double hm_amp_map(const ModeCoeffs& c, double Mf) {
+  if (Mf > c.am_fi) return (Mf > c.am_fr) ? Mf + c.am_br : c.am_am * Mf + c.am_bm;
+  return c.am_ai * Mf;
+}
+
 struct PointOut {
   double amp, phase, tf;
 };
@@ -695,49 +826,11 @@ __device__ inline PointOut phm_eval_point(const ModeCoeffs& c, double f) {
   const double Mf = f * c.M_sec;
   if (c.phenomd_only) {
     o.amp = phenomd_amp(c.d, Mf) * c.amp_scale;
-    double ph = c.cshift + phenomd_phase(c.d, Mf);
-    o.phase = -c.t0 * (Mf - c.Mf_ref) + (ph - 2 * c.phi0);
-    o.tf = c.M_sec * phenomd_dphase(c.d, Mf) / (2 * PI) - (c.t0 / (2. * PI) * c.M_sec);
-    return o;
+  } else {
+    const double Mfa = hm_amp_map(c, Mf);
+    o.amp = phenomd_amp(c.d, Mfa) * hm_amp_factor(c, Mf, Mfa) * c.amp_scale;
   }
-  // amplitude
-  {
-    double Mfa;
-    if (Mf > c.am_fi) {
-      if (Mf > c.am_fr)
-        Mfa = Mf + c.am_br;
-      else
-        Mfa = c.am_am * Mf + c.am_bm;
-    } else {
-      Mfa = c.am_ai * Mf;
-    }
-    double a = phenomd_amp(c.d, Mfa);
-    double t1 = pn_mode_amp(Mf, c.ell, c.mm, c.pn_m1, c.pn_m2, c.pn_chi1, c.pn_chi2);
-    double fac = 0.0;
-    if (t1 != 0.0) {
-      double t2 = pn_mode_amp(2.0 * Mf / c.mm, c.ell, c.mm, c.pn_m1, c.pn_m2, c.pn_chi1, c.pn_chi2);
-      double h1 = pn_mode_amp(Mfa, c.ell, c.mm, c.pn_m1, c.pn_m2, c.pn_chi1, c.pn_chi2);
-      double h2 = pn_mode_amp(Mfa, 2, 2, c.pn_m1, c.pn_m2, 0.0, 0.0);
-      fac = (t1 / t2) * h1 / h2;
-    }
-    o.amp = a * fac * c.amp_scale;
-  }
-  // phase and t(f)
-  {
-    double Mfp, ph;
-    if (!(Mf > c.ph_fi)) {
-      Mfp = c.ph_ai * Mf;
-      ph = phenomd_phase(c.d, Mfp) / c.ph_ai;
-    } else if (!(Mf > c.ph_fr)) {
-      Mfp = c.ph_am * Mf + c.ph_bm;
-      ph = phenomd_phase(c.d, Mfp) / c.ph_am + c.ph_constB;
-    } else {
-      Mfp = c.ph_ar * Mf;
-      ph = phenomd_phase(c.d, Mfp) / c.ph_ar + c.ph_constC;
-    }
-    o.phase = -c.t0 * (Mf - c.Mf_ref) + ((c.cshift + ph) - c.mm * c.phi0);
-    o.tf = c.M_sec * (phenomd_dphase(c.d, Mfp) / (2. * PI)) - (c.t0 / (2. * PI) * c.M_sec);
-  }
+  mode_phase_tf(c, Mf, &o.phase, &o.tf);
   return o;
 }
 

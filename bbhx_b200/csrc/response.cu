@@ -14,13 +14,6 @@
 
 namespace bbhx {
 
-struct OrbitHandle {
-  double* d_x = nullptr;
-  double* d_n = nullptr;
-  OrbitTables tab{};
-  bool ready = false;
-};
-
 __global__ void k_response_setup(ResponseMode* out, const int* ells, const int* mms,
                                  const double* phi_ref, const double* inc, const double* lam,
                                  const double* beta, const double* psi, int M, int B) {

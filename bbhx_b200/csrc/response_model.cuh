@@ -30,6 +30,14 @@ struct OrbitTables {
   double armlength;
 };
 
+// Device-resident orbit tables owned by the C-ABI orbit handle (bbhx_orbits_*).
+struct OrbitHandle {
+  double* d_x = nullptr;
+  double* d_n = nullptr;
+  OrbitTables tab{};
+  bool ready = false;
+};
+
 struct ResponseMode {
   cplx H[9];     // complex mode matrix, row-major
   double k[3];   // propagation direction
@@ -170,9 +178,10 @@ __device__ inline Transfer response_point(const ResponseMode& r, const OrbitTabl
   cplx G31 = c2 * (sinc(pre * (1. - kn2)) * e31);
   cplx G13 = c2 * (sinc(pre * (1. + kn2)) * e31);
 
-  double x = pre;
-  cplx z = expi(2. * x);
-  double s2x = sin(2. * x);
+  // e^{ix}, x = pre, and its powers / sines from one sincos
+  const cplx e1 = expi(pre);
+  const cplx z = e1 * e1;  // e^{2ix}
+  const double s2x = 2. * e1.im * e1.re;
   if (TDItag == 1) {
     cplx fac = rescaled ? mk(1.0, 0.0) : times_i(2. * s2x * z);
     cplx X = G21 + z * G12 - G31 - z * G13;
@@ -189,7 +198,7 @@ __device__ inline Transfer response_point(const ResponseMode& r, const OrbitTabl
     fT = mk(1.0, 0.0);
   } else {
     fAE = times_i(SQRT2 * s2x * z);
-    fT = (2. * SQRT2 * s2x * sin(x)) * expi(3. * x);
+    fT = (2. * SQRT2 * s2x * e1.im) * (z * e1);
   }
   cplx one = mk(1.0, 0.0);
   cplx A = 0.5 * ((one + z) * (G31 + G13) - G23 - z * G32 - G21 - z * G12);
@@ -197,7 +206,7 @@ __device__ inline Transfer response_point(const ResponseMode& r, const OrbitTabl
                               (one + 2. * z) * (G21 - G23));
   cplx T = INVSQRT6 * (G21 - G12 + G32 - G23 + G13 - G31);
   cplx f2 = mk(2.0, 0.0);
-  if (tdi2) f2 = 2.0 * times_i(-2. * sin(4. * x) * expi(4. * x));
+  if (tdi2) f2 = 2.0 * times_i((-2. * (2. * s2x * z.re)) * (z * z));  // -2i sin4x e^{4ix}
   out.L1 = f2 * (fAE * A);
   out.L2 = f2 * (fAE * E);
   out.L3 = f2 * (fT * T);

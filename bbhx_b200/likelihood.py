@@ -90,11 +90,21 @@ class Likelihood:
 
 
 class HeterodynedLikelihood:
+    """Heterodyned (relative-binning) log-likelihood.  ``precision`` selects the fused kernel
+    that evaluates the walkers: "fp64" (default) or "mixed" (FP64 phase, t(f), Roemer delay,
+    ratio and sums; FP32 amplitude, transfer functions and channel products).  ``None``
+    runs the reference's step-by-step chain (sparse templates, ratio, hdyn), which also
+    materialises ``h_sparse``; with a fused precision ``h_sparse`` is produced on first
+    access from the last walkers."""
+
     def __init__(self, template_gen, data_freqs, data_channels, reference_template_params,
                  length_f_het, template_gen_kwargs=None, reference_gen_kwargs=None, sens_mat=None,
-                 force_backend=None):
+                 force_backend=None, precision="fp64"):
         template_gen_kwargs = {} if template_gen_kwargs is None else template_gen_kwargs
         reference_gen_kwargs = {} if reference_gen_kwargs is None else reference_gen_kwargs
+        self.precision = precision
+        self._h_sparse = None
+        self._last = None
         self.template_gen = template_gen
         self.f_dense = to_dev(data_freqs)
         self.d = to_dev(data_channels, torch().complex128)
@@ -149,6 +159,7 @@ class HeterodynedLikelihood:
         freqs_keep = freqs[keep]
         freqs = np.logspace(np.log10(freqs_keep[0]), np.log10(freqs_keep[-1]), self.length_f_het)
         self.h0_sparse = self.template_gen(*p, freqs=freqs, **template_gen_kwargs)[None, :, :]
+        self._h0_flat = self.h0_sparse[0].contiguous()
         fd_all = to_np(self.f_dense)
         inds = (fd_all >= freqs[0]) & (fd_all <= freqs[-1])
         inds_d = to_dev(inds, t.bool)
@@ -184,6 +195,14 @@ class HeterodynedLikelihood:
         template_gen_kwargs["squeeze"] = False
         self.template_gen_kwargs = template_gen_kwargs
 
+    @property
+    def h_sparse(self):
+        """Sparse templates [B, 3, L] of the last walkers (likelihood.py:612)."""
+        if self._h_sparse is None and self._last is not None:
+            params, kw = self._last
+            self._h_sparse = self.template_gen(*params, **kw)
+        return self._h_sparse
+
     def get_ll(self, params, return_extracted_snr=False, phase_marginalize=False,
                **waveform_kwargs):
         """Heterodyned log-likelihood (likelihood.py:550-648)."""
@@ -197,16 +216,31 @@ class HeterodynedLikelihood:
             elif key in self.template_gen_kwargs:
                 waveform_kwargs[key] = waveform_kwargs.get(key, self.template_gen_kwargs[key])
         waveform_kwargs["freqs"] = self.freqs
-        params = np.atleast_2d(np.asarray(params, dtype=np.float64))
-        self.h_sparse = self.template_gen(*params, **waveform_kwargs)
-        r = self.h_sparse / self.h0_sparse
-        B = r.shape[0]
-        residuals = r.permute(2, 1, 0).contiguous().flatten()
-        self.hdyn_d_h = t.zeros(B, dtype=t.complex128, device=device())
-        self.hdyn_h_h = t.zeros(B, dtype=t.complex128, device=device())
-        _lib.call("bbhx_hdyn", _lib.dptr(self.hdyn_d_h), _lib.dptr(self.hdyn_h_h), _lib.dptr(residuals),
-                  _lib.dptr(self.data_constants), _lib.dptr(self.freqs), B, len(self.freqs), 3,
-                  _lib.stream())
+        if isinstance(params, t.Tensor):
+            params = params.to(device=device(), dtype=t.float64, non_blocking=True)
+            if params.ndim == 1:
+                params = params.reshape(-1, 1)
+            params = tuple(params[k].contiguous() for k in range(params.shape[0]))
+        else:
+            params = tuple(np.atleast_2d(np.asarray(params, dtype=np.float64)))
+        if self.precision is not None:
+            kw = {k: v for k, v in waveform_kwargs.items()
+                  if k in ("t_obs_start", "t_obs_end", "modes")}
+            self._last = (params, dict(waveform_kwargs))
+            self._h_sparse = None
+            self.hdyn_d_h, self.hdyn_h_h = self.template_gen.heterodyne_sums(
+                params, self.freqs, self._h0_flat, self.data_constants,
+                precision=self.precision, **kw)
+        else:
+            self._h_sparse = self.template_gen(*params, **waveform_kwargs)
+            r = self._h_sparse / self.h0_sparse
+            B = r.shape[0]
+            residuals = r.permute(2, 1, 0).contiguous().flatten()
+            self.hdyn_d_h = t.zeros(B, dtype=t.complex128, device=device())
+            self.hdyn_h_h = t.zeros(B, dtype=t.complex128, device=device())
+            _lib.call("bbhx_hdyn", _lib.dptr(self.hdyn_d_h), _lib.dptr(self.hdyn_h_h),
+                      _lib.dptr(residuals), _lib.dptr(self.data_constants), _lib.dptr(self.freqs),
+                      B, len(self.freqs), 3, _lib.stream())
         d_h_temp = self.hdyn_d_h if not phase_marginalize else self.hdyn_d_h.abs().to(t.complex128)
         out = (-1 / 2.0 * (self.reference_d_d + self.hdyn_h_h - 2 * d_h_temp).real).cpu().numpy()
         if return_extracted_snr:

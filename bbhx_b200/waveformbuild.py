@@ -252,6 +252,37 @@ class BBHWaveformFD:
             return data_out
         return (template_channels, self.interp_response.start_inds, self.interp_response.lengths)
 
+    def heterodyne_sums(self, params, freqs, h0, constants, t_obs_start=0.0, t_obs_end=1.0,
+                        modes=None, precision="fp64", flags=None, **unused):
+        """Relative-binning sums d_h, h_h (device complex128 [B] each) of the walkers
+        ``params`` in one fused kernel: waveform + response at the sparse grid ``freqs``
+        [L], mode sum, r = h / h0 (``h0`` [3, L]) and the bin terms with ``constants``
+        [4, 3, L] (likelihood.py:550-648, Likelihood.cu:20-123)."""
+        t = torch()
+        (m1, m2, chi1z, chi2z, distance, phi_ref, f_ref, inc, lam, beta, psi, t_ref) = params
+        if isinstance(lam, t.Tensor) and lam.is_cuda:
+            lam_h, beta_h = atleast_1d(lam), atleast_1d(beta)
+        else:
+            lam_h = to_np(atleast_1d(lam)).astype(np.float64)
+            beta_h = to_np(atleast_1d(beta)).astype(np.float64)
+        t_start, t_end = self._time_limits(lam_h, beta_h, t_obs_start, t_obs_end)
+        ap = self.amp_phase_gen
+        ap._setup_records(m1, m2, chi1z, chi2z, distance, t_ref, modes, flags=flags)
+        B, M, L = ap.num_bin_all, ap.num_modes, int(freqs.numel())
+        rg = self.response_gen
+        inc_d, lam_d, beta_d, psi_d, phi_d = (to_dev(atleast_1d(v)) for v in (inc, lam, beta, psi, phi_ref))
+        ts_d = to_dev(t_start)
+        te_d = to_dev(t_end)
+        d_h = t.empty(B, dtype=t.complex128, device=device())
+        h_h = t.empty(B, dtype=t.complex128, device=device())
+        _lib.call("bbhx_hdyn_fused", rg.orbit_handle.ptr, _lib.dptr(d_h), _lib.dptr(h_h),
+                  _lib.dptr(ap._coeffs), _lib.dptr(ap.ells), _lib.dptr(ap.mms), _lib.dptr(phi_d),
+                  _lib.dptr(inc_d), _lib.dptr(lam_d), _lib.dptr(beta_d), _lib.dptr(psi_d),
+                  _lib.dptr(ap.t_ref_dev), float(ap.initial_t_val), _lib.dptr(ts_d), _lib.dptr(te_d),
+                  _lib.dptr(freqs), _lib.dptr(h0), _lib.dptr(constants), rg.TDItag_int,
+                  int(rg.rescaled), int(rg.tdi2), M, L, B, PRECISIONS[precision], _lib.stream())
+        return d_h, h_h
+
     def inner_products(self, params, data_freqs, data_weighted, noise_factors, t_obs_start=0.0,
                        t_obs_end=1.0, length=1024, modes=None, flags=None, timing=None,
                        precision="fp64", **unused):

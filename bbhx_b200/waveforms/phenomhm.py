@@ -129,36 +129,13 @@ class PhenomHMAmpPhase:
         """Shared front half of run_wave: parameter checks, modes, buffers, ringdown
         frequencies and the per-(binary, mode) model records."""
         t = torch()
-        m1 = to_dev(atleast_1d(m1)).clone()
-        m2 = to_dev(atleast_1d(m2)).clone()
-        chi1z = to_dev(atleast_1d(chi1z)).clone()
-        chi2z = to_dev(atleast_1d(chi2z)).clone()
-        m1, m2, chi1z, chi2z = self._sanity_check_params(m1, m2, chi1z, chi2z, flags)
-        if modes is not None:
-            ells = to_dev([ell for ell, mm in modes], t.int32)
-            mms = to_dev([mm for ell, mm in modes], t.int32)
-            self.modes = modes
-            self._sanity_check_modes([e for e, _ in modes], [m for _, m in modes])
-        else:
-            self.modes = self.allowable_modes
-            ells, mms = self.ells_default, self.mms_default
-        if self.run_phenomd:
-            ells = to_dev([2], t.int32)
-            mms = to_dev([2], t.int32)
-            self.modes = self.allowable_modes
-        self.ells, self.mms = ells, mms
-        num_modes = len(ells)
-        num_bin_all = len(m1)
+        self._setup_records(m1, m2, chi1z, chi2z, distance, t_ref, modes, flags)
+        m1, m2 = self._m1, self._m2
+        num_modes, num_bin_all, mms = self.num_modes, self.num_bin_all, self.mms
         self.length = length
-        self.num_modes = num_modes
-        self.num_bin_all = num_bin_all
         self.nparams = 3
         self.num_per_param = length * num_modes * num_bin_all
         self.num_per_bin = length * num_modes
-        distance = to_dev(atleast_1d(distance))
-        self.t_ref_dev = to_dev(atleast_1d(t_ref))
-        if distance.numel() != num_bin_all or self.t_ref_dev.numel() != num_bin_all:
-            raise ValueError("all parameter arrays must have the same length")
         if out_buffer is None:
             self.waveform_carrier = t.zeros(self.nparams * self.num_per_param, dtype=t.float64,
                                             device=device())
@@ -179,6 +156,37 @@ class PhenomHMAmpPhase:
             else:
                 raise ValueError(
                     "If providing freqs, must be 1D array (length,) or 3D array (length, num_modes, length).")
+
+    def _setup_records(self, m1, m2, chi1z, chi2z, distance, t_ref, modes, flags=None):
+        """Parameter checks, mode list, ringdown frequencies and the per-(binary, mode)
+        model records (``self._coeffs``), without any frequency grid or output buffer."""
+        t = torch()
+        m1 = to_dev(atleast_1d(m1)).clone()
+        m2 = to_dev(atleast_1d(m2)).clone()
+        chi1z = to_dev(atleast_1d(chi1z)).clone()
+        chi2z = to_dev(atleast_1d(chi2z)).clone()
+        m1, m2, chi1z, chi2z = self._sanity_check_params(m1, m2, chi1z, chi2z, flags)
+        if modes is not None:
+            ells = to_dev([ell for ell, mm in modes], t.int32)
+            mms = to_dev([mm for ell, mm in modes], t.int32)
+            self.modes = modes
+            self._sanity_check_modes([e for e, _ in modes], [m for _, m in modes])
+        else:
+            self.modes = self.allowable_modes
+            ells, mms = self.ells_default, self.mms_default
+        if self.run_phenomd:
+            ells = to_dev([2], t.int32)
+            mms = to_dev([2], t.int32)
+            self.modes = self.allowable_modes
+        self.ells, self.mms = ells, mms
+        num_modes = len(ells)
+        num_bin_all = len(m1)
+        self.num_modes = num_modes
+        self.num_bin_all = num_bin_all
+        distance = to_dev(atleast_1d(distance))
+        self.t_ref_dev = to_dev(atleast_1d(t_ref))
+        if distance.numel() != num_bin_all or self.t_ref_dev.numel() != num_bin_all:
+            raise ValueError("all parameter arrays must have the same length")
         m1_SI = (m1 * MSUN_SI).contiguous()
         m2_SI = (m2 * MSUN_SI).contiguous()
         ncol = 1 if self.run_phenomd else num_modes + 1

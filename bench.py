@@ -369,7 +369,11 @@ def gpu_arm(args):
 
 
 def het_metric(args, wave, like, f, params):
-    """Heterodyned lnL evals/s: 128 relative-binning bins, B walkers around the injection."""
+    """Heterodyned lnL evals/s: 128 relative-binning bins, B walkers around the injection.
+
+    Three forms on the same walkers: the fused kernel in FP64 ("plain FP64 GPU form") and in
+    mixed precision, and the step-by-step chain of the reference (sparse templates, ratio,
+    hdyn).  |dlnL| of mixed against FP64 is reported over all walkers."""
     import torch
 
     from bbhx_b200 import AET1SensitivityMatrix, HeterodynedLikelihood
@@ -382,22 +386,42 @@ def het_metric(args, wave, like, f, params):
                                 reference_gen_kwargs=dict(kw, length=LENGTH),
                                 sens_mat=AET1SensitivityMatrix(f, tdi2=True, notch=True))
     Bh = args.het_batch
-    walkers = perturb_params(center, Bh, 5)
-    for _ in range(2):
-        het.get_ll(walkers, **kw)
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
+    walkers = torch.as_tensor(perturb_params(center, Bh, 5), device="cuda")
     n = max(2, args.steps // 2)
-    e0.record()
-    for _ in range(n):
-        ll = het.get_ll(walkers, **kw)
-    e1.record()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    return {"heterodyned": {"value": Bh * n / (ms / 1e3), "unit": "lnL evals/s", "batch": Bh,
-                            "bins": 128, "dtype": "f64", "path": "e2e via HeterodynedLikelihood.get_ll",
-                            "finite": bool(np.all(np.isfinite(ll)))}}
+
+    def timed(precision, batch):
+        het.precision = precision
+        w = walkers[:, :batch]
+        for _ in range(2):
+            het.get_ll(w, **kw)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(n):
+            ll = het.get_ll(w, **kw)
+        e1.record()
+        torch.cuda.synchronize()
+        return batch * n / (e0.elapsed_time(e1) / 1e3), ll
+
+    v64, ll64 = timed("fp64", Bh)
+    vmx, llmx = timed("mixed", Bh)
+    chain_batch = min(Bh, 16384)
+    vch, _ = timed(None, chain_batch)
+    d = np.abs(llmx - ll64)
+    return {"heterodyned": {
+        "value": vmx, "unit": "lnL evals/s", "batch": Bh, "bins": 128,
+        "dtype": "mixed: f64 phase/t(f)/Roemer/ratio/sums, f32 amplitude/transfer/products",
+        "fp64_plain": {"value": v64, "unit": "lnL evals/s", "kernel": "k_het_fused<fp64>"},
+        "mixed_over_fp64": vmx / v64,
+        "step_by_step_chain_fp64": {"value": vch, "unit": "lnL evals/s", "batch": chain_batch},
+        "dlnl_mixed_vs_fp64": {"max": float(d.max()), "p99": float(np.percentile(d, 99)),
+                               "median": float(np.median(d)),
+                               "max_over_reference_hh": float(d.max() / het.reference_h_h),
+                               "reference_hh": float(het.reference_h_h)},
+        "lnl_range": [float(ll64.min()), float(ll64.max())],
+        "path": "HeterodynedLikelihood.get_ll with device-resident walkers",
+        "finite": bool(np.all(np.isfinite(ll64)) and np.all(np.isfinite(llmx)))}}
 
 
 def reference_arm(args):

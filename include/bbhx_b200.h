@@ -182,6 +182,21 @@ int bbhx_direct_like_fused(double *d_h, double *h_h, const double *data_freqs, c
                            const double *t_start, const double *t_end, int num_modes, int length,
                            int num_bin_all, int precision, void *stream);
 
+/* fused heterodyned likelihood: PhenomHM + TDI response at the sparse heterodyne grid, mode
+   sum, r = h / h0 and the relative-binning bin sums in one kernel (one CTA per walker).
+   Replaces, as one call, waveform_amp_phase (PhenomHMWaveform.hh:354-371) + LISA_response
+   (Response.hh:27-41) + direct_sum (WaveformBuild.hh:8-10) + the host-side ratio
+   (likelihood.py:606-616) + hdyn (Likelihood.hh:6-9, GPU form: every bin j >= 1).
+   coeffs: records from bbhx_phenomhm_setup [B, M]; freqs [L]; h0 [3, L] complex128;
+   consts [4, 3, L] complex128 (A0, A1, B0, B1); d_h, h_h [B] complex128 (device).
+   precision: 0 = FP64, 1 = mixed (FP64 phase / t(f) / sums, FP32 amplitude / transfer). */
+int bbhx_hdyn_fused(void *orbits, void *d_h, void *h_h, const void *coeffs, const int *ells,
+                    const int *mms, const double *phi_ref, const double *inc, const double *lam,
+                    const double *beta, const double *psi, const double *t_ref, double t_init,
+                    const double *t_start, const double *t_end, const double *freqs,
+                    const void *h0, const void *consts, int TDItag, int rescaled, int tdi2,
+                    int num_modes, int length, int num_bin_all, int precision, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
