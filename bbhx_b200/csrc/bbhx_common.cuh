@@ -39,34 +39,63 @@ enum Status : int {
   ERR_TOO_LARGE = 6,
 };
 
-struct cplx {
-  double re, im;
+// Complex numbers over any real scalar T (double, float, or the dual numbers of the
+// gradient kernels).  In the scalar products the scalar is converted to T, so double
+// constants multiply dual-number complexes directly.
+template <typename T>
+struct cplxT {
+  T re, im;
 };
-struct cplxf {
-  float re, im;
+using cplx = cplxT<double>;
+using cplxf = cplxT<float>;
+
+template <typename T>
+struct ident {
+  using type = T;
 };
 
 __host__ __device__ __forceinline__ cplx mk(double r, double i) { return cplx{r, i}; }
-__host__ __device__ __forceinline__ cplx operator+(cplx a, cplx b) { return {a.re + b.re, a.im + b.im}; }
-__host__ __device__ __forceinline__ cplx operator-(cplx a, cplx b) { return {a.re - b.re, a.im - b.im}; }
-__host__ __device__ __forceinline__ cplx operator*(cplx a, cplx b) {
+template <typename T>
+__host__ __device__ __forceinline__ cplxT<T> cmk(const T& r, const T& i) {
+  return cplxT<T>{r, i};
+}
+template <typename T>
+__host__ __device__ __forceinline__ cplxT<T> operator+(const cplxT<T>& a, const cplxT<T>& b) {
+  return {a.re + b.re, a.im + b.im};
+}
+template <typename T>
+__host__ __device__ __forceinline__ cplxT<T> operator-(const cplxT<T>& a, const cplxT<T>& b) {
+  return {a.re - b.re, a.im - b.im};
+}
+template <typename T>
+__host__ __device__ __forceinline__ cplxT<T> operator*(const cplxT<T>& a, const cplxT<T>& b) {
   return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
 }
-__host__ __device__ __forceinline__ cplx operator*(double s, cplx a) { return {s * a.re, s * a.im}; }
-__host__ __device__ __forceinline__ cplx operator*(cplx a, double s) { return {s * a.re, s * a.im}; }
-__host__ __device__ __forceinline__ cplx conj(cplx a) { return {a.re, -a.im}; }
-__host__ __device__ __forceinline__ cplx times_i(cplx a) { return {-a.im, a.re}; }
-__device__ __forceinline__ cplx expi(double x) {
-  double s, c;
+template <typename T>
+__host__ __device__ __forceinline__ cplxT<T> operator*(typename ident<T>::type s,
+                                                       const cplxT<T>& a) {
+  return {s * a.re, s * a.im};
+}
+template <typename T>
+__host__ __device__ __forceinline__ cplxT<T> operator*(const cplxT<T>& a,
+                                                       typename ident<T>::type s) {
+  return {s * a.re, s * a.im};
+}
+template <typename T>
+__host__ __device__ __forceinline__ cplxT<T> conj(const cplxT<T>& a) {
+  return {a.re, -a.im};
+}
+template <typename T>
+__host__ __device__ __forceinline__ cplxT<T> times_i(const cplxT<T>& a) {
+  return {-a.im, a.re};
+}
+template <typename T>
+__device__ __forceinline__ cplxT<T> expi(const T& x) {
+  T s, c;
   sincos(x, &s, &c);
   return {c, s};
 }
 __device__ __forceinline__ double cabs(cplx a) { return hypot(a.re, a.im); }
-
-__host__ __device__ __forceinline__ cplxf operator+(cplxf a, cplxf b) { return {a.re + b.re, a.im + b.im}; }
-__host__ __device__ __forceinline__ cplxf operator*(cplxf a, cplxf b) {
-  return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
-}
 
 // Phase reduction to [-pi, pi]: k = rint(x / 2pi), then x - k*2pi with 2pi split into a
 // double (hi) and its residual (lo); each FMA forms k*part exactly before its single

@@ -1,0 +1,168 @@
+// Forward-mode (tangent) parts of the gradient chain: dual-number setup of the per-mode
+// PhenomHM and response records, and the contraction of the per-point tangents with the
+// adjoint weights produced by the reverse part (heterodyne bin sums or spline adjoint).
+//
+// Gradient parameters (NGRAD = 11), in this order, with their index in the 12-row
+// parameter array of BBHWaveformFD (waveformbuild.py:338-352):
+//   0 m1 [Msun] (row 0)   1 m2 [Msun] (1)   2 chi1z (2)   3 chi2z (3)   4 distance [m] (4)
+//   5 phi_ref (5)   6 inc (7)   7 lam (8)   8 beta (9)   9 psi (10)   10 t_ref [s] (11)
+// f_ref (row 6) does not enter the model (the reference frequency is the amplitude peak).
+#pragma once
+
+#include "bbhx_common.cuh"
+#include "dual.cuh"
+#include "phenomhm_model.cuh"
+#include "response_model.cuh"
+#include "spline_eval.cuh"
+
+namespace bbhx {
+
+constexpr int NGRAD = 11;
+using GD = ad::Dual<NGRAD>;
+
+__device__ __forceinline__ GD seed(double v, int k) {
+  GD x(v);
+  x.d[k] = 1.0;
+  return x;
+}
+
+struct GradParams {
+  GD m1, m2, chi1, chi2, dist, phi_ref, inc, lam, beta, psi, t_ref;
+};
+
+// P: [12, B] row-major parameter array (device).
+__device__ inline GradParams load_grad_params(const double* P, int B, int b) {
+  GradParams g;
+  g.m1 = seed(P[0 * (size_t)B + b], 0);
+  g.m2 = seed(P[1 * (size_t)B + b], 1);
+  g.chi1 = seed(P[2 * (size_t)B + b], 2);
+  g.chi2 = seed(P[3 * (size_t)B + b], 3);
+  g.dist = seed(P[4 * (size_t)B + b], 4);
+  g.phi_ref = seed(P[5 * (size_t)B + b], 5);
+  g.inc = seed(P[7 * (size_t)B + b], 6);
+  g.lam = seed(P[8 * (size_t)B + b], 7);
+  g.beta = seed(P[9 * (size_t)B + b], 8);
+  g.psi = seed(P[10 * (size_t)B + b], 9);
+  g.t_ref = seed(P[11 * (size_t)B + b], 10);
+  return g;
+}
+
+// Dual-number records of binaries [b0, b0 + nb): the same chain as the forward path
+// (ringdown frequencies -> phm_setup_mode; response_mode_setup), with tangents seeded on the
+// 11 parameters.  qnm: [8, nq] table y/c1/c2/c3 of the ringdown and damping splines.
+static __global__ void k_grad_setup(ModeCoeffsT<GD>* coeffs, ResponseModeT<GD>* rmodes, const double* P,
+                             int B, int b0, int nb, const int* ells, const int* mms, int M,
+                             const double* qnm, int nq, double dspin, int run_phenomd) {
+  const long long n = (long long)nb * M;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int bl = (int)(t / M), i = (int)(t % M);
+    const int b = b0 + bl;
+    const GradParams g = load_grad_params(P, B, b);
+    GD fm, fs;
+    final_mass_spin(g.m1, g.m2, g.chi1, g.chi2, &fm, &fs);
+    // PhenomD 22 ringdown / damping from the tabulated spline (PhenomHMWaveform.cu:1930-1993)
+    const int ind = int((fs.v - (-1.0)) / dspin);
+    const GD x = fs - (dspin * ind + (-1.0));
+    const GD x2 = x * x, x3 = x2 * x;
+    const double* y_rd = qnm;
+    const double* y_dm = qnm + 4 * (size_t)nq;
+    const GD rd22 = (y_rd[ind] + y_rd[nq + ind] * x + y_rd[2 * nq + ind] * x2 +
+                     y_rd[3 * nq + ind] * x3) / fm;
+    const GD dm22 = (y_dm[ind] + y_dm[nq + ind] * x + y_dm[2 * nq + ind] * x2 +
+                     y_dm[3 * nq + ind] * x3) / fm;
+    const int ell = run_phenomd ? 2 : ells[i];
+    const int mm = run_phenomd ? 2 : mms[i];
+    GD rd_lm = rd22, dm_lm = dm22;
+    if (!run_phenomd) {
+      const cplxT<GD> z = qnm_cw(fs, ell, mm);
+      rd_lm = (0.5 / PI) * z.re / fm;
+      dm_lm = (0.5 / PI) * z.im / fm;
+    }
+    phm_setup_mode(coeffs[t], g.m1 * MSUN_SI, g.m2 * MSUN_SI, g.chi1, g.chi2, g.dist, ell, mm,
+                   rd_lm, dm_lm, rd22, dm22, run_phenomd);
+    response_mode_setup(rmodes[t], ell, mm, g.phi_ref, g.inc, g.lam, g.beta, g.psi);
+  }
+}
+
+// Waveform phasor term W_c = T_c A e^{i (phase + Roemer)} of one (mode, frequency) with
+// tangents, and its t(f) (for the observation gate).  Phase and t(f) include the t_ref shift
+// (phenomhm.py:485-507).
+struct PointTangents {
+  cplxT<GD> W[3];
+  GD amp, phase;  // phase including the t_ref shift and the Roemer delay
+  cplxT<GD> T[3];
+  double tf;
+};
+
+__device__ inline PointTangents point_tangents(const ModeCoeffsT<GD>& c, const ResponseModeT<GD>& r,
+                                               const OrbitTables& orb, double f, const GD& t_ref,
+                                               double t_init, int TDItag, int rescaled, int tdi2) {
+  PointTangents o;
+  const PointOutT<GD> w = phm_eval_point(c, GD(f));
+  const GD tf = w.tf + t_ref;
+  o.tf = tf.v;
+  const TransferT<GD> T = response_point(r, orb, f, tf, TDItag, rescaled, tdi2);
+  o.amp = w.amp;
+  o.phase = w.phase + (2 * PI * f) * (t_ref - t_init) + T.phaseRdelay;
+  const cplxT<GD> ap = w.amp * expi(o.phase);
+  o.T[0] = T.L1;
+  o.T[1] = T.L2;
+  o.T[2] = T.L3;
+#pragma unroll
+  for (int ch = 0; ch < 3; ++ch) o.W[ch] = o.T[ch] * ap;
+  return o;
+}
+
+// Sum of NGRAD partials over the block into out[0..NGRAD) (thread 0 writes).
+__device__ inline void block_reduce_grad(double* acc, double* out) {
+  __shared__ double red[NGRAD][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int k = 0; k < NGRAD; ++k) {
+    double v = acc[k];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) red[k][w] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < NGRAD) {
+    double s = 0.0;
+    for (int q = 0; q < nw; ++q) s += red[threadIdx.x][q];
+    out[threadIdx.x] = s;
+  }
+  __syncthreads();
+}
+
+// Heterodyne contraction: grad[b] = sum_{mode, j, channel} Re(gh[b, c, j] dW_c/dtheta) over
+// the sparse grid freqs[j] (lnL depends on h = sum_modes conj(W), and dL = Re(gh dW)).
+// One CTA per binary of [b0, b0 + nb); records indexed relative to b0.
+static __global__ void k_contract_het(double* grad, const ModeCoeffsT<GD>* coeffs,
+                               const ResponseModeT<GD>* rmodes, OrbitTables orb, const double* P,
+                               int B, int b0, int nb, const double* t_start, const double* t_end,
+                               double t_init, const double* freqs, const cplx* gh, int TDItag,
+                               int rescaled, int tdi2, int M, int L) {
+  for (int bl = blockIdx.x; bl < nb; bl += gridDim.x) {
+    const int b = b0 + bl;
+    const GD t_ref = seed(P[11 * (size_t)B + b], 10);
+    const double ts = t_start[b], te = t_end[b];
+    double acc[NGRAD];
+#pragma unroll
+    for (int k = 0; k < NGRAD; ++k) acc[k] = 0.0;
+    for (int p = threadIdx.x; p < M * L; p += blockDim.x) {
+      const int m = p / L, j = p % L;
+      const PointTangents o =
+          point_tangents(coeffs[(size_t)bl * M + m], rmodes[(size_t)bl * M + m], orb, freqs[j],
+                         t_ref, t_init, TDItag, rescaled, tdi2);
+      if (!tf_gate(o.tf, ts, te)) continue;
+#pragma unroll
+      for (int ch = 0; ch < 3; ++ch) {
+        const cplx u = gh[((size_t)b * 3 + ch) * L + j];
+#pragma unroll
+        for (int k = 0; k < NGRAD; ++k) acc[k] += u.re * o.W[ch].re.d[k] - u.im * o.W[ch].im.d[k];
+      }
+    }
+    block_reduce_grad(acc, grad + (size_t)b * NGRAD);
+  }
+}
+
+}  // namespace bbhx

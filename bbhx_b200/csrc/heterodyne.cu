@@ -26,6 +26,7 @@
 #include "phenomhm_model.cuh"
 #include "response_model.cuh"
 #include "spline_eval.cuh"
+#include "gradient_model.cuh"
 
 namespace bbhx {
 
@@ -173,8 +174,6 @@ __device__ __forceinline__ cplxf nHn_f(const cplxf* H, float n0, float n1, float
 
 __device__ __forceinline__ float sinc_f(float x) { return x == 0.0f ? 1.0f : sinf(x) / x; }
 __device__ __forceinline__ cplxf cf(float r, float i) { return cplxf{r, i}; }
-__device__ __forceinline__ cplxf operator-(cplxf a, cplxf b) { return {a.re - b.re, a.im - b.im}; }
-__device__ __forceinline__ cplxf operator*(float s, cplxf a) { return {s * a.re, s * a.im}; }
 __device__ __forceinline__ cplxf ti_f(cplxf a) { return {-a.im, a.re}; }
 __device__ __forceinline__ cplxf ephase(double x) {
   float s, c;
@@ -192,12 +191,12 @@ __device__ inline TransferF response_point_mixed(const RespModeF& r, const Orbit
   TransferF out;
   out.phaseRdelay = 2. * PI / C_SI * f * (k[0] * (AU_SI * ca) + k[1] * (AU_SI * sa));
 
-  V3 p1 = orbit_lerp(orb.x_arr, 9, 0, orb.dt, orb.N, t);
-  V3 p2 = orbit_lerp(orb.x_arr, 9, 3, orb.dt, orb.N, t);
-  V3 p3 = orbit_lerp(orb.x_arr, 9, 6, orb.dt, orb.N, t);
-  V3 n1 = orbit_lerp(orb.n_arr, 18, orb.link_index[0] * 3, orb.dt, orb.N, t);
-  V3 n2 = orbit_lerp(orb.n_arr, 18, orb.link_index[1] * 3, orb.dt, orb.N, t);
-  V3 n3 = orbit_lerp(orb.n_arr, 18, orb.link_index[2] * 3, orb.dt, orb.N, t);
+  V3T<double> p1 = orbit_lerp(orb.x_arr, 9, 0, orb.dt, orb.N, t);
+  V3T<double> p2 = orbit_lerp(orb.x_arr, 9, 3, orb.dt, orb.N, t);
+  V3T<double> p3 = orbit_lerp(orb.x_arr, 9, 6, orb.dt, orb.N, t);
+  V3T<double> n1 = orbit_lerp(orb.n_arr, 18, orb.link_index[0] * 3, orb.dt, orb.N, t);
+  V3T<double> n2 = orbit_lerp(orb.n_arr, 18, orb.link_index[1] * 3, orb.dt, orb.N, t);
+  V3T<double> n3 = orbit_lerp(orb.n_arr, 18, orb.link_index[2] * 3, orb.dt, orb.N, t);
   const float kn1 = (float)(k[0] * n1.x + k[1] * n1.y + k[2] * n1.z);
   const float kn2 = (float)(k[0] * n2.x + k[1] * n2.y + k[2] * n2.z);
   const float kn3 = (float)(k[0] * n3.x + k[1] * n3.y + k[2] * n3.z);
@@ -279,6 +278,7 @@ struct HetArgs {
   const cplx* consts;   // [4, 3, L]: A0, A1, B0, B1
   int TDItag, rescaled, tdi2;
   int M, L, B;
+  cplx* gh;  // optional [B, 3, L]: d lnL / d h (adjoint of the bin sums and of r = h / h0)
 };
 
 // Dynamic shared memory: ModeCoeffs[M] | ResponseMode[M] | AmpModeF[M] | RespModeF[M] |
@@ -408,6 +408,41 @@ __global__ void __launch_bounds__(HET_THREADS) k_het_fused(HetArgs A) {
         him += B0.im * mag2 + 2.0 * B1.im * re01;
       }
     }
+    if (A.gh) {
+      // Adjoint of lnL = Re d_h - (d_d + Re h_h) / 2 through the bin terms: per bin
+      // g_r0 = A0 - Re(B0) r0 - Re(B1) r1, g_r1 = A1 - Re(B1) r0, carried to r_j / r_{j-1}
+      // with the same coefficients as the forward r0, r1; then g_h = g_r / conj(h0).
+      for (int j = threadIdx.x; j < A.L; j += blockDim.x) {
+#pragma unroll
+        for (int ch = 0; ch < 3; ++ch) {
+          cplx g = mk(0.0, 0.0);
+          for (int side = 0; side < 2; ++side) {
+            const int jj = j + side;  // bin jj has cur = r_jj, prv = r_{jj-1}
+            if (jj < 1 || jj >= A.L) continue;
+            const double fj = A.freqs[jj], fp = A.freqs[jj - 1];
+            if (fp == 0.0) continue;
+            const double df = fj - fp;
+            const double fm = (fj + fp) / 2.0;
+            const double a = (fj - fm) / df;
+            const cplx cur = rr[ch * A.L + jj], prv = rr[ch * A.L + jj - 1];
+            const cplx r1 = mk((cur.re - prv.re) / df, (cur.im - prv.im) / df);
+            const cplx r0 = cur - r1 * (fj - fm);
+            const cplx A0 = A.consts[((size_t)0 * 3 + ch) * A.L + jj];
+            const cplx A1 = A.consts[((size_t)1 * 3 + ch) * A.L + jj];
+            const double B0 = A.consts[((size_t)2 * 3 + ch) * A.L + jj].re;
+            const double B1 = A.consts[((size_t)3 * 3 + ch) * A.L + jj].re;
+            const cplx g0 = A0 - B0 * r0 - B1 * r1;
+            const cplx g1 = A1 - B1 * r0;
+            if (side == 0) g = g + (1.0 - a) * g0 + (1.0 / df) * g1;  // r_j is cur of bin j
+            else g = g + a * g0 - (1.0 / df) * g1;                    // r_j is prv of bin j+1
+          }
+          const cplx d = A.h0[(size_t)ch * A.L + j];
+          const double den = d.re * d.re + d.im * d.im;  // g / conj(d) = g d / |d|^2
+          A.gh[((size_t)b * 3 + ch) * A.L + j] =
+              mk((g.re * d.re - g.im * d.im) / den, (g.re * d.im + g.im * d.re) / den);
+        }
+      }
+    }
     for (int o = 16; o > 0; o >>= 1) {
       dre += __shfl_xor_sync(0xffffffffu, dre, o);
       dim += __shfl_xor_sync(0xffffffffu, dim, o);
@@ -455,6 +490,7 @@ using namespace bbhx;
 
 namespace {
 constexpr int kHetMaxL = 2048;
+constexpr int kGradChunk = 4096;  // walkers per dual-number setup / contraction batch
 }
 
 extern "C" {
@@ -498,6 +534,7 @@ int bbhx_hdyn_fused(void* orbits, void* d_h, void* h_h, const void* coeffs, cons
     A.TDItag = TDItag;
     A.rescaled = rescaled;
     A.tdi2 = tdi2;
+    A.gh = nullptr;
     A.M = num_modes;
     A.L = length;
     A.B = num_bin_all;
@@ -518,6 +555,100 @@ int bbhx_hdyn_fused(void* orbits, void* d_h, void* h_h, const void* coeffs, cons
     st = launch_status("k_het_fused");
   }
   cudaFreeAsync(rm, s);
+  return st;
+}
+
+// Heterodyned lnL and its gradient d lnL / d theta for the 11 parameters (order in
+// gradient_model.cuh) of B walkers: FP64 forward pass that also emits d lnL / d h at the
+// sparse grid (reverse part), then dual-number tangents of the waveform + response at every
+// (mode, frequency), contracted with those weights (forward part).  params: [12, B] device.
+int bbhx_hdyn_grad(void* orbits, void* d_h, void* h_h, double* grad, const void* coeffs,
+                   const double* params, const int* ells, const int* mms, const double* qnm_table,
+                   int qnm_n, double dspin, double t_init, const double* t_start,
+                   const double* t_end, const double* freqs, const void* h0, const void* consts,
+                   int TDItag, int rescaled, int tdi2, int run_phenomd, int num_modes, int length,
+                   int num_bin_all, void* stream) {
+  BBHX_REQUIRE(orbits && ((OrbitHandle*)orbits)->ready, "orbit information not added");
+  BBHX_REQUIRE(TDItag == 1 || TDItag == 2, "TDItag must be 1 (XYZ) or 2 (AET)");
+  BBHX_REQUIRE(num_modes > 0 && num_modes <= MAX_MODES, "num_modes must be 1..6");
+  BBHX_REQUIRE(length >= 2 && length <= kHetMaxL, "heterodyne length must be 2..%d", kHetMaxL);
+  BBHX_REQUIRE(qnm_n >= 2 && dspin > 0.0, "bad QNM table");
+  if (num_bin_all == 0) return OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  const long long nbm = (long long)num_bin_all * num_modes;
+  ResponseMode* rm = nullptr;
+  cplx* gh = nullptr;
+  ModeCoeffsT<GD>* cD = nullptr;
+  ResponseModeT<GD>* rD = nullptr;
+  const int chunk = std::min(num_bin_all, kGradChunk);
+  int st = OK;
+  if (pool_alloc((void**)&rm, sizeof(ResponseMode) * nbm, s) != cudaSuccess ||
+      pool_alloc((void**)&gh, sizeof(cplx) * 3 * (size_t)length * num_bin_all, s) != cudaSuccess ||
+      pool_alloc((void**)&cD, sizeof(ModeCoeffsT<GD>) * (size_t)chunk * num_modes, s) != cudaSuccess ||
+      pool_alloc((void**)&rD, sizeof(ResponseModeT<GD>) * (size_t)chunk * num_modes, s) != cudaSuccess) {
+    set_error("device allocation of the gradient scratch failed");
+    st = ERR_CUDA;
+  }
+  if (!st) {
+    k_response_setup_het<<<grid_for(nbm, 128), 128, 0, s>>>(rm, ells, mms, params + 5 * (size_t)num_bin_all,
+                                                            params + 7 * (size_t)num_bin_all,
+                                                            params + 8 * (size_t)num_bin_all,
+                                                            params + 9 * (size_t)num_bin_all,
+                                                            params + 10 * (size_t)num_bin_all,
+                                                            num_modes, num_bin_all);
+    st = launch_status("k_response_setup_het");
+  }
+  if (!st) {
+    HetArgs A;
+    A.d_h = (cplx*)d_h;
+    A.h_h = (cplx*)h_h;
+    A.coeffs = (const ModeCoeffs*)coeffs;
+    A.rmodes = rm;
+    A.orb = ((OrbitHandle*)orbits)->tab;
+    A.t_ref = params + 11 * (size_t)num_bin_all;
+    A.t_init = t_init;
+    A.t_start = t_start;
+    A.t_end = t_end;
+    A.freqs = freqs;
+    A.h0 = (const cplx*)h0;
+    A.consts = (const cplx*)consts;
+    A.TDItag = TDItag;
+    A.rescaled = rescaled;
+    A.tdi2 = tdi2;
+    A.gh = gh;
+    A.M = num_modes;
+    A.L = length;
+    A.B = num_bin_all;
+    const size_t smem = HetSmemLayout(num_modes, length).total;
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const unsigned grid = (unsigned)std::min<long long>(num_bin_all, (long long)nsm * 16);
+    if (cudaFuncSetAttribute(k_het_fused<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess) {
+      set_error("cudaFuncSetAttribute failed for k_het_fused");
+      st = ERR_CUDA;
+    } else {
+      k_het_fused<false><<<grid, HET_THREADS, smem, s>>>(A);
+      st = launch_status("k_het_fused (gradient forward)");
+    }
+    for (int b0 = 0; !st && b0 < num_bin_all; b0 += chunk) {
+      const int nb = std::min(chunk, num_bin_all - b0);
+      const long long n = (long long)nb * num_modes;
+      k_grad_setup<<<grid_for(n, 64), 64, 0, s>>>(cD, rD, params, num_bin_all, b0, nb, ells, mms,
+                                                  num_modes, qnm_table, qnm_n, dspin, run_phenomd);
+      st = launch_status("k_grad_setup");
+      if (st) break;
+      k_contract_het<<<(unsigned)std::min(nb, nsm * 8), 128, 0, s>>>(
+          grad, cD, rD, A.orb, params, num_bin_all, b0, nb, t_start, t_end, t_init, freqs, gh,
+          TDItag, rescaled, tdi2, num_modes, length);
+      st = launch_status("k_contract_het");
+    }
+  }
+  if (rD) cudaFreeAsync(rD, s);
+  if (cD) cudaFreeAsync(cD, s);
+  if (gh) cudaFreeAsync(gh, s);
+  if (rm) cudaFreeAsync(rm, s);
   return st;
 }
 

@@ -21,6 +21,7 @@
 #pragma once
 
 #include "bbhx_common.cuh"
+#include "dual.cuh"
 
 namespace bbhx {
 
@@ -37,12 +38,13 @@ struct Fit11 {
   double c00, c01, c10, c11, c12, c20, c21, c22, c30, c31, c32;
 };
 
-__device__ __forceinline__ double eval_fit(const Fit11& c, double eta, double chi) {
-  double xi = chi - 1.0;
-  double e2 = eta * eta;
-  double t1 = c.c10 + c.c11 * eta + c.c12 * e2;
-  double t2 = c.c20 + c.c21 * eta + c.c22 * e2;
-  double t3 = c.c30 + c.c31 * eta + c.c32 * e2;
+template <typename T>
+__device__ __forceinline__ T eval_fit(const Fit11& c, const T& eta, const T& chi) {
+  T xi = chi - 1.0;
+  T e2 = eta * eta;
+  T t1 = c.c10 + c.c11 * eta + c.c12 * e2;
+  T t2 = c.c20 + c.c21 * eta + c.c22 * e2;
+  T t3 = c.c30 + c.c31 * eta + c.c32 * e2;
   return c.c00 + c.c01 * eta + xi * (t1 + xi * (t2 + xi * t3));
 }
 
@@ -142,50 +144,52 @@ __constant__ QnmFit kQnm[6] = {
      {0.595328, 3.016200, 6.038842, 2.826239, 5.915164}}};
 
 // Complex dimensionless QNM frequency M*omega for mode (l, m, n=0); zero if unsupported.
-__device__ inline cplx qnm_cw(double jf, int ell, int mm) {
+template <typename T>
+__device__ inline cplxT<T> qnm_cw(T jf, int ell, int mm) {
   int idx = -1;
   for (int k = 0; k < 6; ++k)
     if (kQnm[k].ell == ell && kQnm[k].mm == mm) idx = k;
-  if (idx < 0) return mk(0.0, 0.0);
+  if (idx < 0) return cmk(T(0.0), T(0.0));
   const QnmFit& q = kQnm[idx];
-  double kappa = pow(log(2.0 - jf) / log(3.0), 1.0 / (2.0 + ell - abs(mm)));
-  cplx sum = mk(0.0, 0.0);
-  double kp = 1.0;
+  T kappa = pow(log(2.0 - jf) / log(3.0), 1.0 / (2.0 + ell - abs(mm)));
+  cplxT<T> sum = cmk(T(0.0), T(0.0));
+  T kp = 1.0;
   for (int k = 0; k < q.nterms; ++k) {
     double s, c;
     sincos(q.ph[k], &s, &c);
-    sum = sum + mk(q.A[k] * c * kp, q.A[k] * s * kp);
+    sum = sum + cmk(T(q.A[k] * c * kp), T(q.A[k] * s * kp));
     kp *= kappa;
   }
   if (q.shift) sum = kappa * sum;
-  return mk(q.base + sum.re, sum.im);
+  return cmk(T(q.base + sum.re), sum.im);
 }
 
 // Final spin (1508.07250 eq. 3.6) and radiated energy (eqs. 3.7-3.8); masses in any units
 // with m1 >= m2 enforced inside (PhenomHMWaveform.cu:1679-1814).
-__device__ inline void final_mass_spin(double m1, double m2, double chi1, double chi2,
-                                       double* finmass, double* finspin) {
+template <typename T>
+__device__ inline void final_mass_spin(T m1, T m2, T chi1, T chi2,
+                                       T* finmass, T* finspin) {
   if (!(m1 > m2)) {  // the reference swaps unless m1 > m2 strictly
-    double t = m1; m1 = m2; m2 = t;
+    T t = m1; m1 = m2; m2 = t;
     t = chi1; chi1 = chi2; chi2 = t;
   }
-  double M = m1 + m2;
-  double eta = m1 * m2 / (M * M);
-  double Seta = sqrt(1.0 - 4.0 * eta);
-  double q1 = 0.5 * (1.0 + Seta), q2 = 0.5 * (1.0 - Seta);
-  double q1s = q1 * q1, q2s = q2 * q2;
-  double e2 = eta * eta, e3 = e2 * eta, e4 = e3 * eta;
+  T M = m1 + m2;
+  T eta = m1 * m2 / (M * M);
+  T Seta = sqrt(1.0 - 4.0 * eta);
+  T q1 = 0.5 * (1.0 + Seta), q2 = 0.5 * (1.0 - Seta);
+  T q1s = q1 * q1, q2s = q2 * q2;
+  T e2 = eta * eta, e3 = e2 * eta, e4 = e3 * eta;
   // final spin
-  double s = q1s * chi1 + q2s * chi2;
-  double s2 = s * s, s3 = s2 * s, s4 = s3 * s;
+  T s = q1s * chi1 + q2s * chi2;
+  T s2 = s * s, s3 = s2 * s, s4 = s3 * s;
   *finspin = 3.4641016151377544 * eta - 4.399247300629289 * e2 + 9.397292189321194 * e3 -
              13.180949901606242 * e4 + (1 - 0.0850917821418767 * eta - 5.837029316602263 * e2) * s +
              (0.1014665242971878 * eta - 2.0967746996832157 * e2) * s2 +
              (-1.3546806617824356 * eta + 4.108962025369336 * e2) * s3 +
              (-0.8676969352555539 * eta + 2.064046835273906 * e2) * s4;
   // radiated energy
-  double sr = (q1s * chi1 + q2s * chi2) / (q1s + q2s);
-  double erad = ((0.055974469826360077 * eta + 0.5809510763115132 * e2 - 0.9606726679372312 * e3 +
+  T sr = (q1s * chi1 + q2s * chi2) / (q1s + q2s);
+  T erad = ((0.055974469826360077 * eta + 0.5809510763115132 * e2 - 0.9606726679372312 * e3 +
                   3.352411249771192 * e4) *
                  (1. + (-0.0030302335878845507 - 2.0066110851351073 * eta + 7.7050567802399215 * e2) * sr)) /
                 (1. + (-0.6714403054720589 - 1.4756929437702908 * eta + 7.304676214885011 * e2) * sr);
@@ -195,31 +199,36 @@ __device__ inline void final_mass_spin(double m1, double m2, double chi1, double
 // ---------------------------------------------------------------------------------
 // PhenomD coefficients for one (binary, fRD, fDM, Rholm, Taulm)
 // ---------------------------------------------------------------------------------
-struct PhenomD {
-  double eta, etaInv, chi;
-  double fRD, fDM;
+template <typename T>
+struct PhenomDT {
+  T eta, etaInv, chi;
+  T fRD, fDM;
   // amplitude
-  double amp0;        // sqrt(2/3) sqrt(eta) / pi^(1/6)
-  double ains[8];     // Mf^{2/3,1,4/3,5/3,2,7/3,8/3,3} coefficients of the inspiral ansatz
-  double g1, g2, g3;  // gamma_1..3
-  double fpeak;       // fmaxCalc (1508.07253 eq. 20)
-  double hf1, hf2, hf3, hc0, hc1, hc2, hc3, hc4;  // Hermite nodes and Newton coefficients
+  T amp0;        // sqrt(2/3) sqrt(eta) / pi^(1/6)
+  T ains[8];     // Mf^{2/3,1,4/3,5/3,2,7/3,8/3,3} coefficients of the inspiral ansatz
+  T g1, g2, g3;  // gamma_1..3
+  T fpeak;       // fmaxCalc (1508.07253 eq. 20)
+  T hf1, hf2, hf3, hc0, hc1, hc2, hc3, hc4;  // Hermite nodes and Newton coefficients
   // phase
-  double pn_v[8], pn_vlogv5, pn_vlogv6;
-  double sig1, sig2, sig3, sig4, bet1, bet2, bet3, alp1, alp2, alp3, alp4, alp5;
-  double pins_init, pins_23, pins_13, pins_13log, pins_log, pins_m13, pins_m23, pins_m1,
+  T pn_v[8], pn_vlogv5, pn_vlogv6;
+  T sig1, sig2, sig3, sig4, bet1, bet2, bet3, alp1, alp2, alp3, alp4, alp5;
+  T pins_init, pins_23, pins_13, pins_13log, pins_log, pins_m13, pins_m23, pins_m1,
       pins_m53, pins_1, pins_43, pins_53, pins_2;
-  double C1Int, C2Int, C1MRD, C2MRD, fMRDJoin;
-  double Rholm, Taulm;
-  double inv_atan_scale;  // 1 / (Rholm fDM Taulm)
+  T C1Int, C2Int, C1MRD, C2MRD, fMRDJoin;
+  T Rholm, Taulm;
+  T inv_atan_scale;  // 1 / (Rholm fDM Taulm)
 };
+using PhenomD = PhenomDT<double>;
 
-struct Powers {  // PhenomHMWaveform.cu:348-362 (same derivation of the fractional powers)
-  double sixth, third, two_thirds, four_thirds, five_thirds, two, seven_thirds, eight_thirds;
+template <typename T>
+struct PowersT {  // PhenomHMWaveform.cu:348-362 (same derivation of the fractional powers)
+  T sixth, third, two_thirds, four_thirds, five_thirds, two, seven_thirds, eight_thirds;
 };
+using Powers = PowersT<double>;
 
-__device__ __forceinline__ Powers make_powers(double x) {
-  Powers p;
+template <typename T>
+__device__ __forceinline__ PowersT<T> make_powers(T x) {
+  PowersT<T> p;
   p.third = cbrt(x);
   p.sixth = sqrt(p.third);
   p.two_thirds = x / p.third;
@@ -231,54 +240,61 @@ __device__ __forceinline__ Powers make_powers(double x) {
   return p;
 }
 
-__device__ __forceinline__ double amp_ins_ansatz(const PhenomD& d, double Mf, const Powers& p) {
+template <typename T>
+__device__ __forceinline__ T amp_ins_ansatz(const PhenomDT<T>& d, T Mf, const PowersT<T>& p) {
   return 1.0 + p.two_thirds * d.ains[0] + Mf * d.ains[1] + p.four_thirds * d.ains[2] +
          p.five_thirds * d.ains[3] + p.two * d.ains[4] + p.seven_thirds * d.ains[5] +
          p.eight_thirds * d.ains[6] + Mf * p.two * d.ains[7];
 }
 
 // derivative of amp_ins_ansatz: sum_k (k/3) c_k Mf^{k/3-1}
-__device__ __forceinline__ double amp_ins_ansatz_deriv(const PhenomD& d, double Mf) {
-  double t = cbrt(Mf);
-  double t2 = t * t;
+template <typename T>
+__device__ __forceinline__ T amp_ins_ansatz_deriv(const PhenomDT<T>& d, T Mf) {
+  T t = cbrt(Mf);
+  T t2 = t * t;
   return (2.0 / 3.0) * d.ains[0] / t + d.ains[1] + (4.0 / 3.0) * d.ains[2] * t +
          (5.0 / 3.0) * d.ains[3] * t2 + 2.0 * d.ains[4] * Mf + (7.0 / 3.0) * d.ains[5] * Mf * t +
          (8.0 / 3.0) * d.ains[6] * Mf * t2 + 3.0 * d.ains[7] * Mf * Mf;
 }
 
-__device__ __forceinline__ double amp_mrd_ansatz(const PhenomD& d, double f) {
-  double s = d.fDM * d.g3;
-  double x = f - d.fRD;
+template <typename T>
+__device__ __forceinline__ T amp_mrd_ansatz(const PhenomDT<T>& d, T f) {
+  T s = d.fDM * d.g3;
+  T x = f - d.fRD;
   return exp(-x * d.g2 / s) * (s * d.g1) / (x * x + s * s);
 }
 
-__device__ __forceinline__ double amp_mrd_ansatz_deriv(const PhenomD& d, double f) {
-  double s = d.fDM * d.g3;
-  double x = f - d.fRD;
-  double den = x * x + s * s;
+template <typename T>
+__device__ __forceinline__ T amp_mrd_ansatz_deriv(const PhenomDT<T>& d, T f) {
+  T s = d.fDM * d.g3;
+  T x = f - d.fRD;
+  T den = x * x + s * s;
   return amp_mrd_ansatz(d, f) * (-d.g2 / s - 2.0 * x / den);
 }
 
-__device__ __forceinline__ double amp_int_ansatz(const PhenomD& d, double f) {
-  double u = f - d.hf1;
+template <typename T>
+__device__ __forceinline__ T amp_int_ansatz(const PhenomDT<T>& d, T f) {
+  T u = f - d.hf1;
   return d.hc0 + u * (d.hc1 + u * (d.hc2 + (f - d.hf2) * (d.hc3 + (f - d.hf3) * d.hc4)));
 }
 
 // Full PhenomD amplitude (without the distance/mass scale), PhenomHMWaveform.cu:1508-1537
-__device__ __forceinline__ double phenomd_amp(const PhenomD& d, double Mf) {
-  Powers p = make_powers(Mf);
-  double pre = d.amp0 / (Mf * p.sixth);
+template <typename T>
+__device__ __forceinline__ T phenomd_amp(const PhenomDT<T>& d, T Mf) {
+  PowersT<T> p = make_powers(Mf);
+  T pre = d.amp0 / (Mf * p.sixth);
   if (Mf < AMP_FJOIN_INS) return pre * amp_ins_ansatz(d, Mf, p);
   if (Mf >= d.fpeak) return pre * amp_mrd_ansatz(d, Mf);
   return pre * amp_int_ansatz(d, Mf);
 }
 
 // inspiral phase, PhenomHMWaveform.cu:1077-1117
-__device__ __forceinline__ double phi_ins(const PhenomD& d, double Mf, const Powers& p) {
+template <typename T>
+__device__ __forceinline__ T phi_ins(const PhenomDT<T>& d, T Mf, const PowersT<T>& p) {
   const double PI_THIRD = 1.4645918875615231;  // pi^(1/3)
-  double v = p.third * PI_THIRD;
-  double logv = log(v);
-  double ph = d.pins_init;
+  T v = p.third * PI_THIRD;
+  T logv = log(v);
+  T ph = d.pins_init;
   ph += d.pins_23 * p.two_thirds;
   ph += d.pins_13 * p.third;
   ph += d.pins_13log * logv * p.third;
@@ -293,13 +309,14 @@ __device__ __forceinline__ double phi_ins(const PhenomD& d, double Mf, const Pow
 }
 
 // d(phi_ins)/dMf, PhenomHMWaveform.cu:1214-1250
-__device__ __forceinline__ double dphi_ins(const PhenomD& d, double Mf) {
+template <typename T>
+__device__ __forceinline__ T dphi_ins(const PhenomDT<T>& d, T Mf) {
   const double PI_THIRD = 1.4645918875615231;
   const double PI_TWOTHIRDS = 2.1450293971110255;
-  double v = cbrt(PI * Mf);
-  double logv = log(v);
-  double v2 = v * v, v3 = v2 * v, v4 = v3 * v, v5 = v4 * v, v6 = v5 * v, v7 = v6 * v, v8 = v7 * v;
-  double s = 2.0 * d.pn_v[7] * v7;
+  T v = cbrt(PI * Mf);
+  T logv = log(v);
+  T v2 = v * v, v3 = v2 * v, v4 = v3 * v, v5 = v4 * v, v6 = v5 * v, v7 = v6 * v, v8 = v7 * v;
+  T s = 2.0 * d.pn_v[7] * v7;
   s += (d.pn_v[6] + d.pn_vlogv6 * (1.0 + logv)) * v6;
   s += d.pn_vlogv5 * v5;
   s -= d.pn_v[4] * v4;
@@ -312,37 +329,43 @@ __device__ __forceinline__ double dphi_ins(const PhenomD& d, double Mf) {
   return s;
 }
 
-__device__ __forceinline__ double phi_int(const PhenomD& d, double Mf) {
+template <typename T>
+__device__ __forceinline__ T phi_int(const PhenomDT<T>& d, T Mf) {
   return d.bet1 * Mf - d.bet3 / (3.0 * Mf * Mf * Mf) + d.bet2 * log(Mf);
 }
-__device__ __forceinline__ double dphi_int(const PhenomD& d, double Mf) {
-  double Mf2 = Mf * Mf;
+template <typename T>
+__device__ __forceinline__ T dphi_int(const PhenomDT<T>& d, T Mf) {
+  T Mf2 = Mf * Mf;
   return (d.bet1 + d.bet3 / (Mf2 * Mf2) + d.bet2 / Mf) / d.eta;
 }
-__device__ __forceinline__ double phi_mrd(const PhenomD& d, double f, double Rho, double Tau) {
-  double sq = sqrt(f);
-  double f075 = sqrt(f * sq);
+template <typename T>
+__device__ __forceinline__ T phi_mrd(const PhenomDT<T>& d, T f, T Rho, T Tau) {
+  T sq = sqrt(f);
+  T f075 = sqrt(f * sq);
   return -(d.alp2 / f) + (4.0 / 3.0) * (d.alp3 * f075) + d.alp1 * f +
          d.alp4 * Rho * atan((f - d.alp5 * d.fRD) / (Rho * d.fDM * Tau));
 }
-__device__ __forceinline__ double dphi_mrd(const PhenomD& d, double f, double Rho, double Tau) {
-  double x = f - d.alp5 * d.fRD;
-  double w = d.fDM * Tau * Rho;
+template <typename T>
+__device__ __forceinline__ T dphi_mrd(const PhenomDT<T>& d, T f, T Rho, T Tau) {
+  T x = f - d.alp5 * d.fRD;
+  T w = d.fDM * Tau * Rho;
   return (d.alp1 + d.alp2 / (f * f) + d.alp3 / pow(f, 0.25) +
           d.alp4 / (d.fDM * Tau * (1.0 + x * x / (w * w)))) *
          d.etaInv;
 }
 
 // Full PhenomD phase with the mode's connection constants (PhenomHMWaveform.cu:1360-1381)
-__device__ __forceinline__ double phenomd_phase(const PhenomD& d, double Mf) {
+template <typename T>
+__device__ __forceinline__ T phenomd_phase(const PhenomDT<T>& d, T Mf) {
   if (Mf < PHI_FJOIN_INS) {
-    Powers p = make_powers(Mf);
+    PowersT<T> p = make_powers(Mf);
     return phi_ins(d, Mf, p);
   }
   if (Mf >= d.fMRDJoin) return d.etaInv * phi_mrd(d, Mf, d.Rholm, d.Taulm) + d.C1MRD + d.C2MRD * Mf;
   return d.etaInv * phi_int(d, Mf) + d.C1Int + d.C2Int * Mf;
 }
-__device__ __forceinline__ double phenomd_dphase(const PhenomD& d, double Mf) {
+template <typename T>
+__device__ __forceinline__ T phenomd_dphase(const PhenomDT<T>& d, T Mf) {
   if (Mf < PHI_FJOIN_INS) return dphi_ins(d, Mf);
   if (Mf >= d.fMRDJoin) return dphi_mrd(d, Mf, d.Rholm, d.Taulm) + d.C2MRD;
   return dphi_int(d, Mf) + d.C2Int;
@@ -350,16 +373,17 @@ __device__ __forceinline__ double phenomd_dphase(const PhenomD& d, double Mf) {
 
 // Phase and d(phase)/dMf at one frequency together (the two branches of phenomd_phase and
 // phenomd_dphase), sharing the fractional powers, the logarithm and the reciprocals.
-__device__ __forceinline__ void phenomd_phase_dphase(const PhenomD& d, double Mf, double* ph,
-                                                     double* dph) {
+template <typename T>
+__device__ __forceinline__ void phenomd_phase_dphase(const PhenomDT<T>& d, T Mf, T* ph,
+                                                     T* dph) {
   const double PI_THIRD = 1.4645918875615231;  // pi^(1/3)
   if (Mf < PHI_FJOIN_INS) {
-    const double t = cbrt(Mf);  // Mf^(1/3)
-    const double it = 1.0 / t;
-    const double t2 = t * t, it2 = it * it;
-    const double v = t * PI_THIRD;
-    const double logv = log(v);
-    double p = d.pins_init;
+    const T t = cbrt(Mf);  // Mf^(1/3)
+    const T it = 1.0 / t;
+    const T t2 = t * t, it2 = it * it;
+    const T v = t * PI_THIRD;
+    const T logv = log(v);
+    T p = d.pins_init;
     p += d.pins_23 * t2;
     p += d.pins_13 * t;
     p += d.pins_13log * logv * t;
@@ -371,8 +395,8 @@ __device__ __forceinline__ void phenomd_phase_dphase(const PhenomD& d, double Mf
     p += (d.pins_1 * Mf + d.pins_43 * (Mf * t) + d.pins_53 * (Mf * t2) + d.pins_2 * (Mf * Mf)) *
          d.etaInv;
     *ph = p;
-    const double v2 = v * v, v3 = v2 * v, v4 = v3 * v, v5 = v4 * v, v6 = v5 * v, v7 = v6 * v;
-    double s = 2.0 * d.pn_v[7] * v7;
+    const T v2 = v * v, v3 = v2 * v, v4 = v3 * v, v5 = v4 * v, v6 = v5 * v, v7 = v6 * v;
+    T s = 2.0 * d.pn_v[7] * v7;
     s += (d.pn_v[6] + d.pn_vlogv6 * (1.0 + logv)) * v6;
     s += d.pn_vlogv5 * v5;
     s -= d.pn_v[4] * v4;
@@ -380,20 +404,20 @@ __device__ __forceinline__ void phenomd_phase_dphase(const PhenomD& d, double Mf
     s -= 3.0 * d.pn_v[2] * v2;
     s -= 4.0 * d.pn_v[1] * v;
     s -= 5.0 * d.pn_v[0];
-    const double iv = it * (1.0 / PI_THIRD);
-    const double iv2 = iv * iv, iv4 = iv2 * iv2;
+    const T iv = it * (1.0 / PI_THIRD);
+    const T iv2 = iv * iv, iv4 = iv2 * iv2;
     s *= (PI / 3.0) * (iv4 * iv4);
     s += (d.sig1 + d.sig2 * t + d.sig3 * t2 + d.sig4 * Mf) * d.etaInv;
     *dph = s;
     return;
   }
   if (Mf >= d.fMRDJoin) {
-    const double sq = sqrt(Mf);
-    const double q = sqrt(sq);  // Mf^(1/4)
-    const double f075 = sq * q;
-    const double iF = 1.0 / Mf;
-    const double x = Mf - d.alp5 * d.fRD;
-    const double y = x * d.inv_atan_scale;
+    const T sq = sqrt(Mf);
+    const T q = sqrt(sq);  // Mf^(1/4)
+    const T f075 = sq * q;
+    const T iF = 1.0 / Mf;
+    const T x = Mf - d.alp5 * d.fRD;
+    const T y = x * d.inv_atan_scale;
     *ph = d.etaInv * (-(d.alp2 * iF) + (4.0 / 3.0) * (d.alp3 * f075) + d.alp1 * Mf +
                       d.alp4 * d.Rholm * atan(y)) +
           d.C1MRD + d.C2MRD * Mf;
@@ -403,8 +427,8 @@ __device__ __forceinline__ void phenomd_phase_dphase(const PhenomD& d, double Mf
            d.C2MRD;
     return;
   }
-  const double iF = 1.0 / Mf;
-  const double iF2 = iF * iF;
+  const T iF = 1.0 / Mf;
+  const T iF2 = iF * iF;
   *ph = d.etaInv * (d.bet1 * Mf - d.bet3 * (1.0 / 3.0) * (iF2 * iF) + d.bet2 * log(Mf)) + d.C1Int +
         d.C2Int * Mf;
   *dph = (d.bet1 + d.bet3 * (iF2 * iF2) + d.bet2 * iF) * d.etaInv + d.C2Int;
@@ -412,16 +436,17 @@ __device__ __forceinline__ void phenomd_phase_dphase(const PhenomD& d, double Mf
 
 // Build the PhenomD coefficient set.  m1, m2 in solar masses with m1 >= m2 already
 // enforced; fring/fdamp dimensionless; Rholm/Taulm mode ratios (1, 1 for PhenomD).
-__device__ inline void phenomd_setup(PhenomD& d, double m1, double m2, double chi1, double chi2,
-                                     double fring, double fdamp, double Rholm, double Taulm) {
-  const double M = m1 + m2;
-  const double eta = m1 * m2 / (M * M);
+template <typename T>
+__device__ inline void phenomd_setup(PhenomDT<T>& d, T m1, T m2, T chi1, T chi2,
+                                     T fring, T fdamp, T Rholm, T Taulm) {
+  const T M = m1 + m2;
+  const T eta = m1 * m2 / (M * M);
   d.eta = eta;
   d.etaInv = 1.0 / eta;
-  const double Seta = sqrt(1.0 - 4.0 * eta);
+  const T Seta = sqrt(1.0 - 4.0 * eta);
   // reduced spin chi_PN (1107.1267 eq. 5.9)
   d.chi = 0.5 * (chi1 + chi2) * (1.0 - eta * 76.0 / 113.0) + Seta * 0.5 * (chi1 - chi2);
-  const double chi = d.chi;
+  const T chi = d.chi;
   d.fRD = fring;
   d.fDM = fdamp;
   d.Rholm = Rholm;
@@ -431,12 +456,12 @@ __device__ inline void phenomd_setup(PhenomD& d, double m1, double m2, double ch
   // ---------------- amplitude ----------------
   const double pi16 = pow(PI, 1.0 / 6.0);
   d.amp0 = sqrt(2.0 / 3.0) * sqrt(eta) / pi16;
-  Powers pp = make_powers(PI);
+  const PowersT<double> pp = make_powers(PI);
   const double Pi = PI, Pi2 = pp.two;
-  const double c12 = chi1 * chi1, c22 = chi2 * chi2, e2 = eta * eta, e3 = e2 * eta;
-  double rho1 = eval_fit(kFitRho[0], eta, chi);
-  double rho2 = eval_fit(kFitRho[1], eta, chi);
-  double rho3 = eval_fit(kFitRho[2], eta, chi);
+  const T c12 = chi1 * chi1, c22 = chi2 * chi2, e2 = eta * eta, e3 = e2 * eta;
+  T rho1 = eval_fit(kFitRho[0], eta, chi);
+  T rho2 = eval_fit(kFitRho[1], eta, chi);
+  T rho3 = eval_fit(kFitRho[2], eta, chi);
   // TaylorF2-amplitude re-expansion coefficients (1508.07253 eqs. 29-30, appendix B)
   d.ains[0] = ((-969 + 1804 * eta) * pp.two_thirds) / 672.;
   d.ains[1] = ((chi1 * (81 * (1 + Seta) - 44 * eta) + chi2 * (81 - 81 * Seta - 44 * eta)) * Pi) / 48.;
@@ -474,25 +499,25 @@ __device__ inline void phenomd_setup(PhenomD& d, double m1, double m2, double ch
     d.fpeak = fabs(fring + (fdamp * (-1) * d.g3) / d.g2);
   // intermediate amplitude: Hermite data at f1 (value+slope), f2 (value), f3 (value+slope)
   {
-    const double f1 = AMP_FJOIN_INS, f3 = d.fpeak;
-    const double f2 = f1 + (f3 - f1) / 2.0;
-    Powers p1 = make_powers(f1);
-    const double v1 = amp_ins_ansatz(d, f1, p1);
-    const double d1 = amp_ins_ansatz_deriv(d, f1);
-    const double v3 = amp_mrd_ansatz(d, f3);
-    const double d2 = amp_mrd_ansatz_deriv(d, f3);
-    const double v2 = eval_fit(kFitV2, eta, chi);
+    const T f1 = AMP_FJOIN_INS, f3 = d.fpeak;
+    const T f2 = f1 + (f3 - f1) / 2.0;
+    PowersT<T> p1 = make_powers(f1);
+    const T v1 = amp_ins_ansatz(d, f1, p1);
+    const T d1 = amp_ins_ansatz_deriv(d, f1);
+    const T v3 = amp_mrd_ansatz(d, f3);
+    const T d2 = amp_mrd_ansatz_deriv(d, f3);
+    const T v2 = eval_fit(kFitV2, eta, chi);
     // divided differences on nodes (f1, f1, f2, f3, f3)
-    const double z01 = d1;
-    const double z12 = (v2 - v1) / (f2 - f1);
-    const double z23 = (v3 - v2) / (f3 - f2);
-    const double z34 = d2;
-    const double z012 = (z12 - z01) / (f2 - f1);
-    const double z123 = (z23 - z12) / (f3 - f1);
-    const double z234 = (z34 - z23) / (f3 - f2);
-    const double z0123 = (z123 - z012) / (f3 - f1);
-    const double z1234 = (z234 - z123) / (f3 - f1);
-    const double z01234 = (z1234 - z0123) / (f3 - f1);
+    const T z01 = d1;
+    const T z12 = (v2 - v1) / (f2 - f1);
+    const T z23 = (v3 - v2) / (f3 - f2);
+    const T z34 = d2;
+    const T z012 = (z12 - z01) / (f2 - f1);
+    const T z123 = (z23 - z12) / (f3 - f1);
+    const T z234 = (z34 - z23) / (f3 - f2);
+    const T z0123 = (z123 - z012) / (f3 - f1);
+    const T z1234 = (z234 - z123) / (f3 - f1);
+    const T z01234 = (z1234 - z0123) / (f3 - f1);
     d.hf1 = f1;
     d.hf2 = f2;
     d.hf3 = f3;
@@ -519,38 +544,38 @@ __device__ inline void phenomd_setup(PhenomD& d, double m1, double m2, double ch
 
   // TaylorF2 aligned-spin phasing (LAL PNPhasing_F2, PhenomHMWaveform.cu:253-335)
   {
-    const double m1M = m1 / M, m2M = m2 / M;
-    const double dm = (m1 - m2) / M;
-    const double SL = m1M * m1M * chi1 + m2M * m2M * chi2;
-    const double dSigmaL = dm * (m2M * chi2 - m1M * chi1);
-    const double pfaN = 3.0 / (128.0 * eta);
-    double v0 = pfaN;
-    double v1 = 0.0;
-    double v2 = pfaN * (5.0 * (743.0 / 84.0 + 11.0 * eta) / 9.0);
-    double v3 = pfaN * (-16.0 * PI);
-    double v4 = pfaN * (5.0 * (3058.673 / 7.056 + 5429.0 / 7.0 * eta + 617.0 * eta * eta) / 72.0);
-    double v5 = pfaN * (5.0 / 9.0 * (7729.0 / 84.0 - 13.0 * eta) * PI);
-    double vlogv5 = pfaN * (5.0 / 3.0 * (7729.0 / 84.0 - 13.0 * eta) * PI);
-    double v6 = pfaN * ((11583.231236531 / 4.694215680 - 640.0 / 3.0 * PI * PI - 6848.0 / 21.0 * GAMMA_E) +
+    const T m1M = m1 / M, m2M = m2 / M;
+    const T dm = (m1 - m2) / M;
+    const T SL = m1M * m1M * chi1 + m2M * m2M * chi2;
+    const T dSigmaL = dm * (m2M * chi2 - m1M * chi1);
+    const T pfaN = 3.0 / (128.0 * eta);
+    T v0 = pfaN;
+    T v1 = 0.0;
+    T v2 = pfaN * (5.0 * (743.0 / 84.0 + 11.0 * eta) / 9.0);
+    T v3 = pfaN * (-16.0 * PI);
+    T v4 = pfaN * (5.0 * (3058.673 / 7.056 + 5429.0 / 7.0 * eta + 617.0 * eta * eta) / 72.0);
+    T v5 = pfaN * (5.0 / 9.0 * (7729.0 / 84.0 - 13.0 * eta) * PI);
+    T vlogv5 = pfaN * (5.0 / 3.0 * (7729.0 / 84.0 - 13.0 * eta) * PI);
+    T v6 = pfaN * ((11583.231236531 / 4.694215680 - 640.0 / 3.0 * PI * PI - 6848.0 / 21.0 * GAMMA_E) +
                         eta * (-15737.765635 / 3.048192 + 2255. / 12. * PI * PI) +
                         eta * eta * 76055.0 / 1728.0 - eta * eta * eta * 127825.0 / 1296.0);
     v6 += pfaN * (-6848.0 / 21.0) * log(4.);
-    double vlogv6 = pfaN * (-6848.0 / 21.0);
-    double v7 = pfaN * (PI * (77096675.0 / 254016.0 + 378515.0 / 1512.0 * eta - 74045.0 / 756.0 * eta * eta));
+    T vlogv6 = pfaN * (-6848.0 / 21.0);
+    T v7 = pfaN * (PI * (77096675.0 / 254016.0 + 378515.0 / 1512.0 * eta - 74045.0 / 756.0 * eta * eta));
     // spin-spin (2PN) and self-spin terms with qm_def = 1
-    double pn_sigma = eta * (721.0 / 48.0 * chi1 * chi2 - 247.0 / 48.0 * chi1 * chi2);
+    T pn_sigma = eta * (721.0 / 48.0 * chi1 * chi2 - 247.0 / 48.0 * chi1 * chi2);
     pn_sigma += (720.0 - 1.0) / 96.0 * m1M * m1M * chi1 * chi1;
     pn_sigma += (720.0 - 1.0) / 96.0 * m2M * m2M * chi2 * chi2;
     pn_sigma -= (240.0 - 7.0) / 96.0 * m1M * m1M * chi1 * chi1;
     pn_sigma -= (240.0 - 7.0) / 96.0 * m2M * m2M * chi2 * chi2;
-    double pn_ss3 = (326.75 / 1.12 + 557.5 / 1.8 * eta) * eta * chi1 * chi2;
+    T pn_ss3 = (326.75 / 1.12 + 557.5 / 1.8 * eta) * eta * chi1 * chi2;
     pn_ss3 += ((4703.5 / 8.4 + 2935.0 / 6.0 * m1M - 120.0 * m1M * m1M) +
                (-4108.25 / 6.72 - 108.5 / 1.2 * m1M + 125.5 / 3.6 * m1M * m1M)) *
               m1M * m1M * chi1 * chi1;
     pn_ss3 += ((4703.5 / 8.4 + 2935.0 / 6.0 * m2M - 120.0 * m2M * m2M) +
                (-4108.25 / 6.72 - 108.5 / 1.2 * m2M + 125.5 / 3.6 * m2M * m2M)) *
               m2M * m2M * chi2 * chi2;
-    const double pn_gamma = (554345.0 / 1134.0 + 110.0 * eta / 9.0) * SL + (13915.0 / 84.0 - 10.0 * eta / 3.0) * dSigmaL;
+    const T pn_gamma = (554345.0 / 1134.0 + 110.0 * eta / 9.0) * SL + (13915.0 / 84.0 - 10.0 * eta / 3.0) * dSigmaL;
     v7 += pfaN * ((-8980424995.0 / 762048.0 + 6586595.0 * eta / 756.0 - 305.0 * eta * eta / 36.0) * SL -
                   (170978035.0 / 48384.0 - 2876425.0 * eta / 672.0 - 4735.0 * eta * eta / 144.0) * dSigmaL);
     v6 += pfaN * (PI * (3760.0 * SL + 1490.0 * dSigmaL) / 3.0 + pn_ss3);
@@ -582,14 +607,14 @@ __device__ inline void phenomd_setup(PhenomD& d, double m1, double m2, double ch
 
   // C1 joins (PhenomHMWaveform.cu:1263-1303)
   {
-    const double fj = PHI_FJOIN_INS;
+    const T fj = PHI_FJOIN_INS;
     d.C2Int = dphi_ins(d, fj) - dphi_int(d, fj);
-    Powers pj = make_powers(fj);
+    PowersT<T> pj = make_powers(fj);
     d.C1Int = phi_ins(d, fj, pj) - d.etaInv * phi_int(d, fj) - d.C2Int * fj;
     d.fMRDJoin = 0.5 * fring;
-    const double fm = d.fMRDJoin;
-    const double phi_int_val = d.etaInv * phi_int(d, fm) + d.C1Int + d.C2Int * fm;
-    const double dphi_int_val = d.C2Int + dphi_int(d, fm);
+    const T fm = d.fMRDJoin;
+    const T phi_int_val = d.etaInv * phi_int(d, fm) + d.C1Int + d.C2Int * fm;
+    const T dphi_int_val = d.C2Int + dphi_int(d, fm);
     d.C2MRD = dphi_int_val - dphi_mrd(d, fm, Rholm, Taulm);
     d.C1MRD = phi_int_val - d.etaInv * phi_mrd(d, fm, Rholm, Taulm) - d.C2MRD * fm;
   }
@@ -598,23 +623,25 @@ __device__ inline void phenomd_setup(PhenomD& d, double m1, double m2, double ch
 // ---------------------------------------------------------------------------------
 // PhenomHM per-(binary, mode) record
 // ---------------------------------------------------------------------------------
-struct ModeCoeffs {
-  PhenomD d;
+template <typename T>
+struct ModeCoeffsT {
+  PhenomDT<T> d;
   int ell, mm, phenomd_only, pad;
   // phase frequency map Mf22 = a Mf + b by region (PhenomHMWaveform.cu:2130-2369)
-  double ph_fi, ph_fr, ph_ai, ph_am, ph_bm, ph_ar, ph_constB, ph_constC;
+  T ph_fi, ph_fr, ph_ai, ph_am, ph_bm, ph_ar, ph_constB, ph_constC;
   // amplitude frequency map
-  double am_fi, am_fr, am_ai, am_am, am_bm, am_br;
+  T am_fi, am_fr, am_ai, am_am, am_bm, am_br;
   // PN amplitude ratio inputs (PhenomHMWaveform.cu:2375-2455)
-  double pn_m1, pn_m2, pn_chi1, pn_chi2;
+  T pn_m1, pn_m2, pn_chi1, pn_chi2;
   // |H_lm(v)| constants: leading factor, eta, delta, chi_s, chi_a; case 0 = 22 / PhenomD,
   // 1..5 = 21, 33, 32, 44, 43, 6 = no PN amplitude
-  double pn_k, pn_eta, pn_delta, pn_Xs, pn_Xa, pn_2pi_m, pn_4pi_m2;
+  T pn_k, pn_eta, pn_delta, pn_Xs, pn_Xa, pn_2pi_m, pn_4pi_m2;
   int pn_case, pad2;
-  double ph_inv_ai, ph_inv_am, ph_inv_ar;
+  T ph_inv_ai, ph_inv_am, ph_inv_ar;
   // overall shifts / scales
-  double t0, phi0, Mf_ref, amp_scale, M_sec, cshift;
+  T t0, phi0, Mf_ref, amp_scale, M_sec, cshift;
 };
+using ModeCoeffs = ModeCoeffsT<double>;
 
 __device__ __forceinline__ double cshift_of(int mm) {
   // Blanchet arXiv:1310.1528 sec. 9.5 leading-order complex-amplitude phase shifts by m
@@ -630,21 +657,22 @@ __device__ __forceinline__ double cshift_of(int mm) {
 // Set up one (binary, mode) record.  Inputs as the reference's IMRPhenomHM kernel:
 // SI masses (kg), distance (m), the mode's QNM ringdown / damping frequencies and the
 // PhenomD spline values appended after the modes (phenomhm.py:424-463).
-__device__ inline void phm_setup_mode(ModeCoeffs& c, double m1_SI, double m2_SI, double chi1,
-                                      double chi2, double distance, int ell, int mm,
-                                      double Mf_RD_lm, double Mf_DM_lm, double Mf_RD_22_in,
-                                      double Mf_DM_22_in, int run_phenomd) {
-  double m1 = m1_SI / MSUN_SI, m2 = m2_SI / MSUN_SI;
+template <typename T>
+__device__ inline void phm_setup_mode(ModeCoeffsT<T>& c, T m1_SI, T m2_SI, T chi1,
+                                      T chi2, T distance, int ell, int mm,
+                                      T Mf_RD_lm, T Mf_DM_lm, T Mf_RD_22_in,
+                                      T Mf_DM_22_in, int run_phenomd) {
+  T m1 = m1_SI / MSUN_SI, m2 = m2_SI / MSUN_SI;
   if (!(m1 > m2)) {
-    double t = m1; m1 = m2; m2 = t;
+    T t = m1; m1 = m2; m2 = t;
     t = chi1; chi1 = chi2; chi2 = t;
   }
-  const double Mtot = m1 + m2;
-  double finmass, finspin;
+  const T Mtot = m1 + m2;
+  T finmass, finspin;
   final_mass_spin(m1, m2, chi1, chi2, &finmass, &finspin);
-  double Mf_RD_22, Mf_DM_22;
+  T Mf_RD_22, Mf_DM_22;
   if (!run_phenomd) {
-    cplx z = qnm_cw(finspin, 2, 2);
+    cplxT<T> z = qnm_cw(finspin, 2, 2);
     Mf_RD_22 = (0.5 / PI) * z.re / finmass;
     Mf_DM_22 = (0.5 / PI) * z.im / finmass;
   } else {
@@ -652,10 +680,10 @@ __device__ inline void phm_setup_mode(ModeCoeffs& c, double m1_SI, double m2_SI,
     Mf_DM_22 = Mf_DM_lm;
   }
   // 22-mode PhenomD: reference frequency = amplitude peak, t0 and phi0 from there
-  PhenomD d22;
-  phenomd_setup(d22, m1, m2, chi1, chi2, Mf_RD_22_in, Mf_DM_22_in, 1.0, 1.0);
-  const double Mf_ref = d22.fpeak;
-  const double phi22_ref = phenomd_phase(d22, Mf_ref);
+  PhenomDT<T> d22;
+  phenomd_setup(d22, m1, m2, chi1, chi2, Mf_RD_22_in, Mf_DM_22_in, T(1.0), T(1.0));
+  const T Mf_ref = d22.fpeak;
+  const T phi22_ref = phenomd_phase(d22, Mf_ref);
   c.phi0 = 0.5 * phi22_ref;
   c.t0 = phenomd_dphase(d22, Mf_ref);
   c.Mf_ref = Mf_ref;
@@ -669,14 +697,14 @@ __device__ inline void phm_setup_mode(ModeCoeffs& c, double m1_SI, double m2_SI,
   c.pn_chi1 = chi1;
   c.pn_chi2 = chi2;
   {
-    const double M1 = m1 / (m1 + m2), M2 = m2 / (m1 + m2);
-    const double eta = M1 * M2 / ((M1 + M2) * (M1 + M2));
+    const T M1 = m1 / (m1 + m2), M2 = m2 / (m1 + m2);
+    const T eta = M1 * M2 / ((M1 + M2) * (M1 + M2));
     c.pn_eta = eta;
     c.pn_delta = sqrt(1.0 - 4 * eta);
     c.pn_Xs = 0.5 * (chi1 + chi2);
     c.pn_Xa = 0.5 * (chi1 - chi2);
     c.pn_2pi_m = 2.0 * PI / mm;
-    c.pn_4pi_m2 = 4.0 * PI / ((double)mm * mm);
+    c.pn_4pi_m2 = 4.0 * PI / ((T)mm * mm);
     if (run_phenomd || (ell == 2 && mm == 2)) { c.pn_case = 0; c.pn_k = 1.0; }
     else if (ell == 2 && mm == 1) { c.pn_case = 1; c.pn_k = sqrt(2.0) / 3.0; }
     else if (ell == 3 && mm == 3) { c.pn_case = 2; c.pn_k = 0.75 * sqrt(5.0 / 7.0); }
@@ -692,19 +720,19 @@ __device__ inline void phm_setup_mode(ModeCoeffs& c, double m1_SI, double m2_SI,
     return;
   }
   c.cshift = cshift_of(mm);
-  const double Rholm = Mf_RD_22 / Mf_RD_lm;
-  const double Taulm = Mf_DM_lm / Mf_DM_22;
+  const T Rholm = Mf_RD_22 / Mf_RD_lm;
+  const T Taulm = Mf_DM_lm / Mf_DM_22;
   phenomd_setup(c.d, m1, m2, chi1, chi2, Mf_RD_22_in, Mf_DM_22_in, Rholm, Taulm);
   // phase map: inspiral Mf22 = (2/m) Mf; ringdown Mf22 = Rholm Mf; linear in between
   {
-    const double fi = PHI_FJOIN_INS / Rholm;
-    const double fr = Mf_RD_lm;
-    const double ai = 2.0 / mm;
-    const double Trd = Rholm * fr;
-    const double Ti = 2.0 * fi / mm;
-    const double am = (Trd - Ti) / (fr - fi);
-    const double bm = Ti - fi * am;
-    const double ar = Rholm;
+    const T fi = PHI_FJOIN_INS / Rholm;
+    const T fr = Mf_RD_lm;
+    const T ai = 2.0 / mm;
+    const T Trd = Rholm * fr;
+    const T Ti = 2.0 * fi / mm;
+    const T am = (Trd - Ti) / (fr - fi);
+    const T bm = Ti - fi * am;
+    const T ar = Rholm;
     c.ph_fi = fi;
     c.ph_fr = fr;
     c.ph_ai = ai;
@@ -714,20 +742,20 @@ __device__ inline void phm_setup_mode(ModeCoeffs& c, double m1_SI, double m2_SI,
     c.ph_inv_ai = 1.0 / ai;
     c.ph_inv_am = 1.0 / am;
     c.ph_inv_ar = 1.0 / ar;
-    const double PhDBconst = phenomd_phase(c.d, am * fi + bm) / am;
-    const double PhDCconst = phenomd_phase(c.d, ar * fr) / ar;
-    const double PhDBAterm = phenomd_phase(c.d, ai * fi) / ai;
-    const double tmpC = phenomd_phase(c.d, am * fr + bm) / am - PhDBconst + PhDBAterm;
+    const T PhDBconst = phenomd_phase(c.d, am * fi + bm) / am;
+    const T PhDCconst = phenomd_phase(c.d, ar * fr) / ar;
+    const T PhDBAterm = phenomd_phase(c.d, ai * fi) / ai;
+    const T tmpC = phenomd_phase(c.d, am * fr + bm) / am - PhDBconst + PhDBAterm;
     c.ph_constB = -PhDBconst + PhDBAterm;
     c.ph_constC = -PhDCconst + tmpC;
   }
   // amplitude map: inspiral (2/m) Mf; ringdown Mf - Mf_RD_lm + Mf_RD_22
   {
-    const double fi = AMP_FJOIN_INS / Rholm;
-    const double fr = Mf_RD_lm;
-    const double Trd = fr - Mf_RD_lm + Mf_RD_22;
-    const double Ti = 2.0 * fi / mm;
-    const double am = (Trd - Ti) / (fr - fi);
+    const T fi = AMP_FJOIN_INS / Rholm;
+    const T fr = Mf_RD_lm;
+    const T Trd = fr - Mf_RD_lm + Mf_RD_22;
+    const T Ti = 2.0 * fi / mm;
+    const T am = (Trd - Ti) / (fr - fi);
     c.am_fi = fi;
     c.am_fr = fr;
     c.am_ai = 2.0 / mm;
@@ -739,17 +767,18 @@ __device__ inline void phm_setup_mode(ModeCoeffs& c, double m1_SI, double m2_SI,
 
 // |H_lm(v)| of the 1.5PN spinning amplitude (IMRPhenomHMOnePointFiveSpinPN,
 // PhenomHMWaveform.cu:2375-2455) for the non-22 cases.
-__device__ __forceinline__ double pn_habs(const ModeCoeffs& c, double v) {
-  const double v2 = v * v, v3 = v2 * v;
+template <typename T>
+__device__ __forceinline__ T pn_habs(const ModeCoeffsT<T>& c, T v) {
+  const T v2 = v * v, v3 = v2 * v;
   switch (c.pn_case) {
     case 1: {
-      const double v4 = v3 * v;
-      const double re = c.pn_k * (v * c.pn_delta - v2 * 1.5 * (c.pn_Xa + c.pn_delta * c.pn_Xs) +
+      const T v4 = v3 * v;
+      const T re = c.pn_k * (v * c.pn_delta - v2 * 1.5 * (c.pn_Xa + c.pn_delta * c.pn_Xs) +
                                   v3 * c.pn_delta * ((335.0 / 672.0) + (c.pn_eta * 117.0 / 56.0)) +
                                   v4 * (c.pn_Xa * (3427.0 / 1344 - c.pn_eta * 2101.0 / 336) +
                                         c.pn_delta * c.pn_Xs * (3427.0 / 1344 - c.pn_eta * 965 / 336) +
                                         c.pn_delta * (-PI)));
-      const double im = c.pn_k * v4 * c.pn_delta * (-0.5 - 2.0 * 0.69314718056);
+      const T im = c.pn_k * v4 * c.pn_delta * (-0.5 - 2.0 * 0.69314718056);
       return hypot(re, im);
     }
     case 2: return fabs(c.pn_k * (v * c.pn_delta));
@@ -765,19 +794,21 @@ __device__ __forceinline__ double pn_habs(const ModeCoeffs& c, double v) {
 // The v^-3.5 factors cancel exactly (v(2Mf/m) / v(Mf) = (2/m)^(1/3), v_22(Mfa) / v_lm(Mfa)
 // = (m/2)^(1/3)), leaving |H(v(Mf))| |H(v(Mfa))| / |H(v(2Mf/m))|; zero where |H(v(Mf))| = 0
 // (the reference's equal-mass guard).
-__device__ __forceinline__ double hm_amp_factor(const ModeCoeffs& c, double Mf, double Mfa) {
+template <typename T>
+__device__ __forceinline__ T hm_amp_factor(const ModeCoeffsT<T>& c, T Mf, T Mfa) {
   if (c.pn_case == 0) return 1.0;
-  const double t1 = pn_habs(c, cbrt(c.pn_2pi_m * Mf));
+  const T t1 = pn_habs(c, cbrt(c.pn_2pi_m * Mf));
   if (t1 == 0.0) return 0.0;
-  const double t2 = pn_habs(c, cbrt(c.pn_4pi_m2 * Mf));
-  const double h1 = pn_habs(c, cbrt(c.pn_2pi_m * Mfa));
+  const T t2 = pn_habs(c, cbrt(c.pn_4pi_m2 * Mf));
+  const T h1 = pn_habs(c, cbrt(c.pn_2pi_m * Mfa));
   return (t1 / t2) * h1;
 }
 
 // Mapped PhenomD frequency and phase constants of the HM phase map (get_phase,
 // PhenomHMWaveform.cu:2517-2565): ph = phase(Mfp) * inv + add.
-__device__ __forceinline__ void hm_phase_map(const ModeCoeffs& c, double Mf, double* Mfp,
-                                             double* inv, double* add) {
+template <typename T>
+__device__ __forceinline__ void hm_phase_map(const ModeCoeffsT<T>& c, T Mf, T* Mfp,
+                                             T* inv, T* add) {
   if (!(Mf > c.ph_fi)) {
     *Mfp = c.ph_ai * Mf;
     *inv = c.ph_inv_ai;
@@ -794,14 +825,15 @@ __device__ __forceinline__ void hm_phase_map(const ModeCoeffs& c, double Mf, dou
 }
 
 // Phase and t(f) of one mode at Mf (no t_ref shift).
-__device__ __forceinline__ void mode_phase_tf(const ModeCoeffs& c, double Mf, double* phase,
-                                              double* tf) {
-  double ph, dph;
+template <typename T>
+__device__ __forceinline__ void mode_phase_tf(const ModeCoeffsT<T>& c, T Mf, T* phase,
+                                              T* tf) {
+  T ph, dph;
   if (c.phenomd_only) {
     phenomd_phase_dphase(c.d, Mf, &ph, &dph);
     *phase = -c.t0 * (Mf - c.Mf_ref) + ((c.cshift + ph) - 2 * c.phi0);
   } else {
-    double Mfp, inv, add;
+    T Mfp, inv, add;
     hm_phase_map(c, Mf, &Mfp, &inv, &add);
     phenomd_phase_dphase(c.d, Mfp, &ph, &dph);
     *phase = -c.t0 * (Mf - c.Mf_ref) + ((c.cshift + (ph * inv + add)) - c.mm * c.phi0);
@@ -810,24 +842,28 @@ __device__ __forceinline__ void mode_phase_tf(const ModeCoeffs& c, double Mf, do
 }
 
 // Mapped amplitude frequency (IMRPhenomHMFreqDomainMap with AmpFlag, :2295-2315).
-__device__ __forceinline__ double hm_amp_map(const ModeCoeffs& c, double Mf) {
+template <typename T>
+__device__ __forceinline__ T hm_amp_map(const ModeCoeffsT<T>& c, T Mf) {
   if (Mf > c.am_fi) return (Mf > c.am_fr) ? Mf + c.am_br : c.am_am * Mf + c.am_bm;
   return c.am_ai * Mf;
 }
 
-struct PointOut {
-  double amp, phase, tf;
+template <typename T>
+struct PointOutT {
+  T amp, phase, tf;
 };
+using PointOut = PointOutT<double>;
 
 // Amplitude, phase and t(f) of one mode at frequency f (Hz).  t(f) and phase do not yet
 // include the t_ref shift (added by the caller, phenomhm.py:485-507).
-__device__ inline PointOut phm_eval_point(const ModeCoeffs& c, double f) {
-  PointOut o;
-  const double Mf = f * c.M_sec;
+template <typename T>
+__device__ inline PointOutT<T> phm_eval_point(const ModeCoeffsT<T>& c, T f) {
+  PointOutT<T> o;
+  const T Mf = f * c.M_sec;
   if (c.phenomd_only) {
     o.amp = phenomd_amp(c.d, Mf) * c.amp_scale;
   } else {
-    const double Mfa = hm_amp_map(c, Mf);
+    const T Mfa = hm_amp_map(c, Mf);
     o.amp = phenomd_amp(c.d, Mfa) * hm_amp_factor(c, Mf, Mfa) * c.amp_scale;
   }
   mode_phase_tf(c, Mf, &o.phase, &o.tf);

@@ -18,6 +18,7 @@
 #pragma once
 
 #include "bbhx_common.cuh"
+#include "dual.cuh"
 
 namespace bbhx {
 
@@ -38,24 +39,29 @@ struct OrbitHandle {
   bool ready = false;
 };
 
-struct ResponseMode {
-  cplx H[9];     // complex mode matrix, row-major
-  double k[3];   // propagation direction
+template <typename T>
+struct ResponseModeT {
+  cplxT<T> H[9];  // complex mode matrix, row-major
+  T k[3];         // propagation direction
+};
+using ResponseMode = ResponseModeT<double>;
+
+
+template <typename T>
+struct V3T {
+  T x, y, z;
 };
 
-struct V3 {
-  double x, y, z;
-};
-
-__device__ __forceinline__ V3 orbit_lerp(const double* tab, int stride, int offset, double dt,
-                                         int N, double t) {
-  double w = floor(t / dt);
-  if (!(w >= 0.0) || w >= (double)(N - 1)) return V3{0.0, 0.0, 0.0};
+template <typename T>
+__device__ __forceinline__ V3T<T> orbit_lerp(const double* tab, int stride, int offset, double dt,
+                                             int N, const T& t) {
+  double w = floor(value_of(t) / dt);
+  if (!(w >= 0.0) || w >= (double)(N - 1)) return V3T<T>{T(0.0), T(0.0), T(0.0)};
   int wi = (int)w;
   const double* lo = tab + (size_t)wi * stride + offset;
   const double* hi = lo + stride;
-  double tt = t - wi * dt;
-  V3 r;
+  T tt = t - wi * dt;
+  V3T<T> r;
   r.x = __ldg(lo + 0) + (__ldg(hi + 0) - __ldg(lo + 0)) / dt * tt;
   r.y = __ldg(lo + 1) + (__ldg(hi + 1) - __ldg(lo + 1)) / dt * tt;
   r.z = __ldg(lo + 2) + (__ldg(hi + 2) - __ldg(lo + 2)) / dt * tt;
@@ -63,10 +69,11 @@ __device__ __forceinline__ V3 orbit_lerp(const double* tab, int stride, int offs
 }
 
 // spin-weight -2 spherical harmonics for l = 2..4 (Response.cu:383-424)
-__device__ inline cplx sylm_m2(int l, int m, double theta, double phi) {
-  double fac = 0.0;
-  double ct = cos(theta), st = sin(theta);
-  double c2 = cos(theta / 2.0), s2 = sin(theta / 2.0);
+template <typename T>
+__device__ inline cplxT<T> sylm_m2(int l, int m, const T& theta, const T& phi) {
+  T fac = 0.0;
+  T ct = cos(theta), st = sin(theta);
+  T c2 = cos(theta / 2.0), s2 = sin(theta / 2.0);
   if (l == 2) {
     if (m == -2) fac = sqrt(5.0 / (64.0 * PI)) * (1.0 - ct) * (1.0 - ct);
     else if (m == -1) fac = sqrt(5.0 / (16.0 * PI)) * st * (1.0 - ct);
@@ -83,133 +90,141 @@ __device__ inline cplx sylm_m2(int l, int m, double theta, double phi) {
     else if (m == 3) fac = -3.0 * sqrt(7.0 / (2.0 * PI)) * pow(c2, 5.0) * (-1.0 + 2.0 * ct) * s2;
     else if (m == 4) fac = 3.0 * sqrt(7.0 / PI) * pow(c2, 6.0) * pow(s2, 2.0);
   }
-  if (m == 0) return mk(fac, 0.0);
-  double s, c;
+  if (m == 0) return cmk(fac, T(0.0));
+  T s, c;
   sincos(m * phi, &s, &c);
-  return mk(fac * c, fac * s);
+  return cmk(fac * c, fac * s);
 }
 
-__device__ inline void response_mode_setup(ResponseMode& r, int ell, int mm, double phi_ref,
-                                           double inc, double lam, double beta, double psi) {
-  double cl = cos(lam), sl = sin(lam), cb = cos(beta), sb = sin(beta), cp = cos(psi), sp = sin(psi);
+template <typename T>
+__device__ inline void response_mode_setup(ResponseModeT<T>& r, int ell, int mm, const T& phi_ref,
+                                           const T& inc, const T& lam, const T& beta,
+                                           const T& psi) {
+  T cl = cos(lam), sl = sin(lam), cb = cos(beta), sb = sin(beta), cp = cos(psi), sp = sin(psi);
   r.k[0] = -cb * cl;
   r.k[1] = -cb * sl;
   r.k[2] = -sb;
   // rotation from the wave frame to the SSB frame and its inverse
-  double O[9] = {cp * sl - cl * sb * sp, -cl * cp * sb - sl * sp, -cb * cl,
-                 -cl * cp - sb * sl * sp, -cp * sb * sl + cl * sp, -cb * sl,
-                 cb * sp, cb * cp, -sb};
-  double Oi[9] = {O[0], O[3], O[6], O[1], O[4], O[7], O[2], O[5], O[8]};
+  T O[9] = {cp * sl - cl * sb * sp, -cl * cp * sb - sl * sp, -cb * cl,
+            -cl * cp - sb * sl * sp, -cp * sb * sl + cl * sp, -cb * sl,
+            cb * sp, cb * cp, -sb};
+  T Oi[9] = {O[0], O[3], O[6], O[1], O[4], O[7], O[2], O[5], O[8]};
   // H+ = O diag(1,-1,0) O^-1, Hx = O offdiag(1,1) O^-1
-  double Hp[9], Hc[9];
+  T Hp[9], Hc[9];
   for (int i = 0; i < 3; ++i)
     for (int j = 0; j < 3; ++j) {
       // (HS+ O^-1)_{kj} = s_k Oi[k][j] with s = (1,-1,0); (HSx O^-1)_{0j} = Oi[1][j], _{1j} = Oi[0][j]
-      double p = O[i * 3 + 0] * Oi[0 * 3 + j] - O[i * 3 + 1] * Oi[1 * 3 + j];
-      double x = O[i * 3 + 0] * Oi[1 * 3 + j] + O[i * 3 + 1] * Oi[0 * 3 + j];
+      T p = O[i * 3 + 0] * Oi[0 * 3 + j] - O[i * 3 + 1] * Oi[1 * 3 + j];
+      T x = O[i * 3 + 0] * Oi[1 * 3 + j] + O[i * 3 + 1] * Oi[0 * 3 + j];
       Hp[i * 3 + j] = p;
       Hc[i * 3 + j] = x;
     }
-  cplx Ylm = sylm_m2(ell, mm, inc, phi_ref);
-  cplx Ylmm = sylm_m2(ell, -mm, inc, phi_ref);
+  cplxT<T> Ylm = sylm_m2(ell, mm, inc, phi_ref);
+  cplxT<T> Ylmm = sylm_m2(ell, -mm, inc, phi_ref);
   double sgn = (ell % 2 == 0) ? 1.0 : -1.0;
-  cplx Yl_m = sgn * conj(Ylmm);
-  cplx Yp = 0.5 * (Ylm + Yl_m);
-  cplx Yc = times_i(0.5 * (Ylm - Yl_m));
+  cplxT<T> Yl_m = sgn * conj(Ylmm);
+  cplxT<T> Yp = 0.5 * (Ylm + Yl_m);
+  cplxT<T> Yc = times_i(0.5 * (Ylm - Yl_m));
   for (int q = 0; q < 9; ++q) r.H[q] = Yp * Hp[q] + Yc * Hc[q];
 }
 
-struct Transfer {
-  cplx L1, L2, L3;
-  double phaseRdelay;
+template <typename T>
+struct TransferT {
+  cplxT<T> L1, L2, L3;
+  T phaseRdelay;
 };
+using Transfer = TransferT<double>;
 
-__device__ __forceinline__ cplx nHn(const cplx* H, V3 n) {
-  double v[3] = {n.x, n.y, n.z};
-  cplx out = mk(0.0, 0.0);
+template <typename T>
+__device__ __forceinline__ cplxT<T> nHn(const cplxT<T>* H, const V3T<T>& n) {
+  T v[3] = {n.x, n.y, n.z};
+  cplxT<T> out = cmk(T(0.0), T(0.0));
   for (int i = 0; i < 3; ++i) {
-    cplx t = mk(0.0, 0.0);
+    cplxT<T> t = cmk(T(0.0), T(0.0));
     for (int j = 0; j < 3; ++j) t = t + H[i * 3 + j] * v[j];
     out = out + v[i] * t;
   }
   return out;
 }
 
-__device__ __forceinline__ double sinc(double x) { return x == 0.0 ? 1.0 : sin(x) / x; }
+template <typename T>
+__device__ __forceinline__ T sinc(const T& x) { return x == 0.0 ? T(1.0) : sin(x) / x; }
 
 // TDItag: 1 = XYZ, 2 = AET.  f in Hz, t in s.
-__device__ inline Transfer response_point(const ResponseMode& r, const OrbitTables& orb, double f,
-                                          double t, int TDItag, int rescaled, int tdi2) {
-  const double* k = r.k;
+template <typename T>
+__device__ inline TransferT<T> response_point(const ResponseModeT<T>& r, const OrbitTables& orb,
+                                              double f, const T& t, int TDItag, int rescaled,
+                                              int tdi2) {
+  const T* k = r.k;
   // Roemer delay relative to the SSB (circular 1 AU orbit of the guiding centre)
-  double al = Omega0 * t;
-  double sa, ca;
+  T al = Omega0 * t;
+  T sa, ca;
   sincos(al, &sa, &ca);
-  double kR = k[0] * (AU_SI * ca) + k[1] * (AU_SI * sa) + k[2] * (0.0 * t);
-  Transfer out;
+  T kR = k[0] * (AU_SI * ca) + k[1] * (AU_SI * sa) + k[2] * (0.0 * t);
+  TransferT<T> out;
   out.phaseRdelay = 2. * PI / C_SI * f * kR;
 
-  V3 p1 = orbit_lerp(orb.x_arr, 9, 0, orb.dt, orb.N, t);
-  V3 p2 = orbit_lerp(orb.x_arr, 9, 3, orb.dt, orb.N, t);
-  V3 p3 = orbit_lerp(orb.x_arr, 9, 6, orb.dt, orb.N, t);
-  V3 n1 = orbit_lerp(orb.n_arr, 18, orb.link_index[0] * 3, orb.dt, orb.N, t);
-  V3 n2 = orbit_lerp(orb.n_arr, 18, orb.link_index[1] * 3, orb.dt, orb.N, t);
-  V3 n3 = orbit_lerp(orb.n_arr, 18, orb.link_index[2] * 3, orb.dt, orb.N, t);
-  double kn1 = k[0] * n1.x + k[1] * n1.y + k[2] * n1.z;
-  double kn2 = k[0] * n2.x + k[1] * n2.y + k[2] * n2.z;
-  double kn3 = k[0] * n3.x + k[1] * n3.y + k[2] * n3.z;
-  cplx n1H = nHn(r.H, n1), n2H = nHn(r.H, n2), n3H = nHn(r.H, n3);
-  double k12 = k[0] * (p1.x + p2.x) + k[1] * (p1.y + p2.y) + k[2] * (p1.z + p2.z);
-  double k23 = k[0] * (p2.x + p3.x) + k[1] * (p2.y + p3.y) + k[2] * (p2.z + p3.z);
-  double k31 = k[0] * (p3.x + p1.x) + k[1] * (p3.y + p1.y) + k[2] * (p3.z + p1.z);
-  const double L = orb.armlength;
-  double pre = PI * f * L / C_SI;
-  cplx e12 = expi(pre * (1. + k12 / L));
-  cplx e23 = expi(pre * (1. + k23 / L));
-  cplx e31 = expi(pre * (1. + k31 / L));
+  V3T<T> p1 = orbit_lerp(orb.x_arr, 9, 0, orb.dt, orb.N, t);
+  V3T<T> p2 = orbit_lerp(orb.x_arr, 9, 3, orb.dt, orb.N, t);
+  V3T<T> p3 = orbit_lerp(orb.x_arr, 9, 6, orb.dt, orb.N, t);
+  V3T<T> n1 = orbit_lerp(orb.n_arr, 18, orb.link_index[0] * 3, orb.dt, orb.N, t);
+  V3T<T> n2 = orbit_lerp(orb.n_arr, 18, orb.link_index[1] * 3, orb.dt, orb.N, t);
+  V3T<T> n3 = orbit_lerp(orb.n_arr, 18, orb.link_index[2] * 3, orb.dt, orb.N, t);
+  T kn1 = k[0] * n1.x + k[1] * n1.y + k[2] * n1.z;
+  T kn2 = k[0] * n2.x + k[1] * n2.y + k[2] * n2.z;
+  T kn3 = k[0] * n3.x + k[1] * n3.y + k[2] * n3.z;
+  cplxT<T> n1H = nHn(r.H, n1), n2H = nHn(r.H, n2), n3H = nHn(r.H, n3);
+  T k12 = k[0] * (p1.x + p2.x) + k[1] * (p1.y + p2.y) + k[2] * (p1.z + p2.z);
+  T k23 = k[0] * (p2.x + p3.x) + k[1] * (p2.y + p3.y) + k[2] * (p2.z + p3.z);
+  T k31 = k[0] * (p3.x + p1.x) + k[1] * (p3.y + p1.y) + k[2] * (p3.z + p1.z);
+  const T L = orb.armlength;
+  T pre = PI * f * L / C_SI;
+  cplxT<T> e12 = expi(pre * (1. + k12 / L));
+  cplxT<T> e23 = expi(pre * (1. + k23 / L));
+  cplxT<T> e31 = expi(pre * (1. + k31 / L));
   // The constellation-centre phase factor exp(+i 2 pi f k.p0 / c) of the full response and
   // the Roemer-delay factor exp(-i phaseRdelay) cancel identically (Response.cu:166,304-309).
-  cplx common = mk(0.0, pre);
-  cplx c3 = common * n3H, c1 = common * n1H, c2 = common * n2H;
-  cplx G12 = c3 * (sinc(pre * (1. - kn3)) * e12);
-  cplx G21 = c3 * (sinc(pre * (1. + kn3)) * e12);
-  cplx G23 = c1 * (sinc(pre * (1. - kn1)) * e23);
-  cplx G32 = c1 * (sinc(pre * (1. + kn1)) * e23);
-  cplx G31 = c2 * (sinc(pre * (1. - kn2)) * e31);
-  cplx G13 = c2 * (sinc(pre * (1. + kn2)) * e31);
+  cplxT<T> common = cmk(T(0.0), pre);
+  cplxT<T> c3 = common * n3H, c1 = common * n1H, c2 = common * n2H;
+  cplxT<T> G12 = c3 * (sinc(pre * (1. - kn3)) * e12);
+  cplxT<T> G21 = c3 * (sinc(pre * (1. + kn3)) * e12);
+  cplxT<T> G23 = c1 * (sinc(pre * (1. - kn1)) * e23);
+  cplxT<T> G32 = c1 * (sinc(pre * (1. + kn1)) * e23);
+  cplxT<T> G31 = c2 * (sinc(pre * (1. - kn2)) * e31);
+  cplxT<T> G13 = c2 * (sinc(pre * (1. + kn2)) * e31);
 
   // e^{ix}, x = pre, and its powers / sines from one sincos
-  const cplx e1 = expi(pre);
-  const cplx z = e1 * e1;  // e^{2ix}
-  const double s2x = 2. * e1.im * e1.re;
+  const cplxT<T> e1 = expi(pre);
+  const cplxT<T> z = e1 * e1;  // e^{2ix}
+  const T s2x = 2. * e1.im * e1.re;
   if (TDItag == 1) {
-    cplx fac = rescaled ? mk(1.0, 0.0) : times_i(2. * s2x * z);
-    cplx X = G21 + z * G12 - G31 - z * G13;
-    cplx Y = G32 + z * G23 - G12 - z * G21;
-    cplx Z = G13 + z * G31 - G23 - z * G32;
+    cplxT<T> fac = rescaled ? cmk(T(1.0), T(0.0)) : times_i(2. * s2x * z);
+    cplxT<T> X = G21 + z * G12 - G31 - z * G13;
+    cplxT<T> Y = G32 + z * G23 - G12 - z * G21;
+    cplxT<T> Z = G13 + z * G31 - G23 - z * G32;
     out.L1 = fac * X;
     out.L2 = fac * Y;
     out.L3 = fac * Z;
     return out;
   }
-  cplx fAE, fT;
+  cplxT<T> fAE, fT;
   if (rescaled) {
-    fAE = mk(1.0, 0.0);
-    fT = mk(1.0, 0.0);
+    fAE = cmk(T(1.0), T(0.0));
+    fT = cmk(T(1.0), T(0.0));
   } else {
     fAE = times_i(SQRT2 * s2x * z);
     fT = (2. * SQRT2 * s2x * e1.im) * (z * e1);
   }
-  cplx one = mk(1.0, 0.0);
-  cplx A = 0.5 * ((one + z) * (G31 + G13) - G23 - z * G32 - G21 - z * G12);
-  cplx E = (0.5 * INVSQRT3) * ((one - z) * (G13 - G31) + (mk(2.0, 0.0) + z) * (G12 - G32) +
+  cplxT<T> one = cmk(T(1.0), T(0.0));
+  cplxT<T> A = 0.5 * ((one + z) * (G31 + G13) - G23 - z * G32 - G21 - z * G12);
+  cplxT<T> E = (0.5 * INVSQRT3) * ((one - z) * (G13 - G31) + (cmk(T(2.0), T(0.0)) + z) * (G12 - G32) +
                               (one + 2. * z) * (G21 - G23));
-  cplx T = INVSQRT6 * (G21 - G12 + G32 - G23 + G13 - G31);
-  cplx f2 = mk(2.0, 0.0);
+  cplxT<T> Tc = INVSQRT6 * (G21 - G12 + G32 - G23 + G13 - G31);
+  cplxT<T> f2 = cmk(T(2.0), T(0.0));
   if (tdi2) f2 = 2.0 * times_i((-2. * (2. * s2x * z.re)) * (z * z));  // -2i sin4x e^{4ix}
   out.L1 = f2 * (fAE * A);
   out.L2 = f2 * (fAE * E);
-  out.L3 = f2 * (fT * T);
+  out.L3 = f2 * (fT * Tc);
   return out;
 }
 

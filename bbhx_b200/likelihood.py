@@ -195,6 +195,40 @@ class HeterodynedLikelihood:
         template_gen_kwargs["squeeze"] = False
         self.template_gen_kwargs = template_gen_kwargs
 
+    # ------------------------------------------------------------------ gradients
+    def _fused_ll(self, params, kw, precision):
+        """lnL [B] (device) and the raw sums for a [12, B] device parameter tensor."""
+        rows = tuple(params[k].contiguous() for k in range(12))
+        kw = {k: v for k, v in kw.items() if k in ("t_obs_start", "t_obs_end", "modes")}
+        d_h, h_h = self.template_gen.heterodyne_sums(rows, self.freqs, self._h0_flat,
+                                                     self.data_constants, precision=precision, **kw)
+        return -0.5 * (self.reference_d_d + h_h.real - 2 * d_h.real), (d_h, h_h)
+
+    def get_ll_and_grad(self, params, **waveform_kwargs):
+        """lnL [B] and d lnL / d theta [B, 11] (device tensors) for walkers ``params``
+        ([12, B]); theta = (m1, m2, chi1z, chi2z, distance, phi_ref, inc, lam, beta, psi,
+        t_ref).  FP64; the gradient of the plain (not phase-marginalised) lnL."""
+        from .autodiff import as_param_tensor
+
+        P = as_param_tensor(params)
+        kw = dict(self.template_gen_kwargs)
+        kw.update(waveform_kwargs)
+        kw = {k: v for k, v in kw.items() if k in ("t_obs_start", "t_obs_end", "modes")}
+        d_h, h_h, grad = self.template_gen.heterodyne_grad(P, self.freqs, self._h0_flat,
+                                                           self.data_constants, **kw)
+        ll = -0.5 * (self.reference_d_d + h_h.real - 2 * d_h.real)
+        return ll, grad
+
+    def loglike_torch(self, params, **waveform_kwargs):
+        """Differentiable lnL: a [B] tensor whose backward pass runs the gradient kernels
+        (the waveform is recomputed there, nothing is stored)."""
+        from .autodiff import as_param_tensor, function
+
+        kw = dict(self.template_gen_kwargs)
+        kw.update(waveform_kwargs)
+        P = params if (hasattr(params, "requires_grad") and params.requires_grad) else as_param_tensor(params)
+        return function("heterodyned").apply(P, self, kw)
+
     @property
     def h_sparse(self):
         """Sparse templates [B, 3, L] of the last walkers (likelihood.py:612)."""

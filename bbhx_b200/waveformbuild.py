@@ -283,6 +283,33 @@ class BBHWaveformFD:
                   int(rg.rescaled), int(rg.tdi2), M, L, B, PRECISIONS[precision], _lib.stream())
         return d_h, h_h
 
+    def heterodyne_grad(self, params, freqs, h0, constants, t_obs_start=0.0, t_obs_end=1.0,
+                        modes=None, **unused):
+        """Relative-binning sums d_h, h_h [B] and d lnL / d theta [B, 11] of the walkers
+        ``params`` (device tensor [12, B]); theta = rows (0, 1, 2, 3, 4, 5, 7, 8, 9, 10, 11)
+        of ``params`` (f_ref, row 6, does not enter the model)."""
+        t = torch()
+        P = params.to(device=device(), dtype=t.float64).contiguous()
+        rows = tuple(P[k] for k in range(12))
+        m1, m2, chi1z, chi2z, distance, phi_ref, f_ref, inc, lam, beta, psi, t_ref = rows
+        t_start, t_end = self._time_limits(lam, beta, t_obs_start, t_obs_end)
+        ap = self.amp_phase_gen
+        ap._setup_records(m1, m2, chi1z, chi2z, distance, t_ref, modes)
+        B, M, L = ap.num_bin_all, ap.num_modes, int(freqs.numel())
+        rg = self.response_gen
+        d_h = t.empty(B, dtype=t.complex128, device=device())
+        h_h = t.empty(B, dtype=t.complex128, device=device())
+        grad = t.empty((B, 11), dtype=t.float64, device=device())
+        tab = ap.qnm_table
+        from .waveforms.ringdownphenomd import dspin
+        _lib.call("bbhx_hdyn_grad", rg.orbit_handle.ptr, _lib.dptr(d_h), _lib.dptr(h_h),
+                  _lib.dptr(grad), _lib.dptr(ap._coeffs), _lib.dptr(P), _lib.dptr(ap.ells),
+                  _lib.dptr(ap.mms), _lib.dptr(tab), int(tab.shape[1]), float(dspin),
+                  float(ap.initial_t_val), _lib.dptr(t_start), _lib.dptr(t_end), _lib.dptr(freqs),
+                  _lib.dptr(h0), _lib.dptr(constants), rg.TDItag_int, int(rg.rescaled),
+                  int(rg.tdi2), int(ap.run_phenomd), M, L, B, _lib.stream())
+        return d_h, h_h, grad
+
     def inner_products(self, params, data_freqs, data_weighted, noise_factors, t_obs_start=0.0,
                        t_obs_end=1.0, length=1024, modes=None, flags=None, timing=None,
                        precision="fp64", **unused):

@@ -197,6 +197,19 @@ int bbhx_hdyn_fused(void *orbits, void *d_h, void *h_h, const void *coeffs, cons
                     const void *h0, const void *consts, int TDItag, int rescaled, int tdi2,
                     int num_modes, int length, int num_bin_all, int precision, void *stream);
 
+/* Heterodyned lnL terms and the gradient d lnL / d theta of B walkers (no reference
+   counterpart).  theta = (m1, m2, chi1z, chi2z, distance, phi_ref, inc, lam, beta, psi,
+   t_ref): rows 0-5 and 7-11 of params [12, B] (device, row-major); grad [B, 11] (device).
+   Reverse part: adjoint of the relative-binning sums and of r = h / h0 (FP64 forward pass);
+   forward part: dual-number tangents of PhenomHM + TDI at every (mode, frequency).
+   qnm_table [8, qnm_n]: ringdown / damping spline rows (y, c1, c2, c3 each). */
+int bbhx_hdyn_grad(void *orbits, void *d_h, void *h_h, double *grad, const void *coeffs,
+                   const double *params, const int *ells, const int *mms, const double *qnm_table,
+                   int qnm_n, double dspin, double t_init, const double *t_start,
+                   const double *t_end, const double *freqs, const void *h0, const void *consts,
+                   int TDItag, int rescaled, int tdi2, int run_phenomd, int num_modes, int length,
+                   int num_bin_all, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
