@@ -1,0 +1,427 @@
+// Gradient of the direct likelihood, d lnL / d theta for the 11 parameters of
+// gradient_model.cuh, without stored templates.
+//
+// lnL = Re<d|h> - <h|h> / 2 - <d|d> / 2 on the data grid, with h the cubic-spline
+// interpolation of the sparse [9, B, M, L] buffer (amplitude, phase, t(f), six transfer
+// components) summed over modes (TemplateInterpFD + direct_like: waveformbuild.py:89-239,
+// Likelihood.cu:356-471).  The chain, for a batch of binaries:
+//   1. k_adj_gh       d lnL / d h at every (binary, data bin):  g = 4 w (d~ - w h)  (reverse)
+//   2. k_adj_coeffs   warp per (binary, mode, spline segment): d lnL / d (y, c1, c2, c3) of
+//                     the 8 interpolated quantities, summed over the segment's data bins
+//   3. k_spline_adj   CTA per (binary, mode): adjoint of the not-a-knot spline build; the
+//                     slopes' system K s = r is transposed and solved by the same cyclic
+//                     reduction (K^T lambda = s_bar), giving d lnL / d y at the knots
+//   4. k_grad_setup + k_contract_direct: dual-number tangents of the model at the knots,
+//                     contracted with d lnL / d y                                  (forward)
+// The knot frequencies x are held fixed (their dependence on theta through the
+// observation-window regrid is not differentiated).
+#include <algorithm>
+#include <vector>
+
+#include "capi_internal.cuh"
+#include "gradient_model.cuh"
+#include "tridiag.cuh"
+
+extern "C" int bbhx_template_support(int* start, int* len, const double* x, int num_modes,
+                                     int length, int num_bin_all, const double* data_freqs,
+                                     int data_length, void* stream);
+
+namespace bbhx {
+
+// segment of knot row xs[0..L) holding f: s = (#x <= f) - 1 (searchsorted right - 1)
+__device__ __forceinline__ int knot_segment(const double* xs, int L, double f) {
+  int a = 0, c = L;
+  while (a < c) {
+    const int mid = (a + c) >> 1;
+    if (xs[mid] <= f) a = mid + 1;
+    else c = mid;
+  }
+  return a - 1;
+}
+
+// first index k with f[k] >= v
+__device__ __forceinline__ int lower_bound_d(const double* f, int n, double v) {
+  int a = 0, c = n;
+  while (a < c) {
+    const int mid = (a + c) >> 1;
+    if (f[mid] < v) a = mid + 1;
+    else c = mid;
+  }
+  return a;
+}
+
+struct SplineRefs {
+  const double *x, *y, *c1, *c2, *c3;  // x [B, M, L]; y, c1..c3 [9, B, M, L]
+  size_t n;                            // B * M * L
+  int M, L;
+};
+
+// The 9 interpolated quantities of (binary b, mode m) in segment s at u = f - x_s.
+__device__ __forceinline__ void eval_segment(const SplineRefs& S, size_t row, int s, double u,
+                                             double* q) {
+  const size_t o = row * S.L + s;
+#pragma unroll
+  for (int p = 0; p < 9; ++p) {
+    const size_t i = (size_t)p * S.n + o;
+    q[p] = S.y[i] + u * (S.c1[i] + u * (S.c2[i] + u * S.c3[i]));
+  }
+}
+
+// 1. d lnL / d h per (binary, data bin, channel) of binaries [b0, b0 + nb); gh packed by the
+// support offsets off[bl] (local binary bl).
+__global__ void k_adj_gh(cplx* gh, const long long* off, const int* start, const int* len,
+                         SplineRefs S, const double* data_freqs, const cplx* data,
+                         const double* noise, int N, const double* t_start, const double* t_end,
+                         int b0, int nb) {
+  const int bl = blockIdx.y;
+  const int b = b0 + bl;
+  const int st = start[b], n = len[b];
+  const double ts = t_start[b], te = t_end[b];
+  for (int kk = blockIdx.x * blockDim.x + threadIdx.x; kk < n; kk += gridDim.x * blockDim.x) {
+    const int k = st + kk;
+    const double f = data_freqs[k];
+    double h[6] = {0, 0, 0, 0, 0, 0};
+    for (int m = 0; m < S.M; ++m) {
+      const size_t row = (size_t)b * S.M + m;
+      const int s = knot_segment(S.x + row * S.L, S.L, f);
+      if (s < 0 || s >= S.L - 1) continue;
+      double q[9];
+      eval_segment(S, row, s, f - S.x[row * S.L + s], q);
+      if (!tf_gate(q[2], ts, te)) continue;
+      double sn, cs;
+      sincos(q[1], &sn, &cs);
+      const double ar = q[0] * cs, ai = q[0] * sn;
+#pragma unroll
+      for (int ch = 0; ch < 3; ++ch) {  // h += conj(T A e^{i phase})
+        const double tr = q[3 + 2 * ch], ti = q[4 + 2 * ch];
+        h[2 * ch] += tr * ar - ti * ai;
+        h[2 * ch + 1] -= tr * ai + ti * ar;
+      }
+    }
+    cplx* g = gh + (off[bl] + kk) * 3;
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch) {
+      const double w = noise[(size_t)ch * N + k];
+      const cplx d = data[(size_t)ch * N + k];
+      g[ch] = mk(4.0 * w * (d.re - w * h[2 * ch]), 4.0 * w * (d.im - w * h[2 * ch + 1]));
+    }
+  }
+}
+
+// 2. Warp per (local binary, mode, segment s < L-1): sums over the segment's data bins of
+// a_p, a_p u, a_p u^2, a_p u^3 with a_p = d lnL / d q_p (p = amp, phase, 6 transfers), into
+// ybd (d lnL / d y directly) and cb1..cb3 (d lnL / d c1..c3), all [9, B, M, L].
+__global__ void k_adj_coeffs(double* ybd, double* cb1, double* cb2, double* cb3, const cplx* gh,
+                             const long long* off, const int* start, const int* len, SplineRefs S,
+                             const double* data_freqs, int N, const double* t_start,
+                             const double* t_end, int b0, int nb) {
+  const int lane = threadIdx.x & 31;
+  const long long nseg = (long long)S.L - 1;
+  const long long total = (long long)nb * S.M * nseg;
+  for (long long wid = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; wid < total;
+       wid += ((long long)gridDim.x * blockDim.x) >> 5) {
+    const int bl = (int)(wid / (S.M * nseg));
+    const int m = (int)((wid / nseg) % S.M);
+    const int s = (int)(wid % nseg);
+    const int b = b0 + bl;
+    const size_t row = (size_t)b * S.M + m;
+    const double* xs = S.x + row * S.L;
+    const int st = start[b], n = len[b];
+    int k0 = lower_bound_d(data_freqs, N, xs[s]);
+    int k1 = lower_bound_d(data_freqs, N, xs[s + 1]);
+    k0 = max(k0, st);
+    k1 = min(k1, st + n);
+    double acc[32];
+#pragma unroll
+    for (int q = 0; q < 32; ++q) acc[q] = 0.0;
+    const double ts = t_start[b], te = t_end[b];
+    for (int k = k0 + lane; k < k1; k += 32) {
+      const double u = data_freqs[k] - xs[s];
+      double q[9];
+      eval_segment(S, row, s, u, q);
+      if (!tf_gate(q[2], ts, te)) continue;
+      const cplx* g = gh + (off[bl] + (k - st)) * 3;
+      double sn, cs;
+      sincos(q[1], &sn, &cs);
+      const double er = cs, ei = sn;            // e^{i phase}
+      const double aer = q[0] * er, aei = q[0] * ei;  // A e^{i phase}
+      double dA = 0.0, dP = 0.0, dT[6];
+#pragma unroll
+      for (int ch = 0; ch < 3; ++ch) {
+        const cplx u_ = g[ch];
+        const double tr = q[3 + 2 * ch], ti = q[4 + 2 * ch];
+        // dL = Re(u dW), W = T A e^{i phase}
+        const double wr = tr * aer - ti * aei, wi = tr * aei + ti * aer;
+        dA += u_.re * (tr * er - ti * ei) - u_.im * (tr * ei + ti * er);
+        dP += -(u_.re * wi + u_.im * wr);
+        dT[2 * ch] = u_.re * aer - u_.im * aei;
+        dT[2 * ch + 1] = -(u_.re * aei + u_.im * aer);
+      }
+      const double a[8] = {dA, dP, dT[0], dT[1], dT[2], dT[3], dT[4], dT[5]};
+      const double u2 = u * u, u3 = u2 * u;
+#pragma unroll
+      for (int p = 0; p < 8; ++p) {
+        acc[4 * p] += a[p];
+        acc[4 * p + 1] += a[p] * u;
+        acc[4 * p + 2] += a[p] * u2;
+        acc[4 * p + 3] += a[p] * u3;
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 32; ++q) {
+      double v = acc[q];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      acc[q] = v;
+    }
+    if (lane == 0) {
+#pragma unroll
+      for (int p = 0; p < 8; ++p) {
+        const int slot = (p == 0) ? 0 : (p == 1 ? 1 : p + 1);  // skip t(f), slot 2
+        const size_t i = (size_t)slot * S.n + row * S.L + s;
+        ybd[i] = acc[4 * p];
+        cb1[i] = acc[4 * p + 1];
+        cb2[i] = acc[4 * p + 2];
+        cb3[i] = acc[4 * p + 3];
+      }
+    }
+  }
+}
+
+// 3. Adjoint of the not-a-knot spline build of k_spline (spline.cu) for the 9 rows of one
+// (binary, mode): inputs ybd, cb1..cb3 (entries s < L-1), output ybar (d lnL / d y).
+// Forward: m_i = (y_{i+1} - y_i) / h_i; K s = r(m); c1 = s_i, t = (s_i + s_{i+1} - 2 m_i) / h_i,
+// c2 = (m_i - s_i) / h_i - t, c3 = t / h_i.  Shared memory: x, a, b, c, d[9][L].
+__global__ void k_spline_adj(double* ybar, const double* ybd, const double* cb1,
+                             const double* cb2, const double* cb3, SplineRefs S, int b0, int nb) {
+  extern __shared__ double sm[];
+  const int L = S.L;
+  double* xs = sm;
+  double* a = xs + L;
+  double* bb = a + L;
+  double* c = bb + L;
+  double* d = c + L;
+  const int nsys = nb * S.M;
+  for (int sys = blockIdx.x; sys < nsys; sys += gridDim.x) {
+    const size_t row = (size_t)b0 * S.M + sys;
+    for (int i = threadIdx.x; i < L; i += blockDim.x) xs[i] = S.x[row * L + i];
+    __syncthreads();
+    // transposed matrix of the forward rows: a'_i = c_{i-1}, b'_i = b_i, c'_i = a_{i+1}
+    for (int i = threadIdx.x; i < L; i += blockDim.x) {
+      auto fwd = [&](int r, double* fa, double* fb, double* fc) {
+        if (r == 0) {
+          *fa = 0.0; *fb = xs[2] - xs[1]; *fc = xs[2] - xs[0];
+        } else if (r == L - 1) {
+          *fa = xs[L - 1] - xs[L - 3]; *fb = xs[L - 2] - xs[L - 3]; *fc = 0.0;
+        } else {
+          *fa = xs[r + 1] - xs[r]; *fb = 2 * ((xs[r] - xs[r - 1]) + (xs[r + 1] - xs[r]));
+          *fc = xs[r] - xs[r - 1];
+        }
+      };
+      double ta, tb, tc, pa, pb, pc, na, nb_, nc;
+      fwd(i, &ta, &tb, &tc);
+      if (i > 0) fwd(i - 1, &pa, &pb, &pc); else pc = 0.0;
+      if (i < L - 1) fwd(i + 1, &na, &nb_, &nc); else na = 0.0;
+      a[i] = (i > 0) ? pc : 0.0;
+      bb[i] = tb;
+      c[i] = (i < L - 1) ? na : 0.0;
+      // right-hand sides: s_bar from the coefficient adjoints
+      for (int p = 0; p < 9; ++p) {
+        double sb = 0.0;
+        if (p != 2) {
+          const size_t o = (size_t)p * S.n + row * L;
+          if (i < L - 1) {
+            const double h = xs[i + 1] - xs[i];
+            const double tbar = -cb2[o + i] + cb3[o + i] / h;
+            sb += cb1[o + i] - cb2[o + i] / h + tbar / h;
+          }
+          if (i > 0) {
+            const double h = xs[i] - xs[i - 1];
+            const double tbar = -cb2[o + i - 1] + cb3[o + i - 1] / h;
+            sb += tbar / h;
+          }
+        }
+        d[(size_t)p * L + i] = sb;
+      }
+    }
+    __syncthreads();
+    cr_solve(a, bb, c, d, L, 9, L);  // lambda = K^{-T} s_bar (r_bar)
+    // m_bar_i (i < L-1) and y_bar
+    for (int i = threadIdx.x; i < L; i += blockDim.x) {
+      for (int p = 0; p < 9; ++p) {
+        const size_t o = (size_t)p * S.n + row * L;
+        if (p == 2) {
+          ybar[o + i] = 0.0;
+          continue;
+        }
+        const double* lam = d + (size_t)p * L;
+        auto mbar = [&](int j) -> double {  // d lnL / d m_j, j in [0, L-2]
+          const double h = xs[j + 1] - xs[j];
+          const double tbar = -cb2[o + j] + cb3[o + j] / h;
+          double v = (cb2[o + j] - 2.0 * tbar) / h;
+          // interior rows r = 1..L-2: r_r = 3 (h_r m_{r-1} + h_{r-1} m_r)
+          if (j >= 1 && j <= L - 2) v += 3.0 * lam[j] * (xs[j] - xs[j - 1]);
+          if (j + 1 <= L - 2) v += 3.0 * lam[j + 1] * (xs[j + 2] - xs[j + 1]);
+          // row 0: r_0 = ((h0 + 2 d0) h1 m_0 + h0^2 m_1) / d0
+          const double h0 = xs[1] - xs[0], h1 = xs[2] - xs[1], d0 = xs[2] - xs[0];
+          if (j == 0) v += lam[0] * (h0 + 2 * d0) * h1 / d0;
+          if (j == 1) v += lam[0] * h0 * h0 / d0;
+          // row L-1: r = (h_{L-2}^2 m_{L-3} + (2 dL + h_{L-2}) h_{L-3} m_{L-2}) / dL
+          const double hl = xs[L - 1] - xs[L - 2], hp = xs[L - 2] - xs[L - 3];
+          const double dL = xs[L - 1] - xs[L - 3];
+          if (j == L - 3) v += lam[L - 1] * hl * hl / dL;
+          if (j == L - 2) v += lam[L - 1] * (2 * dL + hl) * hp / dL;
+          return v;
+        };
+        double yb = (i < L - 1) ? ybd[o + i] : 0.0;
+        if (i < L - 1) yb -= mbar(i) / (xs[i + 1] - xs[i]);
+        if (i > 0) yb += mbar(i - 1) / (xs[i] - xs[i - 1]);
+        ybar[o + i] = yb;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace bbhx
+
+using namespace bbhx;
+
+namespace {
+constexpr long long kGhBudget = 1ll << 29;  // complex entries of d lnL / d h per batch (8 GB)
+constexpr int kDirectGradChunk = 512;
+}  // namespace
+
+extern "C" {
+
+// d lnL / d theta [B, 11] of the direct likelihood (no reference counterpart).  Inputs are
+// the forward path's sparse buffer y and its spline coefficients c1..c3 ([9, B, M, L]), the
+// knots x [B, M, L], the noise-weighted data [3, N] (complex128) and noise weights [3, N],
+// params [12, B] (device) and the QNM table for the dual-number setup.  The host reads the
+// support lengths once (one synchronisation).
+int bbhx_direct_like_grad(void* orbits, double* grad, const double* params, const int* ells,
+                          const int* mms, const double* qnm_table, int qnm_n, double dspin,
+                          double t_init, const double* data_freqs, const void* data,
+                          const double* noise, int data_length, const double* x, const double* y,
+                          const double* c1, const double* c2, const double* c3,
+                          const double* t_start, const double* t_end, int TDItag, int rescaled,
+                          int tdi2, int run_phenomd, int num_modes, int length, int num_bin_all,
+                          void* stream) {
+  BBHX_REQUIRE(orbits && ((OrbitHandle*)orbits)->ready, "orbit information not added");
+  BBHX_REQUIRE(TDItag == 1 || TDItag == 2, "TDItag must be 1 (XYZ) or 2 (AET)");
+  BBHX_REQUIRE(num_modes > 0 && num_modes <= MAX_MODES, "num_modes must be 1..6");
+  BBHX_REQUIRE(length >= 4 && length <= 2048, "gradient spline length must be 4..2048");
+  BBHX_REQUIRE(qnm_n >= 2 && dspin > 0.0, "bad QNM table");
+  if (num_bin_all == 0) return OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int B = num_bin_all, M = num_modes, L = length;
+  SplineRefs S{x, y, c1, c2, c3, (size_t)B * M * L, M, L};
+  int *start = nullptr, *len = nullptr;
+  int st = OK;
+  BBHX_CHECK_CUDA(pool_alloc((void**)&start, sizeof(int) * 2 * (size_t)B, s));
+  len = start + B;
+  st = bbhx_template_support(start, len, x, M, L, B, data_freqs, data_length, stream);
+  std::vector<int> hlen(B);
+  if (!st) {
+    if (cudaMemcpyAsync(hlen.data(), len, sizeof(int) * B, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+      set_error("reading the template supports failed");
+      st = ERR_CUDA;
+    }
+  }
+  // adjoint arrays over all binaries, dual records and d lnL / d h per batch
+  const size_t nall = (size_t)9 * B * M * L;
+  double *ybd = nullptr, *cb = nullptr, *ybar = nullptr;
+  ModeCoeffsT<GD>* cD = nullptr;
+  ResponseModeT<GD>* rD = nullptr;
+  const int chunk = std::min(B, kDirectGradChunk);
+  if (!st) {
+    if (pool_alloc((void**)&ybd, sizeof(double) * nall * 5, s) != cudaSuccess ||
+        pool_alloc((void**)&cD, sizeof(ModeCoeffsT<GD>) * (size_t)chunk * M, s) != cudaSuccess ||
+        pool_alloc((void**)&rD, sizeof(ResponseModeT<GD>) * (size_t)chunk * M, s) != cudaSuccess) {
+      set_error("device allocation of the gradient scratch failed");
+      st = ERR_CUDA;
+    }
+  }
+  if (!st) {
+    cb = ybd + nall;  // cb1, cb2, cb3
+    ybar = cb + 3 * nall;
+    if (cudaMemsetAsync(ybd, 0, sizeof(double) * nall * 4, s) != cudaSuccess) {
+      set_error("cudaMemsetAsync failed");
+      st = ERR_CUDA;
+    }
+  }
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const size_t smem = sizeof(double) * (size_t)(4 + 9) * L;
+  if (!st && cudaFuncSetAttribute(k_spline_adj, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem) != cudaSuccess) {
+    set_error("cudaFuncSetAttribute failed for k_spline_adj");
+    st = ERR_CUDA;
+  }
+  for (int b0 = 0; !st && b0 < B;) {
+    // batch: at most `chunk` binaries and kGhBudget complex entries of d lnL / d h
+    std::vector<long long> hoff;
+    long long tot = 0;
+    int nb = 0;
+    while (b0 + nb < B && nb < chunk && (nb == 0 || tot + 3ll * hlen[b0 + nb] <= kGhBudget)) {
+      hoff.push_back(tot / 3);
+      tot += 3ll * hlen[b0 + nb];
+      ++nb;
+    }
+    int maxlen = 1;
+    for (int q = 0; q < nb; ++q) maxlen = std::max(maxlen, hlen[b0 + q]);
+    long long* off = nullptr;
+    cplx* gh = nullptr;
+    if (pool_alloc((void**)&off, sizeof(long long) * nb, s) != cudaSuccess ||
+        pool_alloc((void**)&gh, sizeof(cplx) * std::max(tot, 3ll), s) != cudaSuccess) {
+      set_error("device allocation of d lnL / d h failed");
+      st = ERR_CUDA;
+    }
+    if (!st && cudaMemcpyAsync(off, hoff.data(), sizeof(long long) * nb, cudaMemcpyHostToDevice,
+                               s) != cudaSuccess) {
+      set_error("copy of the support offsets failed");
+      st = ERR_CUDA;
+    }
+    if (!st) {
+      const int gx = std::min((maxlen + 255) / 256, std::max(1, nsm * 32 / nb));
+      k_adj_gh<<<dim3(gx, nb), 256, 0, s>>>(gh, off, start, len, S, data_freqs, (const cplx*)data,
+                                            noise, data_length, t_start, t_end, b0, nb);
+      st = launch_status("k_adj_gh");
+    }
+    if (!st) {
+      const long long warps = (long long)nb * M * (L - 1);
+      const unsigned grid = (unsigned)std::min<long long>((warps + 7) / 8, (long long)nsm * 64);
+      k_adj_coeffs<<<grid, 256, 0, s>>>(ybd, cb, cb + nall, cb + 2 * nall, gh, off, start, len, S,
+                                        data_freqs, data_length, t_start, t_end, b0, nb);
+      st = launch_status("k_adj_coeffs");
+    }
+    if (!st) {
+      k_spline_adj<<<(unsigned)std::min(nb * M, nsm * 4), 256, smem, s>>>(ybar, ybd, cb, cb + nall,
+                                                                         cb + 2 * nall, S, b0, nb);
+      st = launch_status("k_spline_adj");
+    }
+    if (!st) {
+      k_grad_setup<<<grid_for((long long)nb * M, 64), 64, 0, s>>>(cD, rD, params, B, b0, nb, ells,
+                                                                  mms, M, qnm_table, qnm_n, dspin,
+                                                                  run_phenomd);
+      st = launch_status("k_grad_setup");
+    }
+    if (!st) {
+      k_contract_direct<<<(unsigned)std::min(nb, nsm * 8), 128, 0, s>>>(
+          grad, cD, rD, ((OrbitHandle*)orbits)->tab, params, B, b0, nb, t_init, x, ybar, TDItag,
+          rescaled, tdi2, M, L);
+      st = launch_status("k_contract_direct");
+    }
+    if (gh) cudaFreeAsync(gh, s);
+    if (off) cudaFreeAsync(off, s);
+    b0 += nb;
+  }
+  if (rD) cudaFreeAsync(rD, s);
+  if (cD) cudaFreeAsync(cD, s);
+  if (ybd) cudaFreeAsync(ybd, s);
+  if (start) cudaFreeAsync(start, s);
+  return st;
+}
+
+}  // extern "C"

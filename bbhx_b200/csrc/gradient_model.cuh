@@ -165,4 +165,47 @@ static __global__ void k_contract_het(double* grad, const ModeCoeffsT<GD>* coeff
   }
 }
 
+// Direct-likelihood contraction at the spline knots: grad[b] = sum_{mode, i} sum_p
+// ybar[p, b, m, i] d q_p / d theta, with q_p the sparse-grid quantities of the [9, B, M, L]
+// buffer (amplitude, phase with t_ref shift and Roemer delay, the six transfer components;
+// t(f), p = 2, only gates).  Knots x [B, M, L] are held fixed.
+static __global__ void k_contract_direct(double* grad, const ModeCoeffsT<GD>* coeffs,
+                                         const ResponseModeT<GD>* rmodes, OrbitTables orb,
+                                         const double* P, int B, int b0, int nb, double t_init,
+                                         const double* x, const double* ybar, int TDItag,
+                                         int rescaled, int tdi2, int M, int L) {
+  const size_t n = (size_t)B * M * L;
+  for (int bl = blockIdx.x; bl < nb; bl += gridDim.x) {
+    const int b = b0 + bl;
+    const GD t_ref = seed(P[11 * (size_t)B + b], 10);
+    double acc[NGRAD];
+#pragma unroll
+    for (int k = 0; k < NGRAD; ++k) acc[k] = 0.0;
+    for (int p = threadIdx.x; p < M * L; p += blockDim.x) {
+      const int m = p / L;
+      const size_t o = ((size_t)b * M + m) * L + (p % L);
+      const double w0 = ybar[o], w1 = ybar[n + o];
+      double wt[6];
+      bool any = (w0 != 0.0) || (w1 != 0.0);
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        wt[q] = ybar[(size_t)(3 + q) * n + o];
+        any = any || (wt[q] != 0.0);
+      }
+      if (!any) continue;
+      const PointTangents pt = point_tangents(coeffs[(size_t)bl * M + m], rmodes[(size_t)bl * M + m],
+                                              orb, x[o], t_ref, t_init, TDItag, rescaled, tdi2);
+#pragma unroll
+      for (int k = 0; k < NGRAD; ++k) {
+        double v = w0 * pt.amp.d[k] + w1 * pt.phase.d[k];
+#pragma unroll
+        for (int ch = 0; ch < 3; ++ch)
+          v += wt[2 * ch] * pt.T[ch].re.d[k] + wt[2 * ch + 1] * pt.T[ch].im.d[k];
+        acc[k] += v;
+      }
+    }
+    block_reduce_grad(acc, grad + (size_t)b * NGRAD);
+  }
+}
+
 }  // namespace bbhx

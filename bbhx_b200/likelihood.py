@@ -89,6 +89,35 @@ class Likelihood:
         return ll
 
 
+    # ------------------------------------------------------------------ gradients
+    def _device_ll(self, params, kw):
+        rows = tuple(params[k].contiguous() for k in range(12))
+        kw = {k: v for k, v in kw.items() if k in ("t_obs_start", "t_obs_end", "length", "modes")}
+        d_h, h_h = self.waveform_gen.inner_products(rows, self.data_freqs, self.data_channels,
+                                                    self.noise_factors, precision="fp64", **kw)
+        return -0.5 * (self.d_d + h_h.real - 2 * d_h.real)
+
+    def get_ll_and_grad(self, params, **waveform_kwargs):
+        """lnL [B] and d lnL / d theta [B, 11] (device tensors); theta = (m1, m2, chi1z,
+        chi2z, distance, phi_ref, inc, lam, beta, psi, t_ref).  FP64, plain lnL; the sparse
+        knots are held fixed in the derivative."""
+        from .autodiff import as_param_tensor
+
+        P = as_param_tensor(params)
+        kw = {k: v for k, v in waveform_kwargs.items()
+              if k in ("t_obs_start", "t_obs_end", "length", "modes")}
+        d_h, h_h, grad = self.waveform_gen.direct_grad(P, self.data_freqs, self.data_channels,
+                                                       self.noise_factors, **kw)
+        return -0.5 * (self.d_d + h_h.real - 2 * d_h.real), grad
+
+    def loglike_torch(self, params, **waveform_kwargs):
+        """Differentiable lnL [B] tensor; the backward pass runs the gradient kernels."""
+        from .autodiff import as_param_tensor, function
+
+        P = params if (hasattr(params, "requires_grad") and params.requires_grad) else as_param_tensor(params)
+        return function("direct").apply(P, self, dict(waveform_kwargs))
+
+
 class HeterodynedLikelihood:
     """Heterodyned (relative-binning) log-likelihood.  ``precision`` selects the fused kernel
     that evaluates the walkers: "fp64" (default) or "mixed" (FP64 phase, t(f), Roemer delay,

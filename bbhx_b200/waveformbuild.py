@@ -310,6 +310,32 @@ class BBHWaveformFD:
                   int(rg.tdi2), int(ap.run_phenomd), M, L, B, _lib.stream())
         return d_h, h_h, grad
 
+    def direct_grad(self, params, data_freqs, data_weighted, noise_factors, t_obs_start=0.0,
+                    t_obs_end=1.0, length=1024, modes=None, **unused):
+        """<d|h>, <h|h> [B] and d lnL / d theta [B, 11] for a [12, B] device parameter tensor
+        (theta: rows 0-5, 7-11).  Forward as inner_products (FP64), then the gradient chain."""
+        t = torch()
+        P = params.to(device=device(), dtype=t.float64).contiguous()
+        rows = tuple(P[k] for k in range(12))
+        d_h, h_h = self.inner_products(rows, data_freqs, data_weighted, noise_factors,
+                                       t_obs_start=t_obs_start, t_obs_end=t_obs_end,
+                                       length=length, modes=modes, precision="fp64")
+        ap, rg = self.amp_phase_gen, self.response_gen
+        B, M, L = self.num_bin_all, self.num_modes, self.length
+        grad = t.empty((B, 11), dtype=t.float64, device=device())
+        tab = ap.qnm_table
+        from .waveforms.ringdownphenomd import dspin
+        buf, c1, c2, c3, x, ts, te = self._last_spline
+        _lib.call("bbhx_direct_like_grad", rg.orbit_handle.ptr, _lib.dptr(grad), _lib.dptr(P),
+                  _lib.dptr(ap.ells), _lib.dptr(ap.mms), _lib.dptr(tab), int(tab.shape[1]),
+                  float(dspin), float(ap.initial_t_val), _lib.dptr(data_freqs),
+                  _lib.dptr(data_weighted), _lib.dptr(noise_factors), int(data_freqs.numel()),
+                  _lib.dptr(x), _lib.dptr(buf), _lib.dptr(c1), _lib.dptr(c2), _lib.dptr(c3),
+                  _lib.dptr(ts), _lib.dptr(te), rg.TDItag_int, int(rg.rescaled), int(rg.tdi2),
+                  int(ap.run_phenomd), M, L, B, _lib.stream())
+        self._last_spline = None
+        return d_h, h_h, grad
+
     def inner_products(self, params, data_freqs, data_weighted, noise_factors, t_obs_start=0.0,
                        t_obs_end=1.0, length=1024, modes=None, flags=None, timing=None,
                        precision="fp64", **unused):
@@ -345,4 +371,5 @@ class BBHWaveformFD:
             ev1.record()
             timing.setdefault("fused", []).append((ev0, ev1))
             self._last_x = x
+        self._last_spline = (buf, c1, c2, c3, x, ts_d, te_d)
         return d_h, h_h

@@ -210,6 +210,21 @@ int bbhx_hdyn_grad(void *orbits, void *d_h, void *h_h, double *grad, const void 
                    int TDItag, int rescaled, int tdi2, int run_phenomd, int num_modes, int length,
                    int num_bin_all, void *stream);
 
+/* Gradient d lnL / d theta [B, 11] of the direct likelihood (no reference counterpart):
+   reverse through the <d|h>, <h|h> reduction, the spline interpolation onto the data grid
+   and the not-a-knot spline build (transposed tridiagonal solve), forward-mode tangents of
+   PhenomHM + TDI at the knots.  x [B, M, L] knots; y, c1, c2, c3 [9, B, M, L] from the forward
+   path (bbhx_waveform_response_fused + bbhx_interpolate); data [3, N] complex128 noise-weighted,
+   noise [3, N]; params [12, B]; theta as for bbhx_hdyn_grad.  Knots are held fixed. */
+int bbhx_direct_like_grad(void *orbits, double *grad, const double *params, const int *ells,
+                          const int *mms, const double *qnm_table, int qnm_n, double dspin,
+                          double t_init, const double *data_freqs, const void *data,
+                          const double *noise, int data_length, const double *x, const double *y,
+                          const double *c1, const double *c2, const double *c3,
+                          const double *t_start, const double *t_end, int TDItag, int rescaled,
+                          int tdi2, int run_phenomd, int num_modes, int length, int num_bin_all,
+                          void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -84,3 +84,43 @@ def test_heterodyned_autograd_backward(golden, golden_data):
     expect[list(ROWS)] = (grad.cpu().numpy() * w.cpu().numpy()[:, None]).T
     np.testing.assert_allclose(x.grad.cpu().numpy(), expect, rtol=1e-12, atol=0)
     assert np.all(x.grad.cpu().numpy()[6] == 0.0)
+
+
+def _direct_setup(golden, golden_data, center_index):
+    from bbhx_b200 import BBHWaveformFD, EqualArmlengthOrbits, Likelihood
+    from bbhx_b200.synthetic import perturb_params
+
+    wave = BBHWaveformFD(amp_phase_kwargs=dict(run_phenomd=False),
+                         response_kwargs=dict(orbits=EqualArmlengthOrbits(), TDItag="AET", tdi2=True))
+    kw = dict(t_obs_start=0.0, t_obs_end=golden_data["tobs"], length=1024)
+    center = golden["params"][:, center_index].copy()
+    inj = wave(*[np.atleast_1d(v) for v in center], freqs=golden_data["f"], fill=True, direct=False,
+               **kw)[0].cpu().numpy()
+    like = Likelihood(wave, golden_data["f"], inj + golden_data["data"], golden_data["psd"])
+    P = perturb_params(center, 3, 29, rel_mass=1e-4, abs_spin_angle=1e-3, t_ref_s=1.0)
+    return like, kw, P
+
+
+@pytest.mark.parametrize("center_index", [0, 2])
+def test_direct_gradient_matches_central_fd(golden, golden_data, center_index):
+    like, kw, P = _direct_setup(golden, golden_data, center_index)
+    ll, grad = like.get_ll_and_grad(P, **kw)
+    ll = ll.cpu().numpy()
+    grad = grad.cpu().numpy()
+    np.testing.assert_allclose(ll, like.get_ll(P, **kw), rtol=1e-12, atol=1e-8)
+    fd = _central_fd(lambda Q: like.get_ll(Q, **kw), P)
+    print("grad", grad[0], "\nfd  ", fd[0])
+    _check(grad, fd, P)
+
+
+def test_direct_autograd_backward(golden, golden_data):
+    import torch
+
+    like, kw, P = _direct_setup(golden, golden_data, 2)
+    x = torch.tensor(P, dtype=torch.float64, device="cuda", requires_grad=True)
+    ll = like.loglike_torch(x, **kw)
+    ll.sum().backward()
+    _, grad = like.get_ll_and_grad(P, **kw)
+    expect = np.zeros((12, P.shape[1]))
+    expect[list(ROWS)] = grad.cpu().numpy().T
+    np.testing.assert_allclose(x.grad.cpu().numpy(), expect, rtol=1e-12, atol=0)
