@@ -52,7 +52,32 @@ def parse():
     ap.add_argument("--no-extra", action="store_true", help="skip the heterodyned metric")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--het-batch", type=int, default=65536)
+    ap.add_argument("--grad-batch", type=int, default=4096)
+    ap.add_argument("--no-grad", action="store_true", help="skip the gradient metric")
     return ap.parse_args()
+
+
+def shard_seed(rank):
+    """Seed of rank's binaries: every rank evaluates its own batch (weak scaling, no
+    data-path collective; binaries are independent)."""
+    return SEED_PARAMS + 1000 * rank
+
+
+def max_over_ranks(value, world, device="cuda"):
+    """Max of a per-rank float over all ranks (device-timed numbers use the slowest rank)."""
+    if world <= 1:
+        return float(value)
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(units_per_rank, world, ms):
+    """Whole-job throughput: units processed by all ranks / the max-over-ranks time."""
+    return units_per_rank * world / (ms / 1e3)
 
 
 def rank_info():
@@ -167,17 +192,23 @@ def ncu_traffic_per_pair():
         return None
 
 
+def make_wave():
+    from bbhx_b200 import BBHWaveformFD, EqualArmlengthOrbits
+
+    return BBHWaveformFD(response_kwargs=dict(orbits=EqualArmlengthOrbits(), TDItag="AET", tdi2=True))
+
+
 def build_problem(B, seed_params=SEED_PARAMS):
     import torch
 
-    from bbhx_b200 import BBHWaveformFD, EqualArmlengthOrbits, Likelihood
+    from bbhx_b200 import Likelihood
     from bbhx_b200.sensitivity import aet_psd
     from bbhx_b200.synthetic import data_grid, draw_params, gaussian_noise, notch_tdi_zeros
 
     f = data_grid(TOBS, F_LO, F_HI)
     df = f[1] - f[0]
     psd = notch_tdi_zeros(f, np.array([aet_psd(f, c, tdi2=True) for c in "AET"]))
-    wave = BBHWaveformFD(response_kwargs=dict(orbits=EqualArmlengthOrbits(), TDItag="AET", tdi2=True))
+    wave = make_wave()
     inj = draw_params(1, TOBS, seed_params + 7)
     h = wave(*inj, freqs=f, length=LENGTH, t_obs_start=0.0, t_obs_end=TOBS, direct=False,
              fill=True, combine=True)
@@ -207,7 +238,7 @@ def gpu_arm(args):
 
     build_ext.build()
     B = args.batch
-    wave, like, params, f = build_problem(B, SEED_PARAMS + 1000 * rank)
+    wave, like, params, f = build_problem(B, shard_seed(rank))
     dev_params = tuple(torch.as_tensor(params[k], device="cuda") for k in range(12))
     kw = dict(length=LENGTH, t_obs_start=0.0, t_obs_end=TOBS)
     flags = torch.zeros(3, dtype=torch.int32, device="cuda")
@@ -263,22 +294,12 @@ def gpu_arm(args):
     clocks = sampler.stop() if sampler else None
     ms_total = e0.elapsed_time(e1)
     fused_ms = [a.elapsed_time(b) for a, b in timing["fused"]]
-    ms = torch.tensor([ms_total], device="cuda", dtype=torch.float64)
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.all_reduce(ms, op=dist.ReduceOp.MAX)
-    ms_total = float(ms.item())
+    ms_total = max_over_ranks(ms_total, world)
     lnl = out.cpu().numpy()
     lnl64 = out64.cpu().numpy()
     assert np.all(np.isfinite(lnl)) and np.all(np.isfinite(lnl64)), "non-finite lnL"
     dl_mixed = np.abs(lnl - lnl64)
-    fp64_ms_t = torch.tensor([fp64_ms], device="cuda", dtype=torch.float64)
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.all_reduce(fp64_ms_t, op=dist.ReduceOp.MAX)
-    fp64_ms = float(fp64_ms_t.item())
+    fp64_ms = max_over_ranks(fp64_ms, world)
 
     # support sizes (sum of per-binary data-grid lengths) for the roofline
     from bbhx_b200 import _lib
@@ -303,17 +324,14 @@ def gpu_arm(args):
         ll_host = like.get_ll(host, **kw)
     t1.record()
     torch.cuda.synchronize()
-    e2e_ms = torch.tensor([t0.elapsed_time(t1)], device="cuda", dtype=torch.float64)
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.all_reduce(e2e_ms, op=dist.ReduceOp.MAX)
-    e2e_ms = float(e2e_ms.item())
+    e2e_ms = max_over_ranks(t0.elapsed_time(t1), world)
     dl = float(np.max(np.abs(ll_host - lnl)))
 
     extra = {}
     if not args.no_extra:
         extra.update(het_metric(args, wave, like, f, params))
+        if not args.no_grad:
+            extra.update(grad_metric(args))
     if world > 1:
         import torch.distributed as dist
 
@@ -328,7 +346,7 @@ def gpu_arm(args):
     n_evals = B * args.steps * world
     res = {
         "metric": "lnL evals/s (direct, heterodyned) mixed vs FP64 plain at |dlnL|<=1e-2; grad/s",
-        "value": n_evals / (ms_total / 1e3),
+        "value": aggregate_rate(B * args.steps, world, ms_total),
         "unit": "lnL evals/s",
         "n_gpus": world,
         "steps": args.steps,
@@ -339,7 +357,7 @@ def gpu_arm(args):
         "vs_baseline": None,
         "dtype": "mixed: f64 phase/t(f)/accumulation, f32 amplitude/transfer/products",
         "data": "synthetic: seeded PhenomHM injection + Gaussian noise from the analytic A/E/T PSD",
-        "fp64_plain": {"value": n_evals / (fp64_ms / 1e3), "unit": "lnL evals/s",
+        "fp64_plain": {"value": aggregate_rate(B * args.steps, world, fp64_ms), "unit": "lnL evals/s",
                        "ms_per_step": fp64_ms / args.steps,
                        "kernel_ms": statistics.mean(a.elapsed_time(b) for a, b in fp64_timing["fused"])},
         "dlnl_mixed_vs_fp64": {"max": float(dl_mixed.max()), "p99": float(np.percentile(dl_mixed, 99)),
@@ -352,7 +370,7 @@ def gpu_arm(args):
                    "binary_bin_pairs_per_step": pairs,
                    "l2": "inputs larger than L2 (data 227 MB + sparse buffers 1.8 GB per step)",
                    "parallelism": f"replicas x{world} (independent binary batches per GPU)"},
-        "e2e": {"value": n_evals / (e2e_ms / 1e3), "unit": "lnL evals/s",
+        "e2e": {"value": aggregate_rate(B * args.steps, world, e2e_ms), "unit": "lnL evals/s",
                 "h2d_bytes_per_step": 12 * B * 8, "d2h_bytes_per_step": 3 * B * 8 + 3 * 8,
                 "max_abs_dlnl_vs_device_path": dl},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -422,6 +440,62 @@ def het_metric(args, wave, like, f, params):
         "lnl_range": [float(ll64.min()), float(ll64.max())],
         "path": "HeterodynedLikelihood.get_ll with device-resident walkers",
         "finite": bool(np.all(np.isfinite(ll64)) and np.all(np.isfinite(llmx)))}}
+
+
+def grad_metric(args):
+    """Gradient evals/s (d lnL / d theta, 11 parameters, FP64) and peak device memory:
+    direct lnL for B = 4096 binaries at Tobs = 0.25 yr (df = 1/Tobs over 1e-5..0.1 Hz), and
+    heterodyned lnL for B = 65536 walkers (128 bins) around the injection.  Each gradient call
+    recomputes the waveform (nothing is kept from the lnL evaluation)."""
+    import torch
+
+    from bbhx_b200 import AET1SensitivityMatrix, HeterodynedLikelihood, Likelihood
+    from bbhx_b200.sensitivity import aet_psd
+    from bbhx_b200.synthetic import (data_grid, draw_params, gaussian_noise, notch_tdi_zeros,
+                                     perturb_params)
+
+    tobs = 0.25
+    f = data_grid(tobs, F_LO, F_HI)
+    df = f[1] - f[0]
+    psd = notch_tdi_zeros(f, np.array([aet_psd(f, c, tdi2=True) for c in "AET"]))
+    wave = make_wave()
+    P = draw_params(args.grad_batch, tobs, SEED_PARAMS + 7)
+    center = P[:, 0]
+    kw = dict(t_obs_start=0.0, t_obs_end=tobs, length=LENGTH)
+    inj = wave(*[np.atleast_1d(v) for v in center], freqs=f, fill=True, direct=False, **kw)[0]
+    data = inj.cpu().numpy() + gaussian_noise(psd, df, SEED_NOISE + 7)
+    like = Likelihood(wave, f, data, psd)
+    Pd = torch.as_tensor(P, device="cuda")
+
+    def timed(fn, n):
+        fn()
+        torch.cuda.synchronize()
+        torch.cuda.reset_peak_memory_stats()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(n):
+            out = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3 / n, torch.cuda.max_memory_allocated() / 1e9, out
+
+    sd, memd, (_, gd) = timed(lambda: like.get_ll_and_grad(Pd, **kw), 2)
+    het = HeterodynedLikelihood(wave, f, data, center, 128,
+                                template_gen_kwargs=dict(t_obs_start=0.0, t_obs_end=tobs),
+                                reference_gen_kwargs=dict(kw),
+                                sens_mat=AET1SensitivityMatrix(f, tdi2=True, notch=True))
+    W = torch.as_tensor(perturb_params(center, args.het_batch, 3), device="cuda")
+    sh, memh, (_, gh) = timed(lambda: het.get_ll_and_grad(W, t_obs_start=0.0, t_obs_end=tobs), 3)
+    return {"gradients": {
+        "direct": {"value": args.grad_batch / sd, "unit": "grad evals/s", "batch": args.grad_batch,
+                   "data_bins": int(len(f)), "tobs_yr": tobs, "peak_mem_gb": memd,
+                   "finite": bool(torch.isfinite(gd).all().item())},
+        "heterodyned": {"value": args.het_batch / sh, "unit": "grad evals/s", "batch": args.het_batch,
+                        "bins": 128, "peak_mem_gb": memh,
+                        "finite": bool(torch.isfinite(gh).all().item())},
+        "parameters": "m1, m2, chi1z, chi2z, distance, phi_ref, inc, lam, beta, psi, t_ref",
+        "method": "adjoint of the reduction / spline chain + dual-number tangents of PhenomHM + TDI"}}
 
 
 def reference_arm(args):
