@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include "bbhx_common.cuh"
+#include "bbhx_b200.h"
 
 namespace bbhx {
 

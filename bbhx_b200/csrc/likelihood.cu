@@ -10,6 +10,8 @@
 //   noise-weights and reduces <d|h>, <h|h> without ever storing a template.
 //
 // Reductions are deterministic: per-(tile, binary) partials in FP64, then a fixed-order sum.
+#include <algorithm>
+#include <cstring>
 #include <type_traits>
 #include <vector>
 
@@ -201,8 +203,11 @@ struct FusedArgs {
   const int* sup_len;
   int B, M, L;
   int ntiles;
+  int tile;            // data bins per tile item (multiple of FD_WARP_BINS)
   double* partials;    // [ntiles * B][3]
   const int2* segtab;  // [ntiles][B][M]: segments of the tile's first and last bin
+  double* d_h;         // [B] complex outputs
+  double* h_h;
 };
 
 // Segment table: for every (tile, binary, mode) the spline segments holding the first and the
@@ -210,7 +215,7 @@ struct FusedArgs {
 // their frequencies), or (1, 0) when the tile misses the support.  One thread per entry.
 __global__ void k_tile_segments(int2* tab, const double* __restrict__ x,
                                 const double* __restrict__ data_freqs, const int* sup_start,
-                                const int* sup_len, int B, int M, int L, int ntiles) {
+                                const int* sup_len, int B, int M, int L, int ntiles, int tile_bins) {
   const long long n = (long long)ntiles * B * M;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
        t += (long long)gridDim.x * blockDim.x) {
@@ -219,7 +224,7 @@ __global__ void k_tile_segments(int2* tab, const double* __restrict__ x,
     const int b = (int)(tb % B);
     const int tile = (int)(tb / B);
     const int s0 = sup_start[b], s1 = s0 + sup_len[b];
-    const int i0 = max(tile * FD_TILE, s0), i1 = min((tile + 1) * FD_TILE, s1) - 1;
+    const int i0 = max(tile * tile_bins, s0), i1 = min((tile + 1) * tile_bins, s1) - 1;
     if (i0 > i1) {
       tab[t] = make_int2(1, 0);
       continue;
@@ -383,30 +388,23 @@ __device__ __forceinline__ void load_seg(SegCoef<R>& cf, const WarpStage<R>& S, 
 // lowest frequencies) take a per-lane walk over global memory instead.
 // MIXED: phase, t(f), the phase reduction and all accumulations in FP64; amplitude, transfer
 // functions, sin/cos of the reduced phase, the mode sum and the per-bin products in FP32.
-template <bool MIXED>
-__global__ void __launch_bounds__(FD_WARPS * 32, MIXED ? 4 : 3) k_direct_fused(FusedArgs A) {
-  using R = typename std::conditional<MIXED, float, double>::type;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int lane = threadIdx.x & 31;
-  const int warp = threadIdx.x >> 5;
-  WarpStage<R>& S = reinterpret_cast<WarpStage<R>*>(smem_raw)[warp];
-  const long long nitems = (long long)A.ntiles * A.B;
+template <bool MIXED, typename R>
+__device__ __forceinline__ void fused_item(const FusedArgs& A, long long q, WarpStage<R>& S,
+                                           int lane) {
   const long long BML = (long long)A.B * A.M * A.L;
   const int L = A.L;
-  const long long gw = (long long)blockIdx.x * FD_WARPS + warp;
-  const long long nw = (long long)gridDim.x * FD_WARPS;
-  for (long long q = gw; q < nitems; q += nw) {
+  {
     const int tile = (int)(q / A.B);
     const int b = (int)(q - (long long)tile * A.B);
     const int s0 = __ldg(A.sup_start + b);
     const int s1 = s0 + __ldg(A.sup_len + b);
-    const int t0 = tile * FD_TILE;
-    if (t0 >= s1 || t0 + FD_TILE <= s0) {
+    const int t0 = tile * A.tile;
+    if (t0 >= s1 || t0 + A.tile <= s0) {
       if (lane == 0) {
         double* P = A.partials + 3 * q;
         P[0] = 0.0; P[1] = 0.0; P[2] = 0.0;
       }
-      continue;
+      return;
     }
     // ---- stage this tile's segments for every mode
     if (lane < A.M) {
@@ -440,7 +438,7 @@ __global__ void __launch_bounds__(FD_WARPS * 32, MIXED ? 4 : 3) k_direct_fused(F
     __syncwarp();
     const double ts = __ldg(A.t_start + b), te = __ldg(A.t_end + b);
     double dr = 0.0, di = 0.0, hh = 0.0;
-    for (int ch0 = 0; ch0 < FD_TILE; ch0 += FD_WARP_BINS) {
+    for (int ch0 = 0; ch0 < A.tile; ch0 += FD_WARP_BINS) {
       const int c0 = t0 + ch0;
       if (c0 >= s1 || c0 + FD_WARP_BINS <= s0) continue;
       double fbin[FD_K];
@@ -560,6 +558,112 @@ __global__ void __launch_bounds__(FD_WARPS * 32, MIXED ? 4 : 3) k_direct_fused(F
       P[2] = hh;
     }
     __syncwarp();
+  }
+}
+
+template <bool MIXED>
+__global__ void __launch_bounds__(FD_WARPS * 32, MIXED ? 4 : 3) k_direct_fused(FusedArgs A) {
+  using R = typename std::conditional<MIXED, float, double>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  WarpStage<R>& S = reinterpret_cast<WarpStage<R>*>(smem_raw)[warp];
+  const long long nitems = (long long)A.ntiles * A.B;
+  const long long gw = (long long)blockIdx.x * FD_WARPS + warp;
+  const long long nw = (long long)gridDim.x * FD_WARPS;
+  for (long long q = gw; q < nitems; q += nw) fused_item<MIXED, R>(A, q, S, lane);
+}
+
+// Several independent problems (groups: own data stream, grid length L, mode count M,
+// binaries) in ONE persistent launch: the items of all groups form one global range that the
+// warps stride over; a warp copies the descriptor of its current group into shared memory
+// when it moves to another group.  Group descriptors and the item offsets are in device
+// memory (written by k_store_groups from kernel parameters, so no host copy is involved).
+constexpr int FD_MAXGROUPS = 64;
+struct MultiArgs {
+  FusedArgs g[FD_MAXGROUPS];
+  long long off[FD_MAXGROUPS + 1];   // item offsets; off[ngroups] = total items
+  long long boff[FD_MAXGROUPS + 1];  // binary offsets; boff[ngroups] = total binaries
+  int ngroups;
+};
+
+__global__ void k_store_groups(MultiArgs M, MultiArgs* dst) {
+  const int n = (int)(sizeof(MultiArgs) / sizeof(unsigned long long));
+  const unsigned long long* src = reinterpret_cast<const unsigned long long*>(&M);
+  unsigned long long* d = reinterpret_cast<unsigned long long*>(dst);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) d[i] = src[i];
+}
+
+template <bool MIXED>
+__global__ void __launch_bounds__(FD_WARPS * 32, MIXED ? 4 : 3)
+    k_direct_fused_multi(const MultiArgs* __restrict__ MA) {
+  using R = typename std::conditional<MIXED, float, double>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ FusedArgs gcur[FD_WARPS];
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  WarpStage<R>& S = reinterpret_cast<WarpStage<R>*>(smem_raw)[warp];
+  const int ng = MA->ngroups;
+  const long long total = MA->off[ng];
+  const long long gw = (long long)blockIdx.x * FD_WARPS + warp;
+  const long long nw = (long long)gridDim.x * FD_WARPS;
+  int g = -1;
+  for (long long q = gw; q < total; q += nw) {
+    if (g < 0 || q >= MA->off[g + 1] || q < MA->off[g]) {
+      int lo = 0, hi = ng;  // last group with off <= q
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (MA->off[mid] <= q) lo = mid; else hi = mid;
+      }
+      g = lo;
+      __syncwarp();
+      const int nw8 = (int)(sizeof(FusedArgs) / sizeof(unsigned long long));
+      const unsigned long long* src = reinterpret_cast<const unsigned long long*>(&MA->g[g]);
+      unsigned long long* dst = reinterpret_cast<unsigned long long*>(&gcur[warp]);
+      for (int i = lane; i < nw8; i += 32) dst[i] = src[i];
+      __syncwarp();
+    }
+    fused_item<MIXED, R>(gcur[warp], q - MA->off[g], S, lane);
+  }
+}
+
+__global__ void k_fused_reduce_multi(const MultiArgs* __restrict__ MA) {
+  const long long* boff = MA->boff;
+  const int lane = threadIdx.x & 31;
+  const int wpb = blockDim.x >> 5;
+  const int ng = MA->ngroups;
+  const long long nb = boff[ng];
+  for (long long gb = blockIdx.x * (long long)wpb + (threadIdx.x >> 5); gb < nb;
+       gb += (long long)gridDim.x * wpb) {
+    int lo = 0, hi = ng;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (boff[mid] <= gb) lo = mid; else hi = mid;
+    }
+    const FusedArgs& A = MA->g[lo];
+    const int b = (int)(gb - boff[lo]);
+    double a = 0, c = 0, h = 0;
+    const int s0 = A.sup_start[b], n = A.sup_len[b];
+    if (n > 0) {
+      const int tlo = s0 / A.tile, thi = (s0 + n - 1) / A.tile;
+      for (int t = tlo + lane; t <= thi; t += 32) {
+        const double* P = A.partials + 3 * ((long long)t * A.B + b);
+        a += P[0];
+        c += P[1];
+        h += P[2];
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_xor_sync(0xffffffffu, a, o);
+      c += __shfl_xor_sync(0xffffffffu, c, o);
+      h += __shfl_xor_sync(0xffffffffu, h, o);
+    }
+    if (lane == 0) {
+      A.d_h[2 * b] = 4.0 * a;
+      A.d_h[2 * b + 1] = 4.0 * c;
+      A.h_h[2 * b] = 4.0 * h;
+      A.h_h[2 * b + 1] = 0.0;
+    }
   }
 }
 
@@ -685,6 +789,123 @@ int bbhx_template_support(int* start, int* len, const double* x, int num_modes, 
   return launch_status("k_support");
 }
 
+// Several direct-likelihood problems in one persistent launch of the fused kernel (see
+// k_direct_fused_multi).  groups: HOST array of descriptors (device pointers inside);
+// tile_bins: data bins per work item (multiple of 128); ctas_per_sm: persistent CTAs per SM.
+int bbhx_direct_like_multi(const bbhx_direct_group* groups, int num_groups, int precision,
+                           int tile_bins, int ctas_per_sm, void* stream) {
+  BBHX_REQUIRE(groups != nullptr && num_groups >= 1 && num_groups <= FD_MAXGROUPS,
+               "num_groups must be 1..%d", FD_MAXGROUPS);
+  BBHX_REQUIRE(precision == 0 || precision == 1, "precision must be 0 (FP64) or 1 (mixed)");
+  BBHX_REQUIRE(tile_bins >= FD_WARP_BINS && tile_bins <= 4096 && tile_bins % FD_WARP_BINS == 0,
+               "tile_bins must be a multiple of %d in [%d, 4096]", FD_WARP_BINS, FD_WARP_BINS);
+  BBHX_REQUIRE(ctas_per_sm >= 1 && ctas_per_sm <= 32, "ctas_per_sm must be 1..32");
+  cudaStream_t s = (cudaStream_t)stream;
+  MultiArgs MA;
+  memset(&MA, 0, sizeof(MA));
+  MA.ngroups = num_groups;
+  std::vector<void*> scratch;
+  int st = OK;
+  long long items = 0, bins = 0;
+  for (int g = 0; g < num_groups && !st; ++g) {
+    const bbhx_direct_group& G = groups[g];
+    if (G.num_bin_all < 0 || G.length < 2 || G.num_modes < 1 || G.num_modes > FD_MAXM ||
+        G.data_length < 1) {
+      set_error("group %d: bad sizes (B=%d M=%d L=%d N=%d)", g, G.num_bin_all, G.num_modes,
+                G.length, G.data_length);
+      st = ERR_BAD_ARG;
+      break;
+    }
+    FusedArgs& A = MA.g[g];
+    A.data_freqs = G.data_freqs;
+    A.data = (const cplx*)G.data;
+    A.noise = G.noise;
+    A.N = G.data_length;
+    A.x = G.x;
+    A.y = G.y;
+    A.c1 = G.c1;
+    A.c2 = G.c2;
+    A.c3 = G.c3;
+    A.t_start = G.t_start;
+    A.t_end = G.t_end;
+    A.B = G.num_bin_all;
+    A.M = G.num_modes;
+    A.L = G.length;
+    A.tile = tile_bins;
+    A.ntiles = (G.data_length + tile_bins - 1) / tile_bins;
+    A.d_h = (double*)G.d_h;
+    A.h_h = (double*)G.h_h;
+    MA.off[g] = items;
+    MA.boff[g] = bins;
+    const long long nit = (long long)A.ntiles * A.B;
+    items += nit;
+    bins += A.B;
+    if (A.B == 0) continue;
+    int* sup = nullptr;
+    double* part = nullptr;
+    int2* segtab = nullptr;
+    if (pool_alloc((void**)&sup, sizeof(int) * 2 * A.B, s) != cudaSuccess ||
+        pool_alloc((void**)&part, sizeof(double) * 3 * nit, s) != cudaSuccess ||
+        pool_alloc((void**)&segtab, sizeof(int2) * nit * A.M, s) != cudaSuccess) {
+      set_error("device allocation for group %d failed", g);
+      st = ERR_CUDA;
+    }
+    if (sup) scratch.push_back(sup);
+    if (part) scratch.push_back(part);
+    if (segtab) scratch.push_back(segtab);
+    if (st) break;
+    A.sup_start = sup;
+    A.sup_len = sup + A.B;
+    A.partials = part;
+    A.segtab = segtab;
+    k_support<<<A.B, 128, 0, s>>>(A.x, A.M, A.L, A.B, A.data_freqs, A.N, sup, sup + A.B);
+    st = launch_status("k_support");
+    if (!st) {
+      k_tile_segments<<<grid_for(nit * A.M, 256, 148 * 64), 256, 0, s>>>(
+          segtab, A.x, A.data_freqs, sup, sup + A.B, A.B, A.M, A.L, A.ntiles, tile_bins);
+      st = launch_status("k_tile_segments");
+    }
+  }
+  MA.off[num_groups] = items;
+  MA.boff[num_groups] = bins;
+  MultiArgs* dMA = nullptr;
+  if (!st) {
+    if (pool_alloc((void**)&dMA, sizeof(MultiArgs), s) != cudaSuccess) {
+      set_error("device allocation of the group table failed");
+      st = ERR_CUDA;
+    } else {
+      scratch.push_back(dMA);
+      k_store_groups<<<1, 256, 0, s>>>(MA, dMA);
+      st = launch_status("k_store_groups");
+    }
+  }
+  if (!st && items > 0) {
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const long long want = (items + FD_WARPS - 1) / FD_WARPS;
+    const unsigned grid = (unsigned)std::min<long long>(want, (long long)nsm * ctas_per_sm);
+    if (precision == 1) {
+      const size_t sm = sizeof(WarpStage<float>) * FD_WARPS;
+      BBHX_CHECK_CUDA(cudaFuncSetAttribute(k_direct_fused_multi<true>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      k_direct_fused_multi<true><<<grid, FD_WARPS * 32, sm, s>>>(dMA);
+    } else {
+      const size_t sm = sizeof(WarpStage<double>) * FD_WARPS;
+      BBHX_CHECK_CUDA(cudaFuncSetAttribute(k_direct_fused_multi<false>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      k_direct_fused_multi<false><<<grid, FD_WARPS * 32, sm, s>>>(dMA);
+    }
+    st = launch_status("k_direct_fused_multi");
+  }
+  if (!st && bins > 0) {
+    k_fused_reduce_multi<<<grid_for(32LL * bins, 128), 128, 0, s>>>(dMA);
+    st = launch_status("k_fused_reduce_multi");
+  }
+  for (void* p : scratch) cudaFreeAsync(p, s);
+  return st;
+}
+
 // Fused direct likelihood: d_h, h_h device complex128 [B] (overwritten, scaled by 4 like the
 // reference), data [3, N] noise-weighted complex128, noise [3, N] = sqrt(df / S).
 int bbhx_direct_like_fused(double* d_h, double* h_h, const double* data_freqs, const double* data,
@@ -710,7 +931,8 @@ int bbhx_direct_like_fused(double* d_h, double* h_h, const double* data_freqs, c
   int st = launch_status("k_support");
   if (!st) {
     k_tile_segments<<<grid_for(nitems * num_modes, 256, 148 * 64), 256, 0, s>>>(
-        segtab, x, data_freqs, sup, sup + num_bin_all, num_bin_all, num_modes, length, ntiles);
+        segtab, x, data_freqs, sup, sup + num_bin_all, num_bin_all, num_modes, length, ntiles,
+        FD_TILE);
     st = launch_status("k_tile_segments");
   }
   if (!st) {
@@ -732,8 +954,11 @@ int bbhx_direct_like_fused(double* d_h, double* h_h, const double* data_freqs, c
     A.M = num_modes;
     A.L = length;
     A.ntiles = ntiles;
+    A.tile = FD_TILE;
     A.partials = part;
     A.segtab = segtab;
+    A.d_h = d_h;
+    A.h_h = h_h;
     const long long warps_needed = (nitems + 0);
     long long g = (warps_needed + FD_WARPS - 1) / FD_WARPS;
     unsigned grid = (unsigned)(g < 148LL * 16 ? g : 148LL * 16);

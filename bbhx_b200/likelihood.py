@@ -225,12 +225,14 @@ class HeterodynedLikelihood:
         self.template_gen_kwargs = template_gen_kwargs
 
     # ------------------------------------------------------------------ gradients
-    def _fused_ll(self, params, kw, precision):
-        """lnL [B] (device) and the raw sums for a [12, B] device parameter tensor."""
+    def _fused_ll(self, params, kw, precision, flags=None):
+        """lnL [B] (device) and the raw sums for a [12, B] device parameter tensor; with a
+        device ``flags`` tensor the spin check is recorded there (no host synchronisation)."""
         rows = tuple(params[k].contiguous() for k in range(12))
         kw = {k: v for k, v in kw.items() if k in ("t_obs_start", "t_obs_end", "modes")}
         d_h, h_h = self.template_gen.heterodyne_sums(rows, self.freqs, self._h0_flat,
-                                                     self.data_constants, precision=precision, **kw)
+                                                     self.data_constants, precision=precision,
+                                                     flags=flags, **kw)
         return -0.5 * (self.reference_d_d + h_h.real - 2 * d_h.real), (d_h, h_h)
 
     def get_ll_and_grad(self, params, **waveform_kwargs):

@@ -1,0 +1,195 @@
+"""Uneven batches: many independent likelihood problems evaluated together.
+
+A batch holds
+  * direct groups — a ``Likelihood`` (its own data stream, hence its own observation span and
+    data grid), binaries ``params`` [12, n], a sparse-grid ``length`` and a mode set;
+  * heterodyned groups — a ``HeterodynedLikelihood`` (its own relative-binning grid of any
+    length) and walkers [12, n].
+``run()`` builds every group's sparse buffers and splines, then evaluates ALL direct groups in
+one persistent launch of the fused likelihood kernel (``bbhx_direct_like_multi``) and every
+heterodyned group with the fused heterodyne kernel.  Nothing in ``run()`` synchronises with the
+host, so ``capture()`` records it once in a CUDA graph and ``replay()`` re-runs it (parameters
+are updated in place with ``set_params``).  The launch shape of the persistent kernel (data bins
+per work item, CTAs per SM) is chosen by ``Autotuner`` by timing the candidates on the batch.
+
+No reference counterpart: the reference evaluates one problem per call.
+"""
+import ctypes
+import itertools
+
+from . import _lib
+from .utils.arrays import device, torch
+from .waveformbuild import PRECISIONS
+
+
+class DirectGroupC(ctypes.Structure):
+    """Mirror of ``bbhx_direct_group`` (include/bbhx_b200.h)."""
+
+    _fields_ = [("data_freqs", ctypes.c_void_p), ("data", ctypes.c_void_p),
+                ("noise", ctypes.c_void_p), ("data_length", ctypes.c_int),
+                ("x", ctypes.c_void_p), ("y", ctypes.c_void_p), ("c1", ctypes.c_void_p),
+                ("c2", ctypes.c_void_p), ("c3", ctypes.c_void_p),
+                ("t_start", ctypes.c_void_p), ("t_end", ctypes.c_void_p),
+                ("num_modes", ctypes.c_int), ("length", ctypes.c_int),
+                ("num_bin_all", ctypes.c_int), ("d_h", ctypes.c_void_p), ("h_h", ctypes.c_void_p)]
+
+
+class DirectGroup:
+    def __init__(self, like, params, length=1024, modes=None, t_obs_start=0.0, t_obs_end=1.0):
+        t = torch()
+        self.like = like
+        self.params = t.as_tensor(params, dtype=t.float64, device=device()).contiguous()
+        self.length, self.modes = length, modes
+        self.t_obs_start, self.t_obs_end = t_obs_start, t_obs_end
+        self.flags = t.zeros(3, dtype=t.int32, device=device())
+
+    @property
+    def size(self):
+        return self.params.shape[1]
+
+    def build(self):
+        """Sparse buffer + splines of this group (device; no host synchronisation)."""
+        t = torch()
+        wave = self.like.waveform_gen
+        rows = tuple(self.params[k] for k in range(12))
+        buf, ts, te = wave._sparse_buffer(rows, self.t_obs_start, self.t_obs_end, None, self.length,
+                                          self.modes, False, flags=self.flags)
+        B, M, L = wave.num_bin_all, wave.num_modes, wave.length
+        x = wave.amp_phase_gen.freqs
+        c1, c2, c3 = t.empty_like(buf), t.empty_like(buf), t.empty_like(buf)
+        _lib.call("bbhx_interpolate", _lib.dptr(x), _lib.dptr(buf), _lib._VP(0), _lib.dptr(c1),
+                  _lib.dptr(c2), _lib.dptr(c3), L, 9, M, B, _lib.stream())
+        self.M, self.L = M, L
+        self.d_h = t.empty(B, dtype=t.complex128, device=device())
+        self.h_h = t.empty(B, dtype=t.complex128, device=device())
+        self._keep = (buf, c1, c2, c3, x, ts, te)
+        lk = self.like
+        return DirectGroupC(_lib.dptr(lk.data_freqs).value, _lib.dptr(lk.data_channels).value,
+                            _lib.dptr(lk.noise_factors).value, int(lk.data_freqs.numel()),
+                            _lib.dptr(x).value, _lib.dptr(buf).value, _lib.dptr(c1).value,
+                            _lib.dptr(c2).value, _lib.dptr(c3).value, _lib.dptr(ts).value,
+                            _lib.dptr(te).value, M, L, B, _lib.dptr(self.d_h).value,
+                            _lib.dptr(self.h_h).value)
+
+    def lnl(self):
+        return -0.5 * (self.like.d_d + self.h_h.real - 2 * self.d_h.real)
+
+
+class HetGroup:
+    def __init__(self, het, walkers, t_obs_start=0.0, t_obs_end=1.0):
+        t = torch()
+        self.het = het
+        self.params = t.as_tensor(walkers, dtype=t.float64, device=device()).contiguous()
+        self.t_obs_start, self.t_obs_end = t_obs_start, t_obs_end
+        self.flags = t.zeros(3, dtype=t.int32, device=device())
+
+    @property
+    def size(self):
+        return self.params.shape[1]
+
+    def run(self, precision):
+        self.ll, _ = self.het._fused_ll(self.params, dict(t_obs_start=self.t_obs_start,
+                                                          t_obs_end=self.t_obs_end), precision,
+                                        flags=self.flags)
+
+    def lnl(self):
+        return self.ll
+
+
+class Autotuner:
+    """Times the persistent kernel's launch shapes on a prepared batch and keeps the fastest
+    per batch signature (in memory; ``table`` can be saved / preloaded by the caller)."""
+
+    TILES = (256, 512, 1024)
+    CTAS = (2, 3, 4, 8)
+
+    def __init__(self, table=None, repeats=2):
+        self.table = dict(table or {})
+        self.repeats = repeats
+
+    @staticmethod
+    def signature(descs, precision):
+        return (precision, len(descs), sum(d.num_bin_all for d in descs),
+                max(d.data_length for d in descs), max(d.length for d in descs))
+
+    def best(self, descs, precision, launch):
+        key = self.signature(descs, precision)
+        if key in self.table:
+            return self.table[key]
+        t = torch()
+        timings = {}
+        for tile, ctas in itertools.product(self.TILES, self.CTAS):
+            launch(tile, ctas)  # warm-up of this shape
+            e0 = t.cuda.Event(enable_timing=True)
+            e1 = t.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(self.repeats):
+                launch(tile, ctas)
+            e1.record()
+            e1.synchronize()
+            timings[(tile, ctas)] = e0.elapsed_time(e1) / self.repeats
+        choice = min(timings, key=timings.get)
+        self.table[key] = choice
+        self.last_timings = timings
+        return choice
+
+
+class UnevenBatch:
+    def __init__(self, direct_groups=(), het_groups=(), precision="mixed", autotuner=None,
+                 shape=None):
+        self.direct = list(direct_groups)
+        self.het = list(het_groups)
+        self.precision = precision
+        self.autotuner = autotuner if autotuner is not None else Autotuner()
+        self.shape = shape  # (tile_bins, ctas_per_sm); None -> autotune on first run
+        self.graph = None
+        if len(self.direct) > 64:
+            raise ValueError("at most 64 direct groups per batch")
+
+    def _launch(self, descs, tile, ctas):
+        arr = (DirectGroupC * len(descs))(*descs)
+        _lib.call("bbhx_direct_like_multi", ctypes.cast(arr, ctypes.c_void_p), len(descs),
+                  PRECISIONS[self.precision], int(tile), int(ctas), _lib.stream())
+
+    def run(self):
+        """All groups' lnL (list of device tensors, direct groups first)."""
+        descs = [g.build() for g in self.direct]
+        if descs:
+            if self.shape is None:
+                self.shape = self.autotuner.best(descs, self.precision,
+                                                 lambda tl, c: self._launch(descs, tl, c))
+            self._launch(descs, *self.shape)
+        for h in self.het:
+            h.run(self.precision)
+        return [g.lnl() for g in self.direct] + [h.lnl() for h in self.het]
+
+    def capture(self):
+        """Record run() in a CUDA graph (after one eager run that also autotunes), execute it
+        once and return the output tensors (refreshed in place by every replay())."""
+        t = torch()
+        self.run()
+        t.cuda.synchronize()
+        s = t.cuda.Stream()
+        s.wait_stream(t.cuda.current_stream())
+        with t.cuda.stream(s):
+            self.run()  # warm the allocator on the capture stream
+        t.cuda.current_stream().wait_stream(s)
+        t.cuda.synchronize()
+        self.graph = t.cuda.CUDAGraph()
+        with t.cuda.graph(self.graph):
+            self.outputs = self.run()
+        self.graph.replay()  # capturing records the work; this executes it once
+        return self.outputs
+
+    def set_params(self, group_index, params):
+        """Copy new parameters into a group's (graph-captured) parameter tensor."""
+        groups = self.direct + self.het
+        groups[group_index].params.copy_(torch().as_tensor(params, dtype=torch().float64))
+
+    def replay(self):
+        self.graph.replay()
+        return self.outputs
+
+    def flags(self):
+        """Device error flags of every group (window search, orbit coverage, spins)."""
+        return [g.flags for g in self.direct + self.het]

@@ -167,10 +167,14 @@ class PhenomHMAmpPhase:
         chi2z = to_dev(atleast_1d(chi2z)).clone()
         m1, m2, chi1z, chi2z = self._sanity_check_params(m1, m2, chi1z, chi2z, flags)
         if modes is not None:
-            ells = to_dev([ell for ell, mm in modes], t.int32)
-            mms = to_dev([mm for ell, mm in modes], t.int32)
+            key = tuple(tuple(md) for md in modes)
+            cache = self.__dict__.setdefault("_mode_tensors", {})
+            if key not in cache:  # device copies made once (no host copy inside graph capture)
+                self._sanity_check_modes([e for e, _ in modes], [m for _, m in modes])
+                cache[key] = (to_dev([ell for ell, mm in modes], t.int32),
+                              to_dev([mm for ell, mm in modes], t.int32))
+            ells, mms = cache[key]
             self.modes = modes
-            self._sanity_check_modes([e for e, _ in modes], [m for _, m in modes])
         else:
             self.modes = self.allowable_modes
             ells, mms = self.ells_default, self.mms_default

@@ -171,6 +171,29 @@ int bbhx_template_support(int *start, int *len, const double *x, int num_modes, 
                           int num_bin_all, const double *data_freqs, int data_length,
                           void *stream);
 
+/* One direct-likelihood problem of a multi-group call: its own data stream (N bins), knots
+   x [B, M, L], sparse buffer y and spline coefficients c1..c3 [9, B, M, L], observation
+   windows t_start / t_end [B], outputs d_h, h_h [B] complex128.  All pointers are device
+   memory. */
+typedef struct {
+  const double *data_freqs;
+  const void *data;
+  const double *noise;
+  int data_length;
+  const double *x, *y, *c1, *c2, *c3;
+  const double *t_start, *t_end;
+  int num_modes, length, num_bin_all;
+  void *d_h, *h_h;
+} bbhx_direct_group;
+
+/* Several direct-likelihood problems (uneven grid lengths, mode sets and observation spans) in
+   ONE persistent launch of the fused kernel; no reference counterpart.  groups is a HOST array
+   of num_groups <= 64 descriptors; tile_bins (multiple of 128) and ctas_per_sm are the launch
+   shape (chosen by bbhx_b200.uneven.Autotuner).  Stream-ordered and free of host
+   synchronisation, so it can be captured in a CUDA graph. */
+int bbhx_direct_like_multi(const bbhx_direct_group *groups, int num_groups, int precision,
+                           int tile_bins, int ctas_per_sm, void *stream);
+
 /* fused interpolate + mode sum + noise weighting + <d|h>, <h|h> reduction; no templates are
  * stored (equivalent to InterpTDI followed by direct_like, waveformbuild.py:641-660 +
  * likelihood.py:177-214); d_h, h_h device complex [B], overwritten.
