@@ -113,8 +113,9 @@ __device__ __forceinline__ double reduce_2pi(double x) {
 
 // sin and cos of an FP64 angle of any size met here (|x| up to ~1e9 rad) for the hot loops.
 // Method: Cody-Waite reduction by pi/2 with pi/2 split into three doubles P1 + P2 + P3 (each
-// FMA forms k*P_i exactly before its one rounding), then the Taylor series of sin and cos on
-// the reduced angle |y| <= pi/4, truncated after the y^17 / y^18 terms (truncation below
+// FMA forms k*P_i exactly before its one rounding), k from the exact product x * 2/pi rounded
+// by adding 1.5 * 2^52 (its low bits give k mod 4), then the Taylor series of sin and cos on
+// the reduced angle |y| <= pi/4 (+ half an ulp of k), truncated after the y^17 / y^18 terms (truncation below
 // 3e-19), evaluated by Horner's rule, and the quadrant k mod 4 applied by swapping / negating.
 // Accuracy ~1e-16 absolute; checked against CUDA's sincos in tests/test_gpu_kernels.py.
 __device__ __forceinline__ void sincos_cw(double x, double* s, double* c) {
@@ -122,7 +123,9 @@ __device__ __forceinline__ void sincos_cw(double x, double* s, double* c) {
   const double P1 = 1.5707963267948966;
   const double P2 = 6.123233995736766e-17;
   const double P3 = -1.4973849048591698e-33;
-  double k = rint(x * TWO_OVER_PI);
+  const double MAGIC = 6755399441055744.0;  // 1.5 * 2^52: rounds to an integer, |x| < 2^50
+  const double t = fma(x, TWO_OVER_PI, MAGIC);
+  const double k = t - MAGIC;
   double y = fma(-k, P1, x);
   y = fma(-k, P2, y);
   y = fma(-k, P3, y);
@@ -146,7 +149,7 @@ __device__ __forceinline__ void sincos_cw(double x, double* s, double* c) {
   pc = fma(pc, y2, 0.041666666666666664);
   pc = fma(pc, y2, -0.5);
   double cy = fma(pc, y2, 1.0);
-  long long q = __double2ll_rn(k) & 3;
+  const int q = __double2loint(t) & 3;
   double ss = (q & 1) ? cy : sy;
   double cc = (q & 1) ? sy : cy;
   *s = (q & 2) ? -ss : ss;
@@ -158,7 +161,11 @@ __device__ __forceinline__ void sincos_cw(double x, double* s, double* c) {
 // (through y^9 and y^10; truncation < 2e-9).
 __device__ __forceinline__ void sincos_mixed(double x, float* s, float* c) {
   const double TWO_OVER_PI = 0.6366197723675814;
-  double k = rint(x * TWO_OVER_PI);
+  // k = nearest integer to x * 2/pi by adding 1.5 * 2^52 (valid for |x| < 2^50); the quadrant
+  // k mod 4 is then the low bits of the sum (no float-to-integer conversion needed)
+  const double MAGIC = 6755399441055744.0;
+  const double t = fma(x, TWO_OVER_PI, MAGIC);
+  const double k = t - MAGIC;
   double yd = fma(-k, 1.5707963267948966, x);
   yd = fma(-k, 6.123233995736766e-17, yd);
   float y = (float)yd;
@@ -169,7 +176,7 @@ __device__ __forceinline__ void sincos_mixed(double x, float* s, float* c) {
   float pc = fmaf(fmaf(fmaf(fmaf(-2.7557319e-07f, y2, 2.4801587e-05f), y2, -1.3888889e-03f), y2,
                        4.1666667e-02f), y2, -0.5f);
   float cy = fmaf(pc, y2, 1.0f);
-  int q = (int)(__double2ll_rn(k) & 3);
+  const int q = __double2loint(t) & 3;
   float ss = (q & 1) ? cy : sy;
   float cc = (q & 1) ? sy : cy;
   *s = (q & 2) ? -ss : ss;

@@ -186,6 +186,7 @@ constexpr int FD_TILE = FD_WARPS * FD_WARP_BINS;  // 512
 constexpr int FD_NSEG = 8;    // spline segments per (tile, mode) staged in shared memory
 constexpr int FD_MAXM = 6;    // modes per binary
 constexpr int FD_NC = 36;     // 9 quantities x (y, c1, c2, c3) per segment
+constexpr int FD_MAXCHUNK = 8;  // 128-bin chunks per tile item (tiles of up to 1024 bins)
 
 struct FusedArgs {
   const double* data_freqs;
@@ -299,6 +300,60 @@ __device__ __forceinline__ void accumulate_bin(const SegCoef<R>& c, double f, do
   }
 }
 
+// The FD_K bins of one lane inside one segment, branch-free so the bins' evaluation chains
+// interleave (G at a time): bins with f < 0 (outside the support) or failing the per-bin t(f)
+// gate (evaluated only when the segment straddles the window, CHECK) contribute zero.  The
+// channel sums are FMA chains.
+template <bool MIXED, typename R, int G, bool CHECK>
+__device__ __forceinline__ void accumulate_chunk(const SegCoef<R>& c, const double* f, double ts,
+                                                 double te, R (*acc)[6]) {
+#pragma unroll
+  for (int j0 = 0; j0 < FD_K; j0 += G) {
+    double u[G], ph[G];
+    bool g[G];
+#pragma unroll
+    for (int j = 0; j < G; ++j) {
+      u[j] = f[j0 + j] - c.xk;
+      g[j] = f[j0 + j] >= 0.0;
+      if (CHECK) {
+        const double tf = fma(fma(fma(c.p3[1], u[j], c.p2[1]), u[j], c.p1[1]), u[j], c.py[1]);
+        g[j] = g[j] && tf_gate(tf, ts, te);
+      }
+      ph[j] = fma(fma(fma(c.p3[0], u[j], c.p2[0]), u[j], c.p1[0]), u[j], c.py[0]);
+    }
+#pragma unroll
+    for (int j = 0; j < G; ++j) {
+      const R ur = (R)u[j];
+      R v[7];
+#pragma unroll
+      for (int a = 0; a < 7; ++a) v[a] = fma(fma(fma(c.a3[a], ur, c.a2[a]), ur, c.a1[a]), ur, c.ay[a]);
+      R sn, cs;
+      if (MIXED) {
+        float sf, cf;
+        sincos_mixed(ph[j], &sf, &cf);
+        sn = (R)sf;
+        cs = (R)cf;
+      } else {
+        double sd, cd;
+        sincos_cw(ph[j], &sd, &cd);
+        sn = (R)sd;
+        cs = (R)cd;
+      }
+      const R amp = g[j] ? v[0] : R(0);
+      const R apr = amp * cs, api = amp * sn;
+      R* a = acc[j0 + j];
+#pragma unroll
+      for (int ch = 0; ch < 3; ++ch) {  // a += conj(T A e^{i phi})
+        const R tr = v[1 + 2 * ch], ti = v[2 + 2 * ch];
+        a[2 * ch] = fma(tr, apr, a[2 * ch]);
+        a[2 * ch] = fma(-ti, api, a[2 * ch]);
+        a[2 * ch + 1] = fma(-tr, api, a[2 * ch + 1]);
+        a[2 * ch + 1] = fma(-ti, apr, a[2 * ch + 1]);
+      }
+    }
+  }
+}
+
 // G bins of one lane that lie in the same spline segment: the same arithmetic as
 // accumulate_bin, written branch-free (invalid or gated-off bins are dropped by selects) so the
 // G independent evaluation chains interleave.
@@ -355,7 +410,47 @@ struct alignas(16) WarpStage {
   R ac[FD_MAXM][FD_NSEG][7][4];
   int klo[FD_MAXM];
   int nseg[FD_MAXM];
+  int gate[FD_MAXM][FD_NSEG];  // t(f) gate over the whole segment: 0 mixed, 1 all in, 2 all out
+  signed char cseg[FD_MAXCHUNK][FD_MAXM];  // staged segment holding a whole 128-bin chunk, or -1
 };
+
+// Whole-segment t(f) gate: bound the cubic t(u) = y + c1 u + c2 u^2 + c3 u^3 over
+// u in [0, h] (end points and stationary points) and classify the segment as entirely inside
+// the observation window (1), entirely outside (2) or straddling it (0, per-bin gate).  A
+// margin of 1e-6 s (tf reaches ~1e8 s, so 1e-6 s is ~1e6 times its rounding) keeps the
+// classification on the safe side of the per-bin test.
+__device__ __forceinline__ int segment_gate(const double* pc, double h, double ts, double te) {
+  const double y = pc[0], c1 = pc[1], c2 = pc[2], c3 = pc[3];
+  double lo = y, hi = y;
+  const double yh = fma(fma(fma(c3, h, c2), h, c1), h, y);
+  lo = fmin(lo, yh);
+  hi = fmax(hi, yh);
+  // stationary points: c1 + 2 c2 u + 3 c3 u^2 = 0
+  double r[2];
+  int nr = 0;
+  if (c3 != 0.0) {
+    const double disc = 4.0 * c2 * c2 - 12.0 * c3 * c1;
+    if (disc >= 0.0) {
+      const double sq = sqrt(disc);
+      r[nr++] = (-2.0 * c2 + sq) / (6.0 * c3);
+      r[nr++] = (-2.0 * c2 - sq) / (6.0 * c3);
+    }
+  } else if (c2 != 0.0) {
+    r[nr++] = -c1 / (2.0 * c2);
+  }
+  for (int i = 0; i < nr; ++i) {
+    if (r[i] > 0.0 && r[i] < h) {
+      const double v = fma(fma(fma(c3, r[i], c2), r[i], c1), r[i], y);
+      lo = fmin(lo, v);
+      hi = fmax(hi, v);
+    }
+  }
+  const double eps = 1e-6;
+  if (!(lo == lo) || !(hi == hi)) return 0;
+  if (lo >= ts + eps && (te <= 0.0 || hi <= te - eps)) return 1;
+  if (hi < ts - eps || (te > 0.0 && lo > te + eps)) return 2;
+  return 0;
+}
 
 template <typename R>
 __device__ __forceinline__ void load_seg(SegCoef<R>& cf, const WarpStage<R>& S, int m, int kl) {
@@ -437,6 +532,31 @@ __device__ __forceinline__ void fused_item(const FusedArgs& A, long long q, Warp
     }
     __syncwarp();
     const double ts = __ldg(A.t_start + b), te = __ldg(A.t_end + b);
+    for (int idx = lane; idx < A.M * FD_NSEG; idx += 32) {
+      const int m = idx / FD_NSEG, sg = idx - m * FD_NSEG;
+      if (sg < S.nseg[m])
+        S.gate[m][sg] = segment_gate(&S.pc[m][sg][1][0], S.x[m][sg + 1] - S.x[m][sg], ts, te);
+    }
+    const int nchunk = A.tile / FD_WARP_BINS;
+    for (int idx = lane; idx < nchunk * A.M; idx += 32) {
+      const int ck = idx / A.M, m = idx - ck * A.M;
+      const int c0 = t0 + ck * FD_WARP_BINS;
+      const int n = S.nseg[m];
+      int seg = -1;
+      if (n > 0 && c0 < s1 && c0 + FD_WARP_BINS > s0) {
+        const double fa = __ldg(A.data_freqs + max(c0, s0));
+        const double fb = __ldg(A.data_freqs + min(c0 + FD_WARP_BINS, s1) - 1);
+        int ka = -1, kz = -1;
+        for (int k = 0; k <= n; ++k) {
+          const double xk = S.x[m][k];
+          ka = (xk <= fa) ? k : ka;
+          kz = (xk <= fb) ? k : kz;
+        }
+        if (ka == kz && ka >= 0 && ka < n) seg = ka;
+      }
+      S.cseg[ck][m] = (signed char)seg;
+    }
+    __syncwarp();
     double dr = 0.0, di = 0.0, hh = 0.0;
     for (int ch0 = 0; ch0 < A.tile; ch0 += FD_WARP_BINS) {
       const int c0 = t0 + ch0;
@@ -450,11 +570,25 @@ __device__ __forceinline__ void fused_item(const FusedArgs& A, long long q, Warp
 #pragma unroll
         for (int c = 0; c < 6; ++c) acc[j][c] = R(0);
       }
+      const int ck = ch0 / FD_WARP_BINS;
       for (int m = 0; m < A.M; ++m) {
         const int n = S.nseg[m];
         if (n == 0) continue;
         SegCoef<R> cf;
         if (n > 0) {
+          // warp-uniform fast path: the whole chunk lies in one staged segment
+          const int ka = S.cseg[ck][m];
+          if (ka >= 0) {
+            const int gate = S.gate[m][ka];
+            if (gate == 2) continue;
+            load_seg<R>(cf, S, m, ka);
+            constexpr int G = MIXED ? 4 : 2;
+            if (gate == 1)
+              accumulate_chunk<MIXED, R, G, false>(cf, fbin, ts, te, acc);
+            else
+              accumulate_chunk<MIXED, R, G, true>(cf, fbin, ts, te, acc);
+            continue;
+          }
           // segment of every bin (local index; n = past the last staged segment)
           int kb[FD_K];
           bool ok[FD_K];
@@ -797,8 +931,10 @@ int bbhx_direct_like_multi(const bbhx_direct_group* groups, int num_groups, int 
   BBHX_REQUIRE(groups != nullptr && num_groups >= 1 && num_groups <= FD_MAXGROUPS,
                "num_groups must be 1..%d", FD_MAXGROUPS);
   BBHX_REQUIRE(precision == 0 || precision == 1, "precision must be 0 (FP64) or 1 (mixed)");
-  BBHX_REQUIRE(tile_bins >= FD_WARP_BINS && tile_bins <= 4096 && tile_bins % FD_WARP_BINS == 0,
-               "tile_bins must be a multiple of %d in [%d, 4096]", FD_WARP_BINS, FD_WARP_BINS);
+  BBHX_REQUIRE(tile_bins >= FD_WARP_BINS && tile_bins <= FD_WARP_BINS * FD_MAXCHUNK &&
+                   tile_bins % FD_WARP_BINS == 0,
+               "tile_bins must be a multiple of %d in [%d, %d]", FD_WARP_BINS, FD_WARP_BINS,
+               FD_WARP_BINS * FD_MAXCHUNK);
   BBHX_REQUIRE(ctas_per_sm >= 1 && ctas_per_sm <= 32, "ctas_per_sm must be 1..32");
   cudaStream_t s = (cudaStream_t)stream;
   MultiArgs MA;
