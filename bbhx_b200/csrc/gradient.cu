@@ -401,16 +401,15 @@ int bbhx_direct_like_grad(void* orbits, double* grad, const double* params, cons
                                                                          cb + 2 * nall, S, b0, nb);
       st = launch_status("k_spline_adj");
     }
-    if (!st) {
+    for (int k0 = 0; !st && k0 < NGRAD; k0 += GRAD_CHUNK) {
       k_grad_setup<<<grid_for((long long)nb * M, 64), 64, 0, s>>>(cD, rD, params, B, b0, nb, ells,
                                                                   mms, M, qnm_table, qnm_n, dspin,
-                                                                  run_phenomd);
+                                                                  run_phenomd, k0);
       st = launch_status("k_grad_setup");
-    }
-    if (!st) {
+      if (st) break;
       k_contract_direct<<<(unsigned)std::min(nb, nsm * 8), 128, 0, s>>>(
           grad, cD, rD, ((OrbitHandle*)orbits)->tab, params, B, b0, nb, t_init, x, ybar, TDItag,
-          rescaled, tdi2, M, L);
+          rescaled, tdi2, M, L, k0);
       st = launch_status("k_contract_direct");
     }
     if (gh) cudaFreeAsync(gh, s);

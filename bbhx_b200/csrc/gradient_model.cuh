@@ -7,6 +7,10 @@
 //   0 m1 [Msun] (row 0)   1 m2 [Msun] (1)   2 chi1z (2)   3 chi2z (3)   4 distance [m] (4)
 //   5 phi_ref (5)   6 inc (7)   7 lam (8)   8 beta (9)   9 psi (10)   10 t_ref [s] (11)
 // f_ref (row 6) does not enter the model (the reference frequency is the amplitude peak).
+//
+// The 11 directions are carried GRAD_CHUNK at a time (passes k0 = 0, GRAD_CHUNK, ...): a
+// dual number of GRAD_CHUNK tangents keeps much more of the model's working set in registers
+// than one of 11 tangents, which spills to local memory.
 #pragma once
 
 #include "bbhx_common.cuh"
@@ -18,11 +22,15 @@
 namespace bbhx {
 
 constexpr int NGRAD = 11;
-using GD = ad::Dual<NGRAD>;
+constexpr int GRAD_CHUNK = 4;
+constexpr int GRAD_PASSES = (NGRAD + GRAD_CHUNK - 1) / GRAD_CHUNK;
+using GD = ad::Dual<GRAD_CHUNK>;
 
-__device__ __forceinline__ GD seed(double v, int k) {
+// x seeded with tangent 1 in direction k (global index) when k is in this pass's chunk
+__device__ __forceinline__ GD seed(double v, int k, int k0) {
   GD x(v);
-  x.d[k] = 1.0;
+  const int i = k - k0;
+  if (i >= 0 && i < GRAD_CHUNK) x.d[i] = 1.0;
   return x;
 }
 
@@ -31,34 +39,36 @@ struct GradParams {
 };
 
 // P: [12, B] row-major parameter array (device).
-__device__ inline GradParams load_grad_params(const double* P, int B, int b) {
+__device__ inline GradParams load_grad_params(const double* P, int B, int b, int k0) {
   GradParams g;
-  g.m1 = seed(P[0 * (size_t)B + b], 0);
-  g.m2 = seed(P[1 * (size_t)B + b], 1);
-  g.chi1 = seed(P[2 * (size_t)B + b], 2);
-  g.chi2 = seed(P[3 * (size_t)B + b], 3);
-  g.dist = seed(P[4 * (size_t)B + b], 4);
-  g.phi_ref = seed(P[5 * (size_t)B + b], 5);
-  g.inc = seed(P[7 * (size_t)B + b], 6);
-  g.lam = seed(P[8 * (size_t)B + b], 7);
-  g.beta = seed(P[9 * (size_t)B + b], 8);
-  g.psi = seed(P[10 * (size_t)B + b], 9);
-  g.t_ref = seed(P[11 * (size_t)B + b], 10);
+  g.m1 = seed(P[0 * (size_t)B + b], 0, k0);
+  g.m2 = seed(P[1 * (size_t)B + b], 1, k0);
+  g.chi1 = seed(P[2 * (size_t)B + b], 2, k0);
+  g.chi2 = seed(P[3 * (size_t)B + b], 3, k0);
+  g.dist = seed(P[4 * (size_t)B + b], 4, k0);
+  g.phi_ref = seed(P[5 * (size_t)B + b], 5, k0);
+  g.inc = seed(P[7 * (size_t)B + b], 6, k0);
+  g.lam = seed(P[8 * (size_t)B + b], 7, k0);
+  g.beta = seed(P[9 * (size_t)B + b], 8, k0);
+  g.psi = seed(P[10 * (size_t)B + b], 9, k0);
+  g.t_ref = seed(P[11 * (size_t)B + b], 10, k0);
   return g;
 }
 
 // Dual-number records of binaries [b0, b0 + nb): the same chain as the forward path
 // (ringdown frequencies -> phm_setup_mode; response_mode_setup), with tangents seeded on the
-// 11 parameters.  qnm: [8, nq] table y/c1/c2/c3 of the ringdown and damping splines.
-static __global__ void k_grad_setup(ModeCoeffsT<GD>* coeffs, ResponseModeT<GD>* rmodes, const double* P,
-                             int B, int b0, int nb, const int* ells, const int* mms, int M,
-                             const double* qnm, int nq, double dspin, int run_phenomd) {
+// directions [k0, k0 + GRAD_CHUNK).  qnm: [8, nq] table y/c1/c2/c3 of the ringdown and damping
+// splines.
+static __global__ void k_grad_setup(ModeCoeffsT<GD>* coeffs, ResponseModeT<GD>* rmodes,
+                                    const double* P, int B, int b0, int nb, const int* ells,
+                                    const int* mms, int M, const double* qnm, int nq,
+                                    double dspin, int run_phenomd, int k0) {
   const long long n = (long long)nb * M;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
        t += (long long)gridDim.x * blockDim.x) {
     const int bl = (int)(t / M), i = (int)(t % M);
     const int b = b0 + bl;
-    const GradParams g = load_grad_params(P, B, b);
+    const GradParams g = load_grad_params(P, B, b, k0);
     GD fm, fs;
     final_mass_spin(g.m1, g.m2, g.chi1, g.chi2, &fm, &fs);
     // PhenomD 22 ringdown / damping from the tabulated spline (PhenomHMWaveform.cu:1930-1993)
@@ -114,21 +124,21 @@ __device__ inline PointTangents point_tangents(const ModeCoeffsT<GD>& c, const R
   return o;
 }
 
-// Sum of NGRAD partials over the block into out[0..NGRAD) (thread 0 writes).
-__device__ inline void block_reduce_grad(double* acc, double* out) {
-  __shared__ double red[NGRAD][32];
+// Sum of the GRAD_CHUNK partials over the block into out[k0 + k] for the directions < NGRAD.
+__device__ inline void block_reduce_grad(double* acc, double* out, int k0) {
+  __shared__ double red[GRAD_CHUNK][32];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
 #pragma unroll
-  for (int k = 0; k < NGRAD; ++k) {
+  for (int k = 0; k < GRAD_CHUNK; ++k) {
     double v = acc[k];
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if (lane == 0) red[k][w] = v;
   }
   __syncthreads();
-  if (threadIdx.x < NGRAD) {
+  if (threadIdx.x < GRAD_CHUNK && k0 + (int)threadIdx.x < NGRAD) {
     double s = 0.0;
     for (int q = 0; q < nw; ++q) s += red[threadIdx.x][q];
-    out[threadIdx.x] = s;
+    out[k0 + threadIdx.x] = s;
   }
   __syncthreads();
 }
@@ -137,17 +147,18 @@ __device__ inline void block_reduce_grad(double* acc, double* out) {
 // the sparse grid freqs[j] (lnL depends on h = sum_modes conj(W), and dL = Re(gh dW)).
 // One CTA per binary of [b0, b0 + nb); records indexed relative to b0.
 static __global__ void k_contract_het(double* grad, const ModeCoeffsT<GD>* coeffs,
-                               const ResponseModeT<GD>* rmodes, OrbitTables orb, const double* P,
-                               int B, int b0, int nb, const double* t_start, const double* t_end,
-                               double t_init, const double* freqs, const cplx* gh, int TDItag,
-                               int rescaled, int tdi2, int M, int L) {
+                                      const ResponseModeT<GD>* rmodes, OrbitTables orb,
+                                      const double* P, int B, int b0, int nb,
+                                      const double* t_start, const double* t_end, double t_init,
+                                      const double* freqs, const cplx* gh, int TDItag,
+                                      int rescaled, int tdi2, int M, int L, int k0) {
   for (int bl = blockIdx.x; bl < nb; bl += gridDim.x) {
     const int b = b0 + bl;
-    const GD t_ref = seed(P[11 * (size_t)B + b], 10);
+    const GD t_ref = seed(P[11 * (size_t)B + b], 10, k0);
     const double ts = t_start[b], te = t_end[b];
-    double acc[NGRAD];
+    double acc[GRAD_CHUNK];
 #pragma unroll
-    for (int k = 0; k < NGRAD; ++k) acc[k] = 0.0;
+    for (int k = 0; k < GRAD_CHUNK; ++k) acc[k] = 0.0;
     for (int p = threadIdx.x; p < M * L; p += blockDim.x) {
       const int m = p / L, j = p % L;
       const PointTangents o =
@@ -158,10 +169,11 @@ static __global__ void k_contract_het(double* grad, const ModeCoeffsT<GD>* coeff
       for (int ch = 0; ch < 3; ++ch) {
         const cplx u = gh[((size_t)b * 3 + ch) * L + j];
 #pragma unroll
-        for (int k = 0; k < NGRAD; ++k) acc[k] += u.re * o.W[ch].re.d[k] - u.im * o.W[ch].im.d[k];
+        for (int k = 0; k < GRAD_CHUNK; ++k)
+          acc[k] += u.re * o.W[ch].re.d[k] - u.im * o.W[ch].im.d[k];
       }
     }
-    block_reduce_grad(acc, grad + (size_t)b * NGRAD);
+    block_reduce_grad(acc, grad + (size_t)b * NGRAD, k0);
   }
 }
 
@@ -173,14 +185,14 @@ static __global__ void k_contract_direct(double* grad, const ModeCoeffsT<GD>* co
                                          const ResponseModeT<GD>* rmodes, OrbitTables orb,
                                          const double* P, int B, int b0, int nb, double t_init,
                                          const double* x, const double* ybar, int TDItag,
-                                         int rescaled, int tdi2, int M, int L) {
+                                         int rescaled, int tdi2, int M, int L, int k0) {
   const size_t n = (size_t)B * M * L;
   for (int bl = blockIdx.x; bl < nb; bl += gridDim.x) {
     const int b = b0 + bl;
-    const GD t_ref = seed(P[11 * (size_t)B + b], 10);
-    double acc[NGRAD];
+    const GD t_ref = seed(P[11 * (size_t)B + b], 10, k0);
+    double acc[GRAD_CHUNK];
 #pragma unroll
-    for (int k = 0; k < NGRAD; ++k) acc[k] = 0.0;
+    for (int k = 0; k < GRAD_CHUNK; ++k) acc[k] = 0.0;
     for (int p = threadIdx.x; p < M * L; p += blockDim.x) {
       const int m = p / L;
       const size_t o = ((size_t)b * M + m) * L + (p % L);
@@ -196,7 +208,7 @@ static __global__ void k_contract_direct(double* grad, const ModeCoeffsT<GD>* co
       const PointTangents pt = point_tangents(coeffs[(size_t)bl * M + m], rmodes[(size_t)bl * M + m],
                                               orb, x[o], t_ref, t_init, TDItag, rescaled, tdi2);
 #pragma unroll
-      for (int k = 0; k < NGRAD; ++k) {
+      for (int k = 0; k < GRAD_CHUNK; ++k) {
         double v = w0 * pt.amp.d[k] + w1 * pt.phase.d[k];
 #pragma unroll
         for (int ch = 0; ch < 3; ++ch)
@@ -204,7 +216,7 @@ static __global__ void k_contract_direct(double* grad, const ModeCoeffsT<GD>* co
         acc[k] += v;
       }
     }
-    block_reduce_grad(acc, grad + (size_t)b * NGRAD);
+    block_reduce_grad(acc, grad + (size_t)b * NGRAD, k0);
   }
 }
 

@@ -635,14 +635,17 @@ int bbhx_hdyn_grad(void* orbits, void* d_h, void* h_h, double* grad, const void*
     for (int b0 = 0; !st && b0 < num_bin_all; b0 += chunk) {
       const int nb = std::min(chunk, num_bin_all - b0);
       const long long n = (long long)nb * num_modes;
-      k_grad_setup<<<grid_for(n, 64), 64, 0, s>>>(cD, rD, params, num_bin_all, b0, nb, ells, mms,
-                                                  num_modes, qnm_table, qnm_n, dspin, run_phenomd);
-      st = launch_status("k_grad_setup");
-      if (st) break;
-      k_contract_het<<<(unsigned)std::min(nb, nsm * 8), 128, 0, s>>>(
-          grad, cD, rD, A.orb, params, num_bin_all, b0, nb, t_start, t_end, t_init, freqs, gh,
-          TDItag, rescaled, tdi2, num_modes, length);
-      st = launch_status("k_contract_het");
+      for (int k0 = 0; !st && k0 < NGRAD; k0 += GRAD_CHUNK) {
+        k_grad_setup<<<grid_for(n, 64), 64, 0, s>>>(cD, rD, params, num_bin_all, b0, nb, ells,
+                                                    mms, num_modes, qnm_table, qnm_n, dspin,
+                                                    run_phenomd, k0);
+        st = launch_status("k_grad_setup");
+        if (st) break;
+        k_contract_het<<<(unsigned)std::min(nb, nsm * 8), 128, 0, s>>>(
+            grad, cD, rD, A.orb, params, num_bin_all, b0, nb, t_start, t_end, t_init, freqs, gh,
+            TDItag, rescaled, tdi2, num_modes, length, k0);
+        st = launch_status("k_contract_het");
+      }
     }
   }
   if (rD) cudaFreeAsync(rD, s);

@@ -582,7 +582,7 @@ __device__ __forceinline__ void fused_item(const FusedArgs& A, long long q, Warp
             const int gate = S.gate[m][ka];
             if (gate == 2) continue;
             load_seg<R>(cf, S, m, ka);
-            constexpr int G = MIXED ? 4 : 2;
+            constexpr int G = 2;  // two interleaved bins: best of 1/2/4 at 4 CTAs per SM
             if (gate == 1)
               accumulate_chunk<MIXED, R, G, false>(cf, fbin, ts, te, acc);
             else
