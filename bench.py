@@ -330,7 +330,9 @@ def gpu_arm(args):
     dl = float(np.max(np.abs(ll_host - lnl)))
 
     extra = {}
-    if not args.no_extra:
+    # the heterodyned / gradient / uneven-batch metrics are single-GPU figures; a multi-rank run
+    # reports the headline direct lnL only (every rank's own batch, no collective)
+    if not args.no_extra and world == 1:
         extra.update(het_metric(args, wave, like, f, params))
         if not args.no_grad:
             extra.update(grad_metric(args))
