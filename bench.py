@@ -301,6 +301,10 @@ def gpu_arm(args):
     lnl64 = out64.cpu().numpy()
     assert np.all(np.isfinite(lnl)) and np.all(np.isfinite(lnl64)), "non-finite lnL"
     dl_mixed = np.abs(lnl - lnl64)
+    # <h|h> of every binary (FP64, outside the timed region) for the relative error
+    _, hh64 = wave.inner_products(dev_params, like.data_freqs, like.data_channels,
+                                  like.noise_factors, flags=flags, precision="fp64", **kw)
+    hh64 = hh64.real.cpu().numpy()
     fp64_ms = max_over_ranks(fp64_ms, world)
 
     # support sizes (sum of per-binary data-grid lengths) for the roofline
@@ -368,7 +372,9 @@ def gpu_arm(args):
                        "kernel_ms": statistics.mean(a.elapsed_time(b) for a, b in fp64_timing["fused"])},
         "dlnl_mixed_vs_fp64": {"max": float(dl_mixed.max()), "p99": float(np.percentile(dl_mixed, 99)),
                                "median": float(np.median(dl_mixed)),
-                               "max_relative_to_hh": float(np.max(dl_mixed / np.maximum(1.0, np.abs(lnl64))))},
+                               "max_over_hh": float(np.max(dl_mixed / np.maximum(1.0, hh64))),
+                               "frac_within_1e-2": float(np.mean(dl_mixed <= 1e-2)),
+                               "median_hh": float(np.median(hh64))},
         "config": {"workload": "direct lnL, mixed precision (FP64 plain beside), B=%d binaries x 6 modes, sparse L=%d, "
                                "Tobs=1 yr, df=1/Tobs over 1e-5..0.1 Hz (N=%d bins), AET TDI2"
                                % (B, LENGTH, len(f)),
@@ -441,6 +447,7 @@ def het_metric(args, wave, like, f, params):
         "step_by_step_chain_fp64": {"value": vch, "unit": "lnL evals/s", "batch": chain_batch},
         "dlnl_mixed_vs_fp64": {"max": float(d.max()), "p99": float(np.percentile(d, 99)),
                                "median": float(np.median(d)),
+                               "frac_within_1e-2": float(np.mean(d <= 1e-2)),
                                "max_over_reference_hh": float(d.max() / het.reference_h_h),
                                "reference_hh": float(het.reference_h_h)},
         "lnl_range": [float(ll64.min()), float(ll64.max())],
@@ -605,6 +612,7 @@ def uneven_metric(args):
         "speedup_vs_fp64_plain": t_fp64 / t_mixed,
         "launch_shape": {"tile_bins": batch.shape[0], "ctas_per_sm": batch.shape[1]},
         "dlnl_mixed_vs_fp64": {"max": float(allerr.max()), "median": float(np.median(allerr)),
+                               "frac_within_1e-2": float(np.mean(allerr <= 1e-2)),
                                "p99": float(np.percentile(allerr, 99)),
                                "max_over_hh": float(allrel.max())},
         "flags_clear": flags_ok,
