@@ -191,12 +191,13 @@ __device__ inline TransferF response_point_mixed(const RespModeF& r, const Orbit
   TransferF out;
   out.phaseRdelay = 2. * PI / C_SI * f * (k[0] * (AU_SI * ca) + k[1] * (AU_SI * sa));
 
-  V3T<double> p1 = orbit_lerp(orb.x_arr, 9, 0, orb.dt, orb.N, t);
-  V3T<double> p2 = orbit_lerp(orb.x_arr, 9, 3, orb.dt, orb.N, t);
-  V3T<double> p3 = orbit_lerp(orb.x_arr, 9, 6, orb.dt, orb.N, t);
-  V3T<double> n1 = orbit_lerp(orb.n_arr, 18, orb.link_index[0] * 3, orb.dt, orb.N, t);
-  V3T<double> n2 = orbit_lerp(orb.n_arr, 18, orb.link_index[1] * 3, orb.dt, orb.N, t);
-  V3T<double> n3 = orbit_lerp(orb.n_arr, 18, orb.link_index[2] * 3, orb.dt, orb.N, t);
+  const OrbitWindow<double> win = orbit_window(orb, t);
+  V3T<double> p1 = orbit_lerp(win.x_lo, 9, 0, win.frac);
+  V3T<double> p2 = orbit_lerp(win.x_lo, 9, 3, win.frac);
+  V3T<double> p3 = orbit_lerp(win.x_lo, 9, 6, win.frac);
+  V3T<double> n1 = orbit_lerp(win.n_lo, 18, orb.link_index[0] * 3, win.frac);
+  V3T<double> n2 = orbit_lerp(win.n_lo, 18, orb.link_index[1] * 3, win.frac);
+  V3T<double> n3 = orbit_lerp(win.n_lo, 18, orb.link_index[2] * 3, win.frac);
   const float kn1 = (float)(k[0] * n1.x + k[1] * n1.y + k[2] * n1.z);
   const float kn2 = (float)(k[0] * n2.x + k[1] * n2.y + k[2] * n2.z);
   const float kn3 = (float)(k[0] * n3.x + k[1] * n3.y + k[2] * n3.z);

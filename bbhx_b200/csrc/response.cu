@@ -134,6 +134,7 @@ int bbhx_orbits_add_orbit_information(void* handle, double dt, int N, const doub
   h->tab.x_arr = h->d_x;
   h->tab.n_arr = h->d_n;
   h->tab.dt = dt;
+  h->tab.inv_dt = 1.0 / dt;
   h->tab.N = N;
   for (int k = 0; k < 3; ++k) h->tab.link_index[k] = slots[k];
   h->tab.armlength = armlength;

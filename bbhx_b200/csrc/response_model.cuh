@@ -14,7 +14,8 @@
 //
 // Orbit tables (bbhx_b200/orbits.py): x_arr[N][3][3], n_arr[N][6][3], link order
 // links[6]; sample k at t = k dt; linear interpolation for 0 <= floor(t/dt) < N-1, zero
-// vector outside.
+// vector outside.  The window and its fraction are found once per time and shared by the six
+// vectors read there.
 #pragma once
 
 #include "bbhx_common.cuh"
@@ -26,6 +27,7 @@ struct OrbitTables {
   const double* x_arr;  // [N][3][3]
   const double* n_arr;  // [N][6][3]
   double dt;
+  double inv_dt;  // 1 / dt
   int N;
   int link_index[3];  // table slots of links 12, 23, 31
   double armlength;
@@ -52,22 +54,46 @@ struct V3T {
   T x, y, z;
 };
 
+// Table window of time t: w = floor(t / dt) (the lookup rule), valid for 0 <= w < N - 1, and the
+// interpolation fraction (t - w dt) / dt shared by all vectors read at that time.
 template <typename T>
-__device__ __forceinline__ V3T<T> orbit_lerp(const double* tab, int stride, int offset, double dt,
-                                             int N, const T& t) {
-  double w = floor(value_of(t) / dt);
-  if (!(w >= 0.0) || w >= (double)(N - 1)) return V3T<T>{T(0.0), T(0.0), T(0.0)};
-  int wi = (int)w;
-  const double* lo = tab + (size_t)wi * stride + offset;
-  const double* hi = lo + stride;
-  T tt = t - wi * dt;
-  V3T<T> r;
-  r.x = __ldg(lo + 0) + (__ldg(hi + 0) - __ldg(lo + 0)) / dt * tt;
-  r.y = __ldg(lo + 1) + (__ldg(hi + 1) - __ldg(lo + 1)) / dt * tt;
-  r.z = __ldg(lo + 2) + (__ldg(hi + 2) - __ldg(lo + 2)) / dt * tt;
-  return r;
+struct OrbitWindow {
+  const double* x_lo;  // first x row of the window (nullptr when outside the table)
+  const double* n_lo;
+  T frac;
+};
+
+template <typename T>
+__device__ __forceinline__ OrbitWindow<T> orbit_window(const OrbitTables& orb, const T& t) {
+  OrbitWindow<T> w;
+  const double f = floor(value_of(t) / orb.dt);
+  if (!(f >= 0.0) || f >= (double)(orb.N - 1)) {
+    w.x_lo = nullptr;
+    w.n_lo = nullptr;
+    w.frac = T(0.0);
+    return w;
+  }
+  const int wi = (int)f;
+  w.x_lo = orb.x_arr + (size_t)wi * 9;
+  w.n_lo = orb.n_arr + (size_t)wi * 18;
+  w.frac = (t - wi * orb.dt) * orb.inv_dt;
+  return w;
 }
 
+// lo + (hi - lo) * frac of the 3-vector at `offset` of rows lo and lo + stride; zero vector
+// outside the table.
+template <typename T>
+__device__ __forceinline__ V3T<T> orbit_lerp(const double* lo, int stride, int offset,
+                                             const T& frac) {
+  if (lo == nullptr) return V3T<T>{T(0.0), T(0.0), T(0.0)};
+  lo += offset;
+  const double* hi = lo + stride;
+  V3T<T> r;
+  r.x = __ldg(lo + 0) + (__ldg(hi + 0) - __ldg(lo + 0)) * frac;
+  r.y = __ldg(lo + 1) + (__ldg(hi + 1) - __ldg(lo + 1)) * frac;
+  r.z = __ldg(lo + 2) + (__ldg(hi + 2) - __ldg(lo + 2)) * frac;
+  return r;
+}
 // spin-weight -2 spherical harmonics for l = 2..4 (Response.cu:383-424)
 template <typename T>
 __device__ inline cplxT<T> sylm_m2(int l, int m, const T& theta, const T& phi) {
@@ -164,12 +190,13 @@ __device__ inline TransferT<T> response_point(const ResponseModeT<T>& r, const O
   TransferT<T> out;
   out.phaseRdelay = 2. * PI / C_SI * f * kR;
 
-  V3T<T> p1 = orbit_lerp(orb.x_arr, 9, 0, orb.dt, orb.N, t);
-  V3T<T> p2 = orbit_lerp(orb.x_arr, 9, 3, orb.dt, orb.N, t);
-  V3T<T> p3 = orbit_lerp(orb.x_arr, 9, 6, orb.dt, orb.N, t);
-  V3T<T> n1 = orbit_lerp(orb.n_arr, 18, orb.link_index[0] * 3, orb.dt, orb.N, t);
-  V3T<T> n2 = orbit_lerp(orb.n_arr, 18, orb.link_index[1] * 3, orb.dt, orb.N, t);
-  V3T<T> n3 = orbit_lerp(orb.n_arr, 18, orb.link_index[2] * 3, orb.dt, orb.N, t);
+  const OrbitWindow<T> win = orbit_window(orb, t);
+  V3T<T> p1 = orbit_lerp(win.x_lo, 9, 0, win.frac);
+  V3T<T> p2 = orbit_lerp(win.x_lo, 9, 3, win.frac);
+  V3T<T> p3 = orbit_lerp(win.x_lo, 9, 6, win.frac);
+  V3T<T> n1 = orbit_lerp(win.n_lo, 18, orb.link_index[0] * 3, win.frac);
+  V3T<T> n2 = orbit_lerp(win.n_lo, 18, orb.link_index[1] * 3, win.frac);
+  V3T<T> n3 = orbit_lerp(win.n_lo, 18, orb.link_index[2] * 3, win.frac);
   T kn1 = k[0] * n1.x + k[1] * n1.y + k[2] * n1.z;
   T kn2 = k[0] * n2.x + k[1] * n2.y + k[2] * n2.z;
   T kn3 = k[0] * n3.x + k[1] * n3.y + k[2] * n3.z;
