@@ -172,7 +172,7 @@ __device__ __forceinline__ cplxf nHn_f(const cplxf* H, float n0, float n1, float
   return out;
 }
 
-__device__ __forceinline__ float sinc_f(float x) { return x == 0.0f ? 1.0f : sinf(x) / x; }
+__device__ __forceinline__ float sinc_f(float x) { return x == 0.0f ? 1.0f : __fdividef(sinf(x), x); }
 __device__ __forceinline__ cplxf cf(float r, float i) { return cplxf{r, i}; }
 __device__ __forceinline__ cplxf ti_f(cplxf a) { return {-a.im, a.re}; }
 __device__ __forceinline__ cplxf ephase(double x) {
@@ -207,11 +207,11 @@ __device__ inline TransferF response_point_mixed(const RespModeF& r, const Orbit
   const double k12 = k[0] * (p1.x + p2.x) + k[1] * (p1.y + p2.y) + k[2] * (p1.z + p2.z);
   const double k23 = k[0] * (p2.x + p3.x) + k[1] * (p2.y + p3.y) + k[2] * (p2.z + p3.z);
   const double k31 = k[0] * (p3.x + p1.x) + k[1] * (p3.y + p1.y) + k[2] * (p3.z + p1.z);
-  const double L = orb.armlength;
-  const double pre = PI * f * L / C_SI;
-  const cplxf e12 = ephase(pre * (1. + k12 / L));
-  const cplxf e23 = ephase(pre * (1. + k23 / L));
-  const cplxf e31 = ephase(pre * (1. + k31 / L));
+  const double invL = orb.inv_armlength;
+  const double pre = f * orb.pi_L_over_c;
+  const cplxf e12 = ephase(pre * (1. + k12 * invL));
+  const cplxf e23 = ephase(pre * (1. + k23 * invL));
+  const cplxf e31 = ephase(pre * (1. + k31 * invL));
   const float pf = (float)pre;
   const cplxf c3 = pf * ti_f(n3H), c1 = pf * ti_f(n1H), c2 = pf * ti_f(n2H);
   const cplxf G12 = sinc_f(pf * (1.f - kn3)) * (c3 * e12);

@@ -231,7 +231,7 @@ __device__ __forceinline__ PowersT<T> make_powers(T x) {
   PowersT<T> p;
   p.third = cbrt(x);
   p.sixth = sqrt(p.third);
-  p.two_thirds = x / p.third;
+  p.two_thirds = p.third * p.third;
   p.four_thirds = x * p.third;
   p.five_thirds = p.four_thirds * p.third;
   p.two = x * x;
@@ -838,7 +838,8 @@ __device__ __forceinline__ void mode_phase_tf(const ModeCoeffsT<T>& c, T Mf, T* 
     phenomd_phase_dphase(c.d, Mfp, &ph, &dph);
     *phase = -c.t0 * (Mf - c.Mf_ref) + ((c.cshift + (ph * inv + add)) - c.mm * c.phi0);
   }
-  *tf = c.M_sec * (dph / (2. * PI)) - (c.t0 / (2. * PI) * c.M_sec);
+  const double INV_2PI = 0.15915494309189533577;  // 1 / (2 pi)
+  *tf = c.M_sec * (dph * INV_2PI) - (c.t0 * INV_2PI * c.M_sec);
 }
 
 // Mapped amplitude frequency (IMRPhenomHMFreqDomainMap with AmpFlag, :2295-2315).

@@ -138,6 +138,8 @@ int bbhx_orbits_add_orbit_information(void* handle, double dt, int N, const doub
   h->tab.N = N;
   for (int k = 0; k < 3; ++k) h->tab.link_index[k] = slots[k];
   h->tab.armlength = armlength;
+  h->tab.inv_armlength = 1.0 / armlength;
+  h->tab.pi_L_over_c = PI * armlength / C_SI;
   h->ready = true;
   return OK;
 }

@@ -31,6 +31,8 @@ struct OrbitTables {
   int N;
   int link_index[3];  // table slots of links 12, 23, 31
   double armlength;
+  double inv_armlength;  // 1 / armlength
+  double pi_L_over_c;    // pi armlength / c
 };
 
 // Device-resident orbit tables owned by the C-ABI orbit handle (bbhx_orbits_*).
@@ -204,11 +206,11 @@ __device__ inline TransferT<T> response_point(const ResponseModeT<T>& r, const O
   T k12 = k[0] * (p1.x + p2.x) + k[1] * (p1.y + p2.y) + k[2] * (p1.z + p2.z);
   T k23 = k[0] * (p2.x + p3.x) + k[1] * (p2.y + p3.y) + k[2] * (p2.z + p3.z);
   T k31 = k[0] * (p3.x + p1.x) + k[1] * (p3.y + p1.y) + k[2] * (p3.z + p1.z);
-  const T L = orb.armlength;
-  T pre = PI * f * L / C_SI;
-  cplxT<T> e12 = expi(pre * (1. + k12 / L));
-  cplxT<T> e23 = expi(pre * (1. + k23 / L));
-  cplxT<T> e31 = expi(pre * (1. + k31 / L));
+  const double invL = orb.inv_armlength;
+  T pre = f * orb.pi_L_over_c;
+  cplxT<T> e12 = expi(pre * (1. + k12 * invL));
+  cplxT<T> e23 = expi(pre * (1. + k23 * invL));
+  cplxT<T> e31 = expi(pre * (1. + k31 * invL));
   // The constellation-centre phase factor exp(+i 2 pi f k.p0 / c) of the full response and
   // the Roemer-delay factor exp(-i phaseRdelay) cancel identically (Response.cu:166,304-309).
   cplxT<T> common = cmk(T(0.0), pre);
