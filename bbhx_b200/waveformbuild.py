@@ -108,16 +108,8 @@ class BBHWaveformFD:
         the host for host inputs, torch on the device for device inputs."""
         t = torch()
         if isinstance(lam, t.Tensor) and lam.is_cuda:
-            from .utils.constants import C_SI, ConstOmega, OrbitR
-
-            def tssb(tL):
-                phase = ConstOmega * tL - lam
-                RoC = OrbitR / C_SI
-                cb = t.cos(beta)
-                return (tL + RoC * cb * t.cos(phase)
-                        - 1.0 / 2 * ConstOmega * (RoC * cb) ** 2 * t.sin(2.0 * phase))
-
-            return tssb(t_obs_start * YRSID_SI).contiguous(), tssb(t_obs_end * YRSID_SI).contiguous()
+            return (tSSBfromLframe(t_obs_start * YRSID_SI, lam, beta, 0.0).contiguous(),
+                    tSSBfromLframe(t_obs_end * YRSID_SI, lam, beta, 0.0).contiguous())
         t_start = np.atleast_1d(tSSBfromLframe(t_obs_start * YRSID_SI, lam, beta, 0.0))
         t_end = np.atleast_1d(tSSBfromLframe(t_obs_end * YRSID_SI, lam, beta, 0.0))
         return t_start, t_end
