@@ -46,7 +46,7 @@ _SIGS = {
     "bbhx_direct_like": [_VP] * 7 + [_I, _I, _VP],
     "bbhx_hdyn": [_VP] * 5 + [_I, _I, _I, _VP],
     "bbhx_template_support": [_VP, _VP, _VP, _I, _I, _I, _VP, _I, _VP],
-    "bbhx_direct_like_fused": [_VP] * 5 + [_I] + [_VP] * 7 + [_I, _I, _I, _I, _VP],
+    "bbhx_direct_like_fused": [_VP] * 5 + [_I] + [_VP] * 7 + [_I, _I, _I, _I, _VP, _VP, _VP],
     "bbhx_hdyn_fused": [_VP] * 12 + [_D] + [_VP] * 5 + [_I] * 7 + [_VP],
     "bbhx_hdyn_grad": [_VP] * 9 + [_I, _D, _D] + [_VP] * 5 + [_I] * 7 + [_VP],
     "bbhx_direct_like_multi": [_VP, _I, _I, _I, _I, _VP],

@@ -209,6 +209,8 @@ struct FusedArgs {
   const int2* segtab;  // [ntiles][B][M]: segments of the tile's first and last bin
   double* d_h;         // [B] complex outputs
   double* h_h;
+  const float2* data32;  // optional FP32 copies of data / noise for the mixed form (or null)
+  const float* noise32;
 };
 
 // Segment table: for every (tile, binary, mode) the spline segments holding the first and the
@@ -663,20 +665,43 @@ __device__ __forceinline__ void fused_item(const FusedArgs& A, long long q, Warp
           }
         }
       }
+      if (MIXED && A.data32 != nullptr) {
+        // FP32 data and weights; one bin's three channels summed in FP32, bins in FP64
 #pragma unroll
-      for (int j = 0; j < FD_K; ++j) {
-        if (fbin[j] < 0.0) continue;
-        const int i = c0 + 32 * j + lane;
+        for (int j = 0; j < FD_K; ++j) {
+          if (fbin[j] < 0.0) continue;
+          const int i = c0 + 32 * j + lane;
+          float cr = 0.f, ci = 0.f, ch = 0.f;
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          const long long gi = (long long)c * A.N + i;
-          const R w = (R)__ldg(A.noise + gi);
-          const double2 d = __ldg(reinterpret_cast<const double2*>(A.data) + gi);
-          const R hr = acc[j][2 * c] * w, hi = acc[j][2 * c + 1] * w;
-          const R dxr = (R)d.x, dyr = (R)d.y;
-          dr += (double)(dxr * hr + dyr * hi);
-          di += (double)(dxr * hi - dyr * hr);
-          hh += (double)(hr * hr + hi * hi);
+          for (int c = 0; c < 3; ++c) {
+            const long long gi = (long long)c * A.N + i;
+            const float w = __ldg(A.noise32 + gi);
+            const float2 d = __ldg(A.data32 + gi);
+            const float hr = (float)acc[j][2 * c] * w, hi = (float)acc[j][2 * c + 1] * w;
+            cr = fmaf(d.x, hr, fmaf(d.y, hi, cr));
+            ci = fmaf(d.x, hi, fmaf(-d.y, hr, ci));
+            ch = fmaf(hr, hr, fmaf(hi, hi, ch));
+          }
+          dr += (double)cr;
+          di += (double)ci;
+          hh += (double)ch;
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < FD_K; ++j) {
+          if (fbin[j] < 0.0) continue;
+          const int i = c0 + 32 * j + lane;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const long long gi = (long long)c * A.N + i;
+            const R w = (R)__ldg(A.noise + gi);
+            const double2 d = __ldg(reinterpret_cast<const double2*>(A.data) + gi);
+            const R hr = acc[j][2 * c] * w, hi = acc[j][2 * c + 1] * w;
+            const R dxr = (R)d.x, dyr = (R)d.y;
+            dr += (double)(dxr * hr + dyr * hi);
+            di += (double)(dxr * hi - dyr * hr);
+            hh += (double)(hr * hr + hi * hi);
+          }
         }
       }
     }
@@ -971,6 +996,8 @@ int bbhx_direct_like_multi(const bbhx_direct_group* groups, int num_groups, int 
     A.ntiles = (G.data_length + tile_bins - 1) / tile_bins;
     A.d_h = (double*)G.d_h;
     A.h_h = (double*)G.h_h;
+    A.data32 = (const float2*)G.data32;
+    A.noise32 = G.noise32;
     MA.off[g] = items;
     MA.boff[g] = bins;
     const long long nit = (long long)A.ntiles * A.B;
@@ -1048,7 +1075,8 @@ int bbhx_direct_like_fused(double* d_h, double* h_h, const double* data_freqs, c
                            const double* noise, int data_length, const double* x, const double* y,
                            const double* c1, const double* c2, const double* c3,
                            const double* t_start, const double* t_end, int num_modes, int length,
-                           int num_bin_all, int precision, void* stream) {
+                           int num_bin_all, int precision, const void* data32,
+                           const float* noise32, void* stream) {
   BBHX_REQUIRE(length >= 2 && num_modes >= 1 && data_length >= 1, "bad sizes");
   BBHX_REQUIRE(precision == 0 || precision == 1, "precision must be 0 (FP64) or 1 (mixed)");
   if (num_bin_all == 0) return OK;
@@ -1095,6 +1123,10 @@ int bbhx_direct_like_fused(double* d_h, double* h_h, const double* data_freqs, c
     A.segtab = segtab;
     A.d_h = d_h;
     A.h_h = h_h;
+    A.data32 = (precision == 1) ? (const float2*)data32 : nullptr;
+    A.noise32 = (precision == 1) ? noise32 : nullptr;
+    BBHX_REQUIRE((A.data32 == nullptr) == (A.noise32 == nullptr),
+                 "data32 and noise32 must be given together");
     const long long warps_needed = (nitems + 0);
     long long g = (warps_needed + FD_WARPS - 1) / FD_WARPS;
     unsigned grid = (unsigned)(g < 148LL * 16 ? g : 148LL * 16);

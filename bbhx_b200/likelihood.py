@@ -37,6 +37,16 @@ class Likelihood:
         self.waveform_gen = template_gen
         self.data_stream_length = len(data_freqs_cpu)
         self.d_d = float((4 * (self.data_channels.conj() * self.data_channels).sum()).real.item())
+        self._fp32 = None
+
+    def fp32_data(self):
+        """FP32 copies of the weighted data and the weights (complex64 / float32 [3 N]) that the
+        mixed form reads; made once, on first use."""
+        if self._fp32 is None:
+            t = torch()
+            self._fp32 = (self.data_channels.to(t.complex64).contiguous(),
+                          self.noise_factors.to(t.float32).contiguous())
+        return self._fp32
 
     @property
     def xp(self):
@@ -63,6 +73,8 @@ class Likelihood:
         for k in ("freqs", "fill", "direct", "compress", "squeeze", "combine"):
             kw.pop(k, None)
         flags = t.zeros(3, dtype=t.int32, device=device())
+        if self.precision == "mixed":
+            kw["data32"] = self.fp32_data()
         d_h, h_h = self.waveform_gen.inner_products(params, self.data_freqs,
                                                     self.data_channels, self.noise_factors,
                                                     flags=flags, precision=self.precision, **kw)

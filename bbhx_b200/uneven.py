@@ -31,7 +31,8 @@ class DirectGroupC(ctypes.Structure):
                 ("c2", ctypes.c_void_p), ("c3", ctypes.c_void_p),
                 ("t_start", ctypes.c_void_p), ("t_end", ctypes.c_void_p),
                 ("num_modes", ctypes.c_int), ("length", ctypes.c_int),
-                ("num_bin_all", ctypes.c_int), ("d_h", ctypes.c_void_p), ("h_h", ctypes.c_void_p)]
+                ("num_bin_all", ctypes.c_int), ("d_h", ctypes.c_void_p), ("h_h", ctypes.c_void_p),
+                ("data32", ctypes.c_void_p), ("noise32", ctypes.c_void_p)]
 
 
 class DirectGroup:
@@ -47,7 +48,7 @@ class DirectGroup:
     def size(self):
         return self.params.shape[1]
 
-    def build(self):
+    def build(self, precision="fp64"):
         """Sparse buffer + splines of this group (device; no host synchronisation)."""
         t = torch()
         wave = self.like.waveform_gen
@@ -64,12 +65,15 @@ class DirectGroup:
         self.h_h = t.empty(B, dtype=t.complex128, device=device())
         self._keep = (buf, c1, c2, c3, x, ts, te)
         lk = self.like
+        d32, n32 = lk.fp32_data() if precision == "mixed" else (None, None)
         return DirectGroupC(_lib.dptr(lk.data_freqs).value, _lib.dptr(lk.data_channels).value,
                             _lib.dptr(lk.noise_factors).value, int(lk.data_freqs.numel()),
                             _lib.dptr(x).value, _lib.dptr(buf).value, _lib.dptr(c1).value,
                             _lib.dptr(c2).value, _lib.dptr(c3).value, _lib.dptr(ts).value,
                             _lib.dptr(te).value, M, L, B, _lib.dptr(self.d_h).value,
-                            _lib.dptr(self.h_h).value)
+                            _lib.dptr(self.h_h).value,
+                            _lib.dptr(d32).value if d32 is not None else None,
+                            _lib.dptr(n32).value if n32 is not None else None)
 
     def lnl(self):
         return -0.5 * (self.like.d_d + self.h_h.real - 2 * self.d_h.real)
@@ -153,7 +157,7 @@ class UnevenBatch:
 
     def run(self):
         """All groups' lnL (list of device tensors, direct groups first)."""
-        descs = [g.build() for g in self.direct]
+        descs = [g.build(self.precision) for g in self.direct]
         if descs:
             if self.shape is None:
                 self.shape = self.autotuner.best(descs, self.precision,

@@ -330,11 +330,12 @@ class BBHWaveformFD:
 
     def inner_products(self, params, data_freqs, data_weighted, noise_factors, t_obs_start=0.0,
                        t_obs_end=1.0, length=1024, modes=None, flags=None, timing=None,
-                       precision="fp64", **unused):
+                       precision="fp64", data32=None, **unused):
         """Fused <d|h>, <h|h> for every binary (device complex128 [B] each).
 
         ``data_weighted`` [3, N] complex = data * sqrt(df / S); ``noise_factors`` [3, N] =
-        sqrt(df / S) (the reference's Likelihood attributes, likelihood.py:99-112)."""
+        sqrt(df / S) (the reference's Likelihood attributes, likelihood.py:99-112).
+        ``data32``: optional (complex64, float32) copies of the two, read by the mixed form."""
         t = torch()
         buf, t_start, t_end = self._sparse_buffer(params, t_obs_start, t_obs_end, None, length,
                                                   modes, False, flags=flags)
@@ -358,7 +359,9 @@ class BBHWaveformFD:
         _lib.call("bbhx_direct_like_fused", _lib.dptr(d_h), _lib.dptr(h_h), _lib.dptr(data_freqs),
                   _lib.dptr(data_weighted), _lib.dptr(noise_factors), int(data_freqs.numel()),
                   _lib.dptr(x), _lib.dptr(buf), _lib.dptr(c1), _lib.dptr(c2), _lib.dptr(c3),
-                  _lib.dptr(ts_d), _lib.dptr(te_d), M, L, B, PRECISIONS[precision], _lib.stream())
+                  _lib.dptr(ts_d), _lib.dptr(te_d), M, L, B, PRECISIONS[precision],
+                  _lib.dptr(data32[0]) if data32 is not None else _lib._VP(0),
+                  _lib.dptr(data32[1]) if data32 is not None else _lib._VP(0), _lib.stream())
         if timing is not None:
             ev1.record()
             timing.setdefault("fused", []).append((ev0, ev1))

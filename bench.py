@@ -248,7 +248,9 @@ def gpu_arm(args):
     def step(timing=None, precision="mixed"):
         d_h, h_h = wave.inner_products(dev_params, like.data_freqs, like.data_channels,
                                        like.noise_factors, flags=flags, timing=timing,
-                                       precision=precision, **kw)
+                                       precision=precision,
+                                       data32=like.fp32_data() if precision == "mixed" else None,
+                                       **kw)
         return -0.5 * (like.d_d + h_h - 2 * d_h).real
 
     def barrier():

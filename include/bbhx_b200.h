@@ -184,6 +184,8 @@ typedef struct {
   const double *t_start, *t_end;
   int num_modes, length, num_bin_all;
   void *d_h, *h_h;
+  const void *data32;    /* optional FP32 copies (complex64 [3, N], float [3, N]) used by the */
+  const float *noise32;  /* mixed form; null to read the FP64 arrays */
 } bbhx_direct_group;
 
 /* Several direct-likelihood problems (uneven grid lengths, mode sets and observation spans) in
@@ -203,7 +205,8 @@ int bbhx_direct_like_fused(double *d_h, double *h_h, const double *data_freqs, c
                            const double *noise, int data_length, const double *x, const double *y,
                            const double *c1, const double *c2, const double *c3,
                            const double *t_start, const double *t_end, int num_modes, int length,
-                           int num_bin_all, int precision, void *stream);
+                           int num_bin_all, int precision, const void *data32,
+                           const float *noise32, void *stream);
 
 /* fused heterodyned likelihood: PhenomHM + TDI response at the sparse heterodyne grid, mode
    sum, r = h / h0 and the relative-binning bin sums in one kernel (one CTA per walker).
