@@ -96,7 +96,9 @@ def _direct_setup(golden, golden_data, center_index):
     center = golden["params"][:, center_index].copy()
     inj = wave(*[np.atleast_1d(v) for v in center], freqs=golden_data["f"], fill=True, direct=False,
                **kw)[0].cpu().numpy()
-    like = Likelihood(wave, golden_data["f"], inj + golden_data["data"], golden_data["psd"])
+    data = inj + golden_data["data"]
+    like = Likelihood(wave, golden_data["f"], data, golden_data["psd"])
+    like.test_data = data
     P = perturb_params(center, 3, 29, rel_mass=1e-4, abs_spin_angle=1e-3, t_ref_s=1.0)
     return like, kw, P
 
@@ -124,3 +126,23 @@ def test_direct_autograd_backward(golden, golden_data):
     expect = np.zeros((12, P.shape[1]))
     expect[list(ROWS)] = grad.cpu().numpy().T
     np.testing.assert_allclose(x.grad.cpu().numpy(), expect, rtol=1e-12, atol=0)
+
+
+def test_direct_gradient_matches_fd_of_oracle_lnl(golden, golden_data):
+    """The GPU gradient against central differences of the oracle's CPU lnL on the same data:
+    the reference's own C++ compiled for CPU (oracle/_ref) when it is built, else the numpy
+    restatement (oracle/kernels_np.py).  One binary near the injection."""
+    import os
+
+    from oracle.build_ref import OUT
+    from oracle.pipeline import RefPipeline
+
+    like, kw, P = _direct_setup(golden, golden_data, 2)
+    P = P[:, :1]
+    _, grad = like.get_ll_and_grad(P, **kw)
+    grad = grad.cpu().numpy()
+    pipe = RefPipeline("ref" if os.path.isfile(OUT) else "np")
+    fd = _central_fd(lambda Q: pipe.direct_lnl(Q, golden_data["f"], like.test_data,
+                                               golden_data["psd"], **kw)[0], P)
+    print(pipe.K.name, "grad", grad[0], "\nfd  ", fd[0])
+    _check(grad, fd, P)
