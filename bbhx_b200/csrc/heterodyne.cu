@@ -409,7 +409,7 @@ __global__ void __launch_bounds__(HET_THREADS) k_het_fused(HetArgs A) {
         him += B0.im * mag2 + 2.0 * B1.im * re01;
       }
     }
-    if (A.gh) {
+    if (!MIXED && A.gh) {  // the adjoint output exists for the FP64 form only
       // Adjoint of lnL = Re d_h - (d_d + Re h_h) / 2 through the bin terms: per bin
       // g_r0 = A0 - Re(B0) r0 - Re(B1) r1, g_r1 = A1 - Re(B1) r0, carried to r_j / r_{j-1}
       // with the same coefficients as the forward r0, r1; then g_h = g_r / conj(h0).
