@@ -14,7 +14,8 @@ products); the plain-FP64 form is timed beside it.
   e2e    : the same through the public API (Likelihood.get_ll) from pinned host params,
            including the H2D copy of the 12 x B parameters and the D2H copy of the B lnL
   roofline: the fused interpolate + reduce kernel against measured HBM bandwidth, with
-           72 B of algorithmic traffic per (binary, data bin)
+           72 B of algorithmic traffic per (binary, data bin) (the FP64 data and weights;
+           frac_vs_mixed_reads uses the 36 B of FP32 copies the mixed form reads)
   cpu_baseline: the reference's own C++ CPU path (oracle/_ref) on a bounded sample
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
@@ -40,6 +41,7 @@ LENGTH = 1024
 SEED_PARAMS = 1234
 SEED_NOISE = 99
 HBM_BYTES_PER_PAIR = 72.0  # 3 x complex128 weighted data + 3 x float64 noise weights
+MIXED_BYTES_PER_PAIR = 36.0  # 3 x complex64 + 3 x float32: the FP32 copies the mixed form reads
 
 
 def parse():
@@ -382,13 +384,18 @@ def gpu_arm(args):
                                % (B, LENGTH, len(f)),
                    "global_batch": n_evals // args.steps, "data_bins": len(f),
                    "binary_bin_pairs_per_step": pairs,
-                   "l2": "inputs larger than L2 (data 227 MB + sparse buffers 1.8 GB per step)",
+                   "l2": "inputs larger than L2: every step writes and reads 1.8 GB of sparse buffers / "
+                         "spline coefficients besides the data (114 MB FP32 copies read by the mixed "
+                         "form, 227 MB FP64 by the plain form)",
                    "parallelism": f"replicas x{world} (independent binary batches per GPU)"},
         "e2e": {"value": aggregate_rate(B * args.steps, world, e2e_ms), "unit": "lnL evals/s",
                 "h2d_bytes_per_step": 12 * B * 8, "d2h_bytes_per_step": 3 * B * 8 + 3 * 8,
                 "max_abs_dlnl_vs_device_path": dl},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak,
+                     "algorithmic_bytes_per_pair": HBM_BYTES_PER_PAIR,
+                     # the mixed kernel reads FP32 copies of data and weights: 36 B per pair
+                     "frac_vs_mixed_reads": achieved * (MIXED_BYTES_PER_PAIR / HBM_BYTES_PER_PAIR) / peak,
                      "traffic": (tpp * pairs if tpp is not None else None),
                      "kernel": "k_direct_fused (bbhx_direct_like_fused)",
                      "kernel_ms": statistics.mean(fused_ms),

@@ -200,7 +200,9 @@ int bbhx_direct_like_multi(const bbhx_direct_group *groups, int num_groups, int 
  * stored (equivalent to InterpTDI followed by direct_like, waveformbuild.py:641-660 +
  * likelihood.py:177-214); d_h, h_h device complex [B], overwritten.
  * precision 0: FP64 throughout (the parity form); 1: mixed -- phase, t(f) and all
- * accumulations in FP64, amplitude / transfer / per-bin products in FP32 */
+ * accumulations in FP64, amplitude / transfer / per-bin products in FP32.
+ * data32 / noise32: optional FP32 copies of data (complex64 [3, N]) and noise (float [3, N])
+ * read by the mixed form instead of data / noise; both null or both given. */
 int bbhx_direct_like_fused(double *d_h, double *h_h, const double *data_freqs, const double *data,
                            const double *noise, int data_length, const double *x, const double *y,
                            const double *c1, const double *c2, const double *c3,
