@@ -3,6 +3,8 @@
 
 #include <cstdarg>
 #include <cstdio>
+#include <initializer_list>
+#include <utility>
 #include <cuda_runtime.h>
 
 #include "bbhx_common.cuh"
@@ -50,6 +52,25 @@ int retain_pool_memory();
 inline cudaError_t pool_alloc(void** p, size_t bytes, cudaStream_t s) {
   retain_pool_memory();
   return cudaMallocAsync(p, bytes, s);
+}
+
+// Several stream-ordered allocations, all or none: on a failure the buffers already obtained
+// are released (stream-ordered) and every pointer is left null.
+inline cudaError_t pool_alloc_all(cudaStream_t s,
+                                  std::initializer_list<std::pair<void**, size_t>> req) {
+  cudaError_t e = cudaSuccess;
+  for (const auto& r : req) *r.first = nullptr;
+  for (const auto& r : req) {
+    e = pool_alloc(r.first, r.second, s);
+    if (e != cudaSuccess) break;
+  }
+  if (e != cudaSuccess) {
+    for (const auto& r : req) {
+      if (*r.first) cudaFreeAsync(*r.first, s);
+      *r.first = nullptr;
+    }
+  }
+  return e;
 }
 
 inline unsigned int grid_for(long long n, int threads, int max_blocks = 148 * 32) {

@@ -891,13 +891,13 @@ int bbhx_direct_like(double* d_h, double* h_h, const double* data, const double*
   DirectJob* d_jobs = nullptr;
   double* d_part = nullptr;
   double* d_out = nullptr;
-  BBHX_CHECK_CUDA(pool_alloc((void**)&d_jobs, sizeof(DirectJob) * num_bin_all, s));
-  BBHX_CHECK_CUDA(pool_alloc((void**)&d_part, sizeof(double) * 3 * (nparts + 1), s));
-  BBHX_CHECK_CUDA(pool_alloc((void**)&d_out, sizeof(double) * 4 * num_bin_all, s));
-  BBHX_CHECK_CUDA(cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(DirectJob) * num_bin_all,
-                                  cudaMemcpyHostToDevice, s));
-  int st = OK;
-  if (maxparts > 0) {
+  BBHX_CHECK_CUDA(pool_alloc_all(s, {{(void**)&d_jobs, sizeof(DirectJob) * num_bin_all},
+                                     {(void**)&d_part, sizeof(double) * 3 * (nparts + 1)},
+                                     {(void**)&d_out, sizeof(double) * 4 * num_bin_all}}));
+  int st = cuda_status(cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(DirectJob) * num_bin_all,
+                                       cudaMemcpyHostToDevice, s),
+                       "direct_like job upload");
+  if (!st && maxparts > 0) {
     unsigned gx = maxparts > 1024 ? 1024 : maxparts;
     k_direct_like_partials<<<dim3(gx, num_bin_all), 256, 0, s>>>(d_jobs, (const cplx*)data, noise,
                                                                  data_stream_length, d_part);
@@ -1079,17 +1079,19 @@ int bbhx_direct_like_fused(double* d_h, double* h_h, const double* data_freqs, c
                            const float* noise32, void* stream) {
   BBHX_REQUIRE(length >= 2 && num_modes >= 1 && data_length >= 1, "bad sizes");
   BBHX_REQUIRE(precision == 0 || precision == 1, "precision must be 0 (FP64) or 1 (mixed)");
+  BBHX_REQUIRE((data32 == nullptr) == (noise32 == nullptr),
+               "data32 and noise32 must be given together");
+  BBHX_REQUIRE(num_modes <= FD_MAXM, "num_modes must be <= 6");
   if (num_bin_all == 0) return OK;
   cudaStream_t s = (cudaStream_t)stream;
   int ntiles = (data_length + FD_TILE - 1) / FD_TILE;
   long long nitems = (long long)ntiles * num_bin_all;
-  BBHX_REQUIRE(num_modes <= FD_MAXM, "num_modes must be <= 6");
   int* sup = nullptr;
   double* part = nullptr;
   int2* segtab = nullptr;
-  BBHX_CHECK_CUDA(pool_alloc((void**)&sup, sizeof(int) * 2 * num_bin_all, s));
-  BBHX_CHECK_CUDA(pool_alloc((void**)&part, sizeof(double) * 3 * nitems, s));
-  BBHX_CHECK_CUDA(pool_alloc((void**)&segtab, sizeof(int2) * nitems * num_modes, s));
+  BBHX_CHECK_CUDA(pool_alloc_all(s, {{(void**)&sup, sizeof(int) * 2 * num_bin_all},
+                                     {(void**)&part, sizeof(double) * 3 * nitems},
+                                     {(void**)&segtab, sizeof(int2) * nitems * num_modes}}));
   k_support<<<num_bin_all, 128, 0, s>>>(x, num_modes, length, num_bin_all, data_freqs, data_length,
                                         sup, sup + num_bin_all);
   int st = launch_status("k_support");
@@ -1125,8 +1127,6 @@ int bbhx_direct_like_fused(double* d_h, double* h_h, const double* data_freqs, c
     A.h_h = h_h;
     A.data32 = (precision == 1) ? (const float2*)data32 : nullptr;
     A.noise32 = (precision == 1) ? noise32 : nullptr;
-    BBHX_REQUIRE((A.data32 == nullptr) == (A.noise32 == nullptr),
-                 "data32 and noise32 must be given together");
     const long long warps_needed = (nitems + 0);
     long long g = (warps_needed + FD_WARPS - 1) / FD_WARPS;
     unsigned grid = (unsigned)(g < 148LL * 16 ? g : 148LL * 16);
