@@ -130,15 +130,17 @@ def test_direct_autograd_backward(golden, golden_data):
 
 def test_direct_gradient_matches_fd_of_oracle_lnl(golden, golden_data):
     """The GPU gradient against central differences of the oracle's CPU lnL on the same data:
-    the reference's own C++ compiled for CPU (oracle/_ref) when it is built, else the numpy
-    restatement (oracle/kernels_np.py).  One binary near the injection."""
+    the reference's own C++ compiled for CPU (oracle/_ref) on 32 samples around the injection
+    when it is built, else the numpy restatement (oracle/kernels_np.py) on one."""
     import os
 
+    from bbhx_b200.synthetic import perturb_params
     from oracle.build_ref import OUT
     from oracle.pipeline import RefPipeline
 
     like, kw, P = _direct_setup(golden, golden_data, 2)
-    P = P[:, :1]
+    n = 32 if os.path.isfile(OUT) else 1
+    P = perturb_params(P[:, 0], n, 31, rel_mass=1e-4, abs_spin_angle=1e-3, t_ref_s=1.0)
     _, grad = like.get_ll_and_grad(P, **kw)
     grad = grad.cpu().numpy()
     pipe = RefPipeline("ref" if os.path.isfile(OUT) else "np")
