@@ -448,6 +448,21 @@ def het_metric(args, wave, like, f, params):
     chain_batch = min(Bh, 16384)
     vch, _ = timed(None, chain_batch)
     d = np.abs(llmx - ll64)
+    # both heterodyned forms against the direct FP64 lnL (the form pinned to the reference) on
+    # the first walkers: relative-binning error plus, for mixed, the precision error.  The
+    # heterodyne keeps only the data inside the reference template's band (as the reference
+    # does), so its <d|d> lacks the rest: that walker-independent constant is removed first.
+    nd = min(Bh, 1024)
+    prev = like.precision
+    like.precision = "fp64"
+    ll_dir = like.get_ll(walkers[:, :nd], length=LENGTH, **kw)
+    like.precision = prev
+    dd_offset = 0.5 * (like.d_d - het.reference_d_d)
+
+    def vs_direct(ll):
+        e = np.abs(ll[:nd] - (ll_dir + dd_offset))
+        return {"max": float(e.max()), "median": float(np.median(e)),
+                "frac_within_1e-2": float(np.mean(e <= 1e-2))}
     return {"heterodyned": {
         "value": vmx, "unit": "lnL evals/s", "batch": Bh, "bins": 128,
         "dtype": "mixed: f64 phase/t(f)/Roemer/ratio/sums, f32 amplitude/transfer/products",
@@ -459,6 +474,8 @@ def het_metric(args, wave, like, f, params):
                                "frac_within_1e-2": float(np.mean(d <= 1e-2)),
                                "max_over_reference_hh": float(d.max() / het.reference_h_h),
                                "reference_hh": float(het.reference_h_h)},
+        "dlnl_vs_direct_fp64": {"walkers": nd, "dd_out_of_band_half": dd_offset,
+                                "mixed": vs_direct(llmx), "fp64": vs_direct(ll64)},
         "lnl_range": [float(ll64.min()), float(ll64.max())],
         "path": "HeterodynedLikelihood.get_ll with device-resident walkers",
         "finite": bool(np.all(np.isfinite(ll64)) and np.all(np.isfinite(llmx)))}}
