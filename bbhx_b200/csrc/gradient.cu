@@ -5,7 +5,8 @@
 // interpolation of the sparse [9, B, M, L] buffer (amplitude, phase, t(f), six transfer
 // components) summed over modes (TemplateInterpFD + direct_like: waveformbuild.py:89-239,
 // Likelihood.cu:356-471).  The chain, for a batch of binaries:
-//   1. k_adj_gh       d lnL / d h at every (binary, data bin):  g = 4 w (d~ - w h)  (reverse)
+//   1. the FP64 fused likelihood kernel (likelihood.cu, direct_fused_gh) writes d lnL / d h
+//                     at every (binary, data bin):  g = 4 w (d~ - w h)                  (reverse)
 //   2. k_adj_coeffs   warp per (binary, mode, spline segment): d lnL / d (y, c1, c2, c3) of
 //                     the 8 interpolated quantities, summed over the segment's data bins
 //   3. k_spline_adj   CTA per (binary, mode): adjoint of the not-a-knot spline build; the
@@ -21,6 +22,14 @@
 #include "capi_internal.cuh"
 #include "gradient_model.cuh"
 #include "tridiag.cuh"
+
+namespace bbhx {
+int direct_fused_gh(cplx* gh, const long long* gh_off, const int* start, const int* len,
+                    const double* data_freqs, const double* data, const double* noise, int N,
+                    const double* x, const double* y, const double* c1, const double* c2,
+                    const double* c3, const double* t_start, const double* t_end, int M, int L,
+                    int B_all, int b0, int nb, cudaStream_t s);
+}  // namespace bbhx
 
 extern "C" int bbhx_template_support(int* start, int* len, const double* x, int num_modes,
                                      int length, int num_bin_all, const double* data_freqs,
@@ -67,55 +76,22 @@ __device__ __forceinline__ void eval_segment(const SplineRefs& S, size_t row, in
   }
 }
 
-// 1. d lnL / d h per (binary, data bin, channel) of binaries [b0, b0 + nb); gh packed by the
-// support offsets off[bl] (local binary bl).
-__global__ void k_adj_gh(cplx* gh, const long long* off, const int* start, const int* len,
-                         SplineRefs S, const double* data_freqs, const cplx* data,
-                         const double* noise, int N, const double* t_start, const double* t_end,
-                         int b0, int nb) {
-  const int bl = blockIdx.y;
-  const int b = b0 + bl;
-  const int st = start[b], n = len[b];
-  const double ts = t_start[b], te = t_end[b];
-  for (int kk = blockIdx.x * blockDim.x + threadIdx.x; kk < n; kk += gridDim.x * blockDim.x) {
-    const int k = st + kk;
-    const double f = data_freqs[k];
-    double h[6] = {0, 0, 0, 0, 0, 0};
-    for (int m = 0; m < S.M; ++m) {
-      const size_t row = (size_t)b * S.M + m;
-      const int s = knot_segment(S.x + row * S.L, S.L, f);
-      if (s < 0 || s >= S.L - 1) continue;
-      double q[9];
-      eval_segment(S, row, s, f - S.x[row * S.L + s], q);
-      if (!tf_gate(q[2], ts, te)) continue;
-      double sn, cs;
-      sincos(q[1], &sn, &cs);
-      const double ar = q[0] * cs, ai = q[0] * sn;
-#pragma unroll
-      for (int ch = 0; ch < 3; ++ch) {  // h += conj(T A e^{i phase})
-        const double tr = q[3 + 2 * ch], ti = q[4 + 2 * ch];
-        h[2 * ch] += tr * ar - ti * ai;
-        h[2 * ch + 1] -= tr * ai + ti * ar;
-      }
-    }
-    cplx* g = gh + (off[bl] + kk) * 3;
-#pragma unroll
-    for (int ch = 0; ch < 3; ++ch) {
-      const double w = noise[(size_t)ch * N + k];
-      const cplx d = data[(size_t)ch * N + k];
-      g[ch] = mk(4.0 * w * (d.re - w * h[2 * ch]), 4.0 * w * (d.im - w * h[2 * ch + 1]));
-    }
-  }
-}
-
 // 2. Warp per (local binary, mode, segment s < L-1): sums over the segment's data bins of
 // a_p, a_p u, a_p u^2, a_p u^3 with a_p = d lnL / d q_p (p = amp, phase, 6 transfers), into
 // ybd (d lnL / d y directly) and cb1..cb3 (d lnL / d c1..c3), all [9, B, M, L].
-__global__ void k_adj_coeffs(double* ybd, double* cb1, double* cb2, double* cb3, const cplx* gh,
-                             const long long* off, const int* start, const int* len, SplineRefs S,
-                             const double* data_freqs, int N, const double* t_start,
-                             const double* t_end, int b0, int nb) {
+// The warp takes 32 bins at a time: lane j evaluates bin j's eight a_p and the powers of u
+// into shared memory, then lane l owns the sum of (p, k) = (l / 4, l % 4) and adds the 32
+// bins' a_p u^k, so each lane keeps one accumulator instead of 32.
+constexpr int ADJ_THREADS = 256;
+__global__ void __launch_bounds__(ADJ_THREADS)
+k_adj_coeffs(double* ybd, double* cb1, double* cb2, double* cb3, const cplx* gh,
+             const long long* off, const int* start, const int* len, SplineRefs S,
+             const double* data_freqs, int N, const double* t_start, const double* t_end, int b0,
+             int nb) {
+  __shared__ double sa[ADJ_THREADS / 32][32][12];  // per bin: a_0..a_7, 1, u, u^2, u^3
   const int lane = threadIdx.x & 31;
+  double (*w)[12] = sa[threadIdx.x >> 5];
+  const int mp = lane >> 2, mk = lane & 3;
   const long long nseg = (long long)S.L - 1;
   const long long total = (long long)nb * S.M * nseg;
   for (long long wid = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; wid < total;
@@ -131,59 +107,50 @@ __global__ void k_adj_coeffs(double* ybd, double* cb1, double* cb2, double* cb3,
     int k1 = lower_bound_d(data_freqs, N, xs[s + 1]);
     k0 = max(k0, st);
     k1 = min(k1, st + n);
-    double acc[32];
-#pragma unroll
-    for (int q = 0; q < 32; ++q) acc[q] = 0.0;
+    double acc = 0.0;
     const double ts = t_start[b], te = t_end[b];
-    for (int k = k0 + lane; k < k1; k += 32) {
-      const double u = data_freqs[k] - xs[s];
-      double q[9];
-      eval_segment(S, row, s, u, q);
-      if (!tf_gate(q[2], ts, te)) continue;
-      const cplx* g = gh + (off[bl] + (k - st)) * 3;
-      double sn, cs;
-      sincos(q[1], &sn, &cs);
-      const double er = cs, ei = sn;            // e^{i phase}
-      const double aer = q[0] * er, aei = q[0] * ei;  // A e^{i phase}
-      double dA = 0.0, dP = 0.0, dT[6];
+    for (int base = k0; base < k1; base += 32) {
+      const int k = base + lane;
+      double a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      double u = 0.0;
+      if (k < k1) {
+        u = data_freqs[k] - xs[s];
+        double q[9];
+        eval_segment(S, row, s, u, q);
+        if (tf_gate(q[2], ts, te)) {
+          const cplx* g = gh + (off[bl] + (k - st)) * 3;
+          double sn, cs;
+          sincos_cw(q[1], &sn, &cs);
+          const double er = cs, ei = sn;                  // e^{i phase}
+          const double aer = q[0] * er, aei = q[0] * ei;  // A e^{i phase}
 #pragma unroll
-      for (int ch = 0; ch < 3; ++ch) {
-        const cplx u_ = g[ch];
-        const double tr = q[3 + 2 * ch], ti = q[4 + 2 * ch];
-        // dL = Re(u dW), W = T A e^{i phase}
-        const double wr = tr * aer - ti * aei, wi = tr * aei + ti * aer;
-        dA += u_.re * (tr * er - ti * ei) - u_.im * (tr * ei + ti * er);
-        dP += -(u_.re * wi + u_.im * wr);
-        dT[2 * ch] = u_.re * aer - u_.im * aei;
-        dT[2 * ch + 1] = -(u_.re * aei + u_.im * aer);
+          for (int ch = 0; ch < 3; ++ch) {
+            const cplx u_ = g[ch];
+            const double tr = q[3 + 2 * ch], ti = q[4 + 2 * ch];
+            // dL = Re(u dW), W = T A e^{i phase}
+            const double wr = tr * aer - ti * aei, wi = tr * aei + ti * aer;
+            a[0] += u_.re * (tr * er - ti * ei) - u_.im * (tr * ei + ti * er);
+            a[1] += -(u_.re * wi + u_.im * wr);
+            a[2 + 2 * ch] = u_.re * aer - u_.im * aei;
+            a[3 + 2 * ch] = -(u_.re * aei + u_.im * aer);
+          }
+        }
       }
-      const double a[8] = {dA, dP, dT[0], dT[1], dT[2], dT[3], dT[4], dT[5]};
-      const double u2 = u * u, u3 = u2 * u;
 #pragma unroll
-      for (int p = 0; p < 8; ++p) {
-        acc[4 * p] += a[p];
-        acc[4 * p + 1] += a[p] * u;
-        acc[4 * p + 2] += a[p] * u2;
-        acc[4 * p + 3] += a[p] * u3;
-      }
+      for (int p = 0; p < 8; ++p) w[lane][p] = a[p];
+      w[lane][8] = 1.0;
+      w[lane][9] = u;
+      w[lane][10] = u * u;
+      w[lane][11] = u * u * u;
+      __syncwarp();
+      const int cnt = min(32, k1 - base);
+      for (int j = 0; j < cnt; ++j) acc = fma(w[j][mp], w[j][8 + mk], acc);
+      __syncwarp();
     }
-#pragma unroll
-    for (int q = 0; q < 32; ++q) {
-      double v = acc[q];
-      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-      acc[q] = v;
-    }
-    if (lane == 0) {
-#pragma unroll
-      for (int p = 0; p < 8; ++p) {
-        const int slot = (p == 0) ? 0 : (p == 1 ? 1 : p + 1);  // skip t(f), slot 2
-        const size_t i = (size_t)slot * S.n + row * S.L + s;
-        ybd[i] = acc[4 * p];
-        cb1[i] = acc[4 * p + 1];
-        cb2[i] = acc[4 * p + 2];
-        cb3[i] = acc[4 * p + 3];
-      }
-    }
+    const int slot = (mp == 0) ? 0 : (mp == 1 ? 1 : mp + 1);  // skip t(f), slot 2
+    const size_t i = (size_t)slot * S.n + row * S.L + s;
+    double* dst = (mk == 0) ? ybd : (mk == 1) ? cb1 : (mk == 2) ? cb2 : cb3;
+    dst[i] = acc;
   }
 }
 
@@ -369,8 +336,6 @@ int bbhx_direct_like_grad(void* orbits, double* grad, const double* params, cons
       tot += 3ll * hlen[b0 + nb];
       ++nb;
     }
-    int maxlen = 1;
-    for (int q = 0; q < nb; ++q) maxlen = std::max(maxlen, hlen[b0 + q]);
     long long* off = nullptr;
     cplx* gh = nullptr;
     if (pool_alloc((void**)&off, sizeof(long long) * nb, s) != cudaSuccess ||
@@ -383,16 +348,13 @@ int bbhx_direct_like_grad(void* orbits, double* grad, const double* params, cons
       set_error("copy of the support offsets failed");
       st = ERR_CUDA;
     }
-    if (!st) {
-      const int gx = std::min((maxlen + 255) / 256, std::max(1, nsm * 32 / nb));
-      k_adj_gh<<<dim3(gx, nb), 256, 0, s>>>(gh, off, start, len, S, data_freqs, (const cplx*)data,
-                                            noise, data_length, t_start, t_end, b0, nb);
-      st = launch_status("k_adj_gh");
-    }
+    if (!st)  // d lnL / d h by the FP64 fused likelihood kernel (staged segments, tile-major)
+      st = direct_fused_gh(gh, off, start, len, data_freqs, (const double*)data, noise,
+                           data_length, x, y, c1, c2, c3, t_start, t_end, M, L, B, b0, nb, s);
     if (!st) {
       const long long warps = (long long)nb * M * (L - 1);
       const unsigned grid = (unsigned)std::min<long long>((warps + 7) / 8, (long long)nsm * 64);
-      k_adj_coeffs<<<grid, 256, 0, s>>>(ybd, cb, cb + nall, cb + 2 * nall, gh, off, start, len, S,
+      k_adj_coeffs<<<grid, ADJ_THREADS, 0, s>>>(ybd, cb, cb + nall, cb + 2 * nall, gh, off, start, len, S,
                                         data_freqs, data_length, t_start, t_end, b0, nb);
       st = launch_status("k_adj_coeffs");
     }

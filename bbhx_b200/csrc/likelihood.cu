@@ -211,6 +211,11 @@ struct FusedArgs {
   double* h_h;
   const float2* data32;  // optional FP32 copies of data / noise for the mixed form (or null)
   const float* noise32;
+  long long qstride;     // distance between the 9 quantities in y, c1..c3 (B M L of those arrays)
+  // optional, FP64 form (gradient chain): d lnL / d h = 4 w (d~ - w h) of every support bin,
+  // written at gh[3 (gh_off[b] + i - sup_start[b]) + channel]; null in the likelihood calls
+  cplx* gh;
+  const long long* gh_off;
 };
 
 // Segment table: for every (tile, binary, mode) the spline segments holding the first and the
@@ -485,10 +490,11 @@ __device__ __forceinline__ void load_seg(SegCoef<R>& cf, const WarpStage<R>& S, 
 // lowest frequencies) take a per-lane walk over global memory instead.
 // MIXED: phase, t(f), the phase reduction and all accumulations in FP64; amplitude, transfer
 // functions, sin/cos of the reduced phase, the mode sum and the per-bin products in FP32.
-template <bool MIXED, typename R>
+// GH (FP64 form only): also write d lnL / d h of every support bin to A.gh (gradient chain).
+template <bool MIXED, typename R, bool GH = false>
 __device__ __forceinline__ void fused_item(const FusedArgs& A, long long q, WarpStage<R>& S,
                                            int lane) {
-  const long long BML = (long long)A.B * A.M * A.L;
+  const long long BML = A.qstride;
   const int L = A.L;
   {
     const int tile = (int)(q / A.B);
@@ -701,6 +707,10 @@ __device__ __forceinline__ void fused_item(const FusedArgs& A, long long q, Warp
             dr += (double)(dxr * hr + dyr * hi);
             di += (double)(dxr * hi - dyr * hr);
             hh += (double)(hr * hr + hi * hi);
+            if (GH) {
+              const long long o = 3 * (__ldg(A.gh_off + b) + (i - s0)) + c;
+              A.gh[o] = mk(4.0 * (double)w * (d.x - (double)hr), 4.0 * (double)w * (d.y - (double)hi));
+            }
           }
         }
       }
@@ -720,8 +730,9 @@ __device__ __forceinline__ void fused_item(const FusedArgs& A, long long q, Warp
   }
 }
 
-template <bool MIXED>
+template <bool MIXED, bool GH = false>
 __global__ void __launch_bounds__(FD_WARPS * 32, MIXED ? 4 : 3) k_direct_fused(FusedArgs A) {
+  static_assert(!(MIXED && GH), "d lnL / d h is written by the FP64 form only");
   using R = typename std::conditional<MIXED, float, double>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31;
@@ -730,7 +741,7 @@ __global__ void __launch_bounds__(FD_WARPS * 32, MIXED ? 4 : 3) k_direct_fused(F
   const long long nitems = (long long)A.ntiles * A.B;
   const long long gw = (long long)blockIdx.x * FD_WARPS + warp;
   const long long nw = (long long)gridDim.x * FD_WARPS;
-  for (long long q = gw; q < nitems; q += nw) fused_item<MIXED, R>(A, q, S, lane);
+  for (long long q = gw; q < nitems; q += nw) fused_item<MIXED, R, GH>(A, q, S, lane);
 }
 
 // Several independent problems (groups: own data stream, grid length L, mode count M,
@@ -856,6 +867,74 @@ __global__ void k_fused_reduce(const double* partials, const int* sup_start, con
       h_h[2 * b + 1] = 0.0;
     }
   }
+}
+
+}  // namespace bbhx
+
+namespace bbhx {
+
+// d lnL / d h of binaries [b0, b0 + nb) of a [B_all, M, L] sparse-buffer / spline set, by the
+// FP64 fused kernel (gradient chain, gradient.cu): gh packed by the batch-local support
+// offsets gh_off; start / len the support of all B_all binaries (bbhx_template_support).
+int direct_fused_gh(cplx* gh, const long long* gh_off, const int* start, const int* len,
+                    const double* data_freqs, const double* data, const double* noise, int N,
+                    const double* x, const double* y, const double* c1, const double* c2,
+                    const double* c3, const double* t_start, const double* t_end, int M, int L,
+                    int B_all, int b0, int nb, cudaStream_t s) {
+  if (nb == 0) return OK;
+  const int ntiles = (N + FD_TILE - 1) / FD_TILE;
+  const long long nitems = (long long)ntiles * nb;
+  const long long row0 = (long long)b0 * M * L;
+  double* part = nullptr;
+  int2* segtab = nullptr;
+  BBHX_CHECK_CUDA(pool_alloc_all(s, {{(void**)&part, sizeof(double) * 3 * nitems},
+                                     {(void**)&segtab, sizeof(int2) * nitems * M}}));
+  k_tile_segments<<<grid_for(nitems * M, 256, 148 * 64), 256, 0, s>>>(
+      segtab, x + row0, data_freqs, start + b0, len + b0, nb, M, L, ntiles, FD_TILE);
+  int st = launch_status("k_tile_segments");
+  if (!st) {
+    FusedArgs A;
+    A.data_freqs = data_freqs;
+    A.data = (const cplx*)data;
+    A.noise = noise;
+    A.N = N;
+    A.x = x + row0;
+    A.y = y + row0;
+    A.c1 = c1 + row0;
+    A.c2 = c2 + row0;
+    A.c3 = c3 + row0;
+    A.t_start = t_start + b0;
+    A.t_end = t_end + b0;
+    A.sup_start = start + b0;
+    A.sup_len = len + b0;
+    A.B = nb;
+    A.M = M;
+    A.L = L;
+    A.ntiles = ntiles;
+    A.tile = FD_TILE;
+    A.partials = part;
+    A.segtab = segtab;
+    A.d_h = nullptr;
+    A.h_h = nullptr;
+    A.data32 = nullptr;
+    A.noise32 = nullptr;
+    A.qstride = (long long)B_all * M * L;
+    A.gh = gh;
+    A.gh_off = gh_off;
+    const long long g = (nitems + FD_WARPS - 1) / FD_WARPS;
+    const unsigned grid = (unsigned)(g < 148LL * 16 ? g : 148LL * 16);
+    const size_t sm = sizeof(WarpStage<double>) * FD_WARPS;
+    st = cuda_status(cudaFuncSetAttribute(k_direct_fused<false, true>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm),
+                     "cudaFuncSetAttribute(k_direct_fused)");
+    if (!st) {
+      k_direct_fused<false, true><<<grid, FD_WARPS * 32, sm, s>>>(A);
+      st = launch_status("k_direct_fused (d lnL / d h)");
+    }
+  }
+  cudaFreeAsync(part, s);
+  cudaFreeAsync(segtab, s);
+  return st;
 }
 
 }  // namespace bbhx
@@ -998,6 +1077,9 @@ int bbhx_direct_like_multi(const bbhx_direct_group* groups, int num_groups, int 
     A.h_h = (double*)G.h_h;
     A.data32 = (const float2*)G.data32;
     A.noise32 = G.noise32;
+    A.qstride = (long long)A.B * A.M * A.L;
+    A.gh = nullptr;
+    A.gh_off = nullptr;
     MA.off[g] = items;
     MA.boff[g] = bins;
     const long long nit = (long long)A.ntiles * A.B;
@@ -1127,6 +1209,9 @@ int bbhx_direct_like_fused(double* d_h, double* h_h, const double* data_freqs, c
     A.h_h = h_h;
     A.data32 = (precision == 1) ? (const float2*)data32 : nullptr;
     A.noise32 = (precision == 1) ? noise32 : nullptr;
+    A.qstride = (long long)num_bin_all * num_modes * length;
+    A.gh = nullptr;
+    A.gh_off = nullptr;
     const long long warps_needed = (nitems + 0);
     long long g = (warps_needed + FD_WARPS - 1) / FD_WARPS;
     unsigned grid = (unsigned)(g < 148LL * 16 ? g : 148LL * 16);
