@@ -7,6 +7,7 @@
 // Likelihood.cu:356-471).  The chain, for a batch of binaries:
 //   1. the FP64 fused likelihood kernel (likelihood.cu, direct_fused_gh) writes d lnL / d h
 //                     at every (binary, data bin):  g = 4 w (d~ - w h)                  (reverse)
+//                     and the batch's <d|h>, <h|h>
 //   2. k_adj_coeffs   warp per (binary, mode, spline segment): d lnL / d (y, c1, c2, c3) of
 //                     the 8 interpolated quantities, summed over the segment's data bins
 //   3. k_spline_adj   CTA per (binary, mode): adjoint of the not-a-knot spline build; the
@@ -24,11 +25,12 @@
 #include "tridiag.cuh"
 
 namespace bbhx {
-int direct_fused_gh(cplx* gh, const long long* gh_off, const int* start, const int* len,
-                    const double* data_freqs, const double* data, const double* noise, int N,
-                    const double* x, const double* y, const double* c1, const double* c2,
-                    const double* c3, const double* t_start, const double* t_end, int M, int L,
-                    int B_all, int b0, int nb, cudaStream_t s);
+int direct_fused_gh(cplx* gh, const long long* gh_off, double* d_h, double* h_h,
+                    const int* start, const int* len, const double* data_freqs,
+                    const double* data, const double* noise, int N, const double* x,
+                    const double* y, const double* c1, const double* c2, const double* c3,
+                    const double* t_start, const double* t_end, int M, int L, int B_all, int b0,
+                    int nb, cudaStream_t s);
 }  // namespace bbhx
 
 extern "C" int bbhx_template_support(int* start, int* len, const double* x, int num_modes,
@@ -265,7 +267,8 @@ extern "C" {
 // knots x [B, M, L], the noise-weighted data [3, N] (complex128) and noise weights [3, N],
 // params [12, B] (device) and the QNM table for the dual-number setup.  The host reads the
 // support lengths once (one synchronisation).
-int bbhx_direct_like_grad(void* orbits, double* grad, const double* params, const int* ells,
+int bbhx_direct_like_grad(void* orbits, void* d_h, void* h_h, double* grad, const double* params,
+                          const int* ells,
                           const int* mms, const double* qnm_table, int qnm_n, double dspin,
                           double t_init, const double* data_freqs, const void* data,
                           const double* noise, int data_length, const double* x, const double* y,
@@ -349,8 +352,9 @@ int bbhx_direct_like_grad(void* orbits, double* grad, const double* params, cons
       st = ERR_CUDA;
     }
     if (!st)  // d lnL / d h by the FP64 fused likelihood kernel (staged segments, tile-major)
-      st = direct_fused_gh(gh, off, start, len, data_freqs, (const double*)data, noise,
-                           data_length, x, y, c1, c2, c3, t_start, t_end, M, L, B, b0, nb, s);
+      st = direct_fused_gh(gh, off, (double*)d_h, (double*)h_h, start, len, data_freqs,
+                           (const double*)data, noise, data_length, x, y, c1, c2, c3, t_start,
+                           t_end, M, L, B, b0, nb, s);
     if (!st) {
       const long long warps = (long long)nb * M * (L - 1);
       const unsigned grid = (unsigned)std::min<long long>((warps + 7) / 8, (long long)nsm * 64);

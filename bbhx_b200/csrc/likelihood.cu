@@ -875,12 +875,14 @@ namespace bbhx {
 
 // d lnL / d h of binaries [b0, b0 + nb) of a [B_all, M, L] sparse-buffer / spline set, by the
 // FP64 fused kernel (gradient chain, gradient.cu): gh packed by the batch-local support
-// offsets gh_off; start / len the support of all B_all binaries (bbhx_template_support).
-int direct_fused_gh(cplx* gh, const long long* gh_off, const int* start, const int* len,
-                    const double* data_freqs, const double* data, const double* noise, int N,
-                    const double* x, const double* y, const double* c1, const double* c2,
-                    const double* c3, const double* t_start, const double* t_end, int M, int L,
-                    int B_all, int b0, int nb, cudaStream_t s) {
+// offsets gh_off; start / len the support of all B_all binaries (bbhx_template_support);
+// d_h, h_h (complex [B_all], may be null) receive the batch's <d|h>, <h|h>.
+int direct_fused_gh(cplx* gh, const long long* gh_off, double* d_h, double* h_h,
+                    const int* start, const int* len, const double* data_freqs,
+                    const double* data, const double* noise, int N, const double* x,
+                    const double* y, const double* c1, const double* c2, const double* c3,
+                    const double* t_start, const double* t_end, int M, int L, int B_all, int b0,
+                    int nb, cudaStream_t s) {
   if (nb == 0) return OK;
   const int ntiles = (N + FD_TILE - 1) / FD_TILE;
   const long long nitems = (long long)ntiles * nb;
@@ -931,6 +933,11 @@ int direct_fused_gh(cplx* gh, const long long* gh_off, const int* start, const i
       k_direct_fused<false, true><<<grid, FD_WARPS * 32, sm, s>>>(A);
       st = launch_status("k_direct_fused (d lnL / d h)");
     }
+  }
+  if (!st && d_h != nullptr && h_h != nullptr) {
+    k_fused_reduce<<<grid_for(32LL * nb, 128), 128, 0, s>>>(part, start + b0, len + b0, nb,
+                                                            d_h + 2LL * b0, h_h + 2LL * b0);
+    st = launch_status("k_fused_reduce");
   }
   cudaFreeAsync(part, s);
   cudaFreeAsync(segtab, s);

@@ -309,33 +309,27 @@ class BBHWaveformFD:
         t = torch()
         P = params.to(device=device(), dtype=t.float64).contiguous()
         rows = tuple(P[k] for k in range(12))
-        d_h, h_h = self.inner_products(rows, data_freqs, data_weighted, noise_factors,
-                                       t_obs_start=t_obs_start, t_obs_end=t_obs_end,
-                                       length=length, modes=modes, precision="fp64")
+        buf, c1, c2, c3, x, ts, te = self._spline_set(rows, t_obs_start, t_obs_end, length, modes)
         ap, rg = self.amp_phase_gen, self.response_gen
         B, M, L = self.num_bin_all, self.num_modes, self.length
         grad = t.empty((B, 11), dtype=t.float64, device=device())
+        d_h = t.empty(B, dtype=t.complex128, device=device())
+        h_h = t.empty(B, dtype=t.complex128, device=device())
         tab = ap.qnm_table
         from .waveforms.ringdownphenomd import dspin
-        buf, c1, c2, c3, x, ts, te = self._last_spline
-        _lib.call("bbhx_direct_like_grad", rg.orbit_handle.ptr, _lib.dptr(grad), _lib.dptr(P),
+        _lib.call("bbhx_direct_like_grad", rg.orbit_handle.ptr, _lib.dptr(d_h), _lib.dptr(h_h),
+                  _lib.dptr(grad), _lib.dptr(P),
                   _lib.dptr(ap.ells), _lib.dptr(ap.mms), _lib.dptr(tab), int(tab.shape[1]),
                   float(dspin), float(ap.initial_t_val), _lib.dptr(data_freqs),
                   _lib.dptr(data_weighted), _lib.dptr(noise_factors), int(data_freqs.numel()),
                   _lib.dptr(x), _lib.dptr(buf), _lib.dptr(c1), _lib.dptr(c2), _lib.dptr(c3),
                   _lib.dptr(ts), _lib.dptr(te), rg.TDItag_int, int(rg.rescaled), int(rg.tdi2),
                   int(ap.run_phenomd), M, L, B, _lib.stream())
-        self._last_spline = None
         return d_h, h_h, grad
 
-    def inner_products(self, params, data_freqs, data_weighted, noise_factors, t_obs_start=0.0,
-                       t_obs_end=1.0, length=1024, modes=None, flags=None, timing=None,
-                       precision="fp64", data32=None, **unused):
-        """Fused <d|h>, <h|h> for every binary (device complex128 [B] each).
-
-        ``data_weighted`` [3, N] complex = data * sqrt(df / S); ``noise_factors`` [3, N] =
-        sqrt(df / S) (the reference's Likelihood attributes, likelihood.py:99-112).
-        ``data32``: optional (complex64, float32) copies of the two, read by the mixed form."""
+    def _spline_set(self, params, t_obs_start, t_obs_end, length, modes, flags=None):
+        """Sparse buffer [9, B, M, L], its spline coefficients c1..c3, the knots and the
+        per-binary observation limits (device), as the fused likelihood consumes them."""
         t = torch()
         buf, t_start, t_end = self._sparse_buffer(params, t_obs_start, t_obs_end, None, length,
                                                   modes, False, flags=flags)
@@ -346,12 +340,24 @@ class BBHWaveformFD:
         c3 = t.empty_like(buf)
         _lib.call("bbhx_interpolate", _lib.dptr(x), _lib.dptr(buf), _lib._VP(0),
                   _lib.dptr(c1), _lib.dptr(c2), _lib.dptr(c3), L, 9, M, B, _lib.stream())
+        return buf, c1, c2, c3, x, to_dev(t_start), to_dev(t_end)
+
+    def inner_products(self, params, data_freqs, data_weighted, noise_factors, t_obs_start=0.0,
+                       t_obs_end=1.0, length=1024, modes=None, flags=None, timing=None,
+                       precision="fp64", data32=None, **unused):
+        """Fused <d|h>, <h|h> for every binary (device complex128 [B] each).
+
+        ``data_weighted`` [3, N] complex = data * sqrt(df / S); ``noise_factors`` [3, N] =
+        sqrt(df / S) (the reference's Likelihood attributes, likelihood.py:99-112).
+        ``data32``: optional (complex64, float32) copies of the two, read by the mixed form."""
+        t = torch()
+        # ts_d / te_d stay referenced across the call: a temporary freed inside the argument
+        # list can be handed back by the caching allocator to the next one
+        buf, c1, c2, c3, x, ts_d, te_d = self._spline_set(params, t_obs_start, t_obs_end, length,
+                                                          modes, flags=flags)
+        B, M, L = self.num_bin_all, self.num_modes, self.length
         d_h = t.empty(B, dtype=t.complex128, device=device())
         h_h = t.empty(B, dtype=t.complex128, device=device())
-        # keep both device copies referenced across the call: a temporary freed inside the
-        # argument list can be handed back by the caching allocator to the next one
-        ts_d = to_dev(t_start)
-        te_d = to_dev(t_end)
         if timing is not None:  # optional CUDA events around the fused kernel (benchmarks)
             ev0 = t.cuda.Event(enable_timing=True)
             ev1 = t.cuda.Event(enable_timing=True)
@@ -366,5 +372,4 @@ class BBHWaveformFD:
             ev1.record()
             timing.setdefault("fused", []).append((ev0, ev1))
             self._last_x = x
-        self._last_spline = (buf, c1, c2, c3, x, ts_d, te_d)
         return d_h, h_h

@@ -243,8 +243,11 @@ int bbhx_hdyn_grad(void *orbits, void *d_h, void *h_h, double *grad, const void 
    and the not-a-knot spline build (transposed tridiagonal solve), forward-mode tangents of
    PhenomHM + TDI at the knots.  x [B, M, L] knots; y, c1, c2, c3 [9, B, M, L] from the forward
    path (bbhx_waveform_response_fused + bbhx_interpolate); data [3, N] complex128 noise-weighted,
-   noise [3, N]; params [12, B]; theta as for bbhx_hdyn_grad.  Knots are held fixed. */
-int bbhx_direct_like_grad(void *orbits, double *grad, const double *params, const int *ells,
+   noise [3, N]; params [12, B]; theta as for bbhx_hdyn_grad.  Knots are held fixed.
+   d_h, h_h: device complex128 [B], overwritten with <d|h>, <h|h> of the same evaluation (as
+   bbhx_direct_like_fused in FP64, so no separate likelihood call is needed). */
+int bbhx_direct_like_grad(void *orbits, void *d_h, void *h_h, double *grad,
+                          const double *params, const int *ells,
                           const int *mms, const double *qnm_table, int qnm_n, double dspin,
                           double t_init, const double *data_freqs, const void *data,
                           const double *noise, int data_length, const double *x, const double *y,
