@@ -15,6 +15,7 @@ import numpy as np
 from . import _lib
 from .sensitivity import AET1SensitivityMatrix, SensitivityMatrix
 from .utils.arrays import device, to_dev, to_np, torch
+from .waveformbuild import PRECISIONS
 
 
 class Likelihood:
@@ -51,6 +52,16 @@ class Likelihood:
     @property
     def xp(self):
         return torch()
+
+    @property
+    def precision(self):
+        return self._precision
+
+    @precision.setter
+    def precision(self, value):
+        if value not in PRECISIONS:
+            raise ValueError(f"precision must be one of {sorted(PRECISIONS)}, got {value!r}")
+        self._precision = value
 
     def get_ll(self, params, return_extracted_snr=False, phase_marginalize=False,
                **waveform_kwargs):
@@ -158,6 +169,16 @@ class HeterodynedLikelihood:
     @property
     def xp(self):
         return torch()
+
+    @property
+    def precision(self):
+        return self._precision
+
+    @precision.setter
+    def precision(self, value):
+        if value is not None and value not in PRECISIONS:
+            raise ValueError(f"precision must be None or one of {sorted(PRECISIONS)}, got {value!r}")
+        self._precision = value
 
     @property
     def sens_mat(self):

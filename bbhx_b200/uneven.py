@@ -143,6 +143,8 @@ class UnevenBatch:
                  shape=None):
         self.direct = list(direct_groups)
         self.het = list(het_groups)
+        if precision not in PRECISIONS:
+            raise ValueError(f"precision must be one of {sorted(PRECISIONS)}, got {precision!r}")
         self.precision = precision
         self.autotuner = autotuner if autotuner is not None else Autotuner()
         self.shape = shape  # (tile_bins, ctas_per_sm); None -> autotune on first run
