@@ -489,7 +489,9 @@ __device__ __forceinline__ void load_seg(SegCoef<R>& cf, const WarpStage<R>& S, 
 // block-wide barrier is involved.  Tiles whose modes span more than FD_NSEG segments (only the
 // lowest frequencies) take a per-lane walk over global memory instead.
 // MIXED: phase, t(f), the phase reduction and all accumulations in FP64; amplitude, transfer
-// functions, sin/cos of the reduced phase, the mode sum and the per-bin products in FP32.
+// functions, sin/cos of the reduced phase and the mode sum (the template) in FP32; the per-bin
+// products with data and weights in FP64 when the FP32 copies of data and weights are given
+// (the path of Likelihood and UnevenBatch), in FP32 without them.
 // GH (FP64 form only): also write d lnL / d h of every support bin to A.gh (gradient chain).
 template <bool MIXED, typename R, bool GH = false>
 __device__ __forceinline__ void fused_item(const FusedArgs& A, long long q, WarpStage<R>& S,
@@ -672,25 +674,25 @@ __device__ __forceinline__ void fused_item(const FusedArgs& A, long long q, Warp
         }
       }
       if (MIXED && A.data32 != nullptr) {
-        // FP32 data and weights; one bin's three channels summed in FP32, bins in FP64
+        // FP32 data and weights, FP32 template; the per-bin products w h, conj(d) w h and
+        // |w h|^2 in FP64: their FP32 rounding (random per bin, ~1e-7 relative) summed over the
+        // loud bins of <h|h> would leave ~1e-2..1e-1 in lnL near the peak of an SNR ~ 5000
+        // source, where the FP32 template error itself enters only through d - h
 #pragma unroll
         for (int j = 0; j < FD_K; ++j) {
           if (fbin[j] < 0.0) continue;
           const int i = c0 + 32 * j + lane;
-          float cr = 0.f, ci = 0.f, ch = 0.f;
 #pragma unroll
           for (int c = 0; c < 3; ++c) {
             const long long gi = (long long)c * A.N + i;
-            const float w = __ldg(A.noise32 + gi);
+            const double w = (double)__ldg(A.noise32 + gi);
             const float2 d = __ldg(A.data32 + gi);
-            const float hr = (float)acc[j][2 * c] * w, hi = (float)acc[j][2 * c + 1] * w;
-            cr = fmaf(d.x, hr, fmaf(d.y, hi, cr));
-            ci = fmaf(d.x, hi, fmaf(-d.y, hr, ci));
-            ch = fmaf(hr, hr, fmaf(hi, hi, ch));
+            const double hr = (double)acc[j][2 * c] * w, hi = (double)acc[j][2 * c + 1] * w;
+            const double dx = (double)d.x, dy = (double)d.y;
+            dr = fma(dx, hr, fma(dy, hi, dr));
+            di = fma(dx, hi, fma(-dy, hr, di));
+            hh = fma(hr, hr, fma(hi, hi, hh));
           }
-          dr += (double)cr;
-          di += (double)ci;
-          hh += (double)ch;
         }
       } else {
 #pragma unroll
