@@ -545,15 +545,17 @@ int bbhx_hdyn_fused(void* orbits, void* d_h, void* h_h, const void* coeffs, cons
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     const unsigned grid = (unsigned)std::min<long long>(num_bin_all, (long long)nsm * 16);
     if (precision == 1) {
-      BBHX_CHECK_CUDA(cudaFuncSetAttribute(k_het_fused<true>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      k_het_fused<true><<<grid, HET_THREADS, smem, s>>>(A);
+      st = cuda_status(cudaFuncSetAttribute(k_het_fused<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem),
+                       "cudaFuncSetAttribute(k_het_fused<true>)");
+      if (!st) k_het_fused<true><<<grid, HET_THREADS, smem, s>>>(A);
     } else {
-      BBHX_CHECK_CUDA(cudaFuncSetAttribute(k_het_fused<false>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      k_het_fused<false><<<grid, HET_THREADS, smem, s>>>(A);
+      st = cuda_status(cudaFuncSetAttribute(k_het_fused<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem),
+                       "cudaFuncSetAttribute(k_het_fused<false>)");
+      if (!st) k_het_fused<false><<<grid, HET_THREADS, smem, s>>>(A);
     }
-    st = launch_status("k_het_fused");
+    if (!st) st = launch_status("k_het_fused");
   }
   cudaFreeAsync(rm, s);
   return st;

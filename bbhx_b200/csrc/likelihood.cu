@@ -1141,16 +1141,18 @@ int bbhx_direct_like_multi(const bbhx_direct_group* groups, int num_groups, int 
     const unsigned grid = (unsigned)std::min<long long>(want, (long long)nsm * ctas_per_sm);
     if (precision == 1) {
       const size_t sm = sizeof(WarpStage<float>) * FD_WARPS;
-      BBHX_CHECK_CUDA(cudaFuncSetAttribute(k_direct_fused_multi<true>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-      k_direct_fused_multi<true><<<grid, FD_WARPS * 32, sm, s>>>(dMA);
+      st = cuda_status(cudaFuncSetAttribute(k_direct_fused_multi<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sm),
+                       "cudaFuncSetAttribute(k_direct_fused_multi<true>)");
+      if (!st) k_direct_fused_multi<true><<<grid, FD_WARPS * 32, sm, s>>>(dMA);
     } else {
       const size_t sm = sizeof(WarpStage<double>) * FD_WARPS;
-      BBHX_CHECK_CUDA(cudaFuncSetAttribute(k_direct_fused_multi<false>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-      k_direct_fused_multi<false><<<grid, FD_WARPS * 32, sm, s>>>(dMA);
+      st = cuda_status(cudaFuncSetAttribute(k_direct_fused_multi<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sm),
+                       "cudaFuncSetAttribute(k_direct_fused_multi<false>)");
+      if (!st) k_direct_fused_multi<false><<<grid, FD_WARPS * 32, sm, s>>>(dMA);
     }
-    st = launch_status("k_direct_fused_multi");
+    if (!st) st = launch_status("k_direct_fused_multi");
   }
   if (!st && bins > 0) {
     k_fused_reduce_multi<<<grid_for(32LL * bins, 128), 128, 0, s>>>(dMA);
@@ -1226,16 +1228,18 @@ int bbhx_direct_like_fused(double* d_h, double* h_h, const double* data_freqs, c
     unsigned grid = (unsigned)(g < 148LL * 16 ? g : 148LL * 16);
     if (precision == 1) {
       const size_t sm = sizeof(WarpStage<float>) * FD_WARPS;
-      BBHX_CHECK_CUDA(cudaFuncSetAttribute(k_direct_fused<true>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-      k_direct_fused<true><<<grid, FD_WARPS * 32, sm, s>>>(A);
+      st = cuda_status(cudaFuncSetAttribute(k_direct_fused<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sm),
+                       "cudaFuncSetAttribute(k_direct_fused<true>)");
+      if (!st) k_direct_fused<true><<<grid, FD_WARPS * 32, sm, s>>>(A);
     } else {
       const size_t sm = sizeof(WarpStage<double>) * FD_WARPS;
-      BBHX_CHECK_CUDA(cudaFuncSetAttribute(k_direct_fused<false>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-      k_direct_fused<false><<<grid, FD_WARPS * 32, sm, s>>>(A);
+      st = cuda_status(cudaFuncSetAttribute(k_direct_fused<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sm),
+                       "cudaFuncSetAttribute(k_direct_fused<false>)");
+      if (!st) k_direct_fused<false><<<grid, FD_WARPS * 32, sm, s>>>(A);
     }
-    st = launch_status("k_direct_fused");
+    if (!st) st = launch_status("k_direct_fused");
   }
   if (!st) {
     k_fused_reduce<<<grid_for(32LL * num_bin_all, 128), 128, 0, s>>>(part, sup, sup + num_bin_all,
