@@ -61,6 +61,28 @@ __device__ __forceinline__ int lower_bound_d(const double* f, int n, double v) {
   return a;
 }
 
+// lower_bound_d with the index guessed from the grid's end points (exact for a uniform grid,
+// the common case) and checked by at most four one-step moves; otherwise the binary search.
+// Same result as lower_bound_d for any sorted grid.
+__device__ __forceinline__ int lower_bound_guess(const double* f, int n, double v) {
+  if (n == 0) return 0;
+  const double f0 = f[0], f1 = f[n - 1];
+  if (!(v > f0)) return 0;
+  if (v > f1) return n;  // here f0 < v <= f1, so n >= 2 and the answer is in [1, n - 1]
+  int k = (int)ceil((v - f0) / (f1 - f0) * (double)(n - 1));
+  k = min(max(k, 1), n - 1);
+  for (int it = 0; it < 4; ++it) {
+    if (f[k] < v) {
+      ++k;  // k < answer <= n - 1
+    } else if (f[k - 1] >= v) {
+      --k;  // k - 1 >= answer >= 1
+    } else {
+      return k;
+    }
+  }
+  return lower_bound_d(f, n, v);
+}
+
 struct SplineRefs {
   const double *x, *y, *c1, *c2, *c3;  // x [B, M, L]; y, c1..c3 [9, B, M, L]
   size_t n;                            // B * M * L
@@ -105,8 +127,8 @@ k_adj_coeffs(double* ybd, double* cb1, double* cb2, double* cb3, const cplx* gh,
     const size_t row = (size_t)b * S.M + m;
     const double* xs = S.x + row * S.L;
     const int st = start[b], n = len[b];
-    int k0 = lower_bound_d(data_freqs, N, xs[s]);
-    int k1 = lower_bound_d(data_freqs, N, xs[s + 1]);
+    int k0 = lower_bound_guess(data_freqs, N, xs[s]);
+    int k1 = lower_bound_guess(data_freqs, N, xs[s + 1]);
     k0 = max(k0, st);
     k1 = min(k1, st + n);
     double acc = 0.0;
