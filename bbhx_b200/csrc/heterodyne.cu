@@ -282,8 +282,9 @@ struct HetArgs {
   cplx* gh;  // optional [B, 3, L]: d lnL / d h (adjoint of the bin sums and of r = h / h0)
 };
 
-// Dynamic shared memory: ModeCoeffs[M] | ResponseMode[M] | AmpModeF[M] | RespModeF[M] |
-// r[3][L] (cplx), each region starting on a 16-byte boundary.
+// Dynamic shared memory of one warp (walker): ModeCoeffs[M] | ResponseMode[M] | AmpModeF[M] |
+// RespModeF[M] | r[3][L] (cplx), each region starting on a 16-byte boundary; a CTA holds one
+// such slice per warp.
 __host__ __device__ __forceinline__ size_t align16(size_t n) { return (n + 15) & ~(size_t)15; }
 
 struct HetSmemLayout {
@@ -297,40 +298,44 @@ struct HetSmemLayout {
   }
 };
 
+// One WARP per walker (each lane takes the frequencies lane, lane + 32, ...), each warp with
+// its own slice of shared memory: no block-wide barrier, so a warp never waits for another
+// walker's slower points or for the serial per-walker set-up of the others.
 template <bool MIXED>
 __global__ void __launch_bounds__(HET_THREADS) k_het_fused(HetArgs A) {
   extern __shared__ __align__(16) unsigned char het_smem[];
   const HetSmemLayout lay(A.M, A.L);
-  ModeCoeffs* sc = (ModeCoeffs*)het_smem;
-  ResponseMode* sr = (ResponseMode*)(het_smem + lay.sr);
-  AmpModeF* sa = (AmpModeF*)(het_smem + lay.sa);
-  RespModeF* sf = (RespModeF*)(het_smem + lay.sf);
-  cplx* rr = (cplx*)(het_smem + lay.rr);
-  __shared__ double red[4][HET_THREADS / 32];
+  const int lane = threadIdx.x & 31;
+  const int nwarps = blockDim.x >> 5;
+  unsigned char* base = het_smem + (size_t)(threadIdx.x >> 5) * align16(lay.total);
+  ModeCoeffs* sc = (ModeCoeffs*)base;
+  ResponseMode* sr = (ResponseMode*)(base + lay.sr);
+  AmpModeF* sa = (AmpModeF*)(base + lay.sa);
+  RespModeF* sf = (RespModeF*)(base + lay.sf);
+  cplx* rr = (cplx*)(base + lay.rr);
 
-  for (int b = blockIdx.x; b < A.B; b += gridDim.x) {
-    __syncthreads();  // previous walker's shared data no longer in use
+  for (int b = blockIdx.x * nwarps + (threadIdx.x >> 5); b < A.B; b += gridDim.x * nwarps) {
+    __syncwarp();  // previous walker's shared data no longer in use
     {
       const unsigned long long* src = (const unsigned long long*)(A.coeffs + (size_t)b * A.M);
       unsigned long long* dst = (unsigned long long*)sc;
       const int n = (int)(sizeof(ModeCoeffs) * A.M / 8);
-      for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+      for (int i = lane; i < n; i += 32) dst[i] = src[i];
       src = (const unsigned long long*)(A.rmodes + (size_t)b * A.M);
       dst = (unsigned long long*)sr;
       const int n2 = (int)(sizeof(ResponseMode) * A.M / 8);
-      for (int i = threadIdx.x; i < n2; i += blockDim.x) dst[i] = src[i];
+      for (int i = lane; i < n2; i += 32) dst[i] = src[i];
     }
-    __syncthreads();
+    __syncwarp();
     if (MIXED) {
-      if (threadIdx.x < A.M) build_amp_f(sa[threadIdx.x], sc[threadIdx.x]);
-      else if (threadIdx.x >= 32 && threadIdx.x < 32 + A.M)
-        build_resp_f(sf[threadIdx.x - 32], sr[threadIdx.x - 32]);
-      __syncthreads();
+      if (lane < A.M) build_amp_f(sa[lane], sc[lane]);
+      else if (lane >= 16 && lane < 16 + A.M) build_resp_f(sf[lane - 16], sr[lane - 16]);
+      __syncwarp();
     }
     const double tr = A.t_ref[b];
     const double ts = A.t_start[b], te = A.t_end[b];
 
-    for (int j = threadIdx.x; j < A.L; j += blockDim.x) {
+    for (int j = lane; j < A.L; j += 32) {
       const double f = A.freqs[j];
       double h[6] = {0, 0, 0, 0, 0, 0};
       for (int m = 0; m < A.M; ++m) {
@@ -382,11 +387,11 @@ __global__ void __launch_bounds__(HET_THREADS) k_het_fused(HetArgs A) {
                               (h[2 * ch + 1] * d.re - h[2 * ch] * d.im) / den);
       }
     }
-    __syncthreads();
+    __syncwarp();
 
     // relative-binning bin terms, hdynLikelihood (Likelihood.cu:20-123): bin j >= 1
     double dre = 0, dim = 0, hre = 0, him = 0;
-    for (int j = 1 + threadIdx.x; j < A.L; j += blockDim.x) {
+    for (int j = 1 + lane; j < A.L; j += 32) {
       const double fj = A.freqs[j], fp = A.freqs[j - 1];
       if (fp == 0.0) continue;
       const double df = fj - fp;
@@ -413,7 +418,7 @@ __global__ void __launch_bounds__(HET_THREADS) k_het_fused(HetArgs A) {
       // Adjoint of lnL = Re d_h - (d_d + Re h_h) / 2 through the bin terms: per bin
       // g_r0 = A0 - Re(B0) r0 - Re(B1) r1, g_r1 = A1 - Re(B1) r0, carried to r_j / r_{j-1}
       // with the same coefficients as the forward r0, r1; then g_h = g_r / conj(h0).
-      for (int j = threadIdx.x; j < A.L; j += blockDim.x) {
+      for (int j = lane; j < A.L; j += 32) {
 #pragma unroll
         for (int ch = 0; ch < 3; ++ch) {
           cplx g = mk(0.0, 0.0);
@@ -450,24 +455,9 @@ __global__ void __launch_bounds__(HET_THREADS) k_het_fused(HetArgs A) {
       hre += __shfl_xor_sync(0xffffffffu, hre, o);
       him += __shfl_xor_sync(0xffffffffu, him, o);
     }
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    if (l == 0) {
-      red[0][w] = dre;
-      red[1][w] = dim;
-      red[2][w] = hre;
-      red[3][w] = him;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double a = 0, bb = 0, c = 0, d = 0;
-      for (int k = 0; k < HET_THREADS / 32; ++k) {
-        a += red[0][k];
-        bb += red[1][k];
-        c += red[2][k];
-        d += red[3][k];
-      }
-      A.d_h[b] = mk(a, bb);
-      A.h_h[b] = mk(c, d);
+    if (lane == 0) {
+      A.d_h[b] = mk(dre, dim);
+      A.h_h[b] = mk(hre, him);
     }
   }
 }
@@ -483,6 +473,24 @@ __global__ void k_response_setup_het(ResponseMode* out, const int* ells, const i
     response_mode_setup(r, ells[i], mms[i], phi_ref[b], inc[b], lam[b], beta[b], psi[b]);
     out[t] = r;
   }
+}
+
+// Warps (walkers) per CTA of k_het_fused and its dynamic shared memory: up to
+// HET_THREADS / 32 warps, as many slices as fit in the opt-in per-block shared memory.
+inline int het_launch_shape(int M, int L, int* threads, size_t* smem) {
+  const size_t slice = align16(HetSmemLayout(M, L).total);
+  int dev = 0, limit = 48 * 1024;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&limit, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  const int w = std::min<int>(HET_THREADS / 32, (int)((size_t)limit / slice));
+  if (w < 1) {
+    set_error("heterodyne length %d needs %zu B of shared memory per walker (limit %d)", L,
+              slice, limit);
+    return ERR_TOO_LARGE;
+  }
+  *threads = 32 * w;
+  *smem = slice * w;
+  return OK;
 }
 
 }  // namespace bbhx
@@ -539,21 +547,25 @@ int bbhx_hdyn_fused(void* orbits, void* d_h, void* h_h, const void* coeffs, cons
     A.M = num_modes;
     A.L = length;
     A.B = num_bin_all;
-    const size_t smem = HetSmemLayout(num_modes, length).total;
+    int threads = HET_THREADS;
+    size_t smem = 0;
+    st = het_launch_shape(num_modes, length, &threads, &smem);
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    const unsigned grid = (unsigned)std::min<long long>(num_bin_all, (long long)nsm * 16);
-    if (precision == 1) {
+    const long long wpc = threads / 32;
+    const unsigned grid =
+        (unsigned)std::min<long long>((num_bin_all + wpc - 1) / wpc, (long long)nsm * 16);
+    if (!st && precision == 1) {
       st = cuda_status(cudaFuncSetAttribute(k_het_fused<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem),
                        "cudaFuncSetAttribute(k_het_fused<true>)");
-      if (!st) k_het_fused<true><<<grid, HET_THREADS, smem, s>>>(A);
-    } else {
+      if (!st) k_het_fused<true><<<grid, threads, smem, s>>>(A);
+    } else if (!st) {
       st = cuda_status(cudaFuncSetAttribute(k_het_fused<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem),
                        "cudaFuncSetAttribute(k_het_fused<false>)");
-      if (!st) k_het_fused<false><<<grid, HET_THREADS, smem, s>>>(A);
+      if (!st) k_het_fused<false><<<grid, threads, smem, s>>>(A);
     }
     if (!st) st = launch_status("k_het_fused");
   }
@@ -622,17 +634,21 @@ int bbhx_hdyn_grad(void* orbits, void* d_h, void* h_h, double* grad, const void*
     A.M = num_modes;
     A.L = length;
     A.B = num_bin_all;
-    const size_t smem = HetSmemLayout(num_modes, length).total;
+    int threads = HET_THREADS;
+    size_t smem = 0;
+    st = het_launch_shape(num_modes, length, &threads, &smem);
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    const unsigned grid = (unsigned)std::min<long long>(num_bin_all, (long long)nsm * 16);
-    if (cudaFuncSetAttribute(k_het_fused<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem) != cudaSuccess) {
+    const long long wpc = threads / 32;
+    const unsigned grid =
+        (unsigned)std::min<long long>((num_bin_all + wpc - 1) / wpc, (long long)nsm * 16);
+    if (!st && cudaFuncSetAttribute(k_het_fused<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem) != cudaSuccess) {
       set_error("cudaFuncSetAttribute failed for k_het_fused");
       st = ERR_CUDA;
-    } else {
-      k_het_fused<false><<<grid, HET_THREADS, smem, s>>>(A);
+    } else if (!st) {
+      k_het_fused<false><<<grid, threads, smem, s>>>(A);
       st = launch_status("k_het_fused (gradient forward)");
     }
     for (int b0 = 0; !st && b0 < num_bin_all; b0 += chunk) {

@@ -213,7 +213,7 @@ int bbhx_direct_like_fused(double *d_h, double *h_h, const double *data_freqs, c
                            const float *noise32, void *stream);
 
 /* fused heterodyned likelihood: PhenomHM + TDI response at the sparse heterodyne grid, mode
-   sum, r = h / h0 and the relative-binning bin sums in one kernel (one CTA per walker).
+   sum, r = h / h0 and the relative-binning bin sums in one kernel (one warp per walker).
    Replaces, as one call, waveform_amp_phase (PhenomHMWaveform.hh:354-371) + LISA_response
    (Response.hh:27-41) + direct_sum (WaveformBuild.hh:8-10) + the host-side ratio
    (likelihood.py:606-616) + hdyn (Likelihood.hh:6-9, GPU form: every bin j >= 1).
