@@ -182,11 +182,14 @@ __global__ void k_support(const double* __restrict__ x, int M, int L, int B,
 constexpr int FD_WARPS = 4;
 constexpr int FD_K = 4;                          // bins per lane per warp chunk
 constexpr int FD_WARP_BINS = 32 * FD_K;          // 128
-constexpr int FD_TILE = FD_WARPS * FD_WARP_BINS;  // 512
+// data bins per (tile, binary) work item of the single-group kernel: large tiles spread the
+// per-item staging, segment table and gate classification over more bins (B = 1024 benchmark:
+// 512 -> 104 ms, 1024 -> 88, 2048 -> 80, 4096 -> 78, 8192 -> 79 ms mixed)
+constexpr int FD_TILE = 4096;
 constexpr int FD_NSEG = 8;    // spline segments per (tile, mode) staged in shared memory
 constexpr int FD_MAXM = 6;    // modes per binary
 constexpr int FD_NC = 36;     // 9 quantities x (y, c1, c2, c3) per segment
-constexpr int FD_MAXCHUNK = 8;  // 128-bin chunks per tile item (tiles of up to 1024 bins)
+constexpr int FD_MAXCHUNK = 32;  // 128-bin chunks per tile item (tiles of up to 4096 bins)
 
 struct FusedArgs {
   const double* data_freqs;

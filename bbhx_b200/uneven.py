@@ -104,7 +104,7 @@ class Autotuner:
     """Times the persistent kernel's launch shapes on a prepared batch and keeps the fastest
     per batch signature (in memory; ``table`` can be saved / preloaded by the caller)."""
 
-    TILES = (256, 512, 1024)
+    TILES = (1024, 2048, 4096)
     CTAS = (2, 3, 4, 8)
 
     def __init__(self, table=None, repeats=2):

@@ -190,7 +190,7 @@ typedef struct {
 
 /* Several direct-likelihood problems (uneven grid lengths, mode sets and observation spans) in
    ONE persistent launch of the fused kernel; no reference counterpart.  groups is a HOST array
-   of num_groups <= 64 descriptors; tile_bins (multiple of 128) and ctas_per_sm are the launch
+   of num_groups <= 64 descriptors; tile_bins (multiple of 128, at most 4096) and ctas_per_sm are the launch
    shape (chosen by bbhx_b200.uneven.Autotuner).  Stream-ordered and free of host
    synchronisation, so it can be captured in a CUDA graph. */
 int bbhx_direct_like_multi(const bbhx_direct_group *groups, int num_groups, int precision,
