@@ -736,7 +736,7 @@ __device__ __forceinline__ void fused_item(const FusedArgs& A, long long q, Warp
 }
 
 template <bool MIXED, bool GH = false>
-__global__ void __launch_bounds__(FD_WARPS * 32, MIXED ? 4 : 3) k_direct_fused(FusedArgs A) {
+__global__ void __launch_bounds__(FD_WARPS * 32, MIXED ? 4 : 2) k_direct_fused(FusedArgs A) {
   static_assert(!(MIXED && GH), "d lnL / d h is written by the FP64 form only");
   using R = typename std::conditional<MIXED, float, double>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -770,7 +770,7 @@ __global__ void k_store_groups(MultiArgs M, MultiArgs* dst) {
 }
 
 template <bool MIXED>
-__global__ void __launch_bounds__(FD_WARPS * 32, MIXED ? 4 : 3)
+__global__ void __launch_bounds__(FD_WARPS * 32, MIXED ? 4 : 2)
     k_direct_fused_multi(const MultiArgs* __restrict__ MA) {
   using R = typename std::conditional<MIXED, float, double>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
