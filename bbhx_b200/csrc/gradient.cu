@@ -89,17 +89,6 @@ struct SplineRefs {
   int M, L;
 };
 
-// The 9 interpolated quantities of (binary b, mode m) in segment s at u = f - x_s.
-__device__ __forceinline__ void eval_segment(const SplineRefs& S, size_t row, int s, double u,
-                                             double* q) {
-  const size_t o = row * S.L + s;
-#pragma unroll
-  for (int p = 0; p < 9; ++p) {
-    const size_t i = (size_t)p * S.n + o;
-    q[p] = S.y[i] + u * (S.c1[i] + u * (S.c2[i] + u * S.c3[i]));
-  }
-}
-
 // 2. Warp per (local binary, mode, segment s < L-1): sums over the segment's data bins of
 // a_p, a_p u, a_p u^2, a_p u^3 with a_p = d lnL / d q_p (p = amp, phase, 6 transfers), into
 // ybd (d lnL / d y directly) and cb1..cb3 (d lnL / d c1..c3), all [9, B, M, L].
@@ -113,8 +102,10 @@ k_adj_coeffs(double* ybd, double* cb1, double* cb2, double* cb3, const cplx* gh,
              const double* data_freqs, int N, const double* t_start, const double* t_end, int b0,
              int nb) {
   __shared__ double sa[ADJ_THREADS / 32][32][12];  // per bin: a_0..a_7, 1, u, u^2, u^3
+  __shared__ double scw[ADJ_THREADS / 32][36];      // the segment's (y, c1, c2, c3) x 9
   const int lane = threadIdx.x & 31;
   double (*w)[12] = sa[threadIdx.x >> 5];
+  double* cw = scw[threadIdx.x >> 5];
   const int mp = lane >> 2, mk = lane & 3;
   const long long nseg = (long long)S.L - 1;
   const long long total = (long long)nb * S.M * nseg;
@@ -133,6 +124,12 @@ k_adj_coeffs(double* ybd, double* cb1, double* cb2, double* cb3, const cplx* gh,
     k1 = min(k1, st + n);
     double acc = 0.0;
     const double ts = t_start[b], te = t_end[b];
+    __syncwarp();  // the previous item's coefficients are no longer read
+    for (int i = lane; i < 36; i += 32) {
+      const double* src = (i & 3) == 0 ? S.y : (i & 3) == 1 ? S.c1 : (i & 3) == 2 ? S.c2 : S.c3;
+      cw[i] = src[(size_t)(i >> 2) * S.n + row * S.L + s];
+    }
+    __syncwarp();
     for (int base = k0; base < k1; base += 32) {
       const int k = base + lane;
       double a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -140,7 +137,9 @@ k_adj_coeffs(double* ybd, double* cb1, double* cb2, double* cb3, const cplx* gh,
       if (k < k1) {
         u = data_freqs[k] - xs[s];
         double q[9];
-        eval_segment(S, row, s, u, q);
+#pragma unroll
+        for (int p = 0; p < 9; ++p)
+          q[p] = cw[4 * p] + u * (cw[4 * p + 1] + u * (cw[4 * p + 2] + u * cw[4 * p + 3]));
         if (tf_gate(q[2], ts, te)) {
           const cplx* g = gh + (off[bl] + (k - st)) * 3;
           double sn, cs;
