@@ -21,6 +21,7 @@ _LL = ctypes.c_longlong
 _SIGS = {
     "bbhx_version": [],
     "bbhx_stream_synchronize": [_VP],
+    "bbhx_take_status": [_VP],
     "bbhx_pointer_is_device": [_VP],
     "bbhx_mode_coeffs_bytes": [],
     "bbhx_response_mode_bytes": [],

@@ -28,16 +28,22 @@ constexpr double INVSQRT3 = 0.577350269189625764509148780501957455;
 constexpr double INVSQRT6 = 0.408248290463863016366214012450981898;
 constexpr double Omega0 = 1.9909865927683788e-07;
 
-// status codes returned by every C-ABI entry point
+// status codes returned by every C-ABI entry point (3 is unused: no kernel of the library
+// waits on another CTA, stream or device, so nothing can time out)
 enum Status : int {
   OK = 0,
   ERR_BAD_ARG = 1,
   ERR_CUDA = 2,
-  ERR_TIMEOUT = 3,
   ERR_NONFINITE = 4,
   ERR_NO_ORBITS = 5,
   ERR_TOO_LARGE = 6,
 };
+
+// Set *word when any of the values is NaN or infinite (the sum is non-finite then).
+__device__ __forceinline__ void note_nonfinite(unsigned* word, double a, double b, double c,
+                                               double d) {
+  if (!isfinite(a + b + c + d)) atomicOr(word, 1u);
+}
 
 // Complex numbers over any real scalar T (double, float, or the dual numbers of the
 // gradient kernels).  In the scalar products the scalar is converted to T, so double

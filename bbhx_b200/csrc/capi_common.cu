@@ -16,6 +16,24 @@ void set_error(const char* fmt, ...) {
 
 const char* get_error() { return g_err; }
 
+int sm_count() {
+  static int cached[256] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) {
+    cudaGetLastError();
+    return 148;
+  }
+  if (cached[dev] == 0) {
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) {
+      cudaGetLastError();
+      return 148;
+    }
+    cached[dev] = n;
+  }
+  return cached[dev];
+}
+
 int retain_pool_memory() {
   static bool done[256] = {};
   int dev = 0;
@@ -58,6 +76,21 @@ int bbhx_selftest_sincos(const double* x, double* out, int n, void* stream) {
 const char* bbhx_last_error_string(void) { return bbhx::get_error(); }
 
 int bbhx_version(void) { return 100; }
+
+// Synchronise the stream, then report (and clear) non-finite likelihood outputs written by
+// any call since the previous check on this device: 4 if a <d|h> or <h|h> was NaN / inf.
+int bbhx_take_status(void* stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned any = 0;
+  int st = bbhx::take_nonfinite_likelihood(s, &any);
+  if (!st) st = bbhx::take_nonfinite_heterodyne(s, &any);
+  if (st) return st;
+  if (any) {
+    bbhx::set_error("a likelihood output (<d|h> or <h|h>) was not finite");
+    return bbhx::ERR_NONFINITE;
+  }
+  return bbhx::OK;
+}
 
 int bbhx_stream_synchronize(void* stream) {
   BBHX_CHECK_CUDA(cudaStreamSynchronize((cudaStream_t)stream));

@@ -73,7 +73,18 @@ inline cudaError_t pool_alloc_all(cudaStream_t s,
   return e;
 }
 
-inline unsigned int grid_for(long long n, int threads, int max_blocks = 148 * 32) {
+// Non-finite output detection.  The kernels that write <d|h>, <h|h> set a device word of
+// their translation unit when a result is not finite; bbhx_take_status() reads and clears
+// the words (one per unit) after synchronising the stream.
+int take_nonfinite_likelihood(cudaStream_t s, unsigned* any);
+int take_nonfinite_heterodyne(cudaStream_t s, unsigned* any);
+
+// Streaming multiprocessors of the current device (queried once per device and cached);
+// grid caps are expressed as multiples of it.
+int sm_count();
+
+inline unsigned int grid_for(long long n, int threads, int max_blocks = -1) {
+  if (max_blocks < 0) max_blocks = sm_count() * 32;
   long long b = (n + threads - 1) / threads;
   if (b < 1) b = 1;
   if (b > max_blocks) b = max_blocks;

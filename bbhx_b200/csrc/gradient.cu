@@ -341,9 +341,7 @@ int bbhx_direct_like_grad(void* orbits, void* d_h, void* h_h, double* grad, cons
       st = ERR_CUDA;
     }
   }
-  int dev = 0, nsm = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const int nsm = sm_count();
   const size_t smem = sizeof(double) * (size_t)(4 + 9) * L;
   if (!st && cudaFuncSetAttribute(k_spline_adj, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)smem) != cudaSuccess) {

@@ -7,8 +7,8 @@
 //   mode sum                      direct_sum          (WaveformBuild.cu:193-296)
 //   r = h / h0, layout transpose  (likelihood.py:606-616, host-side numpy/cupy)
 //   relative-binning sums         hdyn                (Likelihood.cu:20-201)
-// with ONE kernel: a CTA owns one walker, stages its per-mode PhenomHM and response records
-// in shared memory, evaluates amplitude, phase, t(f) and the three TDI transfers at every
+// with ONE kernel: a warp owns one walker, stages its per-mode PhenomHM and response records
+// in its own slice of shared memory, evaluates amplitude, phase, t(f) and the three TDI transfers at every
 // sparse frequency, sums the modes, forms r = h / h0 and reduces the bin terms.  The
 // [9, B, M, L] buffer, the [B, 3, L] templates and the transposed residuals are never
 // written.
@@ -29,6 +29,21 @@
 #include "gradient_model.cuh"
 
 namespace bbhx {
+
+// set when a walker's <d|h> or <h|h> is not finite (read by bbhx_take_status)
+static __device__ unsigned g_nonfinite_heterodyne = 0;
+
+int take_nonfinite_heterodyne(cudaStream_t s, unsigned* any) {
+  static const unsigned zero = 0;
+  unsigned v = 0;
+  BBHX_CHECK_CUDA(cudaMemcpyFromSymbolAsync(&v, g_nonfinite_heterodyne, sizeof(v), 0,
+                                            cudaMemcpyDeviceToHost, s));
+  BBHX_CHECK_CUDA(cudaMemcpyToSymbolAsync(g_nonfinite_heterodyne, &zero, sizeof(zero), 0,
+                                          cudaMemcpyHostToDevice, s));
+  BBHX_CHECK_CUDA(cudaStreamSynchronize(s));
+  *any |= v;
+  return OK;
+}
 
 // ------------------------------------------------------------------ FP32 amplitude model
 // Amplitude coefficients of one (binary, mode) in FP32 (built once per CTA from ModeCoeffs).
@@ -458,6 +473,7 @@ __global__ void __launch_bounds__(HET_THREADS) k_het_fused(HetArgs A) {
     if (lane == 0) {
       A.d_h[b] = mk(dre, dim);
       A.h_h[b] = mk(hre, him);
+      note_nonfinite(&g_nonfinite_heterodyne, dre, dim, hre, him);
     }
   }
 }
@@ -550,9 +566,7 @@ int bbhx_hdyn_fused(void* orbits, void* d_h, void* h_h, const void* coeffs, cons
     int threads = HET_THREADS;
     size_t smem = 0;
     st = het_launch_shape(num_modes, length, &threads, &smem);
-    int dev = 0, nsm = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int nsm = sm_count();
     const long long wpc = threads / 32;
     const unsigned grid =
         (unsigned)std::min<long long>((num_bin_all + wpc - 1) / wpc, (long long)nsm * 16);
@@ -637,9 +651,7 @@ int bbhx_hdyn_grad(void* orbits, void* d_h, void* h_h, double* grad, const void*
     int threads = HET_THREADS;
     size_t smem = 0;
     st = het_launch_shape(num_modes, length, &threads, &smem);
-    int dev = 0, nsm = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int nsm = sm_count();
     const long long wpc = threads / 32;
     const unsigned grid =
         (unsigned)std::min<long long>((num_bin_all + wpc - 1) / wpc, (long long)nsm * 16);

@@ -11,6 +11,7 @@
 //
 // Reductions are deterministic: per-(tile, binary) partials in FP64, then a fixed-order sum.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <type_traits>
 #include <vector>
@@ -19,6 +20,21 @@
 #include "spline_eval.cuh"
 
 namespace bbhx {
+
+// set by the reduce kernels when a <d|h> or <h|h> is not finite (read by bbhx_take_status)
+static __device__ unsigned g_nonfinite_likelihood = 0;
+
+int take_nonfinite_likelihood(cudaStream_t s, unsigned* any) {
+  static const unsigned zero = 0;
+  unsigned v = 0;
+  BBHX_CHECK_CUDA(cudaMemcpyFromSymbolAsync(&v, g_nonfinite_likelihood, sizeof(v), 0,
+                                            cudaMemcpyDeviceToHost, s));
+  BBHX_CHECK_CUDA(cudaMemcpyToSymbolAsync(g_nonfinite_likelihood, &zero, sizeof(zero), 0,
+                                          cudaMemcpyHostToDevice, s));
+  BBHX_CHECK_CUDA(cudaStreamSynchronize(s));
+  *any |= v;
+  return OK;
+}
 
 // ---------------------------------------------------------------------------- direct_like
 struct DirectJob {
@@ -130,6 +146,7 @@ __global__ void k_hdyn(cplx* d_h, cplx* h_h, const cplx* __restrict__ r,
     }
     d_h[b] = dh;
     h_h[b] = mk(hh_re, hh_im);
+    note_nonfinite(&g_nonfinite_likelihood, dh.re, dh.im, hh_re, hh_im);
   }
 }
 
@@ -838,6 +855,7 @@ __global__ void k_fused_reduce_multi(const MultiArgs* __restrict__ MA) {
       A.d_h[2 * b + 1] = 4.0 * c;
       A.h_h[2 * b] = 4.0 * h;
       A.h_h[2 * b + 1] = 0.0;
+      note_nonfinite(&g_nonfinite_likelihood, a, c, h, 0.0);
     }
   }
 }
@@ -870,6 +888,7 @@ __global__ void k_fused_reduce(const double* partials, const int* sup_start, con
       d_h[2 * b + 1] = 4.0 * c;
       h_h[2 * b] = 4.0 * h;
       h_h[2 * b + 1] = 0.0;
+      note_nonfinite(&g_nonfinite_likelihood, a, c, h, 0.0);
     }
   }
 }
@@ -896,7 +915,7 @@ int direct_fused_gh(cplx* gh, const long long* gh_off, double* d_h, double* h_h,
   int2* segtab = nullptr;
   BBHX_CHECK_CUDA(pool_alloc_all(s, {{(void**)&part, sizeof(double) * 3 * nitems},
                                      {(void**)&segtab, sizeof(int2) * nitems * M}}));
-  k_tile_segments<<<grid_for(nitems * M, 256, 148 * 64), 256, 0, s>>>(
+  k_tile_segments<<<grid_for(nitems * M, 256, sm_count() * 64), 256, 0, s>>>(
       segtab, x + row0, data_freqs, start + b0, len + b0, nb, M, L, ntiles, FD_TILE);
   int st = launch_status("k_tile_segments");
   if (!st) {
@@ -929,7 +948,8 @@ int direct_fused_gh(cplx* gh, const long long* gh_off, double* d_h, double* h_h,
     A.gh = gh;
     A.gh_off = gh_off;
     const long long g = (nitems + FD_WARPS - 1) / FD_WARPS;
-    const unsigned grid = (unsigned)(g < 148LL * 16 ? g : 148LL * 16);
+    const long long cap = 16LL * sm_count();
+    const unsigned grid = (unsigned)(g < cap ? g : cap);
     const size_t sm = sizeof(WarpStage<double>) * FD_WARPS;
     st = cuda_status(cudaFuncSetAttribute(k_direct_fused<false, true>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm),
@@ -1009,11 +1029,17 @@ int bbhx_direct_like(double* d_h, double* h_h, const double* data, const double*
   cudaFreeAsync(d_part, s);
   cudaFreeAsync(d_out, s);
   if (st) return st;
+  bool finite = true;
   for (int b = 0; b < num_bin_all; ++b) {
     d_h[2 * b] += host[4 * b];
     d_h[2 * b + 1] += host[4 * b + 1];
     h_h[2 * b] += host[4 * b + 2];
     h_h[2 * b + 1] += host[4 * b + 3];
+    finite = finite && std::isfinite(host[4 * b] + host[4 * b + 1] + host[4 * b + 2]);
+  }
+  if (!finite) {
+    set_error("direct_like: non-finite <d|h> or <h|h> (results written)");
+    return ERR_NONFINITE;
   }
   return OK;
 }
@@ -1118,7 +1144,7 @@ int bbhx_direct_like_multi(const bbhx_direct_group* groups, int num_groups, int 
     k_support<<<A.B, 128, 0, s>>>(A.x, A.M, A.L, A.B, A.data_freqs, A.N, sup, sup + A.B);
     st = launch_status("k_support");
     if (!st) {
-      k_tile_segments<<<grid_for(nit * A.M, 256, 148 * 64), 256, 0, s>>>(
+      k_tile_segments<<<grid_for(nit * A.M, 256, sm_count() * 64), 256, 0, s>>>(
           segtab, A.x, A.data_freqs, sup, sup + A.B, A.B, A.M, A.L, A.ntiles, tile_bins);
       st = launch_status("k_tile_segments");
     }
@@ -1137,9 +1163,7 @@ int bbhx_direct_like_multi(const bbhx_direct_group* groups, int num_groups, int 
     }
   }
   if (!st && items > 0) {
-    int dev = 0, nsm = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int nsm = sm_count();
     const long long want = (items + FD_WARPS - 1) / FD_WARPS;
     const unsigned grid = (unsigned)std::min<long long>(want, (long long)nsm * ctas_per_sm);
     if (precision == 1) {
@@ -1192,7 +1216,7 @@ int bbhx_direct_like_fused(double* d_h, double* h_h, const double* data_freqs, c
                                         sup, sup + num_bin_all);
   int st = launch_status("k_support");
   if (!st) {
-    k_tile_segments<<<grid_for(nitems * num_modes, 256, 148 * 64), 256, 0, s>>>(
+    k_tile_segments<<<grid_for(nitems * num_modes, 256, sm_count() * 64), 256, 0, s>>>(
         segtab, x, data_freqs, sup, sup + num_bin_all, num_bin_all, num_modes, length, ntiles,
         FD_TILE);
     st = launch_status("k_tile_segments");
@@ -1228,7 +1252,8 @@ int bbhx_direct_like_fused(double* d_h, double* h_h, const double* data_freqs, c
     A.gh_off = nullptr;
     const long long warps_needed = (nitems + 0);
     long long g = (warps_needed + FD_WARPS - 1) / FD_WARPS;
-    unsigned grid = (unsigned)(g < 148LL * 16 ? g : 148LL * 16);
+    const long long cap = 16LL * sm_count();
+    unsigned grid = (unsigned)(g < cap ? g : cap);
     if (precision == 1) {
       const size_t sm = sizeof(WarpStage<float>) * FD_WARPS;
       st = cuda_status(cudaFuncSetAttribute(k_direct_fused<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -220,9 +220,10 @@ __global__ void k_default_freqs(double* freqs, const double* m1, const double* m
 // Scratch of bbhx_waveform_amp_phase_noalloc: the per-(binary, mode) model records live in
 // this file-scope device array instead of memory obtained with cudaMalloc / cudaMallocAsync.
 // It is part of the library's device image, so every GPU that loads the library holds it
-// (kNoAllocMaxRecords * sizeof(ModeCoeffs) = 8192 * 752 B, about 6.2 MB) until the process
+// (kNoAllocMaxRecords * sizeof(ModeCoeffs) = 8192 * 848 B, about 6.9 MB) until the process
 // exits.  All calls share it.
 constexpr long long kNoAllocMaxRecords = 8192;
+static_assert(sizeof(ModeCoeffs) == 848, "the documented footprint of the no-alloc array assumes 848-byte records");
 static __device__ __align__(256) ModeCoeffs g_noalloc_records[kNoAllocMaxRecords];
 
 }  // namespace bbhx
@@ -234,7 +235,9 @@ constexpr int kThreads = 256;
 
 // Device address of g_noalloc_records for the current device, looked up once per device.
 // In host code the array's name is only a host-side stand-in, not a device address, so the
-// kernels are given the address that cudaGetSymbolAddress returns.
+// kernels are given the address that cudaGetSymbolAddress returns.  The address is valid for
+// the life of the device's primary context: a cudaDeviceReset (which unloads the module) while
+// the library is in use is not supported.
 std::mutex g_noalloc_mutex;
 void* g_noalloc_addr[256] = {};
 

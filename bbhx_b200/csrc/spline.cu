@@ -129,13 +129,14 @@ int bbhx_interpolate(const double* freqs, const double* y, double* B_, double* u
   size_t smem = sizeof(double) * (size_t)(4 + num_interp_params) * length;
   bool use_smem = smem <= kMaxSplineSmem;
   int threads = 256;
-  unsigned int grid = (unsigned int)(S < 148 * 16 ? S : 148 * 16);
+  const long long nsm = sm_count();
+  unsigned int grid = (unsigned int)(S < nsm * 16 ? S : nsm * 16);
   double* scratch = nullptr;
   if (use_smem) {
     BBHX_CHECK_CUDA(cudaFuncSetAttribute(k_spline, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)kMaxSplineSmem));
   } else {
-    grid = (unsigned int)(S < 148 * 2 ? S : 148 * 2);
+    grid = (unsigned int)(S < nsm * 2 ? S : nsm * 2);
     BBHX_CHECK_CUDA(pool_alloc((void**)&scratch, sizeof(double) * grid * (4 + num_interp_params) * (size_t)length, s));
   }
   k_spline<<<grid, threads, use_smem ? smem : 0, s>>>(freqs, y, B_, upper_diag, diag, lower_diag,

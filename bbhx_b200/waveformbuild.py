@@ -327,9 +327,11 @@ class BBHWaveformFD:
                   int(ap.run_phenomd), M, L, B, _lib.stream())
         return d_h, h_h, grad
 
-    def _spline_set(self, params, t_obs_start, t_obs_end, length, modes, flags=None):
+    def _spline_set(self, params, t_obs_start, t_obs_end, length, modes, flags=None,
+                    timing=None):
         """Sparse buffer [9, B, M, L], its spline coefficients c1..c3, the knots and the
-        per-binary observation limits (device), as the fused likelihood consumes them."""
+        per-binary observation limits (device), as the fused likelihood consumes them.
+        ``timing``: optional dict that receives CUDA events around the spline build."""
         t = torch()
         buf, t_start, t_end = self._sparse_buffer(params, t_obs_start, t_obs_end, None, length,
                                                   modes, False, flags=flags)
@@ -338,8 +340,15 @@ class BBHWaveformFD:
         c1 = t.empty_like(buf)
         c2 = t.empty_like(buf)
         c3 = t.empty_like(buf)
+        if timing is not None:
+            ev0 = t.cuda.Event(enable_timing=True)
+            ev1 = t.cuda.Event(enable_timing=True)
+            ev0.record()
         _lib.call("bbhx_interpolate", _lib.dptr(x), _lib.dptr(buf), _lib._VP(0),
                   _lib.dptr(c1), _lib.dptr(c2), _lib.dptr(c3), L, 9, M, B, _lib.stream())
+        if timing is not None:
+            ev1.record()
+            timing.setdefault("spline", []).append((ev0, ev1))
         return buf, c1, c2, c3, x, to_dev(t_start), to_dev(t_end)
 
     def inner_products(self, params, data_freqs, data_weighted, noise_factors, t_obs_start=0.0,
@@ -354,7 +363,7 @@ class BBHWaveformFD:
         # ts_d / te_d stay referenced across the call: a temporary freed inside the argument
         # list can be handed back by the caching allocator to the next one
         buf, c1, c2, c3, x, ts_d, te_d = self._spline_set(params, t_obs_start, t_obs_end, length,
-                                                          modes, flags=flags)
+                                                          modes, flags=flags, timing=timing)
         B, M, L = self.num_bin_all, self.num_modes, self.length
         d_h = t.empty(B, dtype=t.complex128, device=device())
         h_h = t.empty(B, dtype=t.complex128, device=device())

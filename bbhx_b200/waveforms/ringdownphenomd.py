@@ -1,7 +1,7 @@
 """PhenomD QNM table: final spin -> 22-mode ringdown / damping frequency (1001 points,
 spin step ``dspin``), the model data the reference ships in
 src/bbhx/waveforms/ringdownphenomd.py; loaded from ``bbhx_b200/data/qnm_phenomd.npz``
-(written by ``bbhx_b200/data/make_qnm_table.py``)."""
+(written by the test-side recipe ``oracle/make_qnm_table.py``)."""
 import os
 
 import numpy as np

@@ -7,15 +7,14 @@ PhenomHM with 6 modes on 1024-point sparse grids, 2nd-generation TDI A/E/T, Tobs
 data grid df = 1/Tobs over [1e-5, 0.1] Hz (~3.16e6 bins; complex128 data and real noise
 weights, ~250 MB, larger than L2), synthetic data = seeded injection + Gaussian noise from
 the analytic PSD with the equal-arm TDI noise zeros notched (f = k c / 4L, +-16 bins).
-Headline arithmetic: mixed (FP64 phase, t(f) and sums; FP32 amplitude, transfer and per-bin
-products); the plain-FP64 form is timed beside it.
+Headline arithmetic: plain FP64 (the parity form); the mixed form (FP64 phase, t(f), products
+and sums; FP32 amplitude and transfer) is timed beside it with its |dlnL| against FP64.
 
-  value  : lnL evaluations / s with parameters already resident on the GPU
+  value  : FP64 lnL evaluations / s with parameters already resident on the GPU
   e2e    : the same through the public API (Likelihood.get_ll) from pinned host params,
            including the H2D copy of the 12 x B parameters and the D2H copy of the B lnL
-  roofline: the fused interpolate + reduce kernel against measured HBM bandwidth, with
-           72 B of algorithmic traffic per (binary, data bin) (the FP64 data and weights;
-           frac_vs_mixed_reads uses the 36 B of FP32 copies the mixed form reads)
+  roofline: the fused FP64 interpolate + reduce kernel against measured HBM bandwidth, with
+           72 B of algorithmic traffic per (binary, data bin) (the FP64 data and weights)
   cpu_baseline: the reference's own C++ CPU path (oracle/_ref) on a bounded sample
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
@@ -59,6 +58,11 @@ def parse():
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch metric")
     ap.add_argument("--uneven-batch", type=int, default=16384)
     return ap.parse_args()
+
+
+def workload_name(B, N):
+    return ("direct lnL, plain FP64, B=%d binaries x 6 modes, sparse L=%d, Tobs=1 yr, "
+            "df=1/Tobs over 1e-5..0.1 Hz (N=%d bins), AET TDI2" % (B, LENGTH, N))
 
 
 def shard_seed(rank):
@@ -139,8 +143,10 @@ class ClockSampler:
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu_index):
-        self.path = os.path.join(REPO, "gpurun_out", f"clocks_rank{gpu_index}.csv")
-        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        import tempfile
+
+        fd, self.path = tempfile.mkstemp(prefix=f"bbhx_clocks_gpu{gpu_index}_", suffix=".csv")
+        os.close(fd)
         self.proc = None
         try:
             self.fh = open(self.path, "w")
@@ -173,6 +179,10 @@ class ClockSampler:
             for nm, v in zip(names, parts[5:9]):
                 if v.lower().startswith("active"):
                     reasons.add(nm)
+        try:
+            os.remove(self.path)
+        except OSError:
+            pass
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
@@ -247,7 +257,7 @@ def gpu_arm(args):
     kw = dict(length=LENGTH, t_obs_start=0.0, t_obs_end=TOBS)
     flags = torch.zeros(3, dtype=torch.int32, device="cuda")
 
-    def step(timing=None, precision="mixed"):
+    def step(timing=None, precision="fp64"):
         d_h, h_h = wave.inner_products(dev_params, like.data_freqs, like.data_channels,
                                        like.noise_factors, flags=flags, timing=timing,
                                        precision=precision,
@@ -261,12 +271,13 @@ def gpu_arm(args):
 
             dist.barrier()
 
-    def timed(precision, timing):
+    def timed(precision, timing, sampler_on=False):
         for _ in range(args.warmup):
             step(precision=precision)
         torch.cuda.synchronize()
         barrier()
         torch.cuda.synchronize()
+        sampler = ClockSampler(local) if sampler_on else None
         a = torch.cuda.Event(enable_timing=True)
         z = torch.cuda.Event(enable_timing=True)
         a.record()
@@ -275,41 +286,29 @@ def gpu_arm(args):
         z.record()
         torch.cuda.synchronize()
         barrier()
-        return a.elapsed_time(z), res
+        clk = sampler.stop() if sampler else None
+        return a.elapsed_time(z), res, clk
 
-    # plain FP64 form first (the parity form; reported beside the mixed headline)
-    fp64_timing = {}
-    fp64_ms, out64 = timed("fp64", fp64_timing)
-    for _ in range(args.warmup):
-        out = step()
-    torch.cuda.synchronize()
+    # headline: the plain FP64 form (the parity form, results identical to the reference's
+    # FP64 path within 1e-6 + 2e-11 |lnL|)
+    timing = {}
+    ms_total, out64, clocks = timed("fp64", timing, sampler_on=(rank == 0 or world > 1))
     if int(flags.abs().sum().item()) != 0:
         raise RuntimeError(f"device error flags set: {flags.tolist()}")
-    sampler = ClockSampler(local) if rank == 0 or world > 1 else None
-    barrier()
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    timing = {}
-    e0.record()
-    for _ in range(args.steps):
-        out = step(timing)
-    e1.record()
-    torch.cuda.synchronize()
-    barrier()
-    clocks = sampler.stop() if sampler else None
-    ms_total = e0.elapsed_time(e1)
     fused_ms = [a.elapsed_time(b) for a, b in timing["fused"]]
+    spline_ms = [a.elapsed_time(b) for a, b in timing["spline"]]
     ms_total = max_over_ranks(ms_total, world)
-    lnl = out.cpu().numpy()
+    # mixed form (FP32 amplitude / transfer) beside it, with its error against FP64
+    mixed_timing = {}
+    mixed_ms, outmx, _ = timed("mixed", mixed_timing)
+    mixed_ms = max_over_ranks(mixed_ms, world)
     lnl64 = out64.cpu().numpy()
-    assert np.all(np.isfinite(lnl)) and np.all(np.isfinite(lnl64)), "non-finite lnL"
-    dl_mixed = np.abs(lnl - lnl64)
-    # <h|h> of every binary (FP64, outside the timed region) for the relative error
+    lnlmx = outmx.cpu().numpy()
+    assert np.all(np.isfinite(lnlmx)) and np.all(np.isfinite(lnl64)), "non-finite lnL"
+    dl_mixed = np.abs(lnlmx - lnl64)
     _, hh64 = wave.inner_products(dev_params, like.data_freqs, like.data_channels,
                                   like.noise_factors, flags=flags, precision="fp64", **kw)
     hh64 = hh64.real.cpu().numpy()
-    fp64_ms = max_over_ranks(fp64_ms, world)
 
     # support sizes (sum of per-binary data-grid lengths) for the roofline
     from bbhx_b200 import _lib
@@ -320,28 +319,36 @@ def gpu_arm(args):
               wave.num_modes, LENGTH, B, _lib.dptr(like.data_freqs), len(f), _lib.stream())
     pairs = float(sup[B:].double().sum().item())
 
-    # end to end through the public API from pinned host memory
-    like.precision = "mixed"
+    # end to end through the public API (Likelihood.get_ll) from pinned host memory: the H2D
+    # copy of the parameters and the D2H copy of the results are inside the timed region
     host = torch.tensor(params, dtype=torch.float64).pin_memory()
-    for _ in range(2):
-        like.get_ll(host, **kw)
-    torch.cuda.synchronize()
-    barrier()
-    t0 = torch.cuda.Event(enable_timing=True)
-    t1 = torch.cuda.Event(enable_timing=True)
-    t0.record()
-    for _ in range(args.steps):
-        ll_host = like.get_ll(host, **kw)
-    t1.record()
-    torch.cuda.synchronize()
-    e2e_ms = max_over_ranks(t0.elapsed_time(t1), world)
-    dl = float(np.max(np.abs(ll_host - lnl)))
+
+    def e2e(precision):
+        like.precision = precision
+        for _ in range(2):
+            like.get_ll(host, **kw)
+        torch.cuda.synchronize()
+        barrier()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        for _ in range(args.steps):
+            ll_host = like.get_ll(host, **kw)
+        t1.record()
+        torch.cuda.synchronize()
+        return max_over_ranks(t0.elapsed_time(t1), world), ll_host
+
+    e2e_ms, ll_host = e2e("fp64")
+    e2e_mx_ms, _ = e2e("mixed")
+    like.precision = "fp64"
+    dl = float(np.max(np.abs(ll_host - lnl64)))
     near = near_peak_direct(like, kw)
 
     extra = {}
     # the heterodyned / gradient / uneven-batch metrics are single-GPU figures; a multi-rank run
     # reports the headline direct lnL only (every rank's own batch, no collective)
     if not args.no_extra and world == 1:
+        extra.update(spline_metric(timing, B, wave.num_modes))
         extra.update(het_metric(args, wave, like, f, params))
         if not args.no_grad:
             extra.update(grad_metric(args))
@@ -359,6 +366,7 @@ def gpu_arm(args):
     achieved = HBM_BYTES_PER_PAIR * pairs / fused_avg_s / 1e9
     tpp = ncu_traffic_per_pair()
     n_evals = B * args.steps * world
+    mixed_kernel_ms = statistics.mean(a.elapsed_time(b) for a, b in mixed_timing["fused"])
     res = {
         "metric": "lnL evals/s (direct, heterodyned) mixed vs FP64 plain at |dlnL|<=1e-2; grad/s",
         "value": aggregate_rate(B * args.steps, world, ms_total),
@@ -370,36 +378,34 @@ def gpu_arm(args):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "mixed: f64 phase/t(f)/accumulation, f32 amplitude/transfer/products",
+        "dtype": "f64",
         "data": "synthetic: seeded PhenomHM injection + Gaussian noise from the analytic A/E/T PSD",
-        "fp64_plain": {"value": aggregate_rate(B * args.steps, world, fp64_ms), "unit": "lnL evals/s",
-                       "ms_per_step": fp64_ms / args.steps,
-                       "kernel_ms": statistics.mean(a.elapsed_time(b) for a, b in fp64_timing["fused"])},
-        "dlnl_mixed_vs_fp64": {"max": float(dl_mixed.max()), "p99": float(np.percentile(dl_mixed, 99)),
-                               "median": float(np.median(dl_mixed)),
-                               "max_over_hh": float(np.max(dl_mixed / np.maximum(1.0, hh64))),
-                               "frac_within_1e-2": float(np.mean(dl_mixed <= 1e-2)),
-                               "median_hh": float(np.median(hh64)),
-                               "near_peak": near},
-        "config": {"workload": "direct lnL, mixed precision (FP64 plain beside), B=%d binaries x 6 modes, sparse L=%d, "
-                               "Tobs=1 yr, df=1/Tobs over 1e-5..0.1 Hz (N=%d bins), AET TDI2"
-                               % (B, LENGTH, len(f)),
+        "mixed": {"value": aggregate_rate(B * args.steps, world, mixed_ms), "unit": "lnL evals/s",
+                  "ms_per_step": mixed_ms / args.steps, "kernel_ms": mixed_kernel_ms,
+                  "e2e": aggregate_rate(B * args.steps, world, e2e_mx_ms),
+                  "dtype": "mixed: f64 phase/t(f)/products/accumulation, f32 amplitude/transfer",
+                  "dlnl_vs_fp64": {"max": float(dl_mixed.max()),
+                                   "p99": float(np.percentile(dl_mixed, 99)),
+                                   "median": float(np.median(dl_mixed)),
+                                   "max_over_hh": float(np.max(dl_mixed / np.maximum(1.0, hh64))),
+                                   "frac_within_1e-2": float(np.mean(dl_mixed <= 1e-2)),
+                                   "median_hh": float(np.median(hh64)),
+                                   "near_peak": near}},
+        "config": {"workload": workload_name(B, len(f)),
                    "global_batch": n_evals // args.steps, "data_bins": len(f),
                    "binary_bin_pairs_per_step": pairs,
                    "l2": "inputs larger than L2: every step writes and reads 1.8 GB of sparse buffers / "
-                         "spline coefficients besides the data (114 MB FP32 copies read by the mixed "
-                         "form, 227 MB FP64 by the plain form)",
+                         "spline coefficients besides the 227 MB FP64 data and weights",
                    "parallelism": f"replicas x{world} (independent binary batches per GPU)"},
         "e2e": {"value": aggregate_rate(B * args.steps, world, e2e_ms), "unit": "lnL evals/s",
                 "h2d_bytes_per_step": 12 * B * 8, "d2h_bytes_per_step": 3 * B * 8 + 3 * 8,
+                "path": "Likelihood.get_ll (precision='fp64') from pinned host parameters",
                 "max_abs_dlnl_vs_device_path": dl},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak,
                      "algorithmic_bytes_per_pair": HBM_BYTES_PER_PAIR,
-                     # the mixed kernel reads FP32 copies of data and weights: 36 B per pair
-                     "frac_vs_mixed_reads": achieved * (MIXED_BYTES_PER_PAIR / HBM_BYTES_PER_PAIR) / peak,
                      "traffic": (tpp * pairs if tpp is not None else None),
-                     "kernel": "k_direct_fused (bbhx_direct_like_fused)",
+                     "kernel": "k_direct_fused<FP64> (bbhx_direct_like_fused, precision 0)",
                      "kernel_ms": statistics.mean(fused_ms),
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback"},
         "gpu_launches": 12 * args.steps,
@@ -407,6 +413,22 @@ def gpu_arm(args):
     }
     res.update(extra)
     return res
+
+
+def spline_metric(timing, B, M):
+    """Spline build (bbhx_interpolate) inside the FP64 steps: 9 B M not-a-knot systems of
+    length L per call; 5 x 8 L bytes per system (x and y read, slope and c1..c3 written, the
+    shared x counted once per system)."""
+    ms = statistics.mean(a.elapsed_time(b) for a, b in timing["spline"])
+    systems = 9 * B * M
+    nbytes = 5 * 8 * LENGTH * systems
+    peaks = measured_peaks()
+    peak = peaks["hbm_gbs"] if peaks else 6650.0
+    gbs = nbytes / (ms / 1e3) / 1e9
+    return {"spline": {"solves_per_s": systems / (ms / 1e3), "systems_per_call": systems,
+                       "length": LENGTH, "kernel_ms": ms, "bytes_per_system": 5 * 8 * LENGTH,
+                       "achieved_gbs": gbs, "frac_of_hbm": gbs / peak,
+                       "kernel": "k_spline (cyclic reduction in shared memory, 9 right-hand sides)"}}
 
 
 def near_peak_direct(like, kw, n=64):
@@ -681,6 +703,30 @@ def uneven_metric(args):
                   "[0.8, 0.95] Tobs; heterodyne bins 64/128/192/256 x 1024 walkers; CUDA graph replay"}}
 
 
+CPU_STEPS, CPU_WARMUP = 4, 2  # bounded sample of the GPU line's cpu_baseline leg
+
+
+def cpu_baseline(args):
+    """The reference CPU path on the box's host cores, timed the same way as the reference
+    arm (warm-up steps first, then the mean over timed steps; each step = one binary per
+    process at the full workload size), on a bounded sample: CPU_STEPS timed steps after
+    CPU_WARMUP.  Also the single-thread "as shipped" figure: the reference's CPU build never
+    enables OpenMP, so one binary on one core is what its own build delivers."""
+    from bbhx_b200.synthetic import draw_params
+
+    params = draw_params(args.batch, TOBS, SEED_PARAMS)
+    workers = cpu_workers()
+    val, times = cpu_reference(params, workers, steps=CPU_STEPS, warmup=CPU_WARMUP)
+    val1, times1 = cpu_reference(params, 1, steps=2, warmup=1)
+    return {"value": val, "unit": "lnL evals/s", "cores": workers, "kind": "reference",
+            "sample": f"{CPU_STEPS} steps after {CPU_WARMUP} warm-up, {workers} binaries per step "
+                      "(one per process) at the full workload size; reference C++ CPU path "
+                      "(oracle/_ref) with the reference driver logic",
+            "step_seconds": times,
+            "single_thread_as_shipped": {"value": val1, "unit": "lnL evals/s", "cores": 1,
+                                         "sample": "2 binaries after 1 warm-up, one process"}}
+
+
 def reference_arm(args):
     rank, world, _ = rank_info()
     if rank != 0:
@@ -692,13 +738,13 @@ def reference_arm(args):
     workers = cpu_workers()
     val, times = cpu_reference(params, workers, steps=args.steps, warmup=args.warmup)
     cpu = {"value": val, "unit": "lnL evals/s", "cores": workers, "kind": "reference",
-           "sample": f"{workers} binaries per step (one per process) at the full workload size"}
+           "sample": f"{args.steps} steps after {args.warmup} warm-up, {workers} binaries per step "
+                     "(one per process) at the full workload size"}
     return {"impl": "reference", "metric": "lnL evals/s (direct, heterodyned) mixed vs FP64 plain at |dlnL|<=1e-2; grad/s",
             "value": val, "unit": "lnL evals/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(times),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": "direct lnL, plain FP64, Tobs=1 yr, N=%d bins, 6 modes, L=1024"
-                                             % len(data_grid(TOBS, F_LO, F_HI))},
+            "data": "synthetic", "config": {"workload": workload_name(args.batch, len(data_grid(TOBS, F_LO, F_HI)))},
             "cpu_baseline": cpu,
             "e2e": {"value": val, "unit": "lnL evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
@@ -715,15 +761,7 @@ def main():
     if res is None:
         return
     if not args.no_cpu and world == 1:
-        from bbhx_b200.synthetic import draw_params
-
-        params = draw_params(args.batch, TOBS, SEED_PARAMS)
-        workers = cpu_workers()
-        val, _ = cpu_reference(params, workers, steps=1, warmup=0)
-        res["cpu_baseline"] = {"value": val, "unit": "lnL evals/s", "cores": workers,
-                               "kind": "reference",
-                               "sample": f"{workers} binaries of the same workload, one per process, "
-                                         "reference C++ CPU path (oracle/_ref) with the reference driver logic"}
+        res["cpu_baseline"] = cpu_baseline(args)
     print(json.dumps(res), flush=True)
 
 

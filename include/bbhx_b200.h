@@ -3,8 +3,10 @@
  * waveform -> likelihood path.
  *
  * Conventions (all entry points):
- *   - return int status: 0 ok, 1 bad argument, 2 CUDA error, 3 timeout, 4 non-finite,
- *     5 missing orbit tables, 6 size above a fixed limit;
+ *   - return int status: 0 ok, 1 bad argument, 2 CUDA error, 4 non-finite output,
+ *     5 missing orbit tables, 6 size above a fixed limit (3 is unused: nothing in the library
+ *     waits on another CTA, stream or device); stream-ordered entry points report non-finite
+ *     <d|h> / <h|h> through bbhx_take_status(), the synchronous bbhx_direct_like directly;
  *     bbhx_last_error_string() describes the last failure of the calling thread;
  *   - the last argument is a cudaStream_t passed as void* (NULL = legacy default stream);
  *     work is stream-ordered, nothing synchronises unless stated;
@@ -30,6 +32,10 @@ extern "C" {
 const char *bbhx_last_error_string(void);
 int bbhx_version(void);
 int bbhx_stream_synchronize(void *stream);
+/* synchronise the stream; return 4 if any likelihood output written since the previous call on
+ * this device (direct fused / multi-group / hdyn / heterodyned fused) was NaN or infinite, and
+ * clear that record; 0 otherwise (no reference counterpart: the reference returns NaN silently) */
+int bbhx_take_status(void *stream);
 int bbhx_pointer_is_device(const void *ptr);
 size_t bbhx_mode_coeffs_bytes(void);
 size_t bbhx_response_mode_bytes(void);
@@ -76,10 +82,12 @@ int bbhx_waveform_amp_phase(double *waveform_out, const int *ells, const int *mm
  * callers that must not allocate device memory (a host whose own pool owns the GPU, loops
  * where cudaMalloc's device-wide synchronisation would stall other streams, deployments
  * without the stream-ordered allocator).  Its per-(binary, mode) scratch is a static device
- * array inside the library (8192 records, ~6.2 MB held by every GPU that loads the library):
- * num_bin_all * num_modes must be <= 8192 (else status 6, nothing launched).  The first call
- * on a device looks up that array's address (make it before any stream capture); all calls
- * share the array, so calls that overlap on the GPU race and must be serialised. */
+ * array inside the library (8192 records of 848 B, ~6.9 MB held by every GPU that loads the
+ * library): num_bin_all * num_modes must be <= 8192 (else status 6, nothing launched).  The
+ * first call on a device looks up that array's address (make it before any stream capture)
+ * and keeps it for the life of the device's primary context, so a cudaDeviceReset while the
+ * library is in use is not supported; all calls share the array, so calls that overlap on the
+ * GPU race and must be serialised. */
 int bbhx_waveform_amp_phase_noalloc(double *waveform_out, const int *ells, const int *mms,
                                     const double *freqs, const double *m1_SI,
                                     const double *m2_SI, const double *chi1z, const double *chi2z,

@@ -21,6 +21,9 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT_DIR = os.path.join(HERE, "_ref")
 OUT = os.path.join(OUT_DIR, "libbbhx_ref.so")
+# Location of the reference checkout this recipe compiles from: BBHX_REFERENCE_ROOT, else the
+# checkout directory of the build container.  The golden-fixture scripts and
+# oracle/make_qnm_table.py read it from here; nothing outside oracle/ and tests/golden/ does.
 REF_ROOT = os.environ.get("BBHX_REFERENCE_ROOT", "/root/reference")
 CUTILS = os.path.join(REF_ROOT, "src", "bbhx", "cutils")
 SOURCES = [

@@ -4,7 +4,7 @@
 
 The table is part of the PhenomD model definition (the reference fits a cubic spline
 through it, phenomhm.py:148-163); it is data, not code, and must be identical for parity.
-Run once where the reference checkout exists:  python bbhx_b200/data/make_qnm_table.py
+Test-side recipe, run once where the reference checkout exists:  python oracle/make_qnm_table.py
 """
 import ast
 import os
@@ -12,8 +12,11 @@ import sys
 
 import numpy as np
 
-REF = os.environ.get("BBHX_REFERENCE_ROOT", "/root/reference")
-SRC = os.path.join(REF, "src", "bbhx", "waveforms", "ringdownphenomd.py")
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(HERE))
+from oracle.build_ref import REF_ROOT  # noqa: E402
+
+SRC = os.path.join(REF_ROOT, "src", "bbhx", "waveforms", "ringdownphenomd.py")
 
 
 def main():
@@ -27,7 +30,7 @@ def main():
                 vals[name] = np.array(ast.literal_eval(v.args[0]), dtype=np.float64)
             else:
                 vals[name] = np.float64(ast.literal_eval(v))
-    out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "qnm_phenomd.npz")
+    out = os.path.join(os.path.dirname(HERE), "bbhx_b200", "data", "qnm_phenomd.npz")
     np.savez(out, dspin=vals["dspin"], a=vals["QNMData_a"], fring=vals["QNMData_fring"],
              fdamp=vals["QNMData_fdamp"])
     print(out, {k: np.shape(v) for k, v in vals.items()})

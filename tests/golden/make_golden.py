@@ -21,7 +21,10 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.abspath(os.path.join(HERE, "..", ".."))
-REF_SRC = os.path.join(os.environ.get("BBHX_REFERENCE_ROOT", "/root/reference"), "src")
+sys.path.insert(0, REPO)
+from oracle.build_ref import REF_ROOT  # noqa: E402
+
+REF_SRC = os.path.join(REF_ROOT, "src")
 sys.path.insert(0, os.path.join(REPO, "oracle", "refenv"))
 sys.path.insert(0, REPO)
 sys.path.insert(0, REF_SRC)

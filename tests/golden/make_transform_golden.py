@@ -1,7 +1,7 @@
 """Golden vectors for the frame / sky-mode transforms (tests/golden/transform_golden.npz),
 from the REFERENCE's own src/bbhx/utils/transform.py on seeded random inputs.
 
-Runs only where the reference checkout exists (BBHX_REFERENCE_ROOT, default /root/reference);
+Runs only where the reference checkout exists (its location comes from oracle/build_ref.py);
 the fixture it writes is what the tests read.  Usage: python tests/golden/make_transform_golden.py
 """
 import os
@@ -11,7 +11,10 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.abspath(os.path.join(HERE, "..", ".."))
-REF_SRC = os.path.join(os.environ.get("BBHX_REFERENCE_ROOT", "/root/reference"), "src")
+sys.path.insert(0, REPO)
+from oracle.build_ref import REF_ROOT  # noqa: E402
+
+REF_SRC = os.path.join(REF_ROOT, "src")
 sys.path.insert(0, os.path.join(REPO, "oracle", "refenv"))
 sys.path.insert(0, REPO)
 sys.path.insert(0, REF_SRC)
