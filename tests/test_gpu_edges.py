@@ -122,3 +122,32 @@ def test_reference_rejections_raise_the_same_errors(golden, golden_data):
     # still usable afterwards
     ll = like.get_ll(P, **kw)
     assert np.all(np.isfinite(ll))
+
+
+def test_nonfinite_output_is_status_4():
+    """A NaN in the inputs of the relative-binning sums makes that walker's <d|h>, <h|h> NaN:
+    the stream-ordered call returns 0, bbhx_take_status reports 4 once and clears the record,
+    and finite inputs leave it at 0."""
+    import torch
+
+    from bbhx_b200 import _lib
+
+    s = _lib.stream()
+    take = _raw("bbhx_take_status")
+    take(s)  # clear whatever earlier calls in this process recorded
+    B, L = 3, 16
+    r = torch.ones((L, 3, B), dtype=torch.complex128, device="cuda")
+    consts = torch.ones((4, 3, L), dtype=torch.complex128, device="cuda")
+    f = torch.linspace(1e-3, 2e-3, L, dtype=torch.float64, device="cuda")
+    d_h = torch.zeros(B, dtype=torch.complex128, device="cuda")
+    h_h = torch.zeros(B, dtype=torch.complex128, device="cuda")
+    args = lambda: (_lib.dptr(d_h), _lib.dptr(h_h), _lib.dptr(r), _lib.dptr(consts),
+                    _lib.dptr(f), B, L, 3, s)
+    assert _raw("bbhx_hdyn")(*args()) == 0
+    assert take(s) == 0
+    r[5, 1, 2] = complex(float("nan"), 0.0)
+    assert _raw("bbhx_hdyn")(*args()) == 0
+    assert take(s) == 4
+    assert b"not finite" in _lib.lib().bbhx_last_error_string()
+    assert torch.isnan(d_h[2].real) and torch.isfinite(d_h[0].real)
+    assert take(s) == 0  # the record was cleared
