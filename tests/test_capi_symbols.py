@@ -35,3 +35,30 @@ def test_python_binding_covers_header():
     bound = set(_lib.exported_symbols())
     missing = [n for n in declared_functions() if n not in bound]
     assert not missing, missing
+
+
+def test_backend_methods_mirror_the_reference_table():
+    """bbhx_b200.backend binds exactly BBHx's backend methods (the fields of
+    BBHxBackendMethods, src/bbhx/cutils/__init__.py:13-23) with the positional arity of the
+    reference's Cython wrappers, each onto a declared entry point."""
+    import numpy as np
+    import pytest
+
+    from bbhx_b200 import backend
+
+    reference_fields = {"hdyn_wrap", "direct_like_wrap", "direct_sum_wrap", "InterpTDI_wrap",
+                        "pyFastLISAResponse", "waveform_amp_phase_wrap",
+                        "get_phenomhm_ringdown_frequencies", "get_phenomd_ringdown_frequencies",
+                        "interpolate_wrap"}
+    assert set(backend.METHOD_NAMES) == reference_fields
+    arity = {"waveform_amp_phase_wrap": 16, "get_phenomhm_ringdown_frequencies": 10,
+             "get_phenomd_ringdown_frequencies": 16, "interpolate_wrap": 10, "InterpTDI_wrap": 16,
+             "direct_sum_wrap": 8, "direct_like_wrap": 9, "hdyn_wrap": 8}
+    declared = set(declared_functions())
+    for name, (cname, slots) in backend._METHODS.items():
+        assert len(slots) == arity[name], name
+        assert cname in declared, cname
+    assert len(backend._RESPONSE_SLOTS) == 17  # LISA_response_wrap (lisaresponse.pyx:78-121)
+    # host memory in a device slot is refused before anything reaches the library's kernels
+    with pytest.raises(TypeError, match="device memory"):
+        backend._device_addr(np.zeros(4), "f8", "x")
