@@ -124,7 +124,7 @@ __device__ __forceinline__ double reduce_2pi(double x) {
 // the reduced angle |y| <= pi/4 (+ half an ulp of k), truncated after the y^17 / y^18 terms (truncation below
 // 3e-19), evaluated by Horner's rule, and the quadrant k mod 4 applied by swapping / negating.
 // Accuracy ~1e-16 absolute; checked against CUDA's sincos in tests/test_gpu_kernels.py.
-__device__ __forceinline__ void sincos_cw(double x, double* s, double* c) {
+__device__ __forceinline__ void sincos_cw(double x, double* s, double* c, double x_lo = 0.0) {
   const double TWO_OVER_PI = 0.6366197723675814;
   const double P1 = 1.5707963267948966;
   const double P2 = 6.123233995736766e-17;
@@ -135,6 +135,7 @@ __device__ __forceinline__ void sincos_cw(double x, double* s, double* c) {
   double y = fma(-k, P1, x);
   y = fma(-k, P2, y);
   y = fma(-k, P3, y);
+  y += x_lo;  // angle given as x + x_lo (|x_lo| <= a few ulp of x): folded in after the reduction
   double y2 = y * y;
   double ps = 2.8114572543455206e-15;
   ps = fma(ps, y2, -7.647163731819816e-13);

@@ -236,7 +236,61 @@ struct FusedArgs {
   // written at gh[3 (gh_off[b] + i - sup_start[b]) + channel]; null in the likelihood calls
   cplx* gh;
   const long long* gh_off;
+  // uniform-grid record of data_freqs (k_grid_detect) enabling the phase recurrence, or null
+  const struct GridInfo* grid;
 };
+
+// Data grid of the form f_i = fl((k0 + i) df): numpy's k * df and rfftfreq grids, the form
+// BBHx's data streams take.  k_grid_detect verifies the form bit-exactly on the device for
+// three candidates of df (the rounded f[N-1] / (k0 + N - 1) and its two neighbours); bit c of
+// ok says candidate c reproduces every f_i.  The fused kernel then knows every bin's exact
+// frequency k df (as p + pe, an error-free product), which the phase recurrence needs.
+struct GridInfo {
+  double k0;
+  double df[3];
+  unsigned ok;
+  unsigned pad;
+};
+
+__global__ void k_grid_detect(const double* __restrict__ f, int N, GridInfo* g) {
+  unsigned ok = 0;
+  double k0 = 0.0, cand[3] = {0.0, 0.0, 0.0};
+  if (N >= 2) {
+    const double f0 = f[0], f1 = f[N - 1];
+    const double dfa = (f1 - f0) / (double)(N - 1);
+    k0 = rint(f0 / dfa);
+    const double kN = k0 + (double)(N - 1);
+    const double dc = f1 / kN;
+    cand[0] = dc;
+    cand[1] = nextafter(dc, 0.0);
+    cand[2] = nextafter(dc, 1e300);
+    ok = (f0 > 0.0 && dfa > 0.0 && k0 >= 1.0 && kN < 4.0e15) ? 7u : 0u;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; ok && i < N;
+         i += (long long)gridDim.x * blockDim.x) {
+      const double kd = k0 + (double)i;
+      const double fi = f[i];
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        if (__dmul_rn(kd, cand[c]) != fi) ok &= ~(1u << c);
+    }
+  }
+  ok = __reduce_and_sync(0xffffffffu, ok);
+  if ((threadIdx.x & 31) == 0) atomicAnd(&g->ok, ok);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    g->k0 = k0;
+    g->df[0] = cand[0];
+    g->df[1] = cand[1];
+    g->df[2] = cand[2];
+  }
+}
+
+// Launch the grid detection into g (device) on stream s.
+inline int detect_grid(const double* f, int N, GridInfo* g, cudaStream_t s) {
+  int st = cuda_status(cudaMemsetAsync(&g->ok, 0xff, sizeof(unsigned), s), "grid record init");
+  if (st) return st;
+  k_grid_detect<<<grid_for(N, 256, sm_count() * 8), 256, 0, s>>>(f, N, g);
+  return launch_status("k_grid_detect");
+}
 
 // Segment table: for every (tile, binary, mode) the spline segments holding the first and the
 // last data bin of the binary's support inside the tile (searchsorted(side='right') - 1 of
@@ -381,6 +435,98 @@ __device__ __forceinline__ void accumulate_chunk(const SegCoef<R>& c, const doub
   }
 }
 
+// ---------------------------------------------------------------- phase recurrence
+// Inside one spline segment the phase is a cubic in the data-bin index, so along a lane's bins
+// (stride h = 32 df on a uniform grid) e^{i phi} advances by complex rotations:
+//   E_{j+1} = E_j R_j,  R_{j+1} = R_j Q_j,  Q_{j+1} = Q_j P,
+// with R = e^{i Delta}, Q = e^{i Delta^2}, P = e^{i Delta^3} the first, second and (constant)
+// third differences of the phase cubic.  Three FP64 complex products per bin replace the
+// per-bin phase cubic, range reduction and polynomial sine / cosine.  The state is re-anchored
+// (rot_anchor) at the first chunk of a segment and every kRecChunks chunks; the anchor phase is
+// evaluated at the bin's exact frequency k df (error-free product) with a compensated final sum,
+// so it carries ~1e-12 rad instead of the ~ulp(phi) ~ 1e-9 rad of a plain FP64 evaluation, and
+// the products add < 1e-12 rad over the kRecChunks * FD_K steps between anchors.
+constexpr int kRecChunks = 16;  // chunks (of FD_K steps per lane) between anchors
+
+struct Rot {
+  double er, ei, rr, ri, qr, qi, pr, pi;
+};
+
+// a *= b (complex, FP64)
+__device__ __forceinline__ void cmul_inplace(double& ar, double& ai, double br, double bi) {
+  const double r = fma(ar, br, -ai * bi);
+  const double i = fma(ar, bi, ai * br);
+  ar = r;
+  ai = i;
+}
+
+// Recurrence state at grid bin kd (exact integer k0 + i, as a double) of the segment whose
+// phase cubic is pc = (y, c1, c2, c3) about knot xk; h = 32 df.
+__device__ __forceinline__ void rot_anchor(Rot& z, const double* pc, double xk, double kd,
+                                           double df, double h) {
+  const double p = __dmul_rn(kd, df);     // the grid frequency f_i (bit-exact, see GridInfo)
+  const double pe = fma(kd, df, -p);      // p + pe = kd * df exactly
+  const double u = __dsub_rn(p, xk);      // exact: xk <= p < xk (1 + 1e-2) (Sterbenz)
+  const double y = pc[0], c1 = pc[1], c2 = pc[2], c3 = pc[3];
+  double t = u * fma(fma(c3, u, c2), u, c1);
+  const double d1 = fma(fma(3.0 * c3, u, 2.0 * c2), u, c1);  // phase derivative at u
+  t = fma(d1, pe, t);                     // first-order term of the low part of k df
+  const double sh = __dadd_rn(y, t);      // y + t = sh + se exactly (TwoSum)
+  const double bb = __dsub_rn(sh, y);
+  const double se = __dadd_rn(__dsub_rn(y, __dsub_rn(sh, bb)), __dsub_rn(t, bb));
+  sincos_cw(sh, &z.ei, &z.er, se);
+  const double D1 = h * fma(c3, fma(3.0 * u, u + h, h * h), fma(c2, fma(2.0, u, h), c1));
+  const double D2 = 2.0 * h * h * fma(3.0 * c3, u + h, c2);
+  const double D3 = 6.0 * c3 * h * h * h;
+  sincos_cw(D1, &z.ri, &z.rr);
+  sincos_cw(D2, &z.qi, &z.qr);
+  sincos_cw(D3, &z.pi, &z.pr);
+}
+
+// The FD_K bins of one lane inside one segment with the phase from the recurrence z (advanced
+// past the last bin on return): cubics of amplitude and transfer, conj(T A e^{i phi}) into acc;
+// bins with f < 0 (outside the support) or failing the t(f) gate (CHECK) contribute zero.
+template <typename R, bool CHECK>
+__device__ __forceinline__ void accumulate_chunk_rec(const SegCoef<R>& c, const double* f,
+                                                     double ts, double te, R (*acc)[6], Rot& z) {
+#pragma unroll
+  for (int j = 0; j < FD_K; ++j) {
+    const double u = f[j] - c.xk;
+    bool g = f[j] >= 0.0;
+    if (CHECK) {
+      const double tf = fma(fma(fma(c.p3[1], u, c.p2[1]), u, c.p1[1]), u, c.py[1]);
+      g = g && tf_gate(tf, ts, te);
+    }
+    const R ur = (R)u;
+    R v[7];
+#pragma unroll
+    for (int a = 0; a < 7; ++a) v[a] = fma(fma(fma(c.a3[a], ur, c.a2[a]), ur, c.a1[a]), ur, c.ay[a]);
+    const R amp = g ? v[0] : R(0);
+    const R apr = amp * (R)z.er, api = amp * (R)z.ei;
+    R* a = acc[j];
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch) {  // a += conj(T A e^{i phi})
+      const R tr = v[1 + 2 * ch], ti = v[2 + 2 * ch];
+      a[2 * ch] = fma(tr, apr, a[2 * ch]);
+      a[2 * ch] = fma(-ti, api, a[2 * ch]);
+      a[2 * ch + 1] = fma(-tr, api, a[2 * ch + 1]);
+      a[2 * ch + 1] = fma(-ti, apr, a[2 * ch + 1]);
+    }
+    cmul_inplace(z.er, z.ei, z.rr, z.ri);
+    cmul_inplace(z.rr, z.ri, z.qr, z.qi);
+    cmul_inplace(z.qr, z.qi, z.pr, z.pi);
+  }
+}
+
+// Per-warp recurrence state: E, R, Q, P of every (mode, lane) and, per mode, the chunk and
+// segment the saved state belongs to and the chunks left before the next anchor.
+struct alignas(16) RecStage {
+  double2 st[FD_MAXM][4][32];
+  int next_chunk[FD_MAXM];
+  int seg[FD_MAXM];
+  int left[FD_MAXM];
+};
+
 // G bins of one lane that lie in the same spline segment: the same arithmetic as
 // accumulate_bin, written branch-free (invalid or gated-off bins are dropped by selects) so the
 // G independent evaluation chains interleave.
@@ -513,11 +659,24 @@ __device__ __forceinline__ void load_seg(SegCoef<R>& cf, const WarpStage<R>& S, 
 // products with data and weights in FP64 when the FP32 copies of data and weights are given
 // (the path of Likelihood and UnevenBatch), in FP32 without them.
 // GH (FP64 form only): also write d lnL / d h of every support bin to A.gh (gradient chain).
-template <bool MIXED, typename R, bool GH = false>
+// REC (FP64 form): the phase recurrence in the one-segment chunk path when the data grid is
+// uniform (A.grid), with its state in RS.
+template <bool MIXED, typename R, bool GH = false, bool REC = false>
 __device__ __forceinline__ void fused_item(const FusedArgs& A, long long q, WarpStage<R>& S,
-                                           int lane) {
+                                           RecStage* RS, int lane) {
   const long long BML = A.qstride;
   const int L = A.L;
+  bool uni = false;
+  double gk0 = 0.0, gdf = 0.0;
+  if (REC && A.grid != nullptr) {
+    const unsigned ok = A.grid->ok & 7u;
+    if (ok) {
+      uni = true;
+      gk0 = A.grid->k0;
+      gdf = A.grid->df[(ok & 1u) ? 0 : (ok & 2u) ? 1 : 2];
+    }
+  }
+  const double hstep = 32.0 * gdf;
   {
     const int tile = (int)(q / A.B);
     const int b = (int)(q - (long long)tile * A.B);
@@ -532,6 +691,7 @@ __device__ __forceinline__ void fused_item(const FusedArgs& A, long long q, Warp
       return;
     }
     // ---- stage this tile's segments for every mode
+    if (REC && lane < FD_MAXM) RS->next_chunk[lane] = -1;
     if (lane < A.M) {
       const int2 kk = A.segtab[q * A.M + lane];
       const int klo = max(kk.x, 0), khi = min(kk.y, L - 2);
@@ -596,7 +756,10 @@ __device__ __forceinline__ void fused_item(const FusedArgs& A, long long q, Warp
 #pragma unroll
       for (int j = 0; j < FD_K; ++j) {
         const int i = c0 + 32 * j + lane;
-        fbin[j] = (i >= s0 && i < s1) ? __ldg(A.data_freqs + i) : -1.0;
+        // on a verified uniform grid f_i = fl(k df) is recomputed bit-exactly instead of loaded
+        fbin[j] = (i >= s0 && i < s1) ? (uni ? __dmul_rn(gk0 + (double)i, gdf)
+                                             : __ldg(A.data_freqs + i))
+                                      : -1.0;
 #pragma unroll
         for (int c = 0; c < 6; ++c) acc[j][c] = R(0);
       }
@@ -611,6 +774,39 @@ __device__ __forceinline__ void fused_item(const FusedArgs& A, long long q, Warp
           if (ka >= 0) {
             const int gate = S.gate[m][ka];
             if (gate == 2) continue;
+            if (REC && uni) {
+              // phase by recurrence: continue the saved state when this mode's previous chunk
+              // was the one before in the same segment, else anchor at this lane's first bin
+              const int nc = RS->next_chunk[m], sg = RS->seg[m], left = RS->left[m];
+              const bool cont = (nc == ck) && (sg == ka) && (left > 0);
+              Rot z;
+              if (cont) {
+                const double2 e = RS->st[m][0][lane], r = RS->st[m][1][lane];
+                const double2 qq = RS->st[m][2][lane], pp = RS->st[m][3][lane];
+                z.er = e.x; z.ei = e.y; z.rr = r.x; z.ri = r.y;
+                z.qr = qq.x; z.qi = qq.y; z.pr = pp.x; z.pi = pp.y;
+              } else {
+                rot_anchor(z, &S.pc[m][ka][0][0], S.x[m][ka], gk0 + (double)(c0 + lane), gdf,
+                           hstep);
+              }
+              load_seg<R>(cf, S, m, ka);
+              if (gate == 1)
+                accumulate_chunk_rec<R, false>(cf, fbin, ts, te, acc, z);
+              else
+                accumulate_chunk_rec<R, true>(cf, fbin, ts, te, acc, z);
+              RS->st[m][0][lane] = make_double2(z.er, z.ei);
+              RS->st[m][1][lane] = make_double2(z.rr, z.ri);
+              RS->st[m][2][lane] = make_double2(z.qr, z.qi);
+              RS->st[m][3][lane] = make_double2(z.pr, z.pi);
+              __syncwarp();
+              if (lane == 0) {
+                RS->next_chunk[m] = ck + 1;
+                RS->seg[m] = ka;
+                RS->left[m] = cont ? left - 1 : kRecChunks - 1;
+              }
+              __syncwarp();
+              continue;
+            }
             load_seg<R>(cf, S, m, ka);
             constexpr int G = 2;  // two interleaved bins: best of 1/2/4 at 4 CTAs per SM
             if (gate == 1)
@@ -752,18 +948,29 @@ __device__ __forceinline__ void fused_item(const FusedArgs& A, long long q, Warp
   }
 }
 
+// Shared memory of the fused kernels: FD_WARPS WarpStage slices, then (FP64 form, phase
+// recurrence) FD_WARPS RecStage slices.
+template <bool MIXED>
+constexpr size_t fused_smem_bytes() {
+  using R = typename std::conditional<MIXED, float, double>::type;
+  return FD_WARPS * (sizeof(WarpStage<R>) + (MIXED ? 0 : sizeof(RecStage)));
+}
+
 template <bool MIXED, bool GH = false>
 __global__ void __launch_bounds__(FD_WARPS * 32, MIXED ? 4 : 2) k_direct_fused(FusedArgs A) {
   static_assert(!(MIXED && GH), "d lnL / d h is written by the FP64 form only");
   using R = typename std::conditional<MIXED, float, double>::type;
+  constexpr bool REC = !MIXED;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   WarpStage<R>& S = reinterpret_cast<WarpStage<R>*>(smem_raw)[warp];
+  RecStage* RS = REC ? reinterpret_cast<RecStage*>(smem_raw + FD_WARPS * sizeof(WarpStage<R>)) + warp
+                     : nullptr;
   const long long nitems = (long long)A.ntiles * A.B;
   const long long gw = (long long)blockIdx.x * FD_WARPS + warp;
   const long long nw = (long long)gridDim.x * FD_WARPS;
-  for (long long q = gw; q < nitems; q += nw) fused_item<MIXED, R, GH>(A, q, S, lane);
+  for (long long q = gw; q < nitems; q += nw) fused_item<MIXED, R, GH, REC>(A, q, S, RS, lane);
 }
 
 // Several independent problems (groups: own data stream, grid length L, mode count M,
@@ -790,11 +997,14 @@ template <bool MIXED>
 __global__ void __launch_bounds__(FD_WARPS * 32, MIXED ? 4 : 2)
     k_direct_fused_multi(const MultiArgs* __restrict__ MA) {
   using R = typename std::conditional<MIXED, float, double>::type;
+  constexpr bool REC = !MIXED;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ FusedArgs gcur[FD_WARPS];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   WarpStage<R>& S = reinterpret_cast<WarpStage<R>*>(smem_raw)[warp];
+  RecStage* RS = REC ? reinterpret_cast<RecStage*>(smem_raw + FD_WARPS * sizeof(WarpStage<R>)) + warp
+                     : nullptr;
   const int ng = MA->ngroups;
   const long long total = MA->off[ng];
   const long long gw = (long long)blockIdx.x * FD_WARPS + warp;
@@ -815,7 +1025,7 @@ __global__ void __launch_bounds__(FD_WARPS * 32, MIXED ? 4 : 2)
       for (int i = lane; i < nw8; i += 32) dst[i] = src[i];
       __syncwarp();
     }
-    fused_item<MIXED, R>(gcur[warp], q - MA->off[g], S, lane);
+    fused_item<MIXED, R, false, REC>(gcur[warp], q - MA->off[g], S, RS, lane);
   }
 }
 
@@ -913,11 +1123,14 @@ int direct_fused_gh(cplx* gh, const long long* gh_off, double* d_h, double* h_h,
   const long long row0 = (long long)b0 * M * L;
   double* part = nullptr;
   int2* segtab = nullptr;
+  GridInfo* grid = nullptr;
   BBHX_CHECK_CUDA(pool_alloc_all(s, {{(void**)&part, sizeof(double) * 3 * nitems},
-                                     {(void**)&segtab, sizeof(int2) * nitems * M}}));
+                                     {(void**)&segtab, sizeof(int2) * nitems * M},
+                                     {(void**)&grid, sizeof(GridInfo)}}));
   k_tile_segments<<<grid_for(nitems * M, 256, sm_count() * 64), 256, 0, s>>>(
       segtab, x + row0, data_freqs, start + b0, len + b0, nb, M, L, ntiles, FD_TILE);
   int st = launch_status("k_tile_segments");
+  if (!st) st = detect_grid(data_freqs, N, grid, s);
   if (!st) {
     FusedArgs A;
     A.data_freqs = data_freqs;
@@ -947,10 +1160,11 @@ int direct_fused_gh(cplx* gh, const long long* gh_off, double* d_h, double* h_h,
     A.qstride = (long long)B_all * M * L;
     A.gh = gh;
     A.gh_off = gh_off;
+    A.grid = grid;
     const long long g = (nitems + FD_WARPS - 1) / FD_WARPS;
     const long long cap = 16LL * sm_count();
     const unsigned grid = (unsigned)(g < cap ? g : cap);
-    const size_t sm = sizeof(WarpStage<double>) * FD_WARPS;
+    const size_t sm = fused_smem_bytes<false>();
     st = cuda_status(cudaFuncSetAttribute(k_direct_fused<false, true>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm),
                      "cudaFuncSetAttribute(k_direct_fused)");
@@ -966,6 +1180,7 @@ int direct_fused_gh(cplx* gh, const long long* gh_off, double* d_h, double* h_h,
   }
   cudaFreeAsync(part, s);
   cudaFreeAsync(segtab, s);
+  cudaFreeAsync(grid, s);
   return st;
 }
 
@@ -1118,6 +1333,7 @@ int bbhx_direct_like_multi(const bbhx_direct_group* groups, int num_groups, int 
     A.qstride = (long long)A.B * A.M * A.L;
     A.gh = nullptr;
     A.gh_off = nullptr;
+    A.grid = nullptr;
     MA.off[g] = items;
     MA.boff[g] = bins;
     const long long nit = (long long)A.ntiles * A.B;
@@ -1127,22 +1343,27 @@ int bbhx_direct_like_multi(const bbhx_direct_group* groups, int num_groups, int 
     int* sup = nullptr;
     double* part = nullptr;
     int2* segtab = nullptr;
+    GridInfo* grid = nullptr;
     if (pool_alloc((void**)&sup, sizeof(int) * 2 * A.B, s) != cudaSuccess ||
         pool_alloc((void**)&part, sizeof(double) * 3 * nit, s) != cudaSuccess ||
-        pool_alloc((void**)&segtab, sizeof(int2) * nit * A.M, s) != cudaSuccess) {
+        pool_alloc((void**)&segtab, sizeof(int2) * nit * A.M, s) != cudaSuccess ||
+        pool_alloc((void**)&grid, sizeof(GridInfo), s) != cudaSuccess) {
       set_error("device allocation for group %d failed", g);
       st = ERR_CUDA;
     }
     if (sup) scratch.push_back(sup);
     if (part) scratch.push_back(part);
     if (segtab) scratch.push_back(segtab);
+    if (grid) scratch.push_back(grid);
     if (st) break;
     A.sup_start = sup;
     A.sup_len = sup + A.B;
     A.partials = part;
     A.segtab = segtab;
+    A.grid = grid;
     k_support<<<A.B, 128, 0, s>>>(A.x, A.M, A.L, A.B, A.data_freqs, A.N, sup, sup + A.B);
     st = launch_status("k_support");
+    if (!st) st = detect_grid(A.data_freqs, A.N, grid, s);
     if (!st) {
       k_tile_segments<<<grid_for(nit * A.M, 256, sm_count() * 64), 256, 0, s>>>(
           segtab, A.x, A.data_freqs, sup, sup + A.B, A.B, A.M, A.L, A.ntiles, tile_bins);
@@ -1167,13 +1388,13 @@ int bbhx_direct_like_multi(const bbhx_direct_group* groups, int num_groups, int 
     const long long want = (items + FD_WARPS - 1) / FD_WARPS;
     const unsigned grid = (unsigned)std::min<long long>(want, (long long)nsm * ctas_per_sm);
     if (precision == 1) {
-      const size_t sm = sizeof(WarpStage<float>) * FD_WARPS;
+      const size_t sm = fused_smem_bytes<true>();
       st = cuda_status(cudaFuncSetAttribute(k_direct_fused_multi<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)sm),
                        "cudaFuncSetAttribute(k_direct_fused_multi<true>)");
       if (!st) k_direct_fused_multi<true><<<grid, FD_WARPS * 32, sm, s>>>(dMA);
     } else {
-      const size_t sm = sizeof(WarpStage<double>) * FD_WARPS;
+      const size_t sm = fused_smem_bytes<false>();
       st = cuda_status(cudaFuncSetAttribute(k_direct_fused_multi<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)sm),
                        "cudaFuncSetAttribute(k_direct_fused_multi<false>)");
@@ -1209,12 +1430,15 @@ int bbhx_direct_like_fused(double* d_h, double* h_h, const double* data_freqs, c
   int* sup = nullptr;
   double* part = nullptr;
   int2* segtab = nullptr;
+  GridInfo* grid = nullptr;
   BBHX_CHECK_CUDA(pool_alloc_all(s, {{(void**)&sup, sizeof(int) * 2 * num_bin_all},
                                      {(void**)&part, sizeof(double) * 3 * nitems},
-                                     {(void**)&segtab, sizeof(int2) * nitems * num_modes}}));
+                                     {(void**)&segtab, sizeof(int2) * nitems * num_modes},
+                                     {(void**)&grid, sizeof(GridInfo)}}));
   k_support<<<num_bin_all, 128, 0, s>>>(x, num_modes, length, num_bin_all, data_freqs, data_length,
                                         sup, sup + num_bin_all);
   int st = launch_status("k_support");
+  if (!st) st = detect_grid(data_freqs, data_length, grid, s);
   if (!st) {
     k_tile_segments<<<grid_for(nitems * num_modes, 256, sm_count() * 64), 256, 0, s>>>(
         segtab, x, data_freqs, sup, sup + num_bin_all, num_bin_all, num_modes, length, ntiles,
@@ -1250,18 +1474,19 @@ int bbhx_direct_like_fused(double* d_h, double* h_h, const double* data_freqs, c
     A.qstride = (long long)num_bin_all * num_modes * length;
     A.gh = nullptr;
     A.gh_off = nullptr;
+    A.grid = grid;
     const long long warps_needed = (nitems + 0);
     long long g = (warps_needed + FD_WARPS - 1) / FD_WARPS;
     const long long cap = 16LL * sm_count();
     unsigned grid = (unsigned)(g < cap ? g : cap);
     if (precision == 1) {
-      const size_t sm = sizeof(WarpStage<float>) * FD_WARPS;
+      const size_t sm = fused_smem_bytes<true>();
       st = cuda_status(cudaFuncSetAttribute(k_direct_fused<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)sm),
                        "cudaFuncSetAttribute(k_direct_fused<true>)");
       if (!st) k_direct_fused<true><<<grid, FD_WARPS * 32, sm, s>>>(A);
     } else {
-      const size_t sm = sizeof(WarpStage<double>) * FD_WARPS;
+      const size_t sm = fused_smem_bytes<false>();
       st = cuda_status(cudaFuncSetAttribute(k_direct_fused<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)sm),
                        "cudaFuncSetAttribute(k_direct_fused<false>)");
@@ -1277,6 +1502,7 @@ int bbhx_direct_like_fused(double* d_h, double* h_h, const double* data_freqs, c
   cudaFreeAsync(sup, s);
   cudaFreeAsync(part, s);
   cudaFreeAsync(segtab, s);
+  cudaFreeAsync(grid, s);
   return st;
 }
 
