@@ -44,8 +44,10 @@ _SIGS = {
     "bbhx_interpolate": [_VP] * 6 + [_I] * 4 + [_VP],
     "bbhx_InterpTDI": [_VP] * 9 + [_I] * 4 + [_VP] * 3 + [_VP],
     "bbhx_direct_sum": [_VP, _VP, _I, _I, _I, _I, _VP, _VP, _VP],
+    "bbhx_fill_templates": [_VP, _VP, _VP, _VP, _I, _I, _I, _VP],
     "bbhx_direct_like": [_VP] * 7 + [_I, _I, _VP],
     "bbhx_hdyn": [_VP] * 5 + [_I, _I, _I, _VP],
+    "bbhx_hdyn_constants": [_VP, _VP, _VP, _VP, _I, _VP, _I, _VP, _I, _I, _VP, _I, _D, _VP],
     "bbhx_template_support": [_VP, _VP, _VP, _I, _I, _I, _VP, _I, _VP],
     "bbhx_direct_like_fused": [_VP] * 5 + [_I] + [_VP] * 7 + [_I, _I, _I, _I, _VP, _VP, _VP],
     "bbhx_hdyn_fused": [_VP] * 12 + [_D] + [_VP] * 5 + [_I] * 7 + [_VP],

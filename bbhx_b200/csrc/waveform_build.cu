@@ -9,6 +9,7 @@
 // Pointer conventions follow the reference bindings: InterpTDI's template / index pointer
 // arrays and its start / length / t_start / t_end arrays are HOST arrays (of device
 // addresses where they point at data); direct_sum takes device arrays.
+#include <algorithm>
 #include <vector>
 
 #include "capi_internal.cuh"
@@ -83,6 +84,43 @@ __global__ void k_direct_sum(cplx* out, const double* __restrict__ buf, int B, i
   }
 }
 
+// Template of each binary placed on the full data grid (waveformbuild.py:663-693, fill=True).
+struct FillJob {
+  const cplx* tmpl;  // [3, len]
+  int start, len;
+};
+
+// per binary: out[b, c, start + k] = tmpl[c, k] (out zeroed by the caller)
+__global__ void k_fill_each(cplx* __restrict__ out, const FillJob* __restrict__ jobs, int N) {
+  const int b = blockIdx.y;
+  const FillJob J = jobs[b];
+  const long long n = 3LL * J.len;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(t / J.len), k = (int)(t - (long long)c * J.len);
+    out[((long long)b * 3 + c) * N + J.start + k] = J.tmpl[t];
+  }
+}
+
+// combined: out[c, i] += tmpl_b[c, i - start_b] for every binary covering bin i, added in
+// binary order (the reference's loop of slice additions, so the sums round identically)
+__global__ void k_fill_combine(cplx* __restrict__ out, const FillJob* __restrict__ jobs, int B,
+                               int N, int i0, int i1) {
+  const long long n = 3LL * (i1 - i0);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(t / (i1 - i0));
+    const int i = i0 + (int)(t - (long long)c * (i1 - i0));
+    cplx acc = out[(long long)c * N + i];
+    for (int b = 0; b < B; ++b) {
+      const FillJob& J = jobs[b];
+      const int k = i - J.start;
+      if (k >= 0 && k < J.len) acc = acc + J.tmpl[(long long)c * J.len + k];
+    }
+    out[(long long)c * N + i] = acc;
+  }
+}
+
 }  // namespace bbhx
 
 using namespace bbhx;
@@ -129,6 +167,57 @@ int bbhx_InterpTDI(const int64_t* template_ptrs, const double* data_freqs, const
   // the host job array must outlive the asynchronous copy
   cudaError_t e = cudaStreamSynchronize(s);
   if (!st && e != cudaSuccess) st = cuda_status(e, "InterpTDI sync");
+  return st;
+}
+
+// fill=True placement of per-binary templates on the data grid (waveformbuild.py:663-693; the
+// reference loops over binaries in Python).  template_ptrs, starts, lengths: HOST arrays (the
+// pointers are device addresses of [3, len] complex128 templates, e.g. from InterpTDI).
+// combine = 0: out [B, 3, N] with each binary in its own row; 1: out [3, N], the templates
+// added in binary order.  out (device complex128) must be zeroed or hold the values to add to.
+int bbhx_fill_templates(void* out, const int64_t* template_ptrs, const int* starts,
+                        const int* lengths, int num_bin_all, int data_length, int combine,
+                        void* stream) {
+  BBHX_REQUIRE(num_bin_all >= 0 && num_bin_all <= 65535, "num_bin_all must be 0..65535");
+  if (num_bin_all == 0) return OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  std::vector<FillJob> jobs(num_bin_all);
+  int maxlen = 0, lo = data_length, hi = 0;
+  for (int b = 0; b < num_bin_all; ++b) {
+    BBHX_REQUIRE(lengths[b] >= 0 && starts[b] >= 0 &&
+                     (long long)starts[b] + lengths[b] <= data_length,
+                 "binary %d: data range [%d, %d) outside the data grid", b, starts[b],
+                 starts[b] + lengths[b]);
+    jobs[b].tmpl = (const cplx*)template_ptrs[b];
+    jobs[b].start = starts[b];
+    jobs[b].len = lengths[b];
+    if (lengths[b] > 0) {
+      maxlen = std::max(maxlen, lengths[b]);
+      lo = std::min(lo, starts[b]);
+      hi = std::max(hi, starts[b] + lengths[b]);
+    }
+  }
+  if (maxlen == 0) return OK;
+  FillJob* d_jobs = nullptr;
+  BBHX_CHECK_CUDA(pool_alloc((void**)&d_jobs, sizeof(FillJob) * num_bin_all, s));
+  int st = cuda_status(cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(FillJob) * num_bin_all,
+                                       cudaMemcpyHostToDevice, s),
+                       "fill job upload");
+  if (!st) {
+    if (combine) {
+      k_fill_combine<<<grid_for(3LL * (hi - lo), 256), 256, 0, s>>>((cplx*)out, d_jobs,
+                                                                    num_bin_all, data_length, lo, hi);
+      st = launch_status("k_fill_combine");
+    } else {
+      unsigned gx = (unsigned)std::min<long long>((3LL * maxlen + 255) / 256, 1024);
+      k_fill_each<<<dim3(gx, num_bin_all), 256, 0, s>>>((cplx*)out, d_jobs, data_length);
+      st = launch_status("k_fill_each");
+    }
+  }
+  cudaFreeAsync(d_jobs, s);
+  // the host job array must outlive the asynchronous copy
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (!st && e != cudaSuccess) st = cuda_status(e, "fill sync");
   return st;
 }
 

@@ -222,38 +222,37 @@ class HeterodynedLikelihood:
         freqs = np.logspace(np.log10(freqs_keep[0]), np.log10(freqs_keep[-1]), self.length_f_het)
         self.h0_sparse = self.template_gen(*p, freqs=freqs, **template_gen_kwargs)[None, :, :]
         self._h0_flat = self.h0_sparse[0].contiguous()
+        # the band the reference keeps, (f >= freqs[0]) & (f <= freqs[-1]), is a contiguous run
+        # of the sorted dense grid: [i0, i1)
         fd_all = to_np(self.f_dense)
-        inds = (fd_all >= freqs[0]) & (fd_all <= freqs[-1])
-        inds_d = to_dev(inds, t.bool)
-        self.f_dense = self.f_dense[inds_d]
-        self.d = self.d[:, inds_d]
-        h0 = h0[:, inds_d]
-        f_dense_h = fd_all[inds]
-        bins = np.searchsorted(freqs, f_dense_h, "right") - 1
-        f_m = (freqs[1:] + freqs[:-1]) / 2
+        i0 = int(np.searchsorted(fd_all, freqs[0], "left"))
+        i1 = int(np.searchsorted(fd_all, freqs[-1], "right"))
+        n = i1 - i0
+        f_dense_h = fd_all[i0:i1]
         df = f_dense_h[1] - f_dense_h[0]
         self.sens_mat.update_frequency_arr(f_dense_h)
-        S_n = to_dev(np.asarray([self.sens_mat[0], self.sens_mat[1], self.sens_mat[2]]))
-        bins_d = to_dev(bins, t.int64)
-        fmb = to_dev(f_dense_h - f_m[np.clip(bins, 0, len(f_m) - 1)])
-        A0_flat = 4 * (h0.conj() * self.d) / S_n * df
-        A1_flat = A0_flat * fmb
-        B0_flat = 4 * (h0.conj() * h0) / S_n * df
-        B1_flat = B0_flat * fmb
-        # per-bin sums into slot ind + 1, the last dense point excluded (likelihood.py:512-522)
+        S_n = to_dev(np.ascontiguousarray([self.sens_mat[0], self.sens_mat[1], self.sens_mat[2]]))
+        h0 = h0.contiguous()
+        d_full = self.d.contiguous()
+        N_all = d_full.shape[1]
         L = self.length_f_het
-        consts = []
-        for arr in (A0_flat, A1_flat, B0_flat, B1_flat):
-            acc = t.zeros((3, L), dtype=t.complex128, device=device())
-            acc.index_add_(1, (bins_d[:-1] + 1), arr[:, :-1])
-            consts.append(acc)
-        self.data_constants = t.cat([c.flatten() for c in consts]).contiguous()
-        self.reference_d_d = float((4 * (self.d.conj() * self.d) / S_n * df).sum().real.item())
-        self.reference_h_h = float(B0_flat.sum().real.item())
-        self.reference_d_h = float(A0_flat.sum().real.item())
+        freqs_d = to_dev(freqs)
+        consts = t.empty(4 * 3 * L, dtype=t.complex128, device=device())
+        ref = t.empty(3, dtype=t.float64, device=device())
+        # per-bin A0, A1, B0, B1 sums into slot j + 1 and the band's reference sums on the device
+        # (likelihood.py:480-530): bbhx_hdyn_constants reads the band in place
+        _lib.call("bbhx_hdyn_constants", _lib.dptr(consts), _lib.dptr(ref),
+                  _lib._VP(self.f_dense.data_ptr() + 8 * i0),
+                  _lib._VP(d_full.data_ptr() + 16 * i0), N_all,
+                  _lib._VP(h0.data_ptr() + 16 * i0), int(h0.shape[1]), _lib.dptr(S_n), n, n,
+                  _lib.dptr(freqs_d), L, float(df), _lib.stream())
+        self.f_dense = self.f_dense[i0:i1]
+        self.d = d_full[:, i0:i1]
+        self.data_constants = consts
+        self.reference_d_d, self.reference_h_h, self.reference_d_h = (float(v) for v in ref.cpu())
         self.reference_ll = -1 / 2 * (self.reference_d_d + self.reference_h_h - 2 * self.reference_d_h)
-        self.freqs = to_dev(freqs)
-        self.f_m = f_m
+        self.freqs = freqs_d
+        self.f_m = (freqs[1:] + freqs[:-1]) / 2
         template_gen_kwargs["squeeze"] = False
         self.template_gen_kwargs = template_gen_kwargs
 

@@ -230,17 +230,20 @@ class BBHWaveformFD:
                                         num_interp_params=9, num_modes=M, num_bin_all=B)
         template_channels = self.interp_response(freqs, spline.container, t_start, t_end, L, M, 3)
         if fill:
+            # placement on the full grid in one kernel (waveformbuild.py:663-693 loops over
+            # binaries): combined into [3, N] in binary order, or one row per binary
             nf = len(freqs)
+            ir = self.interp_response
+            tptrs = np.asarray([x.data_ptr() for x in ir.template_carrier], dtype=np.int64)
+            starts = np.ascontiguousarray(ir.start_inds, dtype=np.int32)
+            lengths = np.ascontiguousarray(ir.lengths, dtype=np.int32)
+            shape = (3, nf) if combine else (B, 3, nf)
+            data_out = t.zeros(shape, dtype=t.complex128, device=device())
+            _lib.call("bbhx_fill_templates", _lib.dptr(data_out), _lib.hptr(tptrs),
+                      _lib.hptr(starts), _lib.hptr(lengths), B, nf, int(bool(combine)),
+                      _lib.stream())
             if combine:
-                data_out = t.zeros((3, nf), dtype=t.complex128, device=device())
-                for temp, s, n in zip(template_channels, self.interp_response.start_inds,
-                                      self.interp_response.lengths):
-                    data_out[:, s:s + n] += temp
                 return data_out.squeeze() if squeeze else data_out
-            data_out = t.zeros((B, 3, nf), dtype=t.complex128, device=device())
-            for b, (temp, s, n) in enumerate(zip(template_channels, self.interp_response.start_inds,
-                                                 self.interp_response.lengths)):
-                data_out[b, :, s:s + n] = temp
             return data_out
         return (template_channels, self.interp_response.start_inds, self.interp_response.lengths)
 

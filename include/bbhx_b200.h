@@ -158,6 +158,14 @@ int bbhx_InterpTDI(const int64_t *template_ptrs, const double *data_freqs, const
                    int num_bin_all, int num_modes, const int64_t *inds_ptrs,
                    const int *inds_start, const int *ind_lengths, void *stream);
 
+/* fill=True placement of per-binary templates on the data grid (replaces the Python slice
+ * additions of src/bbhx/waveformbuild.py:663-693; no C counterpart there); template_ptrs,
+ * starts, lengths are [host] arrays (device addresses of [3, len] complex128 templates);
+ * combine 0: out [B, 3, N], 1: out [3, N] summed in binary order; out zeroed by the caller */
+int bbhx_fill_templates(void *out, const int64_t *template_ptrs, const int *starts,
+                        const int *lengths, int num_bin_all, int data_length, int combine,
+                        void *stream);
+
 /* replaces direct_sum (WaveformBuild.hh:8-10) */
 int bbhx_direct_sum(double *templates, const double *buffer, int num_bin_all, int length,
                     int n_channels, int num_modes, const double *t_start, const double *t_end,
@@ -173,6 +181,16 @@ int bbhx_direct_like(double *d_h, double *h_h, const double *data, const double 
 /* replaces hdyn (Likelihood.hh:6-9) */
 int bbhx_hdyn(double *d_h, double *h_h, const double *residuals, const double *constants,
               const double *freqs, int num_bin_all, int length, int n_channels, void *stream);
+
+/* relative-binning constants of the heterodyned likelihood (replaces the per-bin Python loop
+ * of HeterodynedLikelihood.init_heterodyne_info, src/bbhx/likelihood.py:480-530; no C
+ * counterpart there): f [n] the narrowed dense grid, d and h0 complex rows of 3 channels with
+ * row strides ld_d / ld_h, S PSD rows (stride ld_s), freqs [L] the sparse grid, df the dense
+ * bin width.  consts [4, 3, L] complex (A0, A1, B0, B1 summed into slot j + 1, the last dense
+ * point excluded), ref [3] = <d|d>, <h0|h0>, Re<d|h0> over the band (device). */
+int bbhx_hdyn_constants(void *consts, double *ref, const double *f, const void *d, int ld_d,
+                        const void *h0, int ld_h, const double *S, int ld_s, int n,
+                        const double *freqs, int L, double df, void *stream);
 
 /* support [start, start+len) of each binary on the data grid (waveformbuild.py:136-177) */
 int bbhx_template_support(int *start, int *len, const double *x, int num_modes, int length,

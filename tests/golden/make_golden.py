@@ -121,6 +121,26 @@ def direct_like_case(params):
                 buffer0=wave_gen.out_buffer_final[:, :1].copy())
 
 
+def fill_and_modes_case(params):
+    """BBHWaveformFD branches beyond the likelihood's: fill=True combined into one [3, N]
+    stream and one row per binary [B, 3, N] (waveformbuild.py:663-693), stored decimated
+    (every 97th bin) together with exact per-row sums; direct=True, compress=False per-mode
+    templates [B, 3, M, L] (waveformbuild.py:603-636) on a 128-point grid."""
+    orbits = EqualArmlengthOrbits()
+    wave_gen = BBHWaveformFD(amp_phase_kwargs=dict(run_phenomd=False),
+                             response_kwargs=dict(orbits=orbits, TDItag="AET", tdi2=True))
+    f = data_grid(TOBS, F_LO, F_HI)
+    kw = dict(length=1024, t_obs_start=0.0, t_obs_end=TOBS)
+    comb = wave_gen(*params, freqs=f, direct=False, fill=True, combine=True, **kw)
+    each = wave_gen(*params, freqs=f, direct=False, fill=True, combine=False, **kw)
+    fr = np.logspace(-4, -1.5, 128)
+    modes = wave_gen(*params, freqs=fr, direct=True, compress=False, t_obs_start=0.0,
+                     t_obs_end=TOBS)
+    return dict(combine_decim=comb[:, ::97].copy(), combine_abs_sum=np.abs(comb).sum(axis=-1),
+                each_decim=each[:, :, ::97].copy(), each_abs_sum=np.abs(each).sum(axis=-1),
+                modes=np.asarray(modes).copy(), modes_freqs=fr)
+
+
 def het_like_case(center, walkers):
     orbits = EqualArmlengthOrbits()
     wave_gen = BBHWaveformFD(amp_phase_kwargs=dict(run_phenomd=False),
@@ -168,6 +188,9 @@ def main():
     dl = direct_like_case(P)
     for k, v in dl.items():
         out[f"dl_{k}"] = v
+    fm = fill_and_modes_case(P[:, :3])
+    for k, v in fm.items():
+        out[f"wf_{k}"] = v
     W = perturb_params(P[:, 0], 8, SEED_WALK)
     out["het_walkers"] = W
     hl = het_like_case(P[:, 0], W)

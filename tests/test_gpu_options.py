@@ -53,3 +53,34 @@ def test_heterodyned_fused_xyz_matches_chain(golden, golden_data):
                                     precision=prec)
         out[prec] = het.get_ll(golden["het_walkers"], **kw)
     np.testing.assert_allclose(out["fp64"], out[None], rtol=1e-10, atol=1e-6)
+
+
+def test_fill_and_per_mode_outputs_match_reference(golden, golden_data):
+    """BBHWaveformFD's fill=True streams (combined [3, N] and one row per binary [B, 3, N],
+    placed by the fill kernel; waveformbuild.py:663-693) and the direct=True, compress=False
+    per-mode templates [B, 3, M, L] (waveformbuild.py:603-636) against the reference's own
+    outputs (tests/golden, decimated every 97th bin plus exact per-row magnitude sums):
+    row-relative 1e-9, the template bar of the InterpTDI parity test."""
+    from bbhx_b200 import BBHWaveformFD, EqualArmlengthOrbits
+
+    from test_gpu_parity import rowclose
+
+    wave = BBHWaveformFD(amp_phase_kwargs=dict(run_phenomd=False),
+                         response_kwargs=dict(orbits=EqualArmlengthOrbits(), TDItag="AET", tdi2=True))
+    P = golden["params"][:, :3]
+    f, tobs = golden_data["f"], golden_data["tobs"]
+    kw = dict(length=1024, t_obs_start=0.0, t_obs_end=tobs)
+    comb = wave(*P, freqs=f, direct=False, fill=True, combine=True, **kw).cpu().numpy()
+    assert comb.shape == (3, len(f))
+    rowclose(comb[:, ::97], golden["wf_combine_decim"], rtol=1e-9)
+    np.testing.assert_allclose(np.abs(comb).sum(axis=-1), golden["wf_combine_abs_sum"], rtol=1e-9)
+    each = wave(*P, freqs=f, direct=False, fill=True, combine=False, **kw).cpu().numpy()
+    assert each.shape == (3, 3, len(f))
+    rowclose(each[:, :, ::97], golden["wf_each_decim"], rtol=1e-9)
+    np.testing.assert_allclose(np.abs(each).sum(axis=-1), golden["wf_each_abs_sum"], rtol=1e-9)
+    # the combined stream is the sum of the rows (overlapping supports added in binary order)
+    np.testing.assert_allclose(each.sum(axis=0), comb, rtol=0, atol=1e-12 * np.abs(comb).max())
+    modes = wave(*P, freqs=golden["wf_modes_freqs"], direct=True, compress=False,
+                 t_obs_start=0.0, t_obs_end=tobs).cpu().numpy()
+    assert modes.shape == golden["wf_modes"].shape
+    rowclose(modes, golden["wf_modes"], rtol=1e-9)
