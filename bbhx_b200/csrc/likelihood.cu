@@ -203,7 +203,11 @@ constexpr int FD_WARP_BINS = 32 * FD_K;          // 128
 // per-item staging, segment table and gate classification over more bins (B = 1024 benchmark:
 // 512 -> 104 ms, 1024 -> 88, 2048 -> 80, 4096 -> 78, 8192 -> 79 ms mixed)
 constexpr int FD_TILE = 4096;
-constexpr int FD_NSEG = 8;    // spline segments per (tile, mode) staged in shared memory
+// spline segments per (tile, mode) staged in shared memory: 8 for the mixed form, 4 for the
+// FP64 form, whose slices (FP64 coefficients plus the phase-recurrence state) must stay small
+// enough for 3 CTAs per SM
+template <typename R>
+constexpr int fd_nseg() { return sizeof(R) == 8 ? 4 : 8; }
 constexpr int FD_MAXM = 6;    // modes per binary
 constexpr int FD_NC = 36;     // 9 quantities x (y, c1, c2, c3) per segment
 constexpr int FD_MAXCHUNK = 32;  // 128-bin chunks per tile item (tiles of up to 4096 bins)
@@ -435,6 +439,22 @@ __device__ __forceinline__ void accumulate_chunk(const SegCoef<R>& c, const doub
   }
 }
 
+// Per-warp shared-memory copy of the spline segments one (tile, binary) item needs, for every
+// mode: x of the segments' knots, the FP64 cubic coefficients of phase and t(f), and those of
+// the amplitude and six transfer components in R (FP32 when mixed), each quantity's
+// (y, c1, c2, c3) contiguous so a lane reloads a segment with vector loads.
+template <typename R>
+struct alignas(16) WarpStage {
+  static constexpr int NSEG = fd_nseg<R>();
+  double x[FD_MAXM][NSEG + 1];
+  double pc[FD_MAXM][NSEG][2][4];
+  R ac[FD_MAXM][NSEG][7][4];
+  int klo[FD_MAXM];
+  int nseg[FD_MAXM];
+  int gate[FD_MAXM][NSEG];  // t(f) gate over the whole segment: 0 mixed, 1 all in, 2 all out
+  signed char cseg[FD_MAXCHUNK][FD_MAXM];  // staged segment holding a whole 128-bin chunk, or -1
+};
+
 // ---------------------------------------------------------------- phase recurrence
 // Inside one spline segment the phase is a cubic in the data-bin index, so along a lane's bins
 // (stride h = 32 df on a uniform grid) e^{i phi} advances by complex rotations:
@@ -483,45 +503,144 @@ __device__ __forceinline__ void rot_anchor(Rot& z, const double* pc, double xk, 
   sincos_cw(D3, &z.pi, &z.pr);
 }
 
-// The FD_K bins of one lane inside one segment with the phase from the recurrence z (advanced
-// past the last bin on return): cubics of amplitude and transfer, conj(T A e^{i phi}) into acc;
-// bins with f < 0 (outside the support) or failing the t(f) gate (CHECK) contribute zero.
+// The FD_K bins of one lane inside staged segment ka of mode m, with the phase from the
+// recurrence z (advanced past the last bin on return): conj(T A e^{i phi}) into acc; bins with
+// f < 0 (outside the support) or failing the t(f) gate (CHECK) contribute zero.  The cubics
+// are evaluated one quantity at a time for all FD_K bins, reading that quantity's four
+// coefficients from shared memory, which keeps few coefficients and partial values live.
 template <typename R, bool CHECK>
-__device__ __forceinline__ void accumulate_chunk_rec(const SegCoef<R>& c, const double* f,
-                                                     double ts, double te, R (*acc)[6], Rot& z) {
+__device__ __forceinline__ void accumulate_chunk_rec(const WarpStage<R>& S, int m, int ka,
+                                                     const double* f, double ts, double te,
+                                                     R (*acc)[6], Rot& z) {
+  const double xk = S.x[m][ka];
+  double u[FD_K];
+  bool g[FD_K];
 #pragma unroll
   for (int j = 0; j < FD_K; ++j) {
-    const double u = f[j] - c.xk;
-    bool g = f[j] >= 0.0;
-    if (CHECK) {
-      const double tf = fma(fma(fma(c.p3[1], u, c.p2[1]), u, c.p1[1]), u, c.py[1]);
-      g = g && tf_gate(tf, ts, te);
-    }
-    const R ur = (R)u;
-    R v[7];
+    u[j] = f[j] - xk;
+    g[j] = f[j] >= 0.0;
+  }
+  if (CHECK) {
+    const double2 lo = *reinterpret_cast<const double2*>(&S.pc[m][ka][1][0]);
+    const double2 hi = *reinterpret_cast<const double2*>(&S.pc[m][ka][1][2]);
 #pragma unroll
-    for (int a = 0; a < 7; ++a) v[a] = fma(fma(fma(c.a3[a], ur, c.a2[a]), ur, c.a1[a]), ur, c.ay[a]);
-    const R amp = g ? v[0] : R(0);
-    const R apr = amp * (R)z.er, api = amp * (R)z.ei;
-    R* a = acc[j];
-#pragma unroll
-    for (int ch = 0; ch < 3; ++ch) {  // a += conj(T A e^{i phi})
-      const R tr = v[1 + 2 * ch], ti = v[2 + 2 * ch];
-      a[2 * ch] = fma(tr, apr, a[2 * ch]);
-      a[2 * ch] = fma(-ti, api, a[2 * ch]);
-      a[2 * ch + 1] = fma(-tr, api, a[2 * ch + 1]);
-      a[2 * ch + 1] = fma(-ti, apr, a[2 * ch + 1]);
+    for (int j = 0; j < FD_K; ++j) {
+      const double tf = fma(fma(fma(hi.y, u[j], hi.x), u[j], lo.y), u[j], lo.x);
+      g[j] = g[j] && tf_gate(tf, ts, te);
     }
+  }
+  // e^{i phi} of the FD_K bins from the recurrence
+  double er[FD_K], ei[FD_K];
+#pragma unroll
+  for (int j = 0; j < FD_K; ++j) {
+    er[j] = z.er;
+    ei[j] = z.ei;
     cmul_inplace(z.er, z.ei, z.rr, z.ri);
     cmul_inplace(z.rr, z.ri, z.qr, z.qi);
     cmul_inplace(z.qr, z.qi, z.pr, z.pi);
   }
+  auto cubic4 = [&](int a, R* v) {
+    R c[4];
+    if (sizeof(R) == 4) {
+      const float4 q = *reinterpret_cast<const float4*>(&S.ac[m][ka][a][0]);
+      c[0] = (R)q.x; c[1] = (R)q.y; c[2] = (R)q.z; c[3] = (R)q.w;
+    } else {
+      const double2 lo = *reinterpret_cast<const double2*>(&S.ac[m][ka][a][0]);
+      const double2 hi = *reinterpret_cast<const double2*>(&S.ac[m][ka][a][2]);
+      c[0] = (R)lo.x; c[1] = (R)lo.y; c[2] = (R)hi.x; c[3] = (R)hi.y;
+    }
+#pragma unroll
+    for (int j = 0; j < FD_K; ++j) {
+      const R ur = (R)u[j];
+      v[j] = fma(fma(fma(c[3], ur, c[2]), ur, c[1]), ur, c[0]);
+    }
+  };
+  // A e^{i phi}
+  R apr[FD_K], api[FD_K];
+  {
+    R amp[FD_K];
+    cubic4(0, amp);
+#pragma unroll
+    for (int j = 0; j < FD_K; ++j) {
+      const R a = g[j] ? amp[j] : R(0);
+      apr[j] = a * (R)er[j];
+      api[j] = a * (R)ei[j];
+    }
+  }
+  // acc += conj(T_ch A e^{i phi}) channel by channel
+#pragma unroll
+  for (int ch = 0; ch < 3; ++ch) {
+    R tr[FD_K], ti[FD_K];
+    cubic4(1 + 2 * ch, tr);
+    cubic4(2 + 2 * ch, ti);
+#pragma unroll
+    for (int j = 0; j < FD_K; ++j) {
+      R* a = acc[j];
+      a[2 * ch] = fma(tr[j], apr[j], a[2 * ch]);
+      a[2 * ch] = fma(-ti[j], api[j], a[2 * ch]);
+      a[2 * ch + 1] = fma(-tr[j], api[j], a[2 * ch + 1]);
+      a[2 * ch + 1] = fma(-ti[j], apr[j], a[2 * ch + 1]);
+    }
+  }
 }
 
-// Per-warp recurrence state: E, R, Q, P of every (mode, lane) and, per mode, the chunk and
-// segment the saved state belongs to and the chunks left before the next anchor.
+// FP64 form off the recurrence path: one (bin, mode) with each quantity's cubic coefficients
+// read where they are used, from a staged segment in shared memory (SmemCoef) or from the
+// spline arrays in global memory (GlobalCoef), so these less frequent paths hold no segment in
+// registers and stay within the register budget of the recurrence path.
+struct SmemCoef {
+  const WarpStage<double>& S;
+  int m, k;
+  __device__ __forceinline__ double xk() const { return S.x[m][k]; }
+  // quantity p: 0 amplitude, 1 phase, 2 t(f), 3..8 transfer (Re, Im of three channels)
+  __device__ __forceinline__ void get(int p, double* c) const {
+    const double* src = (p == 1 || p == 2) ? &S.pc[m][k][p - 1][0] : &S.ac[m][k][p == 0 ? 0 : p - 2][0];
+    const double2 lo = *reinterpret_cast<const double2*>(src);
+    const double2 hi = *reinterpret_cast<const double2*>(src + 2);
+    c[0] = lo.x; c[1] = lo.y; c[2] = hi.x; c[3] = hi.y;
+  }
+};
+
+struct GlobalCoef {
+  const FusedArgs& A;
+  long long o;  // offset of (binary, mode, segment) in one quantity's [B, M, L] block
+  double x;
+  __device__ __forceinline__ double xk() const { return x; }
+  __device__ __forceinline__ void get(int p, double* c) const {
+    const long long q = p * A.qstride + o;
+    c[0] = __ldg(A.y + q); c[1] = __ldg(A.c1 + q); c[2] = __ldg(A.c2 + q); c[3] = __ldg(A.c3 + q);
+  }
+};
+
+template <typename Src>
+__device__ __forceinline__ void accumulate_bin_src(const Src& src, double f, double ts, double te,
+                                                   double* acc) {
+  const double u = f - src.xk();
+  double c[4];
+  src.get(2, c);
+  if (!tf_gate(fma(fma(fma(c[3], u, c[2]), u, c[1]), u, c[0]), ts, te)) return;
+  src.get(1, c);
+  double sn, cs;
+  sincos_cw(fma(fma(fma(c[3], u, c[2]), u, c[1]), u, c[0]), &sn, &cs);
+  src.get(0, c);
+  const double amp = fma(fma(fma(c[3], u, c[2]), u, c[1]), u, c[0]);
+  const double apr = amp * cs, api = amp * sn;
+#pragma unroll
+  for (int ch = 0; ch < 3; ++ch) {
+    src.get(3 + 2 * ch, c);
+    const double tr = fma(fma(fma(c[3], u, c[2]), u, c[1]), u, c[0]);
+    src.get(4 + 2 * ch, c);
+    const double ti = fma(fma(fma(c[3], u, c[2]), u, c[1]), u, c[0]);
+    acc[2 * ch] += tr * apr - ti * api;
+    acc[2 * ch + 1] -= tr * api + ti * apr;
+  }
+}
+
+// Per-warp recurrence state: E, R, Q of every (mode, lane), P per mode and, per mode, the chunk
+// and segment the saved state belongs to and the chunks left before the next anchor.
 struct alignas(16) RecStage {
-  double2 st[FD_MAXM][4][32];
+  double2 st[FD_MAXM][3][32];  // E, R, Q of every lane
+  double2 P[FD_MAXM];          // e^{i Delta^3}: the same for every lane of a segment
   int next_chunk[FD_MAXM];
   int seg[FD_MAXM];
   int left[FD_MAXM];
@@ -572,20 +691,6 @@ __device__ __forceinline__ void accumulate_group(const SegCoef<R>& c, const doub
   }
 }
 
-// Per-warp shared-memory copy of the spline segments one (tile, binary) item needs, for every
-// mode: x of the segments' knots, the FP64 cubic coefficients of phase and t(f), and those of
-// the amplitude and six transfer components in R (FP32 when mixed), each quantity's
-// (y, c1, c2, c3) contiguous so a lane reloads a segment with vector loads.
-template <typename R>
-struct alignas(16) WarpStage {
-  double x[FD_MAXM][FD_NSEG + 1];
-  double pc[FD_MAXM][FD_NSEG][2][4];
-  R ac[FD_MAXM][FD_NSEG][7][4];
-  int klo[FD_MAXM];
-  int nseg[FD_MAXM];
-  int gate[FD_MAXM][FD_NSEG];  // t(f) gate over the whole segment: 0 mixed, 1 all in, 2 all out
-  signed char cseg[FD_MAXCHUNK][FD_MAXM];  // staged segment holding a whole 128-bin chunk, or -1
-};
 
 // Whole-segment t(f) gate: bound the cubic t(u) = y + c1 u + c2 u^2 + c3 u^3 over
 // u in [0, h] (end points and stationary points) and classify the segment as entirely inside
@@ -652,7 +757,7 @@ __device__ __forceinline__ void load_seg(SegCoef<R>& cf, const WarpStage<R>& S, 
 // The warp stages the tile's segments of every mode (from the segment table) into its slice of
 // shared memory, then walks the tile in FD_TILE / FD_WARP_BINS chunks of 128 bins (lane l owns
 // bins chunk + l + 32 j, j < FD_K) and keeps the <d|h>, <h|h> partial sums in registers; no
-// block-wide barrier is involved.  Tiles whose modes span more than FD_NSEG segments (only the
+// block-wide barrier is involved.  Tiles whose modes span more than NSEG segments (only the
 // lowest frequencies) take a per-lane walk over global memory instead.
 // MIXED: phase, t(f), the phase reduction and all accumulations in FP64; amplitude, transfer
 // functions, sin/cos of the reduced phase and the mode sum (the template) in FP32; the per-bin
@@ -697,7 +802,7 @@ __device__ __forceinline__ void fused_item(const FusedArgs& A, long long q, Warp
       const int klo = max(kk.x, 0), khi = min(kk.y, L - 2);
       const int n = (kk.x > kk.y || khi < klo) ? 0 : khi - klo + 1;
       S.klo[lane] = klo;
-      S.nseg[lane] = (n > FD_NSEG) ? -1 : n;
+      S.nseg[lane] = (n > WarpStage<R>::NSEG) ? -1 : n;
     }
     __syncwarp();
     for (int m = 0; m < A.M; ++m) {
@@ -722,8 +827,9 @@ __device__ __forceinline__ void fused_item(const FusedArgs& A, long long q, Warp
     }
     __syncwarp();
     const double ts = __ldg(A.t_start + b), te = __ldg(A.t_end + b);
-    for (int idx = lane; idx < A.M * FD_NSEG; idx += 32) {
-      const int m = idx / FD_NSEG, sg = idx - m * FD_NSEG;
+    constexpr int NSEG = WarpStage<R>::NSEG;
+    for (int idx = lane; idx < A.M * NSEG; idx += 32) {
+      const int m = idx / NSEG, sg = idx - m * NSEG;
       if (sg < S.nseg[m])
         S.gate[m][sg] = segment_gate(&S.pc[m][sg][1][0], S.x[m][sg + 1] - S.x[m][sg], ts, te);
     }
@@ -782,38 +888,46 @@ __device__ __forceinline__ void fused_item(const FusedArgs& A, long long q, Warp
               Rot z;
               if (cont) {
                 const double2 e = RS->st[m][0][lane], r = RS->st[m][1][lane];
-                const double2 qq = RS->st[m][2][lane], pp = RS->st[m][3][lane];
+                const double2 qq = RS->st[m][2][lane], pp = RS->P[m];
                 z.er = e.x; z.ei = e.y; z.rr = r.x; z.ri = r.y;
                 z.qr = qq.x; z.qi = qq.y; z.pr = pp.x; z.pi = pp.y;
               } else {
                 rot_anchor(z, &S.pc[m][ka][0][0], S.x[m][ka], gk0 + (double)(c0 + lane), gdf,
                            hstep);
               }
-              load_seg<R>(cf, S, m, ka);
+              const double2 pnew = make_double2(z.pr, z.pi);
               if (gate == 1)
-                accumulate_chunk_rec<R, false>(cf, fbin, ts, te, acc, z);
+                accumulate_chunk_rec<R, false>(S, m, ka, fbin, ts, te, acc, z);
               else
-                accumulate_chunk_rec<R, true>(cf, fbin, ts, te, acc, z);
+                accumulate_chunk_rec<R, true>(S, m, ka, fbin, ts, te, acc, z);
               RS->st[m][0][lane] = make_double2(z.er, z.ei);
               RS->st[m][1][lane] = make_double2(z.rr, z.ri);
               RS->st[m][2][lane] = make_double2(z.qr, z.qi);
-              RS->st[m][3][lane] = make_double2(z.pr, z.pi);
               __syncwarp();
               if (lane == 0) {
                 RS->next_chunk[m] = ck + 1;
                 RS->seg[m] = ka;
                 RS->left[m] = cont ? left - 1 : kRecChunks - 1;
+                RS->P[m] = pnew;  // every lane's P of the segment is bitwise the same
               }
               __syncwarp();
               continue;
             }
-            load_seg<R>(cf, S, m, ka);
-            constexpr int G = 2;  // two interleaved bins: best of 1/2/4 at 4 CTAs per SM
-            if (gate == 1)
-              accumulate_chunk<MIXED, R, G, false>(cf, fbin, ts, te, acc);
-            else
-              accumulate_chunk<MIXED, R, G, true>(cf, fbin, ts, te, acc);
-            continue;
+            if constexpr (!MIXED) {
+              const SmemCoef src{S, m, ka};
+#pragma unroll
+              for (int j = 0; j < FD_K; ++j)
+                if (fbin[j] >= 0.0) accumulate_bin_src(src, fbin[j], ts, te, acc[j]);
+              continue;
+            } else {
+              load_seg<R>(cf, S, m, ka);
+              constexpr int G = 2;  // two interleaved bins: best of 1/2/4 at 4 CTAs per SM
+              if (gate == 1)
+                accumulate_chunk<MIXED, R, G, false>(cf, fbin, ts, te, acc);
+              else
+                accumulate_chunk<MIXED, R, G, true>(cf, fbin, ts, te, acc);
+              continue;
+            }
           }
           // segment of every bin (local index; n = past the last staged segment)
           int kb[FD_K];
@@ -827,7 +941,13 @@ __device__ __forceinline__ void fused_item(const FusedArgs& A, long long q, Warp
             ok[j] = ok[j] && kl < n;
             kb[j] = kl;
           }
-          constexpr int G = MIXED ? 1 : 2;  // FP64 gains from 2 interleaved chains; mixed keeps occupancy
+          if constexpr (!MIXED) {
+#pragma unroll
+            for (int j = 0; j < FD_K; ++j)
+              if (ok[j]) accumulate_bin_src(SmemCoef{S, m, kb[j]}, fbin[j], ts, te, acc[j]);
+            continue;
+          }
+          constexpr int G = 1;
           int kc = -1;
 #pragma unroll
           for (int j0 = 0; j0 < FD_K; j0 += G) {
@@ -875,6 +995,14 @@ __device__ __forceinline__ void fused_item(const FusedArgs& A, long long q, Warp
               while (k + 1 < L && __ldg(xrow + k + 1) <= f) ++k;
             }
             if (k < 0 || k >= L - 1) continue;
+            if constexpr (!MIXED) {
+              if (k != kc) {
+                kc = k;
+                xk1 = __ldg(xrow + k + 1);
+              }
+              accumulate_bin_src(GlobalCoef{A, rowi * L + k, __ldg(xrow + k)}, f, ts, te, acc[j]);
+              continue;
+            }
             if (k != kc) {
               kc = k;
               cf.xk = __ldg(xrow + k);
@@ -957,7 +1085,7 @@ constexpr size_t fused_smem_bytes() {
 }
 
 template <bool MIXED, bool GH = false>
-__global__ void __launch_bounds__(FD_WARPS * 32, MIXED ? 4 : 2) k_direct_fused(FusedArgs A) {
+__global__ void __launch_bounds__(FD_WARPS * 32, MIXED ? 4 : 3) k_direct_fused(FusedArgs A) {
   static_assert(!(MIXED && GH), "d lnL / d h is written by the FP64 form only");
   using R = typename std::conditional<MIXED, float, double>::type;
   constexpr bool REC = !MIXED;
@@ -994,7 +1122,7 @@ __global__ void k_store_groups(MultiArgs M, MultiArgs* dst) {
 }
 
 template <bool MIXED>
-__global__ void __launch_bounds__(FD_WARPS * 32, MIXED ? 4 : 2)
+__global__ void __launch_bounds__(FD_WARPS * 32, MIXED ? 4 : 3)
     k_direct_fused_multi(const MultiArgs* __restrict__ MA) {
   using R = typename std::conditional<MIXED, float, double>::type;
   constexpr bool REC = !MIXED;

@@ -80,6 +80,13 @@ def _check(name, k, got, ref, call, row_len):
     if ref.size == 0:
         return
     rows = ref.size // row_len if ref.size % row_len == 0 else 1
+    if name == "interpolate_wrap" and k in (3, 4, 5):
+        # c1, c2, c3 live in the tridiagonal solver's diagonals (Interpolate.cu:332-334); their
+        # last entry of each row is never written as a coefficient and holds what the solver
+        # left there (LAPACK dgtsv's LU factors on the reference's CPU backend, other values on
+        # its GPU backend), and no spline evaluation reads it: compare the L - 1 segments
+        got = got.reshape(rows, row_len)[:, :-1]
+        ref = ref.reshape(rows, row_len)[:, :-1]
     tol = 1e-9 if name in ("direct_sum_wrap", "InterpTDI_wrap", "direct_like_wrap") else 1e-10
     err = _row_rel(got, ref, rows)
     assert err <= tol, f"call {call} {name} arg {k}: row-relative error {err:.2e} > {tol}"
