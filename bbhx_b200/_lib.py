@@ -49,6 +49,12 @@ _SIGS = {
     "bbhx_hdyn": [_VP] * 5 + [_I, _I, _I, _VP],
     "bbhx_hdyn_constants": [_VP, _VP, _VP, _VP, _I, _VP, _I, _VP, _I, _I, _VP, _I, _D, _VP],
     "bbhx_template_support": [_VP, _VP, _VP, _I, _I, _I, _VP, _I, _VP],
+    "bbhx_step_front": [_VP] * 10 + [_I, _I, _D, _D, _VP, _I, _VP],
+    "bbhx_tf_range_check": [_VP, _LL, _D, _D, _VP, _VP],
+    "bbhx_pack_lnl": [_VP, _VP, _VP, _D, _I, _I, _VP, _I, _VP],
+    "bbhx_tssb_from_lframe": [_VP, _VP, _VP, _VP, _I, _D, _I, _VP],
+    "bbhx_frame_transform": [_VP] * 8 + [_I, _D, _I, _VP],
+    "bbhx_sky_mode_transform": [_VP] + [_I] * 8 + [_VP],
     "bbhx_direct_like_fused": [_VP] * 5 + [_I] + [_VP] * 7 + [_I, _I, _I, _I, _VP, _VP, _VP],
     "bbhx_hdyn_fused": [_VP] * 12 + [_D] + [_VP] * 5 + [_I] * 7 + [_VP],
     "bbhx_hdyn_grad": [_VP] * 9 + [_I, _D, _D] + [_VP] * 5 + [_I] * 7 + [_VP],

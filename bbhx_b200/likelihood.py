@@ -16,6 +16,7 @@ from . import _lib
 from .sensitivity import AET1SensitivityMatrix, SensitivityMatrix
 from .utils.arrays import device, to_dev, to_np, torch
 from .waveformbuild import PRECISIONS
+from .waveforms.phenomhm import raise_chi_flag
 
 
 class Likelihood:
@@ -90,10 +91,14 @@ class Likelihood:
                                                     self.data_channels, self.noise_factors,
                                                     flags=flags, precision=self.precision, **kw)
         self.d_h, self.h_h = d_h, h_h
-        d_h_temp = d_h if not phase_marginalize else d_h.abs().to(t.complex128)
-        out = -1.0 / 2.0 * (self.d_d + h_h - 2 * d_h_temp).real
-        packed = t.cat([out, d_h_temp.real, h_h.real, flags.to(t.float64)]).cpu().numpy()
-        B = out.numel()
+        # lnL, Re <d|h> (|<d|h>| when phase-marginalised), Re <h|h> and the status flags in one
+        # device buffer, one copy to the host (likelihood.py:204-225)
+        B = d_h.numel()
+        packed_d = t.empty(3 * B + 3, dtype=t.float64, device=device())
+        _lib.call("bbhx_pack_lnl", _lib.dptr(packed_d), _lib.dptr(d_h), _lib.dptr(h_h),
+                  float(self.d_d), B, int(bool(phase_marginalize)), _lib.dptr(flags), 3,
+                  _lib.stream())
+        packed = packed_d.cpu().numpy()
         fl = packed[3 * B:]
         if fl[0] == 1:
             raise ValueError("The search for a window at x_min did not run correctly. If t_ref is "
@@ -104,8 +109,7 @@ class Likelihood:
                              "crossing zero twice.")
         if fl[1] != 0:
             raise ValueError("Orbital information does not cover the t(f) range of the templates.")
-        if fl[2] != 0:
-            raise ValueError("chi1z or chi2z array contains values with abs(chi) > 1.0 which is not allowed.")
+        raise_chi_flag(int(fl[2]))
         ll = packed[:B]
         if return_extracted_snr:
             return np.array([ll, packed[B:2 * B] / np.sqrt(packed[2 * B:3 * B])]).T
@@ -338,8 +342,13 @@ class HeterodynedLikelihood:
             _lib.call("bbhx_hdyn", _lib.dptr(self.hdyn_d_h), _lib.dptr(self.hdyn_h_h),
                       _lib.dptr(residuals), _lib.dptr(self.data_constants), _lib.dptr(self.freqs),
                       B, len(self.freqs), 3, _lib.stream())
-        d_h_temp = self.hdyn_d_h if not phase_marginalize else self.hdyn_d_h.abs().to(t.complex128)
-        out = (-1 / 2.0 * (self.reference_d_d + self.hdyn_h_h - 2 * d_h_temp).real).cpu().numpy()
+        B = self.hdyn_d_h.numel()
+        packed_d = t.empty(3 * B, dtype=t.float64, device=device())
+        _lib.call("bbhx_pack_lnl", _lib.dptr(packed_d), _lib.dptr(self.hdyn_d_h),
+                  _lib.dptr(self.hdyn_h_h), float(self.reference_d_d), B,
+                  int(bool(phase_marginalize)), _lib._VP(0), 0, _lib.stream())
+        packed = packed_d.cpu().numpy()
+        out = packed[:B]
         if return_extracted_snr:
-            return np.array([out, to_np(d_h_temp.real) / np.sqrt(to_np(self.hdyn_h_h.real))]).T
+            return np.array([out, packed[B:2 * B] / np.sqrt(packed[2 * B:3 * B])]).T
         return out

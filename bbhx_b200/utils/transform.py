@@ -14,6 +14,10 @@ src/bbhx/utils/transform.py), on numpy arrays or torch tensors (CPU or CUDA) ali
 * ``mbh_sky_mode_transform`` (transform.py:296-426): the 8 (4 longitudinal x 2 latitudinal)
   degenerate sky modes of a source.
 * ``mT_q``, ``modpi``, ``mod2pi`` (transform.py:28-72).
+
+numpy inputs are transformed with numpy on the host, as the reference does; CUDA tensors go
+through the library's kernels (bbhx_tssb_from_lframe, bbhx_frame_transform,
+bbhx_sky_mode_transform), one launch per call.
 """
 import math
 
@@ -31,6 +35,21 @@ def _is_torch(x):
         return isinstance(x, torch.Tensor)
     except ImportError:
         return False
+
+
+def _is_cuda(*xs):
+    return any(_is_torch(x) and x.is_cuda for x in xs)
+
+
+def _cuda_args(*xs):
+    """float64 contiguous device tensors of a common broadcast shape, and that shape."""
+    import torch
+
+    ts = [x if _is_torch(x) else torch.as_tensor(x, dtype=torch.float64) for x in xs]
+    dev = next(t.device for t in ts if t.is_cuda)
+    ts = torch.broadcast_tensors(*[t.to(device=dev, dtype=torch.float64) for t in ts])
+    shape = ts[0].shape
+    return [t.contiguous().reshape(-1) for t in ts], shape
 
 
 class _Ops:
@@ -70,7 +89,22 @@ def mod2pi(phase):
     return phase - ops.floor(phase / (2 * np.pi)) * 2 * np.pi
 
 
+def _tssb_cuda(t, lam, beta, t0, inverse):
+    """tSSBfromLframe / tLfromSSBframe of CUDA tensors in one library kernel."""
+    import torch
+
+    from .. import _lib
+
+    (t, lam, beta), shape = _cuda_args(t, lam, beta)
+    out = torch.empty_like(t)
+    _lib.call("bbhx_tssb_from_lframe", _lib.dptr(out), _lib.dptr(t), _lib.dptr(lam),
+              _lib.dptr(beta), t.numel(), float(t0), int(inverse), _lib.stream())
+    return out.reshape(shape)
+
+
 def tSSBfromLframe(tL, lambdaSSB, betaSSB, t0=0.0):
+    if _is_cuda(tL, lambdaSSB, betaSSB):
+        return _tssb_cuda(tL, lambdaSSB, betaSSB, t0, 0)
     ops = _Ops(tL, lambdaSSB, betaSSB)
     phase = ConstOmega * tL + ConstOmega * t0 - lambdaSSB
     RoC = OrbitR / C_SI
@@ -79,6 +113,8 @@ def tSSBfromLframe(tL, lambdaSSB, betaSSB, t0=0.0):
 
 
 def tLfromSSBframe(tSSB, lambdaSSB, betaSSB, t0=0.0):
+    if _is_cuda(tSSB, lambdaSSB, betaSSB):
+        return _tssb_cuda(tSSB, lambdaSSB, betaSSB, t0, 1)
     ops = _Ops(tSSB, lambdaSSB, betaSSB)
     phase = ConstOmega * tSSB + ConstOmega * t0 - lambdaSSB
     return tSSB - OrbitR / C_SI * ops.cos(betaSSB) * ops.cos(phase)
@@ -102,8 +138,23 @@ def _rotate_sky(lam, beta, alpha, zeta, ops):
     return lam_new, beta_new, dpsi
 
 
+def _frame_cuda(t, lam, beta, psi, t0, to_ssb):
+    import torch
+
+    from .. import _lib
+
+    ins, shape = _cuda_args(t, lam, beta, psi)
+    outs = [torch.empty_like(ins[0]) for _ in range(4)]
+    _lib.call("bbhx_frame_transform", *[_lib.dptr(o) for o in outs], *[_lib.dptr(i) for i in ins],
+              ins[0].numel(), float(t0 * YRSID_SI), int(to_ssb), _lib.stream())
+    return tuple(o.reshape(shape) for o in outs)
+
+
 def LISA_to_SSB(tL, lambdaL, betaL, psiL, t0=0.0):
-    """(tSSB, lambdaSSB, betaSSB, psiSSB) from the constellation-frame values; t0 in years."""
+    """(tSSB, lambdaSSB, betaSSB, psiSSB) from the constellation-frame values; t0 in years.
+    CUDA tensors run in one library kernel (bbhx_frame_transform)."""
+    if _is_cuda(tL, lambdaL, betaL, psiL):
+        return _frame_cuda(tL, lambdaL, betaL, psiL, t0, 1)
     ops = _Ops(tL, lambdaL, betaL, psiL)
     t0 = t0 * YRSID_SI
     tSSB = tL
@@ -115,7 +166,10 @@ def LISA_to_SSB(tL, lambdaL, betaL, psiL, t0=0.0):
 
 
 def SSB_to_LISA(tSSB, lambdaSSB, betaSSB, psiSSB, t0=0.0):
-    """(tL, lambdaL, betaL, psiL) from the SSB-frame values; t0 in years."""
+    """(tL, lambdaL, betaL, psiL) from the SSB-frame values; t0 in years.  CUDA tensors run in
+    one library kernel (bbhx_frame_transform)."""
+    if _is_cuda(tSSB, lambdaSSB, betaSSB, psiSSB):
+        return _frame_cuda(tSSB, lambdaSSB, betaSSB, psiSSB, t0, 0)
     ops = _Ops(tSSB, lambdaSSB, betaSSB, psiSSB)
     t0 = t0 * YRSID_SI
     alpha = ConstOmega * tSSB + ConstOmega * t0
@@ -138,6 +192,24 @@ def mbh_sky_mode_transform(coords, ind_map=None, kind="both", inplace=False, cos
                          "longitudinal transformation, or both for both.")
     factor = factors[kind]
     torch_in = _is_torch(coords)
+    if torch_in and coords.is_cuda:
+        import torch
+
+        from .. import _lib
+
+        if inplace and coords.shape[0] % factor != 0:
+            raise ValueError(
+                "If performing an inplace transformation, the coords provided must have a first "
+                "dimension size divisible by {} for a '{}' transformation.".format(factor, kind))
+        out = coords if inplace else coords.repeat(factor, 1)
+        work = out if (out.dtype == torch.float64 and out.is_contiguous()) else \
+            out.to(torch.float64).contiguous()
+        _lib.call("bbhx_sky_mode_transform", _lib.dptr(work), work.shape[0], work.shape[1],
+                  ind_map["inc"], ind_map["lam"], ind_map["beta"], ind_map["psi"],
+                  {"both": 0, "long": 1, "lat": 2}[kind], int(bool(cos_i)), _lib.stream())
+        if work is not out:
+            out.copy_(work)
+        return out
     if inplace:
         if coords.shape[0] % factor != 0:
             raise ValueError(

@@ -19,10 +19,8 @@ import numpy as np
 from . import _lib
 from .response.fastfdresponse import LISATDIResponse
 from .utils.arrays import atleast_1d, device, to_dev, to_np, torch
-from .utils.constants import YRSID_SI
 from .utils.interpolate import CubicSplineInterpolant
-from .utils.transform import tSSBfromLframe
-from .waveforms.phenomhm import PhenomHMAmpPhase
+from .waveforms.phenomhm import PhenomHMAmpPhase, step_front
 
 
 # arithmetic of the fused direct likelihood: "fp64" (parity form) or "mixed" (FP64 phase,
@@ -102,18 +100,6 @@ class BBHWaveformFD:
         return torch()
 
     # ------------------------------------------------------------------ helpers
-    @staticmethod
-    def _time_limits(lam, beta, t_obs_start, t_obs_end):
-        """SSB-frame start / end of the observation (waveformbuild.py:477-484): numpy on
-        the host for host inputs, torch on the device for device inputs."""
-        t = torch()
-        if isinstance(lam, t.Tensor) and lam.is_cuda:
-            return (tSSBfromLframe(t_obs_start * YRSID_SI, lam, beta, 0.0).contiguous(),
-                    tSSBfromLframe(t_obs_end * YRSID_SI, lam, beta, 0.0).contiguous())
-        t_start = np.atleast_1d(tSSBfromLframe(t_obs_start * YRSID_SI, lam, beta, 0.0))
-        t_end = np.atleast_1d(tSSBfromLframe(t_obs_end * YRSID_SI, lam, beta, 0.0))
-        return t_start, t_end
-
     def _sparse_buffer(self, params, t_obs_start, t_obs_end, freqs, length, modes, direct,
                        flags=None):
         """Fill the [9, B, M, L] sparse buffer (amp, phase, t(f), 6 transfer slots).
@@ -124,22 +110,19 @@ class BBHWaveformFD:
         recorded there instead of raising, so the caller can defer the host sync."""
         t = torch()
         (m1, m2, chi1z, chi2z, distance, phi_ref, f_ref, inc, lam, beta, psi, t_ref) = params
-        if isinstance(lam, t.Tensor) and lam.is_cuda:
-            lam_h, beta_h = atleast_1d(lam), atleast_1d(beta)
-        else:
-            lam_h = to_np(atleast_1d(lam)).astype(np.float64)
-            beta_h = to_np(atleast_1d(beta)).astype(np.float64)
-        t_start, t_end = self._time_limits(lam_h, beta_h, t_obs_start, t_obs_end)
         if freqs is None and length is None:
             raise ValueError("Must input freqs or length.")
-        B = len(lam_h)
         ap = self.amp_phase_gen
         if direct:
             length = freqs.shape[-1] if freqs is not None else length
         M = len(modes) if modes is not None else len(ap.allowable_modes)
+        # mass ordering, spin check, SSB observation limits and per-row spans in one kernel
+        pars, t_start, t_end, tobs_rows = step_front(m1, m2, chi1z, chi2z, lam, beta, M,
+                                                     (t_obs_start, t_obs_end), flags=flags)
+        B = pars.shape[1]
         out_buffer = t.zeros(9 * length * M * B, dtype=t.float64, device=device())
         ap._prepare(m1, m2, chi1z, chi2z, distance, None, f_ref, t_ref, length,
-                    freqs if direct else None, out_buffer, modes, flags=flags)
+                    freqs if direct else None, out_buffer, modes, flags=flags, front=pars)
         M = ap.num_modes
         if not direct:
             n = ap.num_per_param
@@ -150,9 +133,8 @@ class BBHWaveformFD:
             new_f = t.empty(n, dtype=t.float64, device=device())
             fminmax = t.empty(2 * rows, dtype=t.float64, device=device())
             err = flags if flags is not None else t.zeros(2, dtype=t.int32, device=device())
-            Tobs = ap._tobs_rows(t_end - t_start)
             _lib.call("bbhx_tf_window_regrid", _lib.dptr(new_f), _lib.dptr(fminmax),
-                      _lib.dptr(ap._freqs), _lib.dptr(tf0), _lib.dptr(Tobs), length, rows,
+                      _lib.dptr(ap._freqs), _lib.dptr(tf0), _lib.dptr(tobs_rows), length, rows,
                       _lib.dptr(err), _lib.stream())
             if flags is None:
                 e = int(err[0].item())
@@ -171,9 +153,8 @@ class BBHWaveformFD:
             tfs = out_buffer[2 * B * M * length:3 * B * M * length]
             tmin, tmax = float(rg.orbits.t_base.min()), float(rg.orbits.t_base.max())
             if flags is not None:
-                mm = t.aminmax(tfs)
-                bad = (mm.min < tmin) | (mm.max > tmax)
-                flags[1] = t.where(bad, t.ones_like(flags[1]), flags[1])
+                _lib.call("bbhx_tf_range_check", _lib.dptr(tfs), tfs.numel(), tmin, tmax,
+                          _lib._VP(flags.data_ptr() + 4), _lib.stream())
             else:
                 lo, hi = float(tfs.min()), float(tfs.max())
                 if lo < tmin or hi > tmax:
@@ -255,19 +236,13 @@ class BBHWaveformFD:
         [4, 3, L] (likelihood.py:550-648, Likelihood.cu:20-123)."""
         t = torch()
         (m1, m2, chi1z, chi2z, distance, phi_ref, f_ref, inc, lam, beta, psi, t_ref) = params
-        if isinstance(lam, t.Tensor) and lam.is_cuda:
-            lam_h, beta_h = atleast_1d(lam), atleast_1d(beta)
-        else:
-            lam_h = to_np(atleast_1d(lam)).astype(np.float64)
-            beta_h = to_np(atleast_1d(beta)).astype(np.float64)
-        t_start, t_end = self._time_limits(lam_h, beta_h, t_obs_start, t_obs_end)
         ap = self.amp_phase_gen
-        ap._setup_records(m1, m2, chi1z, chi2z, distance, t_ref, modes, flags=flags)
+        pars, ts_d, te_d, _ = step_front(m1, m2, chi1z, chi2z, lam, beta, 1,
+                                         (t_obs_start, t_obs_end), flags=flags)
+        ap._setup_records(m1, m2, chi1z, chi2z, distance, t_ref, modes, flags=flags, front=pars)
         B, M, L = ap.num_bin_all, ap.num_modes, int(freqs.numel())
         rg = self.response_gen
         inc_d, lam_d, beta_d, psi_d, phi_d = (to_dev(atleast_1d(v)) for v in (inc, lam, beta, psi, phi_ref))
-        ts_d = to_dev(t_start)
-        te_d = to_dev(t_end)
         d_h = t.empty(B, dtype=t.complex128, device=device())
         h_h = t.empty(B, dtype=t.complex128, device=device())
         _lib.call("bbhx_hdyn_fused", rg.orbit_handle.ptr, _lib.dptr(d_h), _lib.dptr(h_h),
@@ -287,9 +262,10 @@ class BBHWaveformFD:
         P = params.to(device=device(), dtype=t.float64).contiguous()
         rows = tuple(P[k] for k in range(12))
         m1, m2, chi1z, chi2z, distance, phi_ref, f_ref, inc, lam, beta, psi, t_ref = rows
-        t_start, t_end = self._time_limits(lam, beta, t_obs_start, t_obs_end)
+        pars, t_start, t_end, _ = step_front(m1, m2, chi1z, chi2z, lam, beta, 1,
+                                             (t_obs_start, t_obs_end))
         ap = self.amp_phase_gen
-        ap._setup_records(m1, m2, chi1z, chi2z, distance, t_ref, modes)
+        ap._setup_records(m1, m2, chi1z, chi2z, distance, t_ref, modes, front=pars)
         B, M, L = ap.num_bin_all, ap.num_modes, int(freqs.numel())
         rg = self.response_gen
         d_h = t.empty(B, dtype=t.complex128, device=device())

@@ -14,7 +14,7 @@ import numpy as np
 
 from .. import _lib
 from ..utils.arrays import atleast_1d, device, to_dev, torch
-from ..utils.constants import MSUN_SI
+from ..utils.constants import YRSID_SI
 from .ringdownphenomd import QNMData_a, QNMData_fdamp, QNMData_fring, dspin
 
 ALLOWABLE_MODES = [(2, 2), (3, 3), (4, 4), (2, 1), (3, 2), (4, 3)]
@@ -35,6 +35,52 @@ def qnm_spline_table():
               _lib.dptr(c2), _lib.dptr(c3), n, 2, 1, 1, _lib.stream())
     tab = t.stack([y[0, 0], c1[0, 0], c2[0, 0], c3[0, 0], y[1, 0], c1[1, 0], c2[1, 0], c3[1, 0]])
     return tab.contiguous()
+
+
+CHI1_MSG = "chi1z array contains values with abs(chi1z) > 1.0 which is not allowed."
+CHI2_MSG = "chi2z array contains values with abs(chi2z) > 1.0 which is not allowed."
+
+
+def raise_chi_flag(code):
+    """The reference's spin-range errors (phenomhm.py:168-185) from the flag bits set by the
+    step front end (1: chi1z, 2: chi2z; chi1z is reported first, as the reference checks it
+    first)."""
+    if code & 1:
+        raise ValueError(CHI1_MSG)
+    if code & 2:
+        raise ValueError(CHI2_MSG)
+
+
+def step_front(m1, m2, chi1z, chi2z, lam=None, beta=None, num_modes=1, t_obs=(0.0, 0.0),
+               flags=None):
+    """Per-binary front end of a step in one kernel (bbhx_step_front): m1 >= m2 ordering with
+    the spins swapped alongside, SI masses and the |chi| <= 1 check (phenomhm.py:175-199), and,
+    when lam / beta are given, the SSB observation limits (waveformbuild.py:477-484) and the
+    per-(binary, mode) spans the window regrid reads.  ``flags`` (device int32 [3]) is cleared
+    and receives the spin check (flags[2] bits 1 / 2); without it the check raises here.
+    Returns (pars [6, B] = m1, m2, chi1z, chi2z, m1_SI, m2_SI; t_start, t_end, tobs_rows)."""
+    t = torch()
+    cols = [to_dev(atleast_1d(v)).contiguous() for v in (m1, m2, chi1z, chi2z)]
+    B = cols[0].numel()
+    if any(c.numel() != B for c in cols):
+        raise ValueError("all parameter arrays must have the same length")
+    pars = t.empty((6, B), dtype=t.float64, device=device())
+    own = flags is None
+    fl = t.empty(3, dtype=t.int32, device=device()) if own else flags
+    ts = te = tob = None
+    if lam is not None:
+        lam = to_dev(atleast_1d(lam)).contiguous()
+        beta = to_dev(atleast_1d(beta)).contiguous()
+        ts = t.empty(B, dtype=t.float64, device=device())
+        te = t.empty(B, dtype=t.float64, device=device())
+        tob = t.empty(B * num_modes, dtype=t.float64, device=device())
+    _lib.call("bbhx_step_front", _lib.dptr(pars), _lib.dptr(ts), _lib.dptr(te), _lib.dptr(tob),
+              *[_lib.dptr(c) for c in cols], _lib.dptr(lam), _lib.dptr(beta), B, num_modes,
+              float(t_obs[0] * YRSID_SI), float(t_obs[1] * YRSID_SI), _lib.dptr(fl),
+              int(fl.numel()), _lib.stream())
+    if own:
+        raise_chi_flag(int(fl[2].item()))
+    return pars, ts, te, tob
 
 
 class PhenomHMAmpPhase:
@@ -77,24 +123,6 @@ class PhenomHMAmpPhase:
                     "Requested mode [(l,m) = ({},{})] is not available. Allowable modes include {}"
                     .format(ell, mm, self.allowable_modes))
 
-    @staticmethod
-    def _sanity_check_params(m1, m2, chi1z, chi2z, flags=None):
-        """|chi| <= 1 check and m1 >= m2 ordering (phenomhm.py:175-199).  With a device
-        ``flags`` tensor the spin check is recorded in flags[2] instead of raising, so no
-        host synchronisation happens here."""
-        t = torch()
-        if flags is not None:
-            bad = (chi1z.abs() > 1.0).any() | (chi2z.abs() > 1.0).any()
-            flags[2] = t.where(bad, t.ones_like(flags[2]), flags[2])
-        else:
-            if bool((chi1z.abs() > 1.0).any()):
-                raise ValueError("chi1z array contains values with abs(chi1z) > 1.0 which is not allowed.")
-            if bool((chi2z.abs() > 1.0).any()):
-                raise ValueError("chi2z array contains values with abs(chi2z) > 1.0 which is not allowed.")
-        switch = m1 < m2
-        return (t.where(switch, m2, m1), t.where(switch, m1, m2), t.where(switch, chi2z, chi1z),
-                t.where(switch, chi1z, chi2z))
-
     # ------------------------------------------------------------------ views
     @property
     def amp(self):
@@ -125,11 +153,11 @@ class PhenomHMAmpPhase:
 
     # ------------------------------------------------------------------ core
     def _prepare(self, m1, m2, chi1z, chi2z, distance, phi_ref, f_ref, t_ref, length, freqs,
-                 out_buffer, modes, flags=None):
+                 out_buffer, modes, flags=None, front=None):
         """Shared front half of run_wave: parameter checks, modes, buffers, ringdown
         frequencies and the per-(binary, mode) model records."""
         t = torch()
-        self._setup_records(m1, m2, chi1z, chi2z, distance, t_ref, modes, flags)
+        self._setup_records(m1, m2, chi1z, chi2z, distance, t_ref, modes, flags, front)
         m1, m2 = self._m1, self._m2
         num_modes, num_bin_all, mms = self.num_modes, self.num_bin_all, self.mms
         self.length = length
@@ -157,15 +185,14 @@ class PhenomHMAmpPhase:
                 raise ValueError(
                     "If providing freqs, must be 1D array (length,) or 3D array (length, num_modes, length).")
 
-    def _setup_records(self, m1, m2, chi1z, chi2z, distance, t_ref, modes, flags=None):
+    def _setup_records(self, m1, m2, chi1z, chi2z, distance, t_ref, modes, flags=None,
+                       front=None):
         """Parameter checks, mode list, ringdown frequencies and the per-(binary, mode)
-        model records (``self._coeffs``), without any frequency grid or output buffer."""
+        model records (``self._coeffs``), without any frequency grid or output buffer.
+        ``front``: the [6, B] output of step_front when the caller already ran it."""
         t = torch()
-        m1 = to_dev(atleast_1d(m1)).clone()
-        m2 = to_dev(atleast_1d(m2)).clone()
-        chi1z = to_dev(atleast_1d(chi1z)).clone()
-        chi2z = to_dev(atleast_1d(chi2z)).clone()
-        m1, m2, chi1z, chi2z = self._sanity_check_params(m1, m2, chi1z, chi2z, flags)
+        pars = front if front is not None else step_front(m1, m2, chi1z, chi2z, flags=flags)[0]
+        m1, m2, chi1z, chi2z, m1_SI, m2_SI = pars
         if modes is not None:
             key = tuple(tuple(md) for md in modes)
             cache = self.__dict__.setdefault("_mode_tensors", {})
@@ -191,11 +218,9 @@ class PhenomHMAmpPhase:
         self.t_ref_dev = to_dev(atleast_1d(t_ref))
         if distance.numel() != num_bin_all or self.t_ref_dev.numel() != num_bin_all:
             raise ValueError("all parameter arrays must have the same length")
-        m1_SI = (m1 * MSUN_SI).contiguous()
-        m2_SI = (m2 * MSUN_SI).contiguous()
         ncol = 1 if self.run_phenomd else num_modes + 1
-        self.fringdown = t.zeros(num_bin_all * ncol, dtype=t.float64, device=device())
-        self.fdamp = t.zeros_like(self.fringdown)
+        self.fringdown = t.empty(num_bin_all * ncol, dtype=t.float64, device=device())
+        self.fdamp = t.empty_like(self.fringdown)
         tab = self.qnm_table
         _lib.call("bbhx_ringdown_frequencies_all", _lib.dptr(self.fringdown), _lib.dptr(self.fdamp),
                   _lib.dptr(m1), _lib.dptr(m2), _lib.dptr(chi1z), _lib.dptr(chi2z), _lib.dptr(ells),

@@ -192,6 +192,41 @@ int bbhx_hdyn_constants(void *consts, double *ref, const double *f, const void *
                         const void *h0, int ld_h, const double *S, int ld_s, int n,
                         const double *freqs, int L, double df, void *stream);
 
+/* ------------------------------------------------------------------ driver bookkeeping on the
+ * device (each replaces elementwise array code of the reference's Python drivers, so a
+ * likelihood step runs no framework kernels; no C counterparts in the reference) */
+/* front end of a step (phenomhm.py:175-199, waveformbuild.py:477-484): out [6, B] = m1, m2
+ * (ordered m1 >= m2, Msun), chi1z, chi2z (swapped with the masses), m1, m2 in kg; t_start, t_end
+ * [B] = tSSBfromLframe of the observation limits t_obs_start_L / t_obs_end_L (seconds), may be
+ * NULL with lam / beta; tobs_rows [B, M] = t_end - t_start (may be NULL); flags device int
+ * [nflags >= 3] cleared, then flags[2] |= 1 (some |chi1z| > 1), |= 2 (some |chi2z| > 1) */
+int bbhx_step_front(double *out, double *t_start, double *t_end, double *tobs_rows,
+                    const double *m1, const double *m2, const double *chi1z, const double *chi2z,
+                    const double *lam, const double *beta, int num_bin_all, int num_modes,
+                    double t_obs_start_L, double t_obs_end_L, int *flags, int nflags,
+                    void *stream);
+/* orbit-table coverage of t(f) (fastfdresponse.py:427-433): *flag = 1 if any tf[0..n) lies
+ * outside [tmin, tmax] (only ever set) */
+int bbhx_tf_range_check(const double *tf, long long n, double tmin, double tmax, int *flag,
+                        void *stream);
+/* packed [3 B + nflags] = lnL | Re d_h' | Re h_h | flags, lnL = -(d_d + Re h_h - 2 Re d_h') / 2
+ * with d_h' = |d_h| when phase_marginalize (likelihood.py:204-225, :633-648) */
+int bbhx_pack_lnl(double *packed, const void *d_h, const void *h_h, double d_d, int num_bin_all,
+                  int phase_marginalize, const int *flags, int nflags, void *stream);
+/* tSSBfromLframe (inverse 0) / tLfromSSBframe (inverse 1) elementwise (utils/transform.py:75-135),
+ * t0 in seconds */
+int bbhx_tssb_from_lframe(double *out, const double *t, const double *lam, const double *beta,
+                          int n, double t0, int inverse, void *stream);
+/* LISA_to_SSB (to_ssb 1) / SSB_to_LISA (to_ssb 0) elementwise (utils/transform.py:136-294),
+ * t0 in seconds */
+int bbhx_frame_transform(double *t_out, double *lam_out, double *beta_out, double *psi_out,
+                         const double *t_in, const double *lam_in, const double *beta_in,
+                         const double *psi_in, int n, double t0, int to_ssb, void *stream);
+/* mbh_sky_mode_transform (utils/transform.py:296-426) in place on coords [rows, ndim] already
+ * tiled by the mode count; kind 0 = both (8), 1 = long (4), 2 = lat (2) */
+int bbhx_sky_mode_transform(double *coords, int rows, int ndim, int inc, int lam, int beta,
+                            int psi, int kind, int cos_i, void *stream);
+
 /* support [start, start+len) of each binary on the data grid (waveformbuild.py:136-177) */
 int bbhx_template_support(int *start, int *len, const double *x, int num_modes, int length,
                           int num_bin_all, const double *data_freqs, int data_length,
