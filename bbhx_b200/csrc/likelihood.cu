@@ -752,6 +752,67 @@ __device__ __forceinline__ void load_seg(SegCoef<R>& cf, const WarpStage<R>& S, 
   }
 }
 
+// One (chunk, mode) on the phase recurrence: staged segment kl (global segment kg of the mode's
+// grid) holds every support bin of the chunk.  The saved state is continued when this mode's
+// previous chunk was the one before, in the same segment, and fewer than kRecChunks chunks
+// ago; otherwise it is re-anchored at this lane's first bin.
+template <typename R>
+__device__ __forceinline__ void rec_chunk_mode(const WarpStage<R>& S, RecStage* RS, int m, int kl,
+                                               int kg, int gate, int ck, int c0, int lane,
+                                               const double* fbin, double ts, double te,
+                                               R (*acc)[6], double gk0, double gdf, double hstep) {
+  const int nc = RS->next_chunk[m], sg = RS->seg[m], left = RS->left[m];
+  const bool cont = (nc == ck) && (sg == kg) && (left > 0);
+  Rot z;
+  if (cont) {
+    const double2 e = RS->st[m][0][lane], r = RS->st[m][1][lane];
+    const double2 qq = RS->st[m][2][lane], pp = RS->P[m];
+    z.er = e.x; z.ei = e.y; z.rr = r.x; z.ri = r.y;
+    z.qr = qq.x; z.qi = qq.y; z.pr = pp.x; z.pi = pp.y;
+  } else {
+    rot_anchor(z, &S.pc[m][kl][0][0], S.x[m][kl], gk0 + (double)(c0 + lane), gdf, hstep);
+  }
+  const double2 pnew = make_double2(z.pr, z.pi);
+  if (gate == 1)
+    accumulate_chunk_rec<R, false>(S, m, kl, fbin, ts, te, acc, z);
+  else
+    accumulate_chunk_rec<R, true>(S, m, kl, fbin, ts, te, acc, z);
+  RS->st[m][0][lane] = make_double2(z.er, z.ei);
+  RS->st[m][1][lane] = make_double2(z.rr, z.ri);
+  RS->st[m][2][lane] = make_double2(z.qr, z.qi);
+  __syncwarp();
+  if (lane == 0) {
+    RS->next_chunk[m] = ck + 1;
+    RS->seg[m] = kg;
+    RS->left[m] = cont ? left - 1 : kRecChunks - 1;
+    RS->P[m] = pnew;  // every lane's P of the segment is bitwise the same
+  }
+  __syncwarp();
+}
+
+// Copy segments [k0, k0 + n) of (binary b, mode m) into the mode's shared-memory slot: knots
+// x[k0 .. k0 + n], the FP64 phase / t(f) cubics and the amplitude / transfer cubics in R.
+template <typename R>
+__device__ __forceinline__ void stage_segments(const FusedArgs& A, WarpStage<R>& S, int b, int m,
+                                               int k0, int n, int lane) {
+  const long long rowo = ((long long)b * A.M + m) * A.L + k0;
+  const int total = n * FD_NC + n + 1;
+  for (int idx = lane; idx < total; idx += 32) {
+    if (idx < n * FD_NC) {
+      const int sg = idx / FD_NC, r = idx - sg * FD_NC, p = r >> 2, cc = r & 3;
+      const double* src = (cc == 0) ? A.y : (cc == 1) ? A.c1 : (cc == 2) ? A.c2 : A.c3;
+      const double v = __ldg(src + p * A.qstride + rowo + sg);
+      if (p == 1 || p == 2)
+        S.pc[m][sg][p - 1][cc] = v;
+      else
+        S.ac[m][sg][(p == 0) ? 0 : p - 2][cc] = (R)v;
+    } else {
+      const int j = idx - n * FD_NC;
+      S.x[m][j] = __ldg(A.x + rowo + j);
+    }
+  }
+}
+
 // One WARP item = (data tile of FD_TILE bins, binary).  Items are enumerated tile-major, so the
 // warps in flight work on the same data tile for different binaries and share it through L2.
 // The warp stages the tile's segments of every mode (from the segment table) into its slice of
@@ -881,36 +942,8 @@ __device__ __forceinline__ void fused_item(const FusedArgs& A, long long q, Warp
             const int gate = S.gate[m][ka];
             if (gate == 2) continue;
             if (REC && uni) {
-              // phase by recurrence: continue the saved state when this mode's previous chunk
-              // was the one before in the same segment, else anchor at this lane's first bin
-              const int nc = RS->next_chunk[m], sg = RS->seg[m], left = RS->left[m];
-              const bool cont = (nc == ck) && (sg == ka) && (left > 0);
-              Rot z;
-              if (cont) {
-                const double2 e = RS->st[m][0][lane], r = RS->st[m][1][lane];
-                const double2 qq = RS->st[m][2][lane], pp = RS->P[m];
-                z.er = e.x; z.ei = e.y; z.rr = r.x; z.ri = r.y;
-                z.qr = qq.x; z.qi = qq.y; z.pr = pp.x; z.pi = pp.y;
-              } else {
-                rot_anchor(z, &S.pc[m][ka][0][0], S.x[m][ka], gk0 + (double)(c0 + lane), gdf,
-                           hstep);
-              }
-              const double2 pnew = make_double2(z.pr, z.pi);
-              if (gate == 1)
-                accumulate_chunk_rec<R, false>(S, m, ka, fbin, ts, te, acc, z);
-              else
-                accumulate_chunk_rec<R, true>(S, m, ka, fbin, ts, te, acc, z);
-              RS->st[m][0][lane] = make_double2(z.er, z.ei);
-              RS->st[m][1][lane] = make_double2(z.rr, z.ri);
-              RS->st[m][2][lane] = make_double2(z.qr, z.qi);
-              __syncwarp();
-              if (lane == 0) {
-                RS->next_chunk[m] = ck + 1;
-                RS->seg[m] = ka;
-                RS->left[m] = cont ? left - 1 : kRecChunks - 1;
-                RS->P[m] = pnew;  // every lane's P of the segment is bitwise the same
-              }
-              __syncwarp();
+              rec_chunk_mode(S, RS, m, ka, S.klo[m] + ka, gate, ck, c0, lane, fbin, ts, te, acc,
+                             gk0, gdf, hstep);
               continue;
             }
             if constexpr (!MIXED) {
@@ -983,6 +1016,54 @@ __device__ __forceinline__ void fused_item(const FusedArgs& A, long long q, Warp
         } else {
           const long long rowi = (long long)b * A.M + m;
           const double* xrow = A.x + rowi * L;
+          if constexpr (!MIXED) {
+            // the tile spans more segments of this mode than the slot holds (low frequencies):
+            // stage the few segments of this chunk into the mode's slot instead
+            const int ia = max(c0, s0), iz = min(c0 + FD_WARP_BINS, s1) - 1;
+            const double fa = uni ? __dmul_rn(gk0 + (double)ia, gdf) : __ldg(A.data_freqs + ia);
+            const double fz = uni ? __dmul_rn(gk0 + (double)iz, gdf) : __ldg(A.data_freqs + iz);
+            const int ka = warp_segment_search(xrow, L, fa);
+            const int kz = warp_segment_search(xrow, L, fz);
+            const int klo = max(ka, 0), khi = min(kz, L - 2);
+            const int nc = khi - klo + 1;
+            if (nc <= 0) continue;  // no bin of the chunk has a valid segment
+            if (nc <= WarpStage<R>::NSEG) {
+              __syncwarp();
+              stage_segments(A, S, b, m, klo, nc, lane);
+              __syncwarp();
+              if (ka == kz) {  // one segment holds every bin of the chunk
+                const int gate = segment_gate(&S.pc[m][0][1][0], S.x[m][1] - S.x[m][0], ts, te);
+                if (gate != 2) {
+                  if (REC && uni) {
+                    rec_chunk_mode(S, RS, m, 0, klo, gate, ck, c0, lane, fbin, ts, te, acc, gk0,
+                                   gdf, hstep);
+                  } else {
+                    const SmemCoef src{S, m, 0};
+#pragma unroll
+                    for (int j = 0; j < FD_K; ++j)
+                      if (fbin[j] >= 0.0) accumulate_bin_src(src, fbin[j], ts, te, acc[j]);
+                  }
+                }
+              } else {
+                int kb[FD_K];
+                bool ok[FD_K];
+                int kl = 0;
+#pragma unroll
+                for (int j = 0; j < FD_K; ++j) {
+                  const double f = fbin[j];
+                  ok[j] = f >= S.x[m][0];
+                  while (ok[j] && kl < nc && f >= S.x[m][kl + 1]) ++kl;
+                  ok[j] = ok[j] && kl < nc;
+                  kb[j] = kl;
+                }
+#pragma unroll
+                for (int j = 0; j < FD_K; ++j)
+                  if (ok[j]) accumulate_bin_src(SmemCoef{S, m, kb[j]}, fbin[j], ts, te, acc[j]);
+              }
+              __syncwarp();
+              continue;
+            }
+          }
           const double ffirst = __ldg(A.data_freqs + max(c0, s0));
           int k = warp_segment_search(xrow, L, ffirst);
           int kc = -2;
