@@ -451,6 +451,11 @@ struct alignas(16) WarpStage {
   R ac[FD_MAXM][NSEG][7][4];
   int klo[FD_MAXM];
   int nseg[FD_MAXM];
+  // modes whose tile spans more than NSEG segments (nseg = -1, FP64 form): the segment of the
+  // last chunk's first bin (a forward cursor) and the window of segments staged per chunk
+  int kcur[FD_MAXM];
+  int kst[FD_MAXM];
+  int nst[FD_MAXM];
   int gate[FD_MAXM][NSEG];  // t(f) gate over the whole segment: 0 mixed, 1 all in, 2 all out
   signed char cseg[FD_MAXCHUNK][FD_MAXM];  // staged segment holding a whole 128-bin chunk, or -1
 };
@@ -864,6 +869,8 @@ __device__ __forceinline__ void fused_item(const FusedArgs& A, long long q, Warp
       const int n = (kk.x > kk.y || khi < klo) ? 0 : khi - klo + 1;
       S.klo[lane] = klo;
       S.nseg[lane] = (n > WarpStage<R>::NSEG) ? -1 : n;
+      S.kcur[lane] = klo;
+      S.nst[lane] = 0;
     }
     __syncwarp();
     for (int m = 0; m < A.M; ++m) {
@@ -1018,27 +1025,57 @@ __device__ __forceinline__ void fused_item(const FusedArgs& A, long long q, Warp
           const double* xrow = A.x + rowi * L;
           if constexpr (!MIXED) {
             // the tile spans more segments of this mode than the slot holds (low frequencies):
-            // stage the few segments of this chunk into the mode's slot instead
+            // find the chunk's segments from the forward cursor with one warp-wide load of the
+            // next 32 knots, and stage a window of NSEG segments from there when the chunk
+            // leaves the staged window
             const int ia = max(c0, s0), iz = min(c0 + FD_WARP_BINS, s1) - 1;
             const double fa = uni ? __dmul_rn(gk0 + (double)ia, gdf) : __ldg(A.data_freqs + ia);
             const double fz = uni ? __dmul_rn(gk0 + (double)iz, gdf) : __ldg(A.data_freqs + iz);
-            const int ka = warp_segment_search(xrow, L, fa);
-            const int kz = warp_segment_search(xrow, L, fz);
+            const int kc = S.kcur[m];
+            const int kq = kc + lane;
+            const double xv = (kq < L) ? __ldg(xrow + kq) : INFINITY;
+            const unsigned ma = __ballot_sync(0xffffffffu, xv <= fa);
+            const unsigned mz = __ballot_sync(0xffffffffu, xv <= fz);
+            int ka, kz;
+            if (mz != 0xffffffffu && ma != 0u) {
+              ka = kc + __popc(ma) - 1;
+              kz = kc + __popc(mz) - 1;
+            } else {  // more than 32 segments ahead (or behind): full searches
+              ka = warp_segment_search(xrow, L, fa);
+              kz = warp_segment_search(xrow, L, fz);
+            }
             const int klo = max(ka, 0), khi = min(kz, L - 2);
             const int nc = khi - klo + 1;
-            if (nc <= 0) continue;  // no bin of the chunk has a valid segment
-            if (nc <= WarpStage<R>::NSEG) {
+            const int kst0 = S.kst[m], nst0 = S.nst[m];
+            __syncwarp();
+            if (lane == 0) S.kcur[m] = klo;
+            if (nc <= 0) {
               __syncwarp();
-              stage_segments(A, S, b, m, klo, nc, lane);
+              continue;  // no bin of the chunk has a valid segment
+            }
+            constexpr int NSEG = WarpStage<R>::NSEG;
+            if (nc <= NSEG) {
+              int kst = kst0;
+              if (!(nst0 > 0 && klo >= kst0 && khi < kst0 + nst0)) {
+                kst = klo;
+                const int nst = min(NSEG, L - 1 - klo);
+                stage_segments(A, S, b, m, klo, nst, lane);
+                if (lane == 0) {
+                  S.kst[m] = klo;
+                  S.nst[m] = nst;
+                }
+              }
               __syncwarp();
+              const int kl0 = klo - kst, kl1 = khi - kst;
               if (ka == kz) {  // one segment holds every bin of the chunk
-                const int gate = segment_gate(&S.pc[m][0][1][0], S.x[m][1] - S.x[m][0], ts, te);
+                const int gate = segment_gate(&S.pc[m][kl0][1][0], S.x[m][kl0 + 1] - S.x[m][kl0],
+                                              ts, te);
                 if (gate != 2) {
                   if (REC && uni) {
-                    rec_chunk_mode(S, RS, m, 0, klo, gate, ck, c0, lane, fbin, ts, te, acc, gk0,
+                    rec_chunk_mode(S, RS, m, kl0, klo, gate, ck, c0, lane, fbin, ts, te, acc, gk0,
                                    gdf, hstep);
                   } else {
-                    const SmemCoef src{S, m, 0};
+                    const SmemCoef src{S, m, kl0};
 #pragma unroll
                     for (int j = 0; j < FD_K; ++j)
                       if (fbin[j] >= 0.0) accumulate_bin_src(src, fbin[j], ts, te, acc[j]);
@@ -1047,13 +1084,13 @@ __device__ __forceinline__ void fused_item(const FusedArgs& A, long long q, Warp
               } else {
                 int kb[FD_K];
                 bool ok[FD_K];
-                int kl = 0;
+                int kl = kl0;
 #pragma unroll
                 for (int j = 0; j < FD_K; ++j) {
                   const double f = fbin[j];
-                  ok[j] = f >= S.x[m][0];
-                  while (ok[j] && kl < nc && f >= S.x[m][kl + 1]) ++kl;
-                  ok[j] = ok[j] && kl < nc;
+                  ok[j] = f >= S.x[m][kl0];
+                  while (ok[j] && kl <= kl1 && f >= S.x[m][kl + 1]) ++kl;
+                  ok[j] = ok[j] && kl <= kl1;
                   kb[j] = kl;
                 }
 #pragma unroll

@@ -138,33 +138,58 @@ class Autotuner:
         return choice
 
 
+# Mixed form of a direct group: its FP32 amplitude / transfer cubics are evaluated across a
+# whole spline segment, and with coarse sparse grids over long data streams a segment spans
+# ~1e4 data bins; the FP32 rounding of the cubic, largest relative to the template where the
+# transfer functions pass near the TDI zeros (and the weights are largest), then reaches
+# ~1e-5 <h|h> in lnL.  Groups whose segments span more data bins per knot interval than this
+# run in FP64 (a second persistent launch) when the batch is mixed.
+MIXED_MAX_BINS_PER_KNOT = 2048
+
+
 class UnevenBatch:
     def __init__(self, direct_groups=(), het_groups=(), precision="mixed", autotuner=None,
-                 shape=None):
+                 shape=None, mixed_max_bins_per_knot=MIXED_MAX_BINS_PER_KNOT):
         self.direct = list(direct_groups)
         self.het = list(het_groups)
         if precision not in PRECISIONS:
             raise ValueError(f"precision must be one of {sorted(PRECISIONS)}, got {precision!r}")
         self.precision = precision
+        self.mixed_max_bins_per_knot = mixed_max_bins_per_knot
         self.autotuner = autotuner if autotuner is not None else Autotuner()
-        self.shape = shape  # (tile_bins, ctas_per_sm); None -> autotune on first run
+        # launch shape per precision class, {"fp64" | "mixed": (tile_bins, ctas_per_sm)};
+        # a missing entry is autotuned on the first run
+        self.shape = dict(shape or {})
         self.graph = None
         if len(self.direct) > 64:
             raise ValueError("at most 64 direct groups per batch")
 
-    def _launch(self, descs, tile, ctas):
+    def group_precisions(self):
+        """Arithmetic of every group (direct groups first): a mixed batch runs the direct
+        groups whose segments span more than mixed_max_bins_per_knot data bins in FP64."""
+        out = []
+        for g in self.direct:
+            coarse = int(g.like.data_freqs.numel()) / g.length > self.mixed_max_bins_per_knot
+            out.append("fp64" if (self.precision == "fp64" or coarse) else "mixed")
+        return out + [self.precision] * len(self.het)
+
+    def _launch(self, descs, precision, tile, ctas):
         arr = (DirectGroupC * len(descs))(*descs)
         _lib.call("bbhx_direct_like_multi", ctypes.cast(arr, ctypes.c_void_p), len(descs),
-                  PRECISIONS[self.precision], int(tile), int(ctas), _lib.stream())
+                  PRECISIONS[precision], int(tile), int(ctas), _lib.stream())
 
     def run(self):
-        """All groups' lnL (list of device tensors, direct groups first)."""
-        descs = [g.build(self.precision) for g in self.direct]
-        if descs:
-            if self.shape is None:
-                self.shape = self.autotuner.best(descs, self.precision,
-                                                 lambda tl, c: self._launch(descs, tl, c))
-            self._launch(descs, *self.shape)
+        """All groups' lnL (list of device tensors, direct groups first).  Direct groups of
+        each precision class run in one persistent launch."""
+        precs = self.group_precisions()
+        classes = {}
+        for g, pr in zip(self.direct, precs):
+            classes.setdefault(pr, []).append(g.build(pr))
+        for pr, descs in classes.items():
+            if pr not in self.shape:
+                self.shape[pr] = self.autotuner.best(descs, pr,
+                                                     lambda tl, c: self._launch(descs, pr, tl, c))
+            self._launch(descs, pr, *self.shape[pr])
         for h in self.het:
             h.run(self.precision)
         return [g.lnl() for g in self.direct] + [h.lnl() for h in self.het]

@@ -652,7 +652,7 @@ def uneven_metric(args):
     n_inst = sum(d["params"].shape[1] for d in direct) + sum(w.shape[1] for _, w in het_groups)
     dg, hg = groups()
     batch = UnevenBatch(dg, hg, precision="mixed", autotuner=Autotuner(repeats=1))
-    batch.autotuner.CTAS = (2, 4)
+    batch.autotuner.CTAS = (2, 3, 4)
     outs = batch.capture()
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
@@ -688,16 +688,25 @@ def uneven_metric(args):
     rel = [e / np.maximum(h, 1.0) for e, h in zip(err, hh)]
     allerr = np.concatenate(err)
     allrel = np.concatenate(rel)
+    labels = ["direct Tobs=%g L=%d %s bins/knot=%d" % (d["tobs"], d["length"],
+                                                        "22" if d["modes"] else "HM",
+                                                        len(d["like"].data_freqs) // d["length"])
+              for d in direct] + ["het bins=%d" % h.length_f_het for h, _ in het_groups]
+    per_group = [{"group": lb, "precision": pr, "max": float(e.max()),
+                  "frac_within_1e-2": float(np.mean(e <= 1e-2))}
+                 for lb, pr, e in zip(labels, batch.group_precisions(), err)]
     return {"uneven": {
         "value": n_inst / t_mixed, "unit": "lnL evals/s", "instances": int(n_inst),
         "direct_groups": len(direct), "heterodyned_groups": len(het_groups),
         "fp64_plain_per_group": {"value": n_inst / t_fp64, "unit": "lnL evals/s"},
         "speedup_vs_fp64_plain": t_fp64 / t_mixed,
-        "launch_shape": {"tile_bins": batch.shape[0], "ctas_per_sm": batch.shape[1]},
+        "launch_shape": {pr: {"tile_bins": sh[0], "ctas_per_sm": sh[1]} for pr, sh in batch.shape.items()},
+        "groups_in_fp64": sum(1 for pr in batch.group_precisions()[:len(direct)] if pr == "fp64"),
         "dlnl_mixed_vs_fp64": {"max": float(allerr.max()), "median": float(np.median(allerr)),
                                "frac_within_1e-2": float(np.mean(allerr <= 1e-2)),
                                "p99": float(np.percentile(allerr, 99)),
-                               "max_over_hh": float(allrel.max())},
+                               "max_over_hh": float(allrel.max()),
+                               "per_group": per_group},
         "flags_clear": flags_ok,
         "config": "mode sets (2,2) / 6 HM; L 256/512/1024/2048; Tobs 0.1/0.5/1 yr; t_ref in "
                   "[0.8, 0.95] Tobs; heterodyne bins 64/128/192/256 x 1024 walkers; CUDA graph replay"}}

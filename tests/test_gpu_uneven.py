@@ -3,7 +3,9 @@ sets evaluated in one persistent launch, autotuned, captured in a CUDA graph.
 
 Checks: FP64 batch == per-group Likelihood.get_ll to 1e-9 relative (same arithmetic, different
 summation order of the tiles); mixed batch vs FP64 |dlnL| <= 2e-6 <h|h>; graph replay with new
-parameters == an eager run with them; heterodyned groups == HeterodynedLikelihood.get_ll.
+parameters == an eager run with them; heterodyned groups == HeterodynedLikelihood.get_ll; a
+coarse grid over a 1-yr stream (L = 256: ~1.2e4 data bins per knot interval) in a mixed batch
+is routed to FP64 and meets |dlnL| <= 1e-2, while a fine one (L = 2048) stays mixed.
 """
 import numpy as np
 import pytest
@@ -54,7 +56,8 @@ def test_uneven_fp64_matches_per_group(golden, golden_data):
     direct, het, walkers, kw = _problem(golden, golden_data)
     batch = _batch(direct, het, walkers, kw, "fp64")
     out = [o.cpu().numpy() for o in batch.run()]
-    assert batch.shape in [(t, c) for t in batch.autotuner.TILES for c in batch.autotuner.CTAS]
+    shapes = [(t, c) for t in batch.autotuner.TILES for c in batch.autotuner.CTAS]
+    assert batch.shape and all(sh in shapes for sh in batch.shape.values())
     for d, got in zip(direct, out):
         ref = d["like"].get_ll(d["params"], length=d["length"], modes=d["modes"], t_obs_start=0.0,
                                t_obs_end=d["tobs"])
@@ -81,8 +84,38 @@ def test_uneven_mixed_error_and_graph_replay(golden, golden_data):
     rep = [o.cpu().numpy().copy() for o in bm.replay()]
     direct[1]["params"] = newp
     eager = _batch(direct, het, walkers, kw, "mixed")
-    eager.shape = bm.shape
+    eager.shape = dict(bm.shape)
     ev = [o.cpu().numpy() for o in eager.run()]
     for a, b in zip(rep, ev):
         np.testing.assert_allclose(a, b, rtol=1e-12, atol=1e-9)
     assert all(int(f.abs().sum().item()) == 0 for f in bm.flags())
+
+
+def test_uneven_mixed_routes_coarse_grids_to_fp64():
+    from bbhx_b200 import BBHWaveformFD, EqualArmlengthOrbits, Likelihood
+    from bbhx_b200.sensitivity import aet_psd
+    from bbhx_b200.synthetic import data_grid, draw_params, gaussian_noise, notch_tdi_zeros
+    from bbhx_b200.uneven import DirectGroup, UnevenBatch
+    from bbhx_b200.utils.constants import YRSID_SI
+
+    tobs = 1.0
+    f = data_grid(tobs, 1e-5, 0.1)
+    psd = notch_tdi_zeros(f, np.array([aet_psd(f, c, tdi2=True) for c in "AET"]))
+    wave = BBHWaveformFD(response_kwargs=dict(orbits=EqualArmlengthOrbits(), TDItag="AET", tdi2=True))
+    like = Likelihood(wave, f, gaussian_noise(psd, f[1] - f[0], 21), psd)
+    P = draw_params(6, tobs, 77)
+    P[11] = np.random.default_rng(77).uniform(0.8, 0.95, 6) * tobs * YRSID_SI
+    groups = [dict(length=256, params=P[:, :3]), dict(length=2048, params=P[:, 3:])]
+    batch = UnevenBatch([DirectGroup(like, g["params"], length=g["length"], t_obs_start=0.0,
+                                     t_obs_end=tobs) for g in groups], precision="mixed")
+    assert batch.group_precisions() == ["fp64", "mixed"]
+    out = [o.cpu().numpy() for o in batch.run()]
+    for g, got in zip(groups, out):
+        like.precision = "fp64"
+        ref = like.get_ll(g["params"], length=g["length"], t_obs_start=0.0, t_obs_end=tobs)
+        hh = like.h_h.real.cpu().numpy()
+        err = np.abs(got - ref)
+        if g["length"] == 256:
+            assert np.all(err <= 1e-2), err
+        else:
+            assert np.all(err <= 2e-6 * np.maximum(hh, 1.0)), err
