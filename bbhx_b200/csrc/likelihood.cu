@@ -1060,6 +1060,11 @@ __device__ __forceinline__ void fused_item(const FusedArgs& A, long long q, Warp
                 kst = klo;
                 const int nst = min(NSEG, L - 1 - klo);
                 stage_segments(A, S, b, m, klo, nst, lane);
+                __syncwarp();
+                // whole-segment t(f) gates of the window, one segment per lane
+                if (lane < nst)
+                  S.gate[m][lane] = segment_gate(&S.pc[m][lane][1][0],
+                                                 S.x[m][lane + 1] - S.x[m][lane], ts, te);
                 if (lane == 0) {
                   S.kst[m] = klo;
                   S.nst[m] = nst;
@@ -1068,8 +1073,7 @@ __device__ __forceinline__ void fused_item(const FusedArgs& A, long long q, Warp
               __syncwarp();
               const int kl0 = klo - kst, kl1 = khi - kst;
               if (ka == kz) {  // one segment holds every bin of the chunk
-                const int gate = segment_gate(&S.pc[m][kl0][1][0], S.x[m][kl0 + 1] - S.x[m][kl0],
-                                              ts, te);
+                const int gate = S.gate[m][kl0];
                 if (gate != 2) {
                   if (REC && uni) {
                     rec_chunk_mode(S, RS, m, kl0, klo, gate, ck, c0, lane, fbin, ts, te, acc, gk0,
