@@ -516,8 +516,10 @@ def het_metric(args, wave, like, f, params):
         e = np.abs(ll[:nd] - (ll_dir + dd_offset))
         return {"max": float(e.max()), "median": float(np.median(e)),
                 "frac_within_1e-2": float(np.mean(e <= 1e-2))}
+    roof = het_roofline(het, wave, center, v64)
     return {"heterodyned": {
         "value": vmx, "unit": "lnL evals/s", "batch": Bh, "bins": 128,
+        "roofline_fp64": roof,
         "dtype": "mixed: f64 phase/t(f)/Roemer/ratio/sums, f32 amplitude/transfer/products",
         "fp64_plain": {"value": v64, "unit": "lnL evals/s", "kernel": "k_het_fused<fp64>"},
         "mixed_over_fp64": vmx / v64,
@@ -536,6 +538,45 @@ def het_metric(args, wave, like, f, params):
         "lnl_range": [float(ll64.min()), float(ll64.max())],
         "path": "HeterodynedLikelihood.get_ll with device-resident walkers",
         "finite": bool(np.all(np.isfinite(ll64)) and np.all(np.isfinite(llmx)))}}
+
+
+FP64_LANE_OPS_PER_S = 148 * 64 * 1.965e9  # B200: 64 FP64 lanes per SM (nominal, 1965 MHz)
+OPC_NAMES = ("add_sub", "mul", "div", "compare", "sqrt", "cbrt", "log", "exp", "pow", "atan",
+             "sin_cos", "other")
+
+
+def het_roofline(het, wave, center, evals_per_s):
+    """FP64 roofline of the heterodyned form: the algorithmic operations of one (walker, mode,
+    frequency) point, tallied by running the templated FP64 model on an op-counting scalar
+    (bbhx_count_point_ops; the per-binary set-up and the per-bin relative-binning arithmetic
+    are excluded), times the points per second, against the nominal FP64 lane rate (148 SMs x
+    64 lanes x 1965 MHz; no measured FP64 peak exists for this pool)."""
+    import torch
+
+    from bbhx_b200 import _lib
+    from bbhx_b200.waveforms.ringdownphenomd import dspin
+
+    ap, rg = wave.amp_phase_gen, wave.response_gen
+    prm = torch.tensor([center[k] for k in (0, 1, 2, 3, 4, 5, 7, 8, 9, 10, 11)],
+                       dtype=torch.float64, device="cuda")
+    out = torch.zeros(12, dtype=torch.int64, device="cuda")
+    M, L = len(ap.allowable_modes), int(het.freqs.numel())
+    tab = ap.qnm_table
+    _lib.call("bbhx_count_point_ops", rg.orbit_handle.ptr, _lib.dptr(out), _lib.dptr(prm),
+              _lib.dptr(ap.ells_default), _lib.dptr(ap.mms_default), M, _lib.dptr(het.freqs), L,
+              _lib.dptr(tab), int(tab.shape[1]), float(dspin), rg.TDItag_int, int(rg.rescaled),
+              int(rg.tdi2), _lib.stream())
+    tally = out.cpu().numpy() / float(M * L)
+    per_point = {k: float(v) for k, v in zip(OPC_NAMES, tally)}
+    arith = float(tally[0] + tally[1] + tally[2])
+    special = float(tally[4:11].sum())
+    points_per_s = evals_per_s * M * L
+    return {"ops_per_point": per_point, "arith_ops_per_point": arith,
+            "elementary_calls_per_point": special, "points_per_s": points_per_s,
+            "arith_ops_per_s": arith * points_per_s, "peak_lane_ops_per_s": FP64_LANE_OPS_PER_S,
+            "frac_arith": arith * points_per_s / FP64_LANE_OPS_PER_S,
+            "form": "FP64 fused kernel (k_het_fused<FP64>)",
+            "peak_source": "nominal (148 SMs x 64 FP64 lanes x 1965 MHz); cross-check: ncu FP64 pipe % in profiles/"}
 
 
 def grad_metric(args):

@@ -42,6 +42,15 @@ size_t bbhx_response_mode_bytes(void);
 /* self-test (no reference counterpart): out[4i..4i+3] = sin, cos of x[i] from the hot-loop
  * Cody-Waite + Taylor routine and from CUDA's sincos */
 int bbhx_selftest_sincos(const double *x, double *out, int n, void *stream);
+/* diagnostic (no reference counterpart): algorithmic operation tallies of the FP64 heterodyne
+ * point chain (PhenomHM amp / phase / t(f), TDI transfer, phasor, channel products) summed over
+ * num_modes x length points, set-up excluded; out [12] device = add/sub, mul, div, compare,
+ * sqrt, cbrt, log, exp, pow, atan, sin-cos, other; params [11] device = m1, m2 [Msun], chi1z,
+ * chi2z, distance [m], phi_ref, inc, lam, beta, psi, t_ref; one thread, for measurement */
+int bbhx_count_point_ops(void *orbits, unsigned long long *out, const double *params,
+                         const int *ells, const int *mms, int num_modes, const double *freqs,
+                         int length, const double *qnm_table, int qnm_n, double dspin, int TDItag,
+                         int rescaled, int tdi2, void *stream);
 
 /* ------------------------------------------------------------------ PhenomHM */
 /* replaces get_phenomhm_ringdown_frequencies_wrap (src/bbhx/cutils/PhenomHMWaveform.hh:322-333);
