@@ -84,7 +84,7 @@ class Likelihood:
         kw = dict(waveform_kwargs)
         for k in ("freqs", "fill", "direct", "compress", "squeeze", "combine"):
             kw.pop(k, None)
-        flags = t.zeros(3, dtype=t.int32, device=device())
+        flags = t.empty(3, dtype=t.int32, device=device())  # cleared by the step's front end
         if self.precision == "mixed":
             kw["data32"] = self.fp32_data()
         d_h, h_h = self.waveform_gen.inner_products(params, self.data_freqs,
@@ -122,7 +122,11 @@ class Likelihood:
         kw = {k: v for k, v in kw.items() if k in ("t_obs_start", "t_obs_end", "length", "modes")}
         d_h, h_h = self.waveform_gen.inner_products(rows, self.data_freqs, self.data_channels,
                                                     self.noise_factors, precision="fp64", **kw)
-        return -0.5 * (self.d_d + h_h.real - 2 * d_h.real)
+        B = d_h.numel()
+        packed = torch().empty(3 * B, dtype=torch().float64, device=device())
+        _lib.call("bbhx_pack_lnl", _lib.dptr(packed), _lib.dptr(d_h), _lib.dptr(h_h),
+                  float(self.d_d), B, 0, _lib._VP(0), 0, _lib.stream())
+        return packed[:B]
 
     def get_ll_and_grad(self, params, **waveform_kwargs):
         """lnL [B] and d lnL / d theta [B, 11] (device tensors); theta = (m1, m2, chi1z,
@@ -269,7 +273,11 @@ class HeterodynedLikelihood:
         d_h, h_h = self.template_gen.heterodyne_sums(rows, self.freqs, self._h0_flat,
                                                      self.data_constants, precision=precision,
                                                      flags=flags, **kw)
-        return -0.5 * (self.reference_d_d + h_h.real - 2 * d_h.real), (d_h, h_h)
+        B = d_h.numel()
+        packed = torch().empty(3 * B, dtype=torch().float64, device=device())
+        _lib.call("bbhx_pack_lnl", _lib.dptr(packed), _lib.dptr(d_h), _lib.dptr(h_h),
+                  float(self.reference_d_d), B, 0, _lib._VP(0), 0, _lib.stream())
+        return packed[:B], (d_h, h_h)
 
     def get_ll_and_grad(self, params, **waveform_kwargs):
         """lnL [B] and d lnL / d theta [B, 11] (device tensors) for walkers ``params``

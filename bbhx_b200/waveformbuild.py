@@ -120,7 +120,9 @@ class BBHWaveformFD:
         pars, t_start, t_end, tobs_rows = step_front(m1, m2, chi1z, chi2z, lam, beta, M,
                                                      (t_obs_start, t_obs_end), flags=flags)
         B = pars.shape[1]
-        out_buffer = t.zeros(9 * length * M * B, dtype=t.float64, device=device())
+        # every slot of every (binary, mode, frequency) is written by the fused waveform +
+        # response kernel below, so the buffer is not cleared first
+        out_buffer = t.empty(9 * length * M * B, dtype=t.float64, device=device())
         ap._prepare(m1, m2, chi1z, chi2z, distance, None, f_ref, t_ref, length,
                     freqs if direct else None, out_buffer, modes, flags=flags, front=pars)
         M = ap.num_modes
