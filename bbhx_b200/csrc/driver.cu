@@ -9,11 +9,10 @@
 #include <cmath>
 
 #include "capi_internal.cuh"
+#include "frames.cuh"
 
 namespace bbhx {
 
-constexpr double ORBIT_R = AU_SI;                // OrbitR (utils/constants.py)
-constexpr double CONST_OMEGA = 1.99098659277e-7;  // 2 pi / sidereal year (ConstOmega)
 constexpr double ZETA = PI / 3.0;                // inclination of the constellation plane
 
 // numpy's float modulo (result has the sign of the divisor)
@@ -24,15 +23,6 @@ __device__ __forceinline__ double py_mod(double a, double b) {
 }
 
 __device__ __forceinline__ double modpi_dev(double x) { return x - floor(x / PI) * PI; }
-
-// tSSBfromLframe (transform.py:75-105): SSB time of constellation time tL for a source at
-// ecliptic (lambda, beta), first order in R/c plus the R^2/c^2 term
-__device__ __forceinline__ double tssb_from_l(double tL, double lam, double beta, double t0) {
-  const double phase = CONST_OMEGA * tL + CONST_OMEGA * t0 - lam;
-  const double RoC = ORBIT_R / C_SI;
-  const double rc = RoC * cos(beta);
-  return tL + rc * cos(phase) - 0.5 * CONST_OMEGA * (rc * rc) * sin(2.0 * phase);
-}
 
 __device__ __forceinline__ double tl_from_ssb(double tS, double lam, double beta, double t0) {
   const double phase = CONST_OMEGA * tS + CONST_OMEGA * t0 - lam;

@@ -13,14 +13,16 @@
 //   3. k_spline_adj   CTA per (binary, mode): adjoint of the not-a-knot spline build; the
 //                     slopes' system K s = r is transposed and solved by the same cyclic
 //                     reduction (K^T lambda = s_bar), giving d lnL / d y at the knots
-//   4. k_grad_setup + k_contract_direct: dual-number tangents of the model at the knots,
-//                     contracted with d lnL / d y                                  (forward)
-// The knot frequencies x are held fixed (their dependence on theta through the
-// observation-window regrid is not differentiated).
+//                     and d lnL / d x (the knots' positions, y held fixed)
+//   4. k_grad_setup + k_regrid_tangents + k_contract_direct: dual-number tangents of the
+//                     model at the knots and of the knots themselves (the observation-window
+//                     regrid moves them with theta), contracted with d lnL / d y and
+//                     d lnL / d x                                                  (forward)
 #include <algorithm>
 #include <vector>
 
 #include "capi_internal.cuh"
+#include "frames.cuh"
 #include "gradient_model.cuh"
 #include "tridiag.cuh"
 
@@ -177,11 +179,36 @@ k_adj_coeffs(double* ybd, double* cb1, double* cb2, double* cb3, const cplx* gh,
   }
 }
 
+// d lnL / d m_j (j in [0, L-2]) of one row of the spline build: through c2, c3 (the t path)
+// and through the right-hand sides r(m) of the slope system (lam = K^{-T} s_bar).
+__device__ __forceinline__ double spline_mbar(int j, const double* xs, int L, const double* lam,
+                                              const double* cb2, const double* cb3) {
+  const double h = xs[j + 1] - xs[j];
+  const double tbar = -cb2[j] + cb3[j] / h;
+  double v = (cb2[j] - 2.0 * tbar) / h;
+  // interior rows r = 1..L-2: r_r = 3 (h_r m_{r-1} + h_{r-1} m_r)
+  if (j >= 1 && j <= L - 2) v += 3.0 * lam[j] * (xs[j] - xs[j - 1]);
+  if (j + 1 <= L - 2) v += 3.0 * lam[j + 1] * (xs[j + 2] - xs[j + 1]);
+  // row 0: r_0 = ((h0 + 2 d0) h1 m_0 + h0^2 m_1) / d0
+  const double h0 = xs[1] - xs[0], h1 = xs[2] - xs[1], d0 = xs[2] - xs[0];
+  if (j == 0) v += lam[0] * (h0 + 2 * d0) * h1 / d0;
+  if (j == 1) v += lam[0] * h0 * h0 / d0;
+  // row L-1: r = (h_{L-2}^2 m_{L-3} + (2 dL + h_{L-2}) h_{L-3} m_{L-2}) / dL
+  const double hl = xs[L - 1] - xs[L - 2], hp = xs[L - 2] - xs[L - 3];
+  const double dL = xs[L - 1] - xs[L - 3];
+  if (j == L - 3) v += lam[L - 1] * hl * hl / dL;
+  if (j == L - 2) v += lam[L - 1] * (2 * dL + hl) * hp / dL;
+  return v;
+}
+
 // 3. Adjoint of the not-a-knot spline build of k_spline (spline.cu) for the 9 rows of one
-// (binary, mode): inputs ybd, cb1..cb3 (entries s < L-1), output ybar (d lnL / d y).
-// Forward: m_i = (y_{i+1} - y_i) / h_i; K s = r(m); c1 = s_i, t = (s_i + s_{i+1} - 2 m_i) / h_i,
-// c2 = (m_i - s_i) / h_i - t, c3 = t / h_i.  Shared memory: x, a, b, c, d[9][L].
-__global__ void k_spline_adj(double* ybar, const double* ybd, const double* cb1,
+// (binary, mode): inputs ybd, cb1..cb3 (entries s < L-1), outputs ybar (d lnL / d y, x held
+// fixed) and xbar (d lnL / d x at the knots, y held fixed, summed over the rows).
+// Forward: h_i = x_{i+1} - x_i, m_i = (y_{i+1} - y_i) / h_i; K(h) s = r(h, m); c1 = s_i,
+// t = (s_i + s_{i+1} - 2 m_i) / h_i, c2 = (m_i - s_i) / h_i - t, c3 = t / h_i; a data bin f of
+// segment i reads y_i + c1 u + c2 u^2 + c3 u^3 with u = f - x_i.  Shared memory: x, a, b, c,
+// d[9][L].
+__global__ void k_spline_adj(double* ybar, double* xbar, const double* ybd, const double* cb1,
                              const double* cb2, const double* cb3, SplineRefs S, int b0, int nb) {
   extern __shared__ double sm[];
   const int L = S.L;
@@ -235,7 +262,7 @@ __global__ void k_spline_adj(double* ybar, const double* ybd, const double* cb1,
     }
     __syncthreads();
     cr_solve(a, bb, c, d, L, 9, L);  // lambda = K^{-T} s_bar (r_bar)
-    // m_bar_i (i < L-1) and y_bar
+    // y_bar from m_bar
     for (int i = threadIdx.x; i < L; i += blockDim.x) {
       for (int p = 0; p < 9; ++p) {
         const size_t o = (size_t)p * S.n + row * L;
@@ -244,31 +271,146 @@ __global__ void k_spline_adj(double* ybar, const double* ybd, const double* cb1,
           continue;
         }
         const double* lam = d + (size_t)p * L;
-        auto mbar = [&](int j) -> double {  // d lnL / d m_j, j in [0, L-2]
-          const double h = xs[j + 1] - xs[j];
-          const double tbar = -cb2[o + j] + cb3[o + j] / h;
-          double v = (cb2[o + j] - 2.0 * tbar) / h;
-          // interior rows r = 1..L-2: r_r = 3 (h_r m_{r-1} + h_{r-1} m_r)
-          if (j >= 1 && j <= L - 2) v += 3.0 * lam[j] * (xs[j] - xs[j - 1]);
-          if (j + 1 <= L - 2) v += 3.0 * lam[j + 1] * (xs[j + 2] - xs[j + 1]);
-          // row 0: r_0 = ((h0 + 2 d0) h1 m_0 + h0^2 m_1) / d0
-          const double h0 = xs[1] - xs[0], h1 = xs[2] - xs[1], d0 = xs[2] - xs[0];
-          if (j == 0) v += lam[0] * (h0 + 2 * d0) * h1 / d0;
-          if (j == 1) v += lam[0] * h0 * h0 / d0;
-          // row L-1: r = (h_{L-2}^2 m_{L-3} + (2 dL + h_{L-2}) h_{L-3} m_{L-2}) / dL
-          const double hl = xs[L - 1] - xs[L - 2], hp = xs[L - 2] - xs[L - 3];
-          const double dL = xs[L - 1] - xs[L - 3];
-          if (j == L - 3) v += lam[L - 1] * hl * hl / dL;
-          if (j == L - 2) v += lam[L - 1] * (2 * dL + hl) * hp / dL;
-          return v;
-        };
         double yb = (i < L - 1) ? ybd[o + i] : 0.0;
-        if (i < L - 1) yb -= mbar(i) / (xs[i + 1] - xs[i]);
-        if (i > 0) yb += mbar(i - 1) / (xs[i] - xs[i - 1]);
+        if (i < L - 1) yb -= spline_mbar(i, xs, L, lam, cb2 + o, cb3 + o) / (xs[i + 1] - xs[i]);
+        if (i > 0) yb += spline_mbar(i - 1, xs, L, lam, cb2 + o, cb3 + o) / (xs[i] - xs[i - 1]);
         ybar[o + i] = yb;
       }
     }
+    // x_bar.  Per segment i: e_i = d lnL / d u-shift (evaluation, u = f - x_i) and
+    // hb_i = d lnL / d h_i (coefficients c2, c3 explicitly, m_i = (y_{i+1} - y_i) / h_i, and
+    // the rows of K(h) s = r(h, m): lam^T (dr/dh - dK/dh s)); then
+    // x_bar_i = -e_i - hb_i + hb_{i-1}.  The slopes are s_j = c1_j (j < L-1) and
+    // s_{L-1} = c3_{L-2} h^2 - s_{L-2} + 2 m_{L-2}.  a[] and bb[] are free after the solve.
+    for (int i = threadIdx.x; i < L - 1; i += blockDim.x) {
+      double e = 0.0, hb = 0.0;
+      for (int p = 0; p < 9; ++p) {
+        if (p == 2) continue;
+        const size_t o = (size_t)p * S.n + row * L;
+        const double* lam = d + (size_t)p * L;
+        const double* y = S.y + o;
+        const double* s1 = S.c1 + o;
+        auto hh = [&](int j) { return xs[j + 1] - xs[j]; };
+        auto mm = [&](int j) { return (y[j + 1] - y[j]) / hh(j); };
+        auto sl = [&](int j) {
+          if (j < L - 1) return s1[j];
+          const double h = hh(L - 2);
+          return S.c3[o + L - 2] * h * h - s1[L - 2] + 2.0 * mm(L - 2);
+        };
+        const double h = hh(i);
+        const double c2i = S.c2[o + i], c3i = S.c3[o + i];
+        e += s1[i] * ybd[o + i] + 2.0 * c2i * cb1[o + i] + 3.0 * c3i * cb2[o + i];
+        hb -= (cb2[o + i] * c2i + 2.0 * cb3[o + i] * c3i) / h;
+        hb -= spline_mbar(i, xs, L, lam, cb2 + o, cb3 + o) * mm(i) / h;
+        if (i >= 1 && i <= L - 2) hb += lam[i] * (3.0 * mm(i - 1) - sl(i - 1) - 2.0 * sl(i));
+        if (i <= L - 3) hb += lam[i + 1] * (3.0 * mm(i + 1) - 2.0 * sl(i + 1) - sl(i + 2));
+        if (i <= 1) {  // row 0: h1 s0 + d0 s1 = ((3 h0 + 2 h1) h1 m0 + h0^2 m1) / d0
+          const double h0 = hh(0), h1 = hh(1), d0 = h0 + h1;
+          const double rhs = ((3.0 * h0 + 2.0 * h1) * h1 * mm(0) + h0 * h0 * mm(1)) / d0;
+          if (i == 0) hb += lam[0] * ((3.0 * h1 * mm(0) + 2.0 * h0 * mm(1) - rhs) / d0 - sl(1));
+          else hb += lam[0] * (((3.0 * h0 + 4.0 * h1) * mm(0) - rhs) / d0 - sl(0) - sl(1));
+        }
+        if (i >= L - 3) {  // row L-1: dL s_{L-2} + A s_{L-1} = (Bh^2 m_{L-3} + (2A + 3Bh) A m_{L-2}) / dL
+          const double A = hh(L - 3), Bh = hh(L - 2), dL = A + Bh;
+          const double mq = mm(L - 3), mr = mm(L - 2);
+          const double rhs = (Bh * Bh * mq + (2.0 * A + 3.0 * Bh) * A * mr) / dL;
+          if (i == L - 3) hb += lam[L - 1] * (((4.0 * A + 3.0 * Bh) * mr - rhs) / dL - sl(L - 2) - sl(L - 1));
+          else hb += lam[L - 1] * ((2.0 * Bh * mq + 3.0 * A * mr - rhs) / dL - sl(L - 2));
+        }
+      }
+      a[i] = e;
+      bb[i] = hb;
+    }
     __syncthreads();
+    for (int i = threadIdx.x; i < L; i += blockDim.x) {
+      double v = 0.0;
+      if (i < L - 1) v -= a[i] + bb[i];
+      if (i > 0) v += bb[i - 1];
+      xbar[row * L + i] = v;
+    }
+    __syncthreads();
+  }
+}
+
+// 4a. Knot motion of the observation-window regrid (forward: k_tf_window, phenomhm.cu; the
+// reference's phenomhm.py:520-610).  Row (b, m) has knots x_k = flo^(1 - r_k) fhi^(r_k),
+// r_k = k / (L - 1), between band edges that are either the default grid's end points (which
+// scale as 1 / (m1 + m2)) or where the linear interpolation of t(f) over the default grid
+// crosses 0 (lower edge) or the SSB observation span To = tSSB(t_end) - tSSB(t_start) (upper
+// edge).  t(f) at a default-grid point moves with the intrinsic parameters, t_ref and the
+// point's own frequency; To moves with lam and beta.  One thread per (local binary, mode)
+// repeats the forward's crossing search on the forward's default grid f0 and its t(f) tf0
+// ([B, M, L] each), evaluates the straddling points as duals and writes
+// wreg[row][0][k] = d flo / flo and wreg[row][1][k] = d fhi / fhi for the pass's directions.
+__global__ void k_regrid_tangents(double* wreg, const ModeCoeffsT<GD>* coeffs, const double* P,
+                                  int B, int b0, int nb, int M, int L, const double* f0,
+                                  const double* tf0, const double* t_start, const double* t_end,
+                                  double tL_start, double tL_end, int k0) {
+  const long long n = (long long)nb * M;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int bl = (int)(t / M), m = (int)(t % M);
+    const int b = b0 + bl;
+    const size_t row = ((size_t)b * M + m) * L;
+    const double* f = f0 + row;
+    const double* x = tf0 + row;
+    const ModeCoeffsT<GD>& c = coeffs[t];
+    const GD msum = seed(P[0 * (size_t)B + b], 0, k0) + seed(P[1 * (size_t)B + b], 1, k0);
+    const GD t_ref = seed(P[11 * (size_t)B + b], 10, k0);
+    // default-grid point j: f_j proportional to 1 / (m1 + m2)
+    auto fdual = [&](int j) {
+      GD r(f[j]);
+#pragma unroll
+      for (int k = 0; k < GRAD_CHUNK; ++k) r.d[k] = -f[j] / msum.v * msum.d[k];
+      return r;
+    };
+    // t(f_j) + t_ref along the moving point (value: the forward's)
+    auto tdual = [&](int j) {
+      const GD fj = fdual(j);
+      GD ph, tf;
+      mode_phase_tf(c, fj * c.M_sec, &ph, &tf);
+      GD r = tf + t_ref;
+      r.v = x[j];
+      return r;
+    };
+    // f where the chord of t(f) over [f_s, f_s+1] reaches T
+    auto cross = [&](int s, const GD& T) {
+      const GD fa = fdual(s), fb = fdual(s + 1), ta = tdual(s), tb = tdual(s + 1);
+      return (fb - fa) / (tb - ta) * (T - ta) + fa;
+    };
+    double tmin = x[0], tmax = x[0];
+    for (int i = 1; i < L; ++i) {
+      tmin = fmin(tmin, x[i]);
+      tmax = fmax(tmax, x[i]);
+    }
+    GD flo = fdual(0), fhi = fdual(L - 1);
+    if (tmin < 0.0) {
+      int cnt = 0, seg = -1;
+      for (int i = 0; i < L - 1; ++i)
+        if ((0.0 < x[i + 1]) && (0.0 > x[i])) {
+          if (cnt == 0) seg = i;
+          ++cnt;
+        }
+      if (cnt == 1) flo = cross(seg, GD(0.0));
+    }
+    const GD lam = seed(P[8 * (size_t)B + b], 7, k0), beta = seed(P[9 * (size_t)B + b], 8, k0);
+    GD To = tssb_from_l(tL_end, lam, beta, 0.0) - tssb_from_l(tL_start, lam, beta, 0.0);
+    To.v = t_end[b] - t_start[b];  // the forward's span
+    if (tmax > To.v) {
+      int cnt = 0, seg = -1;
+      for (int i = 0; i < L - 1; ++i)
+        if ((To.v < x[i + 1]) && (To.v > x[i])) {
+          if (cnt == 0) seg = i;
+          ++cnt;
+        }
+      if (cnt == 1) fhi = cross(seg, To);
+    }
+    double* w = wreg + (size_t)t * 2 * GRAD_CHUNK;
+#pragma unroll
+    for (int k = 0; k < GRAD_CHUNK; ++k) {
+      w[k] = flo.d[k] / flo.v;
+      w[GRAD_CHUNK + k] = fhi.d[k] / fhi.v;
+    }
   }
 }
 
@@ -286,17 +428,21 @@ extern "C" {
 // d lnL / d theta [B, 11] of the direct likelihood (no reference counterpart).  Inputs are
 // the forward path's sparse buffer y and its spline coefficients c1..c3 ([9, B, M, L]), the
 // knots x [B, M, L], the noise-weighted data [3, N] (complex128) and noise weights [3, N],
-// params [12, B] (device) and the QNM table for the dual-number setup.  The host reads the
-// support lengths once (one synchronisation).
+// params [12, B] (device) and the QNM table for the dual-number setup.  The knots' own motion
+// (the observation-window regrid) is differentiated from the forward's default grid f_default
+// and its t(f) tf_default ([B, M, L], t_ref included) and the L-frame observation limits
+// t_obs_start_L, t_obs_end_L [s]; with f_default or tf_default null the knots are held fixed.
+// The host reads the support lengths once (one synchronisation).
 int bbhx_direct_like_grad(void* orbits, void* d_h, void* h_h, double* grad, const double* params,
                           const int* ells,
                           const int* mms, const double* qnm_table, int qnm_n, double dspin,
                           double t_init, const double* data_freqs, const void* data,
                           const double* noise, int data_length, const double* x, const double* y,
                           const double* c1, const double* c2, const double* c3,
-                          const double* t_start, const double* t_end, int TDItag, int rescaled,
-                          int tdi2, int run_phenomd, int num_modes, int length, int num_bin_all,
-                          void* stream) {
+                          const double* t_start, const double* t_end, const double* f_default,
+                          const double* tf_default, double t_obs_start_L, double t_obs_end_L,
+                          int TDItag, int rescaled, int tdi2, int run_phenomd, int num_modes,
+                          int length, int num_bin_all, void* stream) {
   BBHX_REQUIRE(orbits && ((OrbitHandle*)orbits)->ready, "orbit information not added");
   BBHX_REQUIRE(TDItag == 1 || TDItag == 2, "TDItag must be 1 (XYZ) or 2 (AET)");
   BBHX_REQUIRE(num_modes > 0 && num_modes <= MAX_MODES, "num_modes must be 1..6");
@@ -321,12 +467,14 @@ int bbhx_direct_like_grad(void* orbits, void* d_h, void* h_h, double* grad, cons
   }
   // adjoint arrays over all binaries, dual records and d lnL / d h per batch
   const size_t nall = (size_t)9 * B * M * L;
-  double *ybd = nullptr, *cb = nullptr, *ybar = nullptr;
+  const bool moving = f_default != nullptr && tf_default != nullptr;
+  double *ybd = nullptr, *cb = nullptr, *ybar = nullptr, *xbar = nullptr, *wreg = nullptr;
   ModeCoeffsT<GD>* cD = nullptr;
   ResponseModeT<GD>* rD = nullptr;
   const int chunk = std::min(B, kDirectGradChunk);
   if (!st) {
-    if (pool_alloc((void**)&ybd, sizeof(double) * nall * 5, s) != cudaSuccess ||
+    const size_t nscratch = nall * 5 + (size_t)B * M * L + (size_t)chunk * M * 2 * GRAD_CHUNK;
+    if (pool_alloc((void**)&ybd, sizeof(double) * nscratch, s) != cudaSuccess ||
         pool_alloc((void**)&cD, sizeof(ModeCoeffsT<GD>) * (size_t)chunk * M, s) != cudaSuccess ||
         pool_alloc((void**)&rD, sizeof(ResponseModeT<GD>) * (size_t)chunk * M, s) != cudaSuccess) {
       set_error("device allocation of the gradient scratch failed");
@@ -336,7 +484,11 @@ int bbhx_direct_like_grad(void* orbits, void* d_h, void* h_h, double* grad, cons
   if (!st) {
     cb = ybd + nall;  // cb1, cb2, cb3
     ybar = cb + 3 * nall;
-    if (cudaMemsetAsync(ybd, 0, sizeof(double) * nall * 4, s) != cudaSuccess) {
+    xbar = ybar + nall;
+    wreg = xbar + (size_t)B * M * L;
+    // ybd / cb rows not written by k_adj_coeffs stay zero; wreg is zero for fixed knots
+    if (cudaMemsetAsync(ybd, 0, sizeof(double) * nall * 4, s) != cudaSuccess ||
+        cudaMemsetAsync(wreg, 0, sizeof(double) * (size_t)chunk * M * 2 * GRAD_CHUNK, s) != cudaSuccess) {
       set_error("cudaMemsetAsync failed");
       st = ERR_CUDA;
     }
@@ -382,8 +534,8 @@ int bbhx_direct_like_grad(void* orbits, void* d_h, void* h_h, double* grad, cons
       st = launch_status("k_adj_coeffs");
     }
     if (!st) {
-      k_spline_adj<<<(unsigned)std::min(nb * M, nsm * 4), 256, smem, s>>>(ybar, ybd, cb, cb + nall,
-                                                                         cb + 2 * nall, S, b0, nb);
+      k_spline_adj<<<(unsigned)std::min(nb * M, nsm * 4), 256, smem, s>>>(
+          ybar, xbar, ybd, cb, cb + nall, cb + 2 * nall, S, b0, nb);
       st = launch_status("k_spline_adj");
     }
     for (int k0 = 0; !st && k0 < NGRAD; k0 += GRAD_CHUNK) {
@@ -392,9 +544,16 @@ int bbhx_direct_like_grad(void* orbits, void* d_h, void* h_h, double* grad, cons
                                                                   run_phenomd, k0);
       st = launch_status("k_grad_setup");
       if (st) break;
+      if (moving) {
+        k_regrid_tangents<<<grid_for((long long)nb * M, 64), 64, 0, s>>>(
+            wreg, cD, params, B, b0, nb, M, L, f_default, tf_default, t_start, t_end,
+            t_obs_start_L, t_obs_end_L, k0);
+        st = launch_status("k_regrid_tangents");
+        if (st) break;
+      }
       k_contract_direct<<<(unsigned)std::min(nb, nsm * 8), 128, 0, s>>>(
-          grad, cD, rD, ((OrbitHandle*)orbits)->tab, params, B, b0, nb, t_init, x, ybar, TDItag,
-          rescaled, tdi2, M, L, k0);
+          grad, cD, rD, ((OrbitHandle*)orbits)->tab, params, B, b0, nb, t_init, x, ybar, xbar,
+          wreg, TDItag, rescaled, tdi2, M, L, k0);
       st = launch_status("k_contract_direct");
     }
     if (gh) cudaFreeAsync(gh, s);

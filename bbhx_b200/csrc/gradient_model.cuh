@@ -105,8 +105,11 @@ struct PointTangents {
   double tf;
 };
 
+// The frequency is a double (fixed grid) or a GD whose tangents are the knot's own motion
+// dx/dtheta, in which case the tangents are total derivatives along the moving knot.
+template <typename F>
 __device__ inline PointTangents point_tangents(const ModeCoeffsT<GD>& c, const ResponseModeT<GD>& r,
-                                               const OrbitTables& orb, double f, const GD& t_ref,
+                                               const OrbitTables& orb, const F& f, const GD& t_ref,
                                                double t_init, int TDItag, int rescaled, int tdi2) {
   PointTangents o;
   const PointOutT<GD> w = phm_eval_point(c, GD(f));
@@ -177,16 +180,22 @@ static __global__ void k_contract_het(double* grad, const ModeCoeffsT<GD>* coeff
   }
 }
 
-// Direct-likelihood contraction at the spline knots: grad[b] = sum_{mode, i} sum_p
-// ybar[p, b, m, i] d q_p / d theta, with q_p the sparse-grid quantities of the [9, B, M, L]
-// buffer (amplitude, phase with t_ref shift and Roemer delay, the six transfer components;
-// t(f), p = 2, only gates).  Knots x [B, M, L] are held fixed.
+// Direct-likelihood contraction at the spline knots: grad[b] = sum_{mode, i} (sum_p
+// ybar[p, b, m, i] d q_p / d theta + xbar[b, m, i] d x_i / d theta), with q_p the sparse-grid
+// quantities of the [9, B, M, L] buffer (amplitude, phase with t_ref shift and Roemer delay,
+// the six transfer components; t(f), p = 2, only gates) and x_i the knots.  The knots move
+// with theta through the observation-window regrid: d x_i = x_i ((1 - r_i) wlo + r_i whi),
+// r_i = i / (L - 1), with (wlo, whi) = (d flo / flo, d fhi / fhi) of the row from
+// k_regrid_tangents (wreg [nb * M][2][GRAD_CHUNK], local rows); q_p is differentiated along the
+// moving knot (the frequency is a dual carrying d x_i).
 static __global__ void k_contract_direct(double* grad, const ModeCoeffsT<GD>* coeffs,
                                          const ResponseModeT<GD>* rmodes, OrbitTables orb,
                                          const double* P, int B, int b0, int nb, double t_init,
-                                         const double* x, const double* ybar, int TDItag,
-                                         int rescaled, int tdi2, int M, int L, int k0) {
+                                         const double* x, const double* ybar, const double* xbar,
+                                         const double* wreg, int TDItag, int rescaled, int tdi2,
+                                         int M, int L, int k0) {
   const size_t n = (size_t)B * M * L;
+  const double inv_span = 1.0 / (double)(L - 1);
   for (int bl = blockIdx.x; bl < nb; bl += gridDim.x) {
     const int b = b0 + bl;
     const GD t_ref = seed(P[11 * (size_t)B + b], 10, k0);
@@ -194,22 +203,28 @@ static __global__ void k_contract_direct(double* grad, const ModeCoeffsT<GD>* co
 #pragma unroll
     for (int k = 0; k < GRAD_CHUNK; ++k) acc[k] = 0.0;
     for (int p = threadIdx.x; p < M * L; p += blockDim.x) {
-      const int m = p / L;
-      const size_t o = ((size_t)b * M + m) * L + (p % L);
-      const double w0 = ybar[o], w1 = ybar[n + o];
+      const int m = p / L, i = p % L;
+      const size_t o = ((size_t)b * M + m) * L + i;
+      const double w0 = ybar[o], w1 = ybar[n + o], xb = xbar[o];
       double wt[6];
-      bool any = (w0 != 0.0) || (w1 != 0.0);
+      bool any = (w0 != 0.0) || (w1 != 0.0) || (xb != 0.0);
 #pragma unroll
       for (int q = 0; q < 6; ++q) {
         wt[q] = ybar[(size_t)(3 + q) * n + o];
         any = any || (wt[q] != 0.0);
       }
       if (!any) continue;
+      const double* wr = wreg + ((size_t)bl * M + m) * 2 * GRAD_CHUNK;
+      const double r = i * inv_span;
+      GD fk(x[o]);
+#pragma unroll
+      for (int k = 0; k < GRAD_CHUNK; ++k)
+        fk.d[k] = x[o] * ((1.0 - r) * wr[k] + r * wr[GRAD_CHUNK + k]);
       const PointTangents pt = point_tangents(coeffs[(size_t)bl * M + m], rmodes[(size_t)bl * M + m],
-                                              orb, x[o], t_ref, t_init, TDItag, rescaled, tdi2);
+                                              orb, fk, t_ref, t_init, TDItag, rescaled, tdi2);
 #pragma unroll
       for (int k = 0; k < GRAD_CHUNK; ++k) {
-        double v = w0 * pt.amp.d[k] + w1 * pt.phase.d[k];
+        double v = w0 * pt.amp.d[k] + w1 * pt.phase.d[k] + xb * fk.d[k];
 #pragma unroll
         for (int ch = 0; ch < 3; ++ch)
           v += wt[2 * ch] * pt.T[ch].re.d[k] + wt[2 * ch + 1] * pt.T[ch].im.d[k];

@@ -178,10 +178,11 @@ __device__ __forceinline__ cplxT<T> nHn(const cplxT<T>* H, const V3T<T>& n) {
 template <typename T>
 __device__ __forceinline__ T sinc(const T& x) { return x == 0.0 ? T(1.0) : sin(x) / x; }
 
-// TDItag: 1 = XYZ, 2 = AET.  f in Hz, t in s.
-template <typename T>
+// TDItag: 1 = XYZ, 2 = AET.  f in Hz, t in s.  The frequency has its own type F: double, or
+// the dual type T when the frequency itself carries tangents (knots that move with theta).
+template <typename T, typename F = double>
 __device__ inline TransferT<T> response_point(const ResponseModeT<T>& r, const OrbitTables& orb,
-                                              double f, const T& t, int TDItag, int rescaled,
+                                              const F& f, const T& t, int TDItag, int rescaled,
                                               int tdi2) {
   const T* k = r.k;
   // Roemer delay relative to the SSB (circular 1 AU orbit of the guiding centre)

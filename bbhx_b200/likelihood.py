@@ -130,8 +130,8 @@ class Likelihood:
 
     def get_ll_and_grad(self, params, **waveform_kwargs):
         """lnL [B] and d lnL / d theta [B, 11] (device tensors); theta = (m1, m2, chi1z,
-        chi2z, distance, phi_ref, inc, lam, beta, psi, t_ref).  FP64, plain lnL; the sparse
-        knots are held fixed in the derivative."""
+        chi2z, distance, phi_ref, inc, lam, beta, psi, t_ref).  FP64, plain lnL; the
+        derivative follows the sparse knots as the observation-window regrid moves them."""
         from .autodiff import as_param_tensor
 
         P = as_param_tensor(params)

@@ -19,6 +19,7 @@ import numpy as np
 from . import _lib
 from .response.fastfdresponse import LISATDIResponse
 from .utils.arrays import atleast_1d, device, to_dev, to_np, torch
+from .utils.constants import YRSID_SI
 from .utils.interpolate import CubicSplineInterpolant
 from .waveforms.phenomhm import PhenomHMAmpPhase, step_front
 
@@ -143,6 +144,8 @@ class BBHWaveformFD:
                 if e:
                     raise ValueError("The search for a window at x_%s did not run correctly."
                                      % ("min" if e == 1 else "max"))
+            # what the regrid read, for the knots' derivative in direct_grad
+            self._regrid_inputs = (ap._freqs, tf0)
             ap._freqs = new_f
         rg = self.response_gen
         inc_d, lam_d, beta_d, psi_d, phi_d = (to_dev(atleast_1d(v)) for v in (inc, lam, beta, psi, phi_ref))
@@ -291,6 +294,7 @@ class BBHWaveformFD:
         P = params.to(device=device(), dtype=t.float64).contiguous()
         rows = tuple(P[k] for k in range(12))
         buf, c1, c2, c3, x, ts, te = self._spline_set(rows, t_obs_start, t_obs_end, length, modes)
+        f_default, tf_default = self._regrid_inputs
         ap, rg = self.amp_phase_gen, self.response_gen
         B, M, L = self.num_bin_all, self.num_modes, self.length
         grad = t.empty((B, 11), dtype=t.float64, device=device())
@@ -304,8 +308,9 @@ class BBHWaveformFD:
                   float(dspin), float(ap.initial_t_val), _lib.dptr(data_freqs),
                   _lib.dptr(data_weighted), _lib.dptr(noise_factors), int(data_freqs.numel()),
                   _lib.dptr(x), _lib.dptr(buf), _lib.dptr(c1), _lib.dptr(c2), _lib.dptr(c3),
-                  _lib.dptr(ts), _lib.dptr(te), rg.TDItag_int, int(rg.rescaled), int(rg.tdi2),
-                  int(ap.run_phenomd), M, L, B, _lib.stream())
+                  _lib.dptr(ts), _lib.dptr(te), _lib.dptr(f_default), _lib.dptr(tf_default),
+                  float(t_obs_start * YRSID_SI), float(t_obs_end * YRSID_SI), rg.TDItag_int,
+                  int(rg.rescaled), int(rg.tdi2), int(ap.run_phenomd), M, L, B, _lib.stream())
         return d_h, h_h, grad
 
     def _spline_set(self, params, t_obs_start, t_obs_end, length, modes, flags=None,

@@ -315,7 +315,11 @@ int bbhx_hdyn_grad(void *orbits, void *d_h, void *h_h, double *grad, const void 
    and the not-a-knot spline build (transposed tridiagonal solve), forward-mode tangents of
    PhenomHM + TDI at the knots.  x [B, M, L] knots; y, c1, c2, c3 [9, B, M, L] from the forward
    path (bbhx_waveform_response_fused + bbhx_interpolate); data [3, N] complex128 noise-weighted,
-   noise [3, N]; params [12, B]; theta as for bbhx_hdyn_grad.  Knots are held fixed.
+   noise [3, N]; params [12, B]; theta as for bbhx_hdyn_grad.  The knots' motion through the
+   observation-window regrid (bbhx_tf_window_regrid) is differentiated from f_default, the
+   default grid the regrid read (bbhx_default_freqs), and tf_default, its t(f) with t_ref
+   (bbhx_phenomhm_tf), both [B, M, L], and the L-frame observation limits t_obs_start_L,
+   t_obs_end_L [s]; f_default or tf_default null holds the knots fixed.
    d_h, h_h: device complex128 [B], overwritten with <d|h>, <h|h> of the same evaluation (as
    bbhx_direct_like_fused in FP64, so no separate likelihood call is needed). */
 int bbhx_direct_like_grad(void *orbits, void *d_h, void *h_h, double *grad,
@@ -324,9 +328,10 @@ int bbhx_direct_like_grad(void *orbits, void *d_h, void *h_h, double *grad,
                           double t_init, const double *data_freqs, const void *data,
                           const double *noise, int data_length, const double *x, const double *y,
                           const double *c1, const double *c2, const double *c3,
-                          const double *t_start, const double *t_end, int TDItag, int rescaled,
-                          int tdi2, int run_phenomd, int num_modes, int length, int num_bin_all,
-                          void *stream);
+                          const double *t_start, const double *t_end, const double *f_default,
+                          const double *tf_default, double t_obs_start_L, double t_obs_end_L,
+                          int TDItag, int rescaled, int tdi2, int run_phenomd, int num_modes,
+                          int length, int num_bin_all, void *stream);
 
 #ifdef __cplusplus
 }

@@ -3,8 +3,9 @@ lnL, and the torch.autograd front end.
 
 Finite-difference steps (central, FP64): relative 1e-6 for masses and distance, absolute
 1e-6 for spins and angles, 1e-3 s for t_ref.  Agreement bound per component:
-|g - fd| <= 1e-4 |fd| + 1e-7 max_k |fd_k * step_scale_k| (the second term absorbs
-components that are zero to FD accuracy).
+direct likelihood |g - fd| <= 1e-4 |fd| (the derivative follows the sparse knots as the
+observation-window regrid moves them); heterodyned |g - fd| <= 1e-4 |fd| + 1e-7 max_k
+|fd_k * step_scale_k| (the second term absorbs components that are zero to FD accuracy).
 """
 import numpy as np
 import pytest
@@ -33,10 +34,10 @@ def _central_fd(fn, P):
     return out
 
 
-def _check(grad, fd, P):
+def _check(grad, fd, P, floor=1e-7):
     for b in range(grad.shape[0]):
         scale = np.max(np.abs(fd[b] * _steps(P[:, b]))) / 1e-6
-        tol = 1e-4 * np.abs(fd[b]) + 1e-7 * scale
+        tol = 1e-4 * np.abs(fd[b]) + floor * scale
         bad = np.abs(grad[b] - fd[b]) > tol
         assert not np.any(bad), (b, np.array(ROWS)[bad], grad[b][bad], fd[b][bad])
 
@@ -111,8 +112,8 @@ def test_direct_gradient_matches_central_fd(golden, golden_data, center_index):
     grad = grad.cpu().numpy()
     np.testing.assert_allclose(ll, like.get_ll(P, **kw), rtol=1e-12, atol=1e-8)
     fd = _central_fd(lambda Q: like.get_ll(Q, **kw), P)
-    print("grad", grad[0], "\nfd  ", fd[0])
-    _check(grad, fd, P)
+    print("grad", grad[0], "\nfd  ", fd[0], "\nrel ", np.max(np.abs(grad - fd) / np.abs(fd), axis=0))
+    _check(grad, fd, P, floor=0.0)
 
 
 def test_direct_autograd_backward(golden, golden_data):
@@ -146,5 +147,5 @@ def test_direct_gradient_matches_fd_of_oracle_lnl(golden, golden_data):
     pipe = RefPipeline("ref" if os.path.isfile(OUT) else "np")
     fd = _central_fd(lambda Q: pipe.direct_lnl(Q, golden_data["f"], like.test_data,
                                                golden_data["psd"], **kw)[0], P)
-    print(pipe.K.name, "grad", grad[0], "\nfd  ", fd[0])
-    _check(grad, fd, P)
+    print(pipe.K.name, "grad", grad[0], "\nfd  ", fd[0], "\nrel ", np.max(np.abs(grad - fd) / np.abs(fd), axis=0))
+    _check(grad, fd, P, floor=0.0)
