@@ -13,20 +13,12 @@
 // [9, B, M, L] buffer, the [B, 3, L] templates and the transposed residuals are never
 // written.
 //
-// Precision variants (template flag MIXED):
-//   FP64  : everything in FP64 (phm_eval_point / response_point of the direct path).
-//   mixed : phase, t(f), the Roemer delay, the orbit positions, the arguments of the
-//           transfer phasors, the waveform phasor e^{i phase}, the distance / mass scale and
-//           the channel products in FP64; the shape of the amplitude (PhenomD ansatz and PN
-//           ratios), the sinc factors and the transfer algebra in FP32; r = h / h0 and the
-//           bin sums in FP64.
+// Precision variants (FP64, mixed): het_item.cuh.
 #include <algorithm>
 
 #include "capi_internal.cuh"
-#include "phenomhm_model.cuh"
-#include "response_model.cuh"
-#include "spline_eval.cuh"
 #include "gradient_model.cuh"
+#include "het_item.cuh"
 
 namespace bbhx {
 
@@ -45,456 +37,25 @@ int take_nonfinite_heterodyne(cudaStream_t s, unsigned* any) {
   return OK;
 }
 
-// ------------------------------------------------------------------ FP32 amplitude model
-// Amplitude coefficients of one (binary, mode) in FP32 (built once per CTA from ModeCoeffs).
-struct __align__(16) AmpModeF {
-  float amp0, ains[8], g1, g2, g3, fRD, fDM, fpeak;
-  float hf1, hf2, hf3, hc0, hc1, hc2, hc3, hc4;
-  float am_fi, am_fr, am_ai, am_am, am_bm, am_br;
-  // PN amplitude |H_lm(v)| (IMRPhenomHMOnePointFiveSpinPN, PhenomHMWaveform.cu:2375-2455)
-  float eta, delta, Xs, Xa, two_pi_over_m, four_pi_over_m2, pn_k;
-  int pn_case;  // 0: (2,2) or PhenomD only; 1: 21; 2: 33; 3: 32; 4: 44; 5: 43; 6: none
-};
-
-__device__ inline void build_amp_f(AmpModeF& a, const ModeCoeffs& c) {
-  const PhenomD& d = c.d;
-  a.amp0 = (float)d.amp0;
-  for (int k = 0; k < 8; ++k) a.ains[k] = (float)d.ains[k];
-  a.g1 = (float)d.g1;
-  a.g2 = (float)d.g2;
-  a.g3 = (float)d.g3;
-  a.fRD = (float)d.fRD;
-  a.fDM = (float)d.fDM;
-  a.fpeak = (float)d.fpeak;
-  a.hf1 = (float)d.hf1;
-  a.hf2 = (float)d.hf2;
-  a.hf3 = (float)d.hf3;
-  a.hc0 = (float)d.hc0;
-  a.hc1 = (float)d.hc1;
-  a.hc2 = (float)d.hc2;
-  a.hc3 = (float)d.hc3;
-  a.hc4 = (float)d.hc4;
-  a.am_fi = (float)c.am_fi;
-  a.am_fr = (float)c.am_fr;
-  a.am_ai = (float)c.am_ai;
-  a.am_am = (float)c.am_am;
-  a.am_bm = (float)c.am_bm;
-  a.am_br = (float)c.am_br;
-  a.eta = (float)c.pn_eta;
-  a.delta = (float)c.pn_delta;
-  a.Xs = (float)c.pn_Xs;
-  a.Xa = (float)c.pn_Xa;
-  a.two_pi_over_m = (float)c.pn_2pi_m;
-  a.four_pi_over_m2 = (float)c.pn_4pi_m2;
-  a.pn_k = (float)c.pn_k;
-  a.pn_case = c.pn_case;
-}
-
-// |H_lm(v)| of the 1.5PN spinning amplitude for the non-22 cases.
-__device__ __forceinline__ float pn_habs_f(const AmpModeF& a, float v) {
-  const float v2 = v * v, v3 = v2 * v;
-  switch (a.pn_case) {
-    case 1: {
-      const float v4 = v3 * v;
-      const float re = a.pn_k * (v * a.delta - v2 * 1.5f * (a.Xa + a.delta * a.Xs) +
-                                 v3 * a.delta * (335.0f / 672.0f + a.eta * (117.0f / 56.0f)) +
-                                 v4 * (a.Xa * (3427.0f / 1344.0f - a.eta * (2101.0f / 336.0f)) +
-                                       a.delta * a.Xs * (3427.0f / 1344.0f - a.eta * (965.0f / 336.0f)) -
-                                       a.delta * (float)PI));
-      const float im = a.pn_k * v4 * a.delta * (-0.5f - 2.0f * 0.69314718056f);
-      return sqrtf(re * re + im * im);
-    }
-    case 2: return fabsf(a.pn_k * v * a.delta);
-    case 3: return fabsf(a.pn_k * v2 * (1.0f - 3.0f * a.eta));
-    case 4: return fabsf(a.pn_k * v2 * (1.0f - 3.0f * a.eta));
-    case 5: return fabsf(a.pn_k * v3 * a.delta * (1.0f - 2.0f * a.eta));
-    default: return 0.0f;
-  }
-}
-
-
-// PhenomD amplitude without the distance / mass scale (PhenomHMWaveform.cu:1508-1537).
-__device__ __forceinline__ float phenomd_amp_f(const AmpModeF& a, float Mf) {
-  const float third = cbrtf(Mf);
-  const float sixth = sqrtf(third);
-  const float pre = a.amp0 / (Mf * sixth);
-  if (Mf < (float)AMP_FJOIN_INS) {
-    const float two_thirds = Mf / third, four_thirds = Mf * third;
-    const float five_thirds = four_thirds * third, two = Mf * Mf;
-    const float seven_thirds = third * two, eight_thirds = two_thirds * two;
-    const float ins = 1.0f + two_thirds * a.ains[0] + Mf * a.ains[1] + four_thirds * a.ains[2] +
-                      five_thirds * a.ains[3] + two * a.ains[4] + seven_thirds * a.ains[5] +
-                      eight_thirds * a.ains[6] + Mf * two * a.ains[7];
-    return pre * ins;
-  }
-  if (Mf >= a.fpeak) {
-    const float s = a.fDM * a.g3;
-    const float x = Mf - a.fRD;
-    return pre * expf(-x * a.g2 / s) * (s * a.g1) / (x * x + s * s);
-  }
-  const float u = Mf - a.hf1;
-  return pre * (a.hc0 + u * (a.hc1 + u * (a.hc2 + (Mf - a.hf2) * (a.hc3 + (Mf - a.hf3) * a.hc4))));
-}
-
-// Mode amplitude at geometric frequency Mf without the distance / mass scale: PhenomD at the
-// mapped frequency times the PN ratio (get_amp, PhenomHMWaveform.cu:2461-2514).  With v_lm(x) = (2 pi x / m)^(1/3), the
-// four v^-3.5 |H| factors of the reference reduce to |H(v(Mf))| |H(v(Mfa))| / |H(v(2Mf/m))|
-// because the v^-3.5 powers cancel exactly: v(2Mf/m) / v(Mf) = (2/m)^(1/3) and
-// v_22(Mfa) / v_lm(Mfa) = (m/2)^(1/3).
-__device__ __forceinline__ float mode_amp_f(const AmpModeF& a, float Mf) {
-  float Mfa;
-  if (Mf > a.am_fi) Mfa = (Mf > a.am_fr) ? Mf + a.am_br : fmaf(a.am_am, Mf, a.am_bm);
-  else Mfa = a.am_ai * Mf;
-  const float amp = phenomd_amp_f(a, Mfa);
-  if (a.pn_case == 0) return amp;
-  const float t1 = pn_habs_f(a, cbrtf(a.two_pi_over_m * Mf));
-  if (t1 == 0.0f) return 0.0f;
-  const float t2 = pn_habs_f(a, cbrtf(a.four_pi_over_m2 * Mf));
-  const float h1 = pn_habs_f(a, cbrtf(a.two_pi_over_m * Mfa));
-  return amp * (t1 / t2) * h1;
-}
-
-// ------------------------------------------------------------------ FP32 response algebra
-struct __align__(16) RespModeF {
-  cplxf H[9];
-  double k[3];
-};
-
-__device__ inline void build_resp_f(RespModeF& o, const ResponseMode& r) {
-  for (int q = 0; q < 9; ++q) o.H[q] = cplxf{(float)r.H[q].re, (float)r.H[q].im};
-  for (int q = 0; q < 3; ++q) o.k[q] = r.k[q];
-}
-
-struct TransferF {
-  cplxf L1, L2, L3;
-  double phaseRdelay;
-};
-
-__device__ __forceinline__ cplxf nHn_f(const cplxf* H, float n0, float n1, float n2) {
-  const float v[3] = {n0, n1, n2};
-  cplxf out{0.f, 0.f};
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    cplxf t{0.f, 0.f};
-#pragma unroll
-    for (int j = 0; j < 3; ++j) {
-      t.re = fmaf(H[i * 3 + j].re, v[j], t.re);
-      t.im = fmaf(H[i * 3 + j].im, v[j], t.im);
-    }
-    out.re = fmaf(v[i], t.re, out.re);
-    out.im = fmaf(v[i], t.im, out.im);
-  }
-  return out;
-}
-
-__device__ __forceinline__ float sinc_f(float x) { return x == 0.0f ? 1.0f : __fdividef(sinf(x), x); }
-__device__ __forceinline__ cplxf cf(float r, float i) { return cplxf{r, i}; }
-__device__ __forceinline__ cplxf ti_f(cplxf a) { return {-a.im, a.re}; }
-__device__ __forceinline__ cplxf ephase(double x) {
-  float s, c;
-  sincos_mixed(x, &s, &c);
-  return cplxf{c, s};
-}
-
-// Same transfer as response_point (Response.cu:54-314) with the split described above.
-__device__ inline TransferF response_point_mixed(const RespModeF& r, const OrbitTables& orb,
-                                                 double f, double t, int TDItag, int rescaled,
-                                                 int tdi2) {
-  const double* k = r.k;
-  double sa, ca;
-  sincos_cw(Omega0 * t, &sa, &ca);
-  TransferF out;
-  out.phaseRdelay = 2. * PI / C_SI * f * (k[0] * (AU_SI * ca) + k[1] * (AU_SI * sa));
-
-  const OrbitWindow<double> win = orbit_window(orb, t);
-  V3T<double> p1 = orbit_lerp(win.x_lo, 9, 0, win.frac);
-  V3T<double> p2 = orbit_lerp(win.x_lo, 9, 3, win.frac);
-  V3T<double> p3 = orbit_lerp(win.x_lo, 9, 6, win.frac);
-  V3T<double> n1 = orbit_lerp(win.n_lo, 18, orb.link_index[0] * 3, win.frac);
-  V3T<double> n2 = orbit_lerp(win.n_lo, 18, orb.link_index[1] * 3, win.frac);
-  V3T<double> n3 = orbit_lerp(win.n_lo, 18, orb.link_index[2] * 3, win.frac);
-  const float kn1 = (float)(k[0] * n1.x + k[1] * n1.y + k[2] * n1.z);
-  const float kn2 = (float)(k[0] * n2.x + k[1] * n2.y + k[2] * n2.z);
-  const float kn3 = (float)(k[0] * n3.x + k[1] * n3.y + k[2] * n3.z);
-  const cplxf n1H = nHn_f(r.H, (float)n1.x, (float)n1.y, (float)n1.z);
-  const cplxf n2H = nHn_f(r.H, (float)n2.x, (float)n2.y, (float)n2.z);
-  const cplxf n3H = nHn_f(r.H, (float)n3.x, (float)n3.y, (float)n3.z);
-  const double k12 = k[0] * (p1.x + p2.x) + k[1] * (p1.y + p2.y) + k[2] * (p1.z + p2.z);
-  const double k23 = k[0] * (p2.x + p3.x) + k[1] * (p2.y + p3.y) + k[2] * (p2.z + p3.z);
-  const double k31 = k[0] * (p3.x + p1.x) + k[1] * (p3.y + p1.y) + k[2] * (p3.z + p1.z);
-  const double invL = orb.inv_armlength;
-  const double pre = f * orb.pi_L_over_c;
-  const cplxf e12 = ephase(pre * (1. + k12 * invL));
-  const cplxf e23 = ephase(pre * (1. + k23 * invL));
-  const cplxf e31 = ephase(pre * (1. + k31 * invL));
-  const float pf = (float)pre;
-  const cplxf c3 = pf * ti_f(n3H), c1 = pf * ti_f(n1H), c2 = pf * ti_f(n2H);
-  const cplxf G12 = sinc_f(pf * (1.f - kn3)) * (c3 * e12);
-  const cplxf G21 = sinc_f(pf * (1.f + kn3)) * (c3 * e12);
-  const cplxf G23 = sinc_f(pf * (1.f - kn1)) * (c1 * e23);
-  const cplxf G32 = sinc_f(pf * (1.f + kn1)) * (c1 * e23);
-  const cplxf G31 = sinc_f(pf * (1.f - kn2)) * (c2 * e31);
-  const cplxf G13 = sinc_f(pf * (1.f + kn2)) * (c2 * e31);
-
-  // powers of e^{ix}, x = pre, from one reduction
-  const cplxf e1 = ephase(pre);
-  const cplxf z = e1 * e1;  // e^{2ix}
-  const float s1 = e1.im, s2x = 2.f * e1.im * e1.re;
-  if (TDItag == 1) {
-    const cplxf fac = rescaled ? cf(1.f, 0.f) : ti_f((2.f * s2x) * z);
-    const cplxf X = G21 + z * G12 - G31 - z * G13;
-    const cplxf Y = G32 + z * G23 - G12 - z * G21;
-    const cplxf Z = G13 + z * G31 - G23 - z * G32;
-    out.L1 = fac * X;
-    out.L2 = fac * Y;
-    out.L3 = fac * Z;
-    return out;
-  }
-  cplxf fAE, fT;
-  if (rescaled) {
-    fAE = cf(1.f, 0.f);
-    fT = cf(1.f, 0.f);
-  } else {
-    fAE = ti_f((float)SQRT2 * s2x * z);
-    fT = (2.f * (float)SQRT2 * s2x * s1) * (z * e1);
-  }
-  const cplxf one = cf(1.f, 0.f);
-  const cplxf A = 0.5f * ((one + z) * (G31 + G13) - G23 - z * G32 - G21 - z * G12);
-  const cplxf E = (0.5f * (float)INVSQRT3) *
-                  ((one - z) * (G13 - G31) + (cf(2.f, 0.f) + z) * (G12 - G32) +
-                   (one + 2.f * z) * (G21 - G23));
-  const cplxf T = (float)INVSQRT6 * (G21 - G12 + G32 - G23 + G13 - G31);
-  cplxf f2 = cf(2.f, 0.f);
-  if (tdi2) {
-    const cplxf z2 = z * z;                                // e^{4ix}
-    const float s4x = 2.f * s2x * (e1.re * e1.re - e1.im * e1.im);  // sin 4x
-    f2 = 2.f * ti_f((-2.f * s4x) * z2);
-  }
-  out.L1 = f2 * (fAE * A);
-  out.L2 = f2 * (fAE * E);
-  out.L3 = f2 * (fT * T);
-  return out;
-}
-
 // ------------------------------------------------------------------ fused kernel
-constexpr int HET_THREADS = 128;
-
-struct HetArgs {
-  cplx* d_h;
-  cplx* h_h;
-  const ModeCoeffs* coeffs;  // [B, M]
-  const ResponseMode* rmodes;  // [B, M]
-  OrbitTables orb;
-  const double* t_ref;
-  double t_init;
-  const double* t_start;
-  const double* t_end;
-  const double* freqs;  // [L]
-  const cplx* h0;       // [3, L]
-  const cplx* consts;   // [4, 3, L]: A0, A1, B0, B1
-  int TDItag, rescaled, tdi2;
-  int M, L, B;
-  cplx* gh;  // optional [B, 3, L]: d lnL / d h (adjoint of the bin sums and of r = h / h0)
-};
-
-// Dynamic shared memory of one warp (walker): ModeCoeffs[M] | ResponseMode[M] | AmpModeF[M] |
-// RespModeF[M] | r[3][L] (cplx), each region starting on a 16-byte boundary; a CTA holds one
-// such slice per warp.
-__host__ __device__ __forceinline__ size_t align16(size_t n) { return (n + 15) & ~(size_t)15; }
-
-struct HetSmemLayout {
-  size_t sr, sa, sf, rr, total;
-  __host__ __device__ HetSmemLayout(int M, int L) {
-    sr = align16(sizeof(ModeCoeffs) * M);
-    sa = sr + align16(sizeof(ResponseMode) * M);
-    sf = sa + align16(sizeof(AmpModeF) * M);
-    rr = sf + align16(sizeof(RespModeF) * M);
-    total = rr + sizeof(cplx) * 3 * (size_t)L;
-  }
-};
-
-// One WARP per walker (each lane takes the frequencies lane, lane + 32, ...), each warp with
-// its own slice of shared memory: no block-wide barrier, so a warp never waits for another
-// walker's slower points or for the serial per-walker set-up of the others.
-template <bool MIXED>
+// One WARP per walker (het_item, het_item.cuh), each warp with its own slice of shared memory:
+// no block-wide barrier, so a warp never waits for another walker's slower points or for the
+// serial per-walker set-up of the others.
+template <bool MIXED, bool GH>
 __global__ void __launch_bounds__(HET_THREADS) k_het_fused(HetArgs A) {
   extern __shared__ __align__(16) unsigned char het_smem[];
-  const HetSmemLayout lay(A.M, A.L);
   const int lane = threadIdx.x & 31;
   const int nwarps = blockDim.x >> 5;
-  unsigned char* base = het_smem + (size_t)(threadIdx.x >> 5) * align16(lay.total);
-  ModeCoeffs* sc = (ModeCoeffs*)base;
-  ResponseMode* sr = (ResponseMode*)(base + lay.sr);
-  AmpModeF* sa = (AmpModeF*)(base + lay.sa);
-  RespModeF* sf = (RespModeF*)(base + lay.sf);
-  cplx* rr = (cplx*)(base + lay.rr);
-
-  for (int b = blockIdx.x * nwarps + (threadIdx.x >> 5); b < A.B; b += gridDim.x * nwarps) {
-    __syncwarp();  // previous walker's shared data no longer in use
-    {
-      const unsigned long long* src = (const unsigned long long*)(A.coeffs + (size_t)b * A.M);
-      unsigned long long* dst = (unsigned long long*)sc;
-      const int n = (int)(sizeof(ModeCoeffs) * A.M / 8);
-      for (int i = lane; i < n; i += 32) dst[i] = src[i];
-      src = (const unsigned long long*)(A.rmodes + (size_t)b * A.M);
-      dst = (unsigned long long*)sr;
-      const int n2 = (int)(sizeof(ResponseMode) * A.M / 8);
-      for (int i = lane; i < n2; i += 32) dst[i] = src[i];
-    }
-    __syncwarp();
-    if (MIXED) {
-      if (lane < A.M) build_amp_f(sa[lane], sc[lane]);
-      else if (lane >= 16 && lane < 16 + A.M) build_resp_f(sf[lane - 16], sr[lane - 16]);
-      __syncwarp();
-    }
-    const double tr = A.t_ref[b];
-    const double ts = A.t_start[b], te = A.t_end[b];
-
-    for (int j = lane; j < A.L; j += 32) {
-      const double f = A.freqs[j];
-      double h[6] = {0, 0, 0, 0, 0, 0};
-      for (int m = 0; m < A.M; ++m) {
-        if (MIXED) {
-          const ModeCoeffs& c = sc[m];
-          const double Mf = f * c.M_sec;
-          double ph, tf;
-          mode_phase_tf(c, Mf, &ph, &tf);  // FP64
-          ph += f * (tr - A.t_init) * 2 * PI;
-          tf += tr;
-          if (!tf_gate(tf, ts, te)) continue;
-          const float ampf = c.phenomd_only ? phenomd_amp_f(sa[m], (float)Mf)
-                                            : mode_amp_f(sa[m], (float)Mf);
-          const TransferF T = response_point_mixed(sf[m], A.orb, f, tf, A.TDItag, A.rescaled, A.tdi2);
-          // phasor and channel products in FP64 (the scale factor stays FP64 as well)
-          double sn, cs;
-          sincos_cw(ph + T.phaseRdelay, &sn, &cs);
-          const double amp = (double)ampf * c.amp_scale;
-          const double apr = amp * cs, api = amp * sn;
-          const cplxf Tc[3] = {T.L1, T.L2, T.L3};
-#pragma unroll
-          for (int ch = 0; ch < 3; ++ch) {
-            const double trr = Tc[ch].re, tii = Tc[ch].im;
-            h[2 * ch] += trr * apr - tii * api;
-            h[2 * ch + 1] -= trr * api + tii * apr;
-          }
-        } else {
-          PointOut o = phm_eval_point(sc[m], f);
-          o.phase += f * (tr - A.t_init) * 2 * PI;
-          o.tf += tr;
-          if (!tf_gate(o.tf, ts, te)) continue;
-          const Transfer T = response_point(sr[m], A.orb, f, o.tf, A.TDItag, A.rescaled, A.tdi2);
-          const cplx ap = o.amp * expi(o.phase + T.phaseRdelay);
-          const cplx Tc[3] = {T.L1, T.L2, T.L3};
-#pragma unroll
-          for (int ch = 0; ch < 3; ++ch) {
-            const cplx v = Tc[ch] * ap;
-            h[2 * ch] += v.re;
-            h[2 * ch + 1] -= v.im;
-          }
-        }
-      }
-      // r = h / h0 per channel
-#pragma unroll
-      for (int ch = 0; ch < 3; ++ch) {
-        const cplx d = A.h0[(size_t)ch * A.L + j];
-        const double den = d.re * d.re + d.im * d.im;
-        rr[ch * A.L + j] = mk((h[2 * ch] * d.re + h[2 * ch + 1] * d.im) / den,
-                              (h[2 * ch + 1] * d.re - h[2 * ch] * d.im) / den);
-      }
-    }
-    __syncwarp();
-
-    // relative-binning bin terms, hdynLikelihood (Likelihood.cu:20-123): bin j >= 1
-    double dre = 0, dim = 0, hre = 0, him = 0;
-    for (int j = 1 + lane; j < A.L; j += 32) {
-      const double fj = A.freqs[j], fp = A.freqs[j - 1];
-      if (fp == 0.0) continue;
-      const double df = fj - fp;
-      const double fm = (fj + fp) / 2.0;
-#pragma unroll
-      for (int ch = 0; ch < 3; ++ch) {
-        const cplx cur = rr[ch * A.L + j], prv = rr[ch * A.L + j - 1];
-        const cplx r1 = mk((cur.re - prv.re) / df, (cur.im - prv.im) / df);
-        const cplx r0 = cur - r1 * (fj - fm);
-        const cplx A0 = A.consts[((size_t)0 * 3 + ch) * A.L + j];
-        const cplx A1 = A.consts[((size_t)1 * 3 + ch) * A.L + j];
-        const cplx B0 = A.consts[((size_t)2 * 3 + ch) * A.L + j];
-        const cplx B1 = A.consts[((size_t)3 * 3 + ch) * A.L + j];
-        const cplx t = A0 * conj(r0) + A1 * conj(r1);
-        dre += t.re;
-        dim += t.im;
-        const double mag2 = r0.re * r0.re + r0.im * r0.im;
-        const double re01 = r0.re * r1.re + r0.im * r1.im;
-        hre += B0.re * mag2 + 2.0 * B1.re * re01;
-        him += B0.im * mag2 + 2.0 * B1.im * re01;
-      }
-    }
-    if (!MIXED && A.gh) {  // the adjoint output exists for the FP64 form only
-      // Adjoint of lnL = Re d_h - (d_d + Re h_h) / 2 through the bin terms: per bin
-      // g_r0 = A0 - Re(B0) r0 - Re(B1) r1, g_r1 = A1 - Re(B1) r0, carried to r_j / r_{j-1}
-      // with the same coefficients as the forward r0, r1; then g_h = g_r / conj(h0).
-      for (int j = lane; j < A.L; j += 32) {
-#pragma unroll
-        for (int ch = 0; ch < 3; ++ch) {
-          cplx g = mk(0.0, 0.0);
-          for (int side = 0; side < 2; ++side) {
-            const int jj = j + side;  // bin jj has cur = r_jj, prv = r_{jj-1}
-            if (jj < 1 || jj >= A.L) continue;
-            const double fj = A.freqs[jj], fp = A.freqs[jj - 1];
-            if (fp == 0.0) continue;
-            const double df = fj - fp;
-            const double fm = (fj + fp) / 2.0;
-            const double a = (fj - fm) / df;
-            const cplx cur = rr[ch * A.L + jj], prv = rr[ch * A.L + jj - 1];
-            const cplx r1 = mk((cur.re - prv.re) / df, (cur.im - prv.im) / df);
-            const cplx r0 = cur - r1 * (fj - fm);
-            const cplx A0 = A.consts[((size_t)0 * 3 + ch) * A.L + jj];
-            const cplx A1 = A.consts[((size_t)1 * 3 + ch) * A.L + jj];
-            const double B0 = A.consts[((size_t)2 * 3 + ch) * A.L + jj].re;
-            const double B1 = A.consts[((size_t)3 * 3 + ch) * A.L + jj].re;
-            const cplx g0 = A0 - B0 * r0 - B1 * r1;
-            const cplx g1 = A1 - B1 * r0;
-            if (side == 0) g = g + (1.0 - a) * g0 + (1.0 / df) * g1;  // r_j is cur of bin j
-            else g = g + a * g0 - (1.0 / df) * g1;                    // r_j is prv of bin j+1
-          }
-          const cplx d = A.h0[(size_t)ch * A.L + j];
-          const double den = d.re * d.re + d.im * d.im;  // g / conj(d) = g d / |d|^2
-          A.gh[((size_t)b * 3 + ch) * A.L + j] =
-              mk((g.re * d.re - g.im * d.im) / den, (g.re * d.im + g.im * d.re) / den);
-        }
-      }
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-      dre += __shfl_xor_sync(0xffffffffu, dre, o);
-      dim += __shfl_xor_sync(0xffffffffu, dim, o);
-      hre += __shfl_xor_sync(0xffffffffu, hre, o);
-      him += __shfl_xor_sync(0xffffffffu, him, o);
-    }
-    if (lane == 0) {
-      A.d_h[b] = mk(dre, dim);
-      A.h_h[b] = mk(hre, him);
-      note_nonfinite(&g_nonfinite_heterodyne, dre, dim, hre, him);
-    }
-  }
-}
-
-__global__ void k_response_setup_het(ResponseMode* out, const int* ells, const int* mms,
-                                     const double* phi_ref, const double* inc, const double* lam,
-                                     const double* beta, const double* psi, int M, int B) {
-  long long n = (long long)B * M;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
-       t += (long long)gridDim.x * blockDim.x) {
-    int b = (int)(t / M), i = (int)(t % M);
-    ResponseMode r;
-    response_mode_setup(r, ells[i], mms[i], phi_ref[b], inc[b], lam[b], beta[b], psi[b]);
-    out[t] = r;
-  }
+  unsigned char* base =
+      het_smem + (size_t)(threadIdx.x >> 5) * align16(HetSmemLayout(A.M, A.L, GH).total);
+  for (int b = blockIdx.x * nwarps + (threadIdx.x >> 5); b < A.B; b += gridDim.x * nwarps)
+    het_item<MIXED, GH>(A, b, base, lane, &g_nonfinite_heterodyne);
 }
 
 // Warps (walkers) per CTA of k_het_fused and its dynamic shared memory: up to
 // HET_THREADS / 32 warps, as many slices as fit in the opt-in per-block shared memory.
-inline int het_launch_shape(int M, int L, int* threads, size_t* smem) {
-  const size_t slice = align16(HetSmemLayout(M, L).total);
+inline int het_launch_shape(int M, int L, bool full_r, int* threads, size_t* smem) {
+  const size_t slice = align16(HetSmemLayout(M, L, full_r).total);
   int dev = 0, limit = 48 * 1024;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&limit, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
@@ -509,6 +70,23 @@ inline int het_launch_shape(int M, int L, int* threads, size_t* smem) {
   return OK;
 }
 
+template <bool MIXED, bool GH>
+int launch_het(const HetArgs& A, cudaStream_t s) {
+  int threads = HET_THREADS;
+  size_t smem = 0;
+  int st = het_launch_shape(A.M, A.L, GH, &threads, &smem);
+  if (st) return st;
+  const long long wpc = threads / 32;
+  const unsigned grid =
+      (unsigned)std::min<long long>((A.B + wpc - 1) / wpc, (long long)sm_count() * 16);
+  st = cuda_status(cudaFuncSetAttribute(k_het_fused<MIXED, GH>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                   "cudaFuncSetAttribute(k_het_fused)");
+  if (st) return st;
+  k_het_fused<MIXED, GH><<<grid, threads, smem, s>>>(A);
+  return launch_status("k_het_fused");
+}
+
 }  // namespace bbhx
 
 using namespace bbhx;
@@ -517,6 +95,55 @@ namespace {
 constexpr int kHetMaxL = 2048;
 constexpr int kGradChunk = 4096;  // walkers per dual-number setup / contraction batch
 }
+
+namespace bbhx {
+
+// Walker description of one heterodyned problem (validated by the caller).
+HetArgs het_args(void* orbits, void* d_h, void* h_h, const void* coeffs, const int* ells,
+                 const int* mms, const double* phi_ref, const double* inc, const double* lam,
+                 const double* beta, const double* psi, const double* t_ref, double t_init,
+                 const double* t_start, const double* t_end, const double* freqs, const void* h0,
+                 const void* consts, int TDItag, int rescaled, int tdi2, int num_modes,
+                 int length, int num_bin_all) {
+  HetArgs A;
+  A.d_h = (cplx*)d_h;
+  A.h_h = (cplx*)h_h;
+  A.coeffs = (const ModeCoeffs*)coeffs;
+  A.ells = ells;
+  A.mms = mms;
+  A.phi_ref = phi_ref;
+  A.inc = inc;
+  A.lam = lam;
+  A.beta = beta;
+  A.psi = psi;
+  A.orb = ((OrbitHandle*)orbits)->tab;
+  A.t_ref = t_ref;
+  A.t_init = t_init;
+  A.t_start = t_start;
+  A.t_end = t_end;
+  A.freqs = freqs;
+  A.h0 = (const cplx*)h0;
+  A.consts = (const cplx*)consts;
+  A.TDItag = TDItag;
+  A.rescaled = rescaled;
+  A.tdi2 = tdi2;
+  A.gh = nullptr;
+  A.M = num_modes;
+  A.L = length;
+  A.B = num_bin_all;
+  return A;
+}
+
+int het_check(void* orbits, int TDItag, int num_modes, int length, int precision) {
+  BBHX_REQUIRE(orbits && ((OrbitHandle*)orbits)->ready, "orbit information not added");
+  BBHX_REQUIRE(TDItag == 1 || TDItag == 2, "TDItag must be 1 (XYZ) or 2 (AET)");
+  BBHX_REQUIRE(num_modes > 0 && num_modes <= MAX_MODES, "num_modes must be 1..6");
+  BBHX_REQUIRE(length >= 2 && length <= kHetMaxL, "heterodyne length must be 2..%d", kHetMaxL);
+  BBHX_REQUIRE(precision == 0 || precision == 1, "precision must be 0 (fp64) or 1 (mixed)");
+  return OK;
+}
+
+}  // namespace bbhx
 
 extern "C" {
 
@@ -529,62 +156,14 @@ int bbhx_hdyn_fused(void* orbits, void* d_h, void* h_h, const void* coeffs, cons
                     const double* t_start, const double* t_end, const double* freqs,
                     const void* h0, const void* consts, int TDItag, int rescaled, int tdi2,
                     int num_modes, int length, int num_bin_all, int precision, void* stream) {
-  BBHX_REQUIRE(orbits && ((OrbitHandle*)orbits)->ready, "orbit information not added");
-  BBHX_REQUIRE(TDItag == 1 || TDItag == 2, "TDItag must be 1 (XYZ) or 2 (AET)");
-  BBHX_REQUIRE(num_modes > 0 && num_modes <= MAX_MODES, "num_modes must be 1..6");
-  BBHX_REQUIRE(length >= 2 && length <= kHetMaxL, "heterodyne length must be 2..%d", kHetMaxL);
-  BBHX_REQUIRE(precision == 0 || precision == 1, "precision must be 0 (fp64) or 1 (mixed)");
+  int st = het_check(orbits, TDItag, num_modes, length, precision);
+  if (st) return st;
   if (num_bin_all == 0) return OK;
+  const HetArgs A = het_args(orbits, d_h, h_h, coeffs, ells, mms, phi_ref, inc, lam, beta, psi,
+                             t_ref, t_init, t_start, t_end, freqs, h0, consts, TDItag, rescaled,
+                             tdi2, num_modes, length, num_bin_all);
   cudaStream_t s = (cudaStream_t)stream;
-  const long long nbm = (long long)num_bin_all * num_modes;
-  ResponseMode* rm = nullptr;
-  BBHX_CHECK_CUDA(pool_alloc((void**)&rm, sizeof(ResponseMode) * nbm, s));
-  k_response_setup_het<<<grid_for(nbm, 128), 128, 0, s>>>(rm, ells, mms, phi_ref, inc, lam, beta,
-                                                          psi, num_modes, num_bin_all);
-  int st = launch_status("k_response_setup_het");
-  if (!st) {
-    HetArgs A;
-    A.d_h = (cplx*)d_h;
-    A.h_h = (cplx*)h_h;
-    A.coeffs = (const ModeCoeffs*)coeffs;
-    A.rmodes = rm;
-    A.orb = ((OrbitHandle*)orbits)->tab;
-    A.t_ref = t_ref;
-    A.t_init = t_init;
-    A.t_start = t_start;
-    A.t_end = t_end;
-    A.freqs = freqs;
-    A.h0 = (const cplx*)h0;
-    A.consts = (const cplx*)consts;
-    A.TDItag = TDItag;
-    A.rescaled = rescaled;
-    A.tdi2 = tdi2;
-    A.gh = nullptr;
-    A.M = num_modes;
-    A.L = length;
-    A.B = num_bin_all;
-    int threads = HET_THREADS;
-    size_t smem = 0;
-    st = het_launch_shape(num_modes, length, &threads, &smem);
-    const int nsm = sm_count();
-    const long long wpc = threads / 32;
-    const unsigned grid =
-        (unsigned)std::min<long long>((num_bin_all + wpc - 1) / wpc, (long long)nsm * 16);
-    if (!st && precision == 1) {
-      st = cuda_status(cudaFuncSetAttribute(k_het_fused<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem),
-                       "cudaFuncSetAttribute(k_het_fused<true>)");
-      if (!st) k_het_fused<true><<<grid, threads, smem, s>>>(A);
-    } else if (!st) {
-      st = cuda_status(cudaFuncSetAttribute(k_het_fused<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem),
-                       "cudaFuncSetAttribute(k_het_fused<false>)");
-      if (!st) k_het_fused<false><<<grid, threads, smem, s>>>(A);
-    }
-    if (!st) st = launch_status("k_het_fused");
-  }
-  cudaFreeAsync(rm, s);
-  return st;
+  return precision == 1 ? launch_het<true, false>(A, s) : launch_het<false, false>(A, s);
 }
 
 // Heterodyned lnL and its gradient d lnL / d theta for the 11 parameters (order in
@@ -597,72 +176,30 @@ int bbhx_hdyn_grad(void* orbits, void* d_h, void* h_h, double* grad, const void*
                    const double* t_end, const double* freqs, const void* h0, const void* consts,
                    int TDItag, int rescaled, int tdi2, int run_phenomd, int num_modes, int length,
                    int num_bin_all, void* stream) {
-  BBHX_REQUIRE(orbits && ((OrbitHandle*)orbits)->ready, "orbit information not added");
-  BBHX_REQUIRE(TDItag == 1 || TDItag == 2, "TDItag must be 1 (XYZ) or 2 (AET)");
-  BBHX_REQUIRE(num_modes > 0 && num_modes <= MAX_MODES, "num_modes must be 1..6");
-  BBHX_REQUIRE(length >= 2 && length <= kHetMaxL, "heterodyne length must be 2..%d", kHetMaxL);
+  int st = het_check(orbits, TDItag, num_modes, length, 0);
+  if (st) return st;
   BBHX_REQUIRE(qnm_n >= 2 && dspin > 0.0, "bad QNM table");
   if (num_bin_all == 0) return OK;
   cudaStream_t s = (cudaStream_t)stream;
-  const long long nbm = (long long)num_bin_all * num_modes;
-  ResponseMode* rm = nullptr;
   cplx* gh = nullptr;
   ModeCoeffsT<GD>* cD = nullptr;
   ResponseModeT<GD>* rD = nullptr;
   const int chunk = std::min(num_bin_all, kGradChunk);
-  int st = OK;
-  if (pool_alloc((void**)&rm, sizeof(ResponseMode) * nbm, s) != cudaSuccess ||
-      pool_alloc((void**)&gh, sizeof(cplx) * 3 * (size_t)length * num_bin_all, s) != cudaSuccess ||
+  const int nsm = sm_count();
+  if (pool_alloc((void**)&gh, sizeof(cplx) * 3 * (size_t)length * num_bin_all, s) != cudaSuccess ||
       pool_alloc((void**)&cD, sizeof(ModeCoeffsT<GD>) * (size_t)chunk * num_modes, s) != cudaSuccess ||
       pool_alloc((void**)&rD, sizeof(ResponseModeT<GD>) * (size_t)chunk * num_modes, s) != cudaSuccess) {
     set_error("device allocation of the gradient scratch failed");
     st = ERR_CUDA;
   }
   if (!st) {
-    k_response_setup_het<<<grid_for(nbm, 128), 128, 0, s>>>(rm, ells, mms, params + 5 * (size_t)num_bin_all,
-                                                            params + 7 * (size_t)num_bin_all,
-                                                            params + 8 * (size_t)num_bin_all,
-                                                            params + 9 * (size_t)num_bin_all,
-                                                            params + 10 * (size_t)num_bin_all,
-                                                            num_modes, num_bin_all);
-    st = launch_status("k_response_setup_het");
-  }
-  if (!st) {
-    HetArgs A;
-    A.d_h = (cplx*)d_h;
-    A.h_h = (cplx*)h_h;
-    A.coeffs = (const ModeCoeffs*)coeffs;
-    A.rmodes = rm;
-    A.orb = ((OrbitHandle*)orbits)->tab;
-    A.t_ref = params + 11 * (size_t)num_bin_all;
-    A.t_init = t_init;
-    A.t_start = t_start;
-    A.t_end = t_end;
-    A.freqs = freqs;
-    A.h0 = (const cplx*)h0;
-    A.consts = (const cplx*)consts;
-    A.TDItag = TDItag;
-    A.rescaled = rescaled;
-    A.tdi2 = tdi2;
+    const size_t B = (size_t)num_bin_all;
+    HetArgs A = het_args(orbits, d_h, h_h, coeffs, ells, mms, params + 5 * B, params + 7 * B,
+                         params + 8 * B, params + 9 * B, params + 10 * B, params + 11 * B, t_init,
+                         t_start, t_end, freqs, h0, consts, TDItag, rescaled, tdi2, num_modes,
+                         length, num_bin_all);
     A.gh = gh;
-    A.M = num_modes;
-    A.L = length;
-    A.B = num_bin_all;
-    int threads = HET_THREADS;
-    size_t smem = 0;
-    st = het_launch_shape(num_modes, length, &threads, &smem);
-    const int nsm = sm_count();
-    const long long wpc = threads / 32;
-    const unsigned grid =
-        (unsigned)std::min<long long>((num_bin_all + wpc - 1) / wpc, (long long)nsm * 16);
-    if (!st && cudaFuncSetAttribute(k_het_fused<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem) != cudaSuccess) {
-      set_error("cudaFuncSetAttribute failed for k_het_fused");
-      st = ERR_CUDA;
-    } else if (!st) {
-      k_het_fused<false><<<grid, threads, smem, s>>>(A);
-      st = launch_status("k_het_fused (gradient forward)");
-    }
+    st = launch_het<false, true>(A, s);
     for (int b0 = 0; !st && b0 < num_bin_all; b0 += chunk) {
       const int nb = std::min(chunk, num_bin_all - b0);
       const long long n = (long long)nb * num_modes;
@@ -682,7 +219,6 @@ int bbhx_hdyn_grad(void* orbits, void* d_h, void* h_h, double* grad, const void*
   if (rD) cudaFreeAsync(rD, s);
   if (cD) cudaFreeAsync(cD, s);
   if (gh) cudaFreeAsync(gh, s);
-  if (rm) cudaFreeAsync(rm, s);
   return st;
 }
 

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "capi_internal.cuh"
+#include "het_item.cuh"
 #include "spline_eval.cuh"
 
 namespace bbhx {
@@ -1243,39 +1244,84 @@ __global__ void k_store_groups(MultiArgs M, MultiArgs* dst) {
   for (int i = threadIdx.x; i < n; i += blockDim.x) d[i] = src[i];
 }
 
-template <bool MIXED>
-__global__ void __launch_bounds__(FD_WARPS * 32, MIXED ? 4 : 3)
-    k_direct_fused_multi(const MultiArgs* __restrict__ MA) {
+// Heterodyned problems of an uneven batch: their walkers form one item range in front of the
+// direct items of k_uneven.  Stored in device memory by k_store_het (from kernel parameters).
+struct HetMulti {
+  HetArgs g[FD_MAXGROUPS];
+  long long woff[FD_MAXGROUPS + 1];  // walker offsets; woff[ngroups] = total walkers
+  int ngroups;
+};
+
+__global__ void k_store_het(HetMulti H, HetMulti* dst) {
+  const int n = (int)(sizeof(HetMulti) / sizeof(unsigned long long));
+  const unsigned long long* src = reinterpret_cast<const unsigned long long*>(&H);
+  unsigned long long* d = reinterpret_cast<unsigned long long*>(dst);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) d[i] = src[i];
+}
+
+// Last index i in [0, n) with off[i] <= q (off ascending, off[0] = 0 <= q).
+__device__ __forceinline__ int group_of(const long long* off, int n, long long q) {
+  int lo = 0, hi = n;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (off[mid] <= q) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+// An uneven batch in ONE persistent launch: the walkers of every heterodyned problem (one
+// warp item each, het_item) followed by the (tile, binary) items of every direct problem
+// (fused_item), enumerated as one range that the warps stride through.  Each warp owns a
+// shared-memory slot of `slot` bytes that holds either a direct item's staged segments (and
+// recurrence state) or a walker's records and residual strip; the problem's argument block is
+// copied to shared memory when the warp moves to another problem.  HET = false compiles the
+// walker path out (batches without heterodyned problems): the mixed direct items then run
+// within 128 registers, 4 CTAs per SM; with walkers the mixed kernel takes the FP64 budget
+// (168 registers, 3 CTAs per SM), which the FP32 heterodyne models need without spilling.
+template <bool MIXED, bool HET>
+__global__ void __launch_bounds__(FD_WARPS * 32, (MIXED && !HET) ? 4 : 3)
+    k_uneven(const MultiArgs* __restrict__ MA, const HetMulti* __restrict__ HM, int slot) {
   using R = typename std::conditional<MIXED, float, double>::type;
   constexpr bool REC = !MIXED;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ FusedArgs gcur[FD_WARPS];
+  __shared__ HetArgs hcur[FD_WARPS];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
-  WarpStage<R>& S = reinterpret_cast<WarpStage<R>*>(smem_raw)[warp];
-  RecStage* RS = REC ? reinterpret_cast<RecStage*>(smem_raw + FD_WARPS * sizeof(WarpStage<R>)) + warp
-                     : nullptr;
-  const int ng = MA->ngroups;
-  const long long total = MA->off[ng];
+  unsigned char* mine = smem_raw + (size_t)warp * slot;
+  WarpStage<R>& S = *reinterpret_cast<WarpStage<R>*>(mine);
+  RecStage* RS = REC ? reinterpret_cast<RecStage*>(mine + sizeof(WarpStage<R>)) : nullptr;
+  const long long nh = HM->woff[HM->ngroups];
+  const long long total = nh + MA->off[MA->ngroups];
   const long long gw = (long long)blockIdx.x * FD_WARPS + warp;
   const long long nw = (long long)gridDim.x * FD_WARPS;
-  int g = -1;
+  int g = -1, hg = -1;
   for (long long q = gw; q < total; q += nw) {
-    if (g < 0 || q >= MA->off[g + 1] || q < MA->off[g]) {
-      int lo = 0, hi = ng;  // last group with off <= q
-      while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (MA->off[mid] <= q) lo = mid; else hi = mid;
+    if (HET && q < nh) {
+      if (hg < 0 || q >= HM->woff[hg + 1] || q < HM->woff[hg]) {
+        hg = group_of(HM->woff, HM->ngroups, q);
+        __syncwarp();
+        const int n8 = (int)(sizeof(HetArgs) / sizeof(unsigned long long));
+        const unsigned long long* src = reinterpret_cast<const unsigned long long*>(&HM->g[hg]);
+        unsigned long long* dst = reinterpret_cast<unsigned long long*>(&hcur[warp]);
+        for (int i = lane; i < n8; i += 32) dst[i] = src[i];
+        __syncwarp();
       }
-      g = lo;
-      __syncwarp();
-      const int nw8 = (int)(sizeof(FusedArgs) / sizeof(unsigned long long));
-      const unsigned long long* src = reinterpret_cast<const unsigned long long*>(&MA->g[g]);
-      unsigned long long* dst = reinterpret_cast<unsigned long long*>(&gcur[warp]);
-      for (int i = lane; i < nw8; i += 32) dst[i] = src[i];
-      __syncwarp();
+      het_item<MIXED, false>(hcur[warp], (int)(q - HM->woff[hg]), mine, lane,
+                             &g_nonfinite_likelihood);
+    } else {
+      const long long qd = q - nh;
+      if (g < 0 || qd >= MA->off[g + 1] || qd < MA->off[g]) {
+        g = group_of(MA->off, MA->ngroups, qd);
+        __syncwarp();
+        const int n8 = (int)(sizeof(FusedArgs) / sizeof(unsigned long long));
+        const unsigned long long* src = reinterpret_cast<const unsigned long long*>(&MA->g[g]);
+        unsigned long long* dst = reinterpret_cast<unsigned long long*>(&gcur[warp]);
+        for (int i = lane; i < n8; i += 32) dst[i] = src[i];
+        __syncwarp();
+      }
+      fused_item<MIXED, R, false, REC>(gcur[warp], qd - MA->off[g], S, RS, lane);
     }
-    fused_item<MIXED, R, false, REC>(gcur[warp], q - MA->off[g], S, RS, lane);
   }
 }
 
@@ -1530,20 +1576,56 @@ int bbhx_template_support(int* start, int* len, const double* x, int num_modes, 
   return launch_status("k_support");
 }
 
-// Several direct-likelihood problems in one persistent launch of the fused kernel (see
-// k_direct_fused_multi).  groups: HOST array of descriptors (device pointers inside);
-// tile_bins: data bins per work item (multiple of 128); ctas_per_sm: persistent CTAs per SM.
-int bbhx_direct_like_multi(const bbhx_direct_group* groups, int num_groups, int precision,
-                           int tile_bins, int ctas_per_sm, void* stream) {
-  BBHX_REQUIRE(groups != nullptr && num_groups >= 1 && num_groups <= FD_MAXGROUPS,
-               "num_groups must be 1..%d", FD_MAXGROUPS);
+}  // extern "C"
+
+namespace bbhx {
+HetArgs het_args(void* orbits, void* d_h, void* h_h, const void* coeffs, const int* ells,
+                 const int* mms, const double* phi_ref, const double* inc, const double* lam,
+                 const double* beta, const double* psi, const double* t_ref, double t_init,
+                 const double* t_start, const double* t_end, const double* freqs, const void* h0,
+                 const void* consts, int TDItag, int rescaled, int tdi2, int num_modes,
+                 int length, int num_bin_all);
+int het_check(void* orbits, int TDItag, int num_modes, int length, int precision);
+static_assert(sizeof(HetArgs) % 8 == 0 && sizeof(FusedArgs) % 8 == 0,
+              "argument blocks are copied in 8-byte words");
+
+// Direct and heterodyned problems in ONE persistent launch of k_uneven (direct groups only:
+// the same kernel with an empty walker range).  groups / hgroups: HOST arrays of descriptors
+// (device pointers inside).
+static int uneven_like(const bbhx_direct_group* groups, int num_groups,
+                       const bbhx_hdyn_group* hgroups, int num_het, int precision, int tile_bins,
+                       int ctas_per_sm, cudaStream_t s) {
+  BBHX_REQUIRE(num_groups >= 0 && num_groups <= FD_MAXGROUPS && (groups != nullptr || num_groups == 0),
+               "num_direct must be 0..%d", FD_MAXGROUPS);
+  BBHX_REQUIRE(num_het >= 0 && num_het <= FD_MAXGROUPS && (hgroups != nullptr || num_het == 0),
+               "num_het must be 0..%d", FD_MAXGROUPS);
+  BBHX_REQUIRE(num_groups + num_het >= 1, "no problems in the batch");
   BBHX_REQUIRE(precision == 0 || precision == 1, "precision must be 0 (FP64) or 1 (mixed)");
   BBHX_REQUIRE(tile_bins >= FD_WARP_BINS && tile_bins <= FD_WARP_BINS * FD_MAXCHUNK &&
                    tile_bins % FD_WARP_BINS == 0,
                "tile_bins must be a multiple of %d in [%d, %d]", FD_WARP_BINS, FD_WARP_BINS,
                FD_WARP_BINS * FD_MAXCHUNK);
   BBHX_REQUIRE(ctas_per_sm >= 1 && ctas_per_sm <= 32, "ctas_per_sm must be 1..32");
-  cudaStream_t s = (cudaStream_t)stream;
+  // heterodyned problems: validated, walker offsets, the largest per-warp slice
+  HetMulti HM;
+  memset(&HM, 0, sizeof(HM));
+  HM.ngroups = num_het;
+  long long walkers = 0;
+  size_t het_slot = 0;
+  for (int g = 0; g < num_het; ++g) {
+    const bbhx_hdyn_group& H = hgroups[g];
+    const int hs = het_check(H.orbits, H.TDItag, H.num_modes, H.length, precision);
+    if (hs) return hs;
+    BBHX_REQUIRE(H.num_bin_all >= 0, "heterodyned group %d: bad walker count %d", g, H.num_bin_all);
+    HM.g[g] = het_args(H.orbits, H.d_h, H.h_h, H.coeffs, H.ells, H.mms, H.phi_ref, H.inc, H.lam,
+                       H.beta, H.psi, H.t_ref, H.t_init, H.t_start, H.t_end, H.freqs, H.h0,
+                       H.consts, H.TDItag, H.rescaled, H.tdi2, H.num_modes, H.length,
+                       H.num_bin_all);
+    HM.woff[g] = walkers;
+    walkers += H.num_bin_all;
+    het_slot = std::max(het_slot, align16(HetSmemLayout(H.num_modes, H.length, false).total));
+  }
+  HM.woff[num_het] = walkers;
   MultiArgs MA;
   memset(&MA, 0, sizeof(MA));
   MA.ngroups = num_groups;
@@ -1623,34 +1705,43 @@ int bbhx_direct_like_multi(const bbhx_direct_group* groups, int num_groups, int 
   MA.off[num_groups] = items;
   MA.boff[num_groups] = bins;
   MultiArgs* dMA = nullptr;
+  HetMulti* dHM = nullptr;
   if (!st) {
-    if (pool_alloc((void**)&dMA, sizeof(MultiArgs), s) != cudaSuccess) {
-      set_error("device allocation of the group table failed");
+    if (pool_alloc((void**)&dMA, sizeof(MultiArgs), s) != cudaSuccess ||
+        pool_alloc((void**)&dHM, sizeof(HetMulti), s) != cudaSuccess) {
+      set_error("device allocation of the group tables failed");
       st = ERR_CUDA;
-    } else {
-      scratch.push_back(dMA);
+    }
+    if (dMA) scratch.push_back(dMA);
+    if (dHM) scratch.push_back(dHM);
+    if (!st) {
       k_store_groups<<<1, 256, 0, s>>>(MA, dMA);
       st = launch_status("k_store_groups");
     }
-  }
-  if (!st && items > 0) {
-    const int nsm = sm_count();
-    const long long want = (items + FD_WARPS - 1) / FD_WARPS;
-    const unsigned grid = (unsigned)std::min<long long>(want, (long long)nsm * ctas_per_sm);
-    if (precision == 1) {
-      const size_t sm = fused_smem_bytes<true>();
-      st = cuda_status(cudaFuncSetAttribute(k_direct_fused_multi<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)sm),
-                       "cudaFuncSetAttribute(k_direct_fused_multi<true>)");
-      if (!st) k_direct_fused_multi<true><<<grid, FD_WARPS * 32, sm, s>>>(dMA);
-    } else {
-      const size_t sm = fused_smem_bytes<false>();
-      st = cuda_status(cudaFuncSetAttribute(k_direct_fused_multi<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)sm),
-                       "cudaFuncSetAttribute(k_direct_fused_multi<false>)");
-      if (!st) k_direct_fused_multi<false><<<grid, FD_WARPS * 32, sm, s>>>(dMA);
+    if (!st) {
+      k_store_het<<<1, 256, 0, s>>>(HM, dHM);
+      st = launch_status("k_store_het");
     }
-    if (!st) st = launch_status("k_direct_fused_multi");
+  }
+  if (!st && items + walkers > 0) {
+    const int nsm = sm_count();
+    const long long want = (items + walkers + FD_WARPS - 1) / FD_WARPS;
+    const unsigned grid = (unsigned)std::min<long long>(want, (long long)nsm * ctas_per_sm);
+    const size_t dslot = (precision == 1 ? fused_smem_bytes<true>() : fused_smem_bytes<false>()) / FD_WARPS;
+    const size_t slot = align16(std::max(dslot, het_slot));
+    const size_t sm = slot * FD_WARPS;
+    auto launch = [&](auto kernel) {
+      int r = cuda_status(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)sm),
+                          "cudaFuncSetAttribute(k_uneven)");
+      if (!r) kernel<<<grid, FD_WARPS * 32, sm, s>>>(dMA, dHM, (int)slot);
+      return r;
+    };
+    if (precision == 1)
+      st = walkers > 0 ? launch(k_uneven<true, true>) : launch(k_uneven<true, false>);
+    else
+      st = walkers > 0 ? launch(k_uneven<false, true>) : launch(k_uneven<false, false>);
+    if (!st) st = launch_status("k_uneven");
   }
   if (!st && bins > 0) {
     k_fused_reduce_multi<<<grid_for(32LL * bins, 128), 128, 0, s>>>(dMA);
@@ -1658,6 +1749,29 @@ int bbhx_direct_like_multi(const bbhx_direct_group* groups, int num_groups, int 
   }
   for (void* p : scratch) cudaFreeAsync(p, s);
   return st;
+}
+
+}  // namespace bbhx
+
+extern "C" {
+
+// Several direct-likelihood problems in one persistent launch of the fused kernel (k_uneven
+// with no heterodyned problems).  groups: HOST array of descriptors (device pointers inside);
+// tile_bins: data bins per work item (multiple of 128); ctas_per_sm: persistent CTAs per SM.
+int bbhx_direct_like_multi(const bbhx_direct_group* groups, int num_groups, int precision,
+                           int tile_bins, int ctas_per_sm, void* stream) {
+  BBHX_REQUIRE(groups != nullptr && num_groups >= 1 && num_groups <= FD_MAXGROUPS,
+               "num_groups must be 1..%d", FD_MAXGROUPS);
+  return uneven_like(groups, num_groups, nullptr, 0, precision, tile_bins, ctas_per_sm,
+                     (cudaStream_t)stream);
+}
+
+// Direct and heterodyned problems (uneven grid lengths, mode sets, observation spans, sparse
+// grids) in one persistent launch (k_uneven).
+int bbhx_uneven_like(const bbhx_direct_group* direct, int num_direct, const bbhx_hdyn_group* het,
+                     int num_het, int precision, int tile_bins, int ctas_per_sm, void* stream) {
+  return uneven_like(direct, num_direct, het, num_het, precision, tile_bins, ctas_per_sm,
+                     (cudaStream_t)stream);
 }
 
 // Fused direct likelihood: d_h, h_h device complex128 [B] (overwritten, scaled by 4 like the

@@ -5,12 +5,14 @@ A batch holds
     data grid), binaries ``params`` [12, n], a sparse-grid ``length`` and a mode set;
   * heterodyned groups — a ``HeterodynedLikelihood`` (its own relative-binning grid of any
     length) and walkers [12, n].
-``run()`` builds every group's sparse buffers and splines, then evaluates ALL direct groups in
-one persistent launch of the fused likelihood kernel (``bbhx_direct_like_multi``) and every
-heterodyned group with the fused heterodyne kernel.  Nothing in ``run()`` synchronises with the
-host, so ``capture()`` records it once in a CUDA graph and ``replay()`` re-runs it (parameters
-are updated in place with ``set_params``).  The launch shape of the persistent kernel (data bins
-per work item, CTAs per SM) is chosen by ``Autotuner`` by timing the candidates on the batch.
+``run()`` builds every group's inputs on the device -- sparse buffers and splines of the direct
+groups, per-walker model records of the heterodyned ones -- then evaluates ALL groups of a
+precision class in ONE persistent launch (``bbhx_uneven_like``): the heterodyned walkers and the
+direct (data tile, binary) items form one work range.  Nothing in ``run()`` synchronises with
+the host, so ``capture()`` records it once in a CUDA graph and ``replay()`` re-runs it
+(parameters are updated in place with ``set_params``).  The launch shape of the persistent
+kernel (data bins per work item, CTAs per SM) is chosen by ``Autotuner`` by timing the
+candidates on the batch.
 
 No reference counterpart: the reference evaluates one problem per call.
 """
@@ -33,6 +35,20 @@ class DirectGroupC(ctypes.Structure):
                 ("num_modes", ctypes.c_int), ("length", ctypes.c_int),
                 ("num_bin_all", ctypes.c_int), ("d_h", ctypes.c_void_p), ("h_h", ctypes.c_void_p),
                 ("data32", ctypes.c_void_p), ("noise32", ctypes.c_void_p)]
+
+
+class HdynGroupC(ctypes.Structure):
+    """Mirror of ``bbhx_hdyn_group`` (include/bbhx_b200.h)."""
+
+    _fields_ = [("orbits", ctypes.c_void_p), ("d_h", ctypes.c_void_p), ("h_h", ctypes.c_void_p),
+                ("coeffs", ctypes.c_void_p), ("ells", ctypes.c_void_p), ("mms", ctypes.c_void_p),
+                ("phi_ref", ctypes.c_void_p), ("inc", ctypes.c_void_p), ("lam", ctypes.c_void_p),
+                ("beta", ctypes.c_void_p), ("psi", ctypes.c_void_p), ("t_ref", ctypes.c_void_p),
+                ("t_init", ctypes.c_double), ("t_start", ctypes.c_void_p),
+                ("t_end", ctypes.c_void_p), ("freqs", ctypes.c_void_p), ("h0", ctypes.c_void_p),
+                ("consts", ctypes.c_void_p), ("TDItag", ctypes.c_int), ("rescaled", ctypes.c_int),
+                ("tdi2", ctypes.c_int), ("num_modes", ctypes.c_int), ("length", ctypes.c_int),
+                ("num_bin_all", ctypes.c_int)]
 
 
 class DirectGroup:
@@ -91,13 +107,20 @@ class HetGroup:
     def size(self):
         return self.params.shape[1]
 
-    def run(self, precision):
-        self.ll, _ = self.het._fused_ll(self.params, dict(t_obs_start=self.t_obs_start,
-                                                          t_obs_end=self.t_obs_end), precision,
-                                        flags=self.flags)
+    def build(self, precision="fp64"):
+        """Per-walker records and outputs of this group (device; no host synchronisation)."""
+        het = self.het
+        rows = tuple(self.params[k] for k in range(12))
+        a = het.template_gen.heterodyne_setup(rows, het.freqs, het._h0_flat, het.data_constants,
+                                              self.t_obs_start, self.t_obs_end, flags=self.flags)
+        self._keep = a
+        self.d_h, self.h_h = a["d_h"], a["h_h"]
+        fields = {k: (a[k] if isinstance(a[k], (int, float)) else _lib.dptr(a[k]).value)
+                  for k in het.template_gen.HDYN_ARGS}
+        return HdynGroupC(orbits=het.template_gen.response_gen.orbit_handle.ptr.value, **fields)
 
     def lnl(self):
-        return self.ll
+        return -0.5 * (self.het.reference_d_d + self.h_h.real - 2 * self.d_h.real)
 
 
 class Autotuner:
@@ -112,12 +135,14 @@ class Autotuner:
         self.repeats = repeats
 
     @staticmethod
-    def signature(descs, precision):
+    def signature(descs, hdescs, precision):
         return (precision, len(descs), sum(d.num_bin_all for d in descs),
-                max(d.data_length for d in descs), max(d.length for d in descs))
+                max((d.data_length for d in descs), default=0),
+                max((d.length for d in descs), default=0), len(hdescs),
+                sum(h.num_bin_all for h in hdescs), max((h.length for h in hdescs), default=0))
 
-    def best(self, descs, precision, launch):
-        key = self.signature(descs, precision)
+    def best(self, descs, hdescs, precision, launch):
+        key = self.signature(descs, hdescs, precision)
         if key in self.table:
             return self.table[key]
         t = torch()
@@ -161,8 +186,8 @@ class UnevenBatch:
         # a missing entry is autotuned on the first run
         self.shape = dict(shape or {})
         self.graph = None
-        if len(self.direct) > 64:
-            raise ValueError("at most 64 direct groups per batch")
+        if len(self.direct) > 64 or len(self.het) > 64:
+            raise ValueError("at most 64 direct and 64 heterodyned groups per batch")
 
     def group_precisions(self):
         """Arithmetic of every group (direct groups first): a mixed batch runs the direct
@@ -173,25 +198,27 @@ class UnevenBatch:
             out.append("fp64" if (self.precision == "fp64" or coarse) else "mixed")
         return out + [self.precision] * len(self.het)
 
-    def _launch(self, descs, precision, tile, ctas):
-        arr = (DirectGroupC * len(descs))(*descs)
-        _lib.call("bbhx_direct_like_multi", ctypes.cast(arr, ctypes.c_void_p), len(descs),
-                  PRECISIONS[precision], int(tile), int(ctas), _lib.stream())
+    def _launch(self, descs, hdescs, precision, tile, ctas):
+        arr = (DirectGroupC * max(len(descs), 1))(*descs)
+        harr = (HdynGroupC * max(len(hdescs), 1))(*hdescs)
+        _lib.call("bbhx_uneven_like", ctypes.cast(arr, ctypes.c_void_p), len(descs),
+                  ctypes.cast(harr, ctypes.c_void_p), len(hdescs), PRECISIONS[precision],
+                  int(tile), int(ctas), _lib.stream())
 
     def run(self):
-        """All groups' lnL (list of device tensors, direct groups first).  Direct groups of
-        each precision class run in one persistent launch."""
+        """All groups' lnL (list of device tensors, direct groups first).  The groups of each
+        precision class (direct and heterodyned) run in one persistent launch."""
         precs = self.group_precisions()
         classes = {}
         for g, pr in zip(self.direct, precs):
-            classes.setdefault(pr, []).append(g.build(pr))
-        for pr, descs in classes.items():
+            classes.setdefault(pr, ([], []))[0].append(g.build(pr))
+        for h, pr in zip(self.het, precs[len(self.direct):]):
+            classes.setdefault(pr, ([], []))[1].append(h.build(pr))
+        for pr, (descs, hdescs) in classes.items():
             if pr not in self.shape:
-                self.shape[pr] = self.autotuner.best(descs, pr,
-                                                     lambda tl, c: self._launch(descs, pr, tl, c))
-            self._launch(descs, pr, *self.shape[pr])
-        for h in self.het:
-            h.run(self.precision)
+                self.shape[pr] = self.autotuner.best(
+                    descs, hdescs, pr, lambda tl, c: self._launch(descs, hdescs, pr, tl, c))
+            self._launch(descs, hdescs, pr, *self.shape[pr])
         return [g.lnl() for g in self.direct] + [h.lnl() for h in self.het]
 
     def capture(self):

@@ -233,12 +233,12 @@ class BBHWaveformFD:
             return data_out
         return (template_channels, self.interp_response.start_inds, self.interp_response.lengths)
 
-    def heterodyne_sums(self, params, freqs, h0, constants, t_obs_start=0.0, t_obs_end=1.0,
-                        modes=None, precision="fp64", flags=None, **unused):
-        """Relative-binning sums d_h, h_h (device complex128 [B] each) of the walkers
-        ``params`` in one fused kernel: waveform + response at the sparse grid ``freqs``
-        [L], mode sum, r = h / h0 (``h0`` [3, L]) and the bin terms with ``constants``
-        [4, 3, L] (likelihood.py:550-648, Likelihood.cu:20-123)."""
+    def heterodyne_setup(self, params, freqs, h0, constants, t_obs_start=0.0, t_obs_end=1.0,
+                         modes=None, flags=None):
+        """Everything a fused heterodyned evaluation of the walkers ``params`` reads, without
+        the evaluation: per-walker model records, observation limits and the output tensors.
+        Returns the arguments of ``bbhx_hdyn_fused`` (after ``orbits``, before ``precision``)
+        by name; the tensors stay referenced by the returned dict."""
         t = torch()
         (m1, m2, chi1z, chi2z, distance, phi_ref, f_ref, inc, lam, beta, psi, t_ref) = params
         ap = self.amp_phase_gen
@@ -248,15 +248,30 @@ class BBHWaveformFD:
         B, M, L = ap.num_bin_all, ap.num_modes, int(freqs.numel())
         rg = self.response_gen
         inc_d, lam_d, beta_d, psi_d, phi_d = (to_dev(atleast_1d(v)) for v in (inc, lam, beta, psi, phi_ref))
-        d_h = t.empty(B, dtype=t.complex128, device=device())
-        h_h = t.empty(B, dtype=t.complex128, device=device())
-        _lib.call("bbhx_hdyn_fused", rg.orbit_handle.ptr, _lib.dptr(d_h), _lib.dptr(h_h),
-                  _lib.dptr(ap._coeffs), _lib.dptr(ap.ells), _lib.dptr(ap.mms), _lib.dptr(phi_d),
-                  _lib.dptr(inc_d), _lib.dptr(lam_d), _lib.dptr(beta_d), _lib.dptr(psi_d),
-                  _lib.dptr(ap.t_ref_dev), float(ap.initial_t_val), _lib.dptr(ts_d), _lib.dptr(te_d),
-                  _lib.dptr(freqs), _lib.dptr(h0), _lib.dptr(constants), rg.TDItag_int,
-                  int(rg.rescaled), int(rg.tdi2), M, L, B, PRECISIONS[precision], _lib.stream())
-        return d_h, h_h
+        return dict(d_h=t.empty(B, dtype=t.complex128, device=device()),
+                    h_h=t.empty(B, dtype=t.complex128, device=device()),
+                    coeffs=ap._coeffs, ells=ap.ells, mms=ap.mms, phi_ref=phi_d, inc=inc_d,
+                    lam=lam_d, beta=beta_d, psi=psi_d, t_ref=ap.t_ref_dev,
+                    t_init=float(ap.initial_t_val), t_start=ts_d, t_end=te_d, freqs=freqs, h0=h0,
+                    consts=constants, TDItag=rg.TDItag_int, rescaled=int(rg.rescaled),
+                    tdi2=int(rg.tdi2), num_modes=M, length=L, num_bin_all=B)
+
+    HDYN_ARGS = ("d_h", "h_h", "coeffs", "ells", "mms", "phi_ref", "inc", "lam", "beta", "psi",
+                 "t_ref", "t_init", "t_start", "t_end", "freqs", "h0", "consts", "TDItag",
+                 "rescaled", "tdi2", "num_modes", "length", "num_bin_all")
+
+    def heterodyne_sums(self, params, freqs, h0, constants, t_obs_start=0.0, t_obs_end=1.0,
+                        modes=None, precision="fp64", flags=None, **unused):
+        """Relative-binning sums d_h, h_h (device complex128 [B] each) of the walkers
+        ``params`` in one fused kernel: waveform + response at the sparse grid ``freqs``
+        [L], mode sum, r = h / h0 (``h0`` [3, L]) and the bin terms with ``constants``
+        [4, 3, L] (likelihood.py:550-648, Likelihood.cu:20-123)."""
+        a = self.heterodyne_setup(params, freqs, h0, constants, t_obs_start, t_obs_end, modes,
+                                  flags)
+        vals = [a[k] if isinstance(a[k], (int, float)) else _lib.dptr(a[k]) for k in self.HDYN_ARGS]
+        _lib.call("bbhx_hdyn_fused", self.response_gen.orbit_handle.ptr, *vals,
+                  PRECISIONS[precision], _lib.stream())
+        return a["d_h"], a["h_h"]
 
     def heterodyne_grad(self, params, freqs, h0, constants, t_obs_start=0.0, t_obs_end=1.0,
                         modes=None, **unused):

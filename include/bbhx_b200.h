@@ -266,6 +266,33 @@ typedef struct {
 int bbhx_direct_like_multi(const bbhx_direct_group *groups, int num_groups, int precision,
                            int tile_bins, int ctas_per_sm, void *stream);
 
+/* One heterodyned (relative-binning) problem of an uneven batch: the arguments of
+   bbhx_hdyn_fused for its walkers (orbits handle, records from bbhx_phenomhm_setup, the
+   response inputs and t_ref [B], observation limits [B], its own sparse grid freqs [L],
+   h0 [3, L] and consts [4, 3, L] complex128); d_h, h_h [B] complex128 are overwritten. */
+typedef struct {
+  void *orbits;
+  void *d_h, *h_h;
+  const void *coeffs;
+  const int *ells, *mms;
+  const double *phi_ref, *inc, *lam, *beta, *psi, *t_ref;
+  double t_init;
+  const double *t_start, *t_end;
+  const double *freqs;
+  const void *h0, *consts;
+  int TDItag, rescaled, tdi2, num_modes, length, num_bin_all;
+} bbhx_hdyn_group;
+
+/* Direct and heterodyned problems with uneven grid lengths, mode sets, observation spans and
+   sparse grids in ONE persistent launch: the walkers of every heterodyned problem and the
+   (data tile, binary) items of every direct problem form one work range that the warps stride
+   through (no reference counterpart).  direct / het: HOST arrays of at most 64 descriptors
+   each (either may be empty); precision, tile_bins and ctas_per_sm as for
+   bbhx_direct_like_multi (the heterodyned walkers use the same precision).  Stream-ordered,
+   free of host synchronisation (graph-capturable). */
+int bbhx_uneven_like(const bbhx_direct_group *direct, int num_direct, const bbhx_hdyn_group *het,
+                     int num_het, int precision, int tile_bins, int ctas_per_sm, void *stream);
+
 /* fused interpolate + mode sum + noise weighting + <d|h>, <h|h> reduction; no templates are
  * stored (equivalent to InterpTDI followed by direct_like, waveformbuild.py:641-660 +
  * likelihood.py:177-214); d_h, h_h device complex [B], overwritten.

@@ -1,5 +1,6 @@
-"""Uneven batch: groups with different data streams (observation spans), grid lengths and mode
-sets evaluated in one persistent launch, autotuned, captured in a CUDA graph.
+"""Uneven batch: direct groups with different data streams (observation spans), grid lengths and
+mode sets, and heterodyned groups with different sparse grids, evaluated in one persistent
+launch, autotuned, captured in a CUDA graph.
 
 Checks: FP64 batch == per-group Likelihood.get_ll to 1e-9 relative (same arithmetic, different
 summation order of the tiles); mixed batch vs FP64 |dlnL| <= 2e-6 <h|h>; graph replay with new
@@ -40,21 +41,26 @@ def _problem(golden, golden_data):
                                 template_gen_kwargs=dict(kw), reference_gen_kwargs=dict(kw, length=1024),
                                 sens_mat=AET1SensitivityMatrix(golden_data["f"], tdi2=True))
     walkers = perturb_params(P[:, 0], 5, 3)
-    return direct, het, walkers, kw
+    # a second heterodyned problem: another reference point, a 96-point sparse grid
+    het2 = HeterodynedLikelihood(wave(), golden_data["f"], golden_data["data"], P[:, 2], 96,
+                                 template_gen_kwargs=dict(kw), reference_gen_kwargs=dict(kw, length=1024),
+                                 sens_mat=AET1SensitivityMatrix(golden_data["f"], tdi2=True))
+    walkers2 = perturb_params(P[:, 2], 7, 5)
+    return direct, [(het, walkers), (het2, walkers2)], kw
 
 
-def _batch(direct, het, walkers, kw, precision):
+def _batch(direct, hets, kw, precision):
     from bbhx_b200.uneven import DirectGroup, HetGroup, UnevenBatch
 
     dg = [DirectGroup(d["like"], d["params"], length=d["length"], modes=d["modes"], t_obs_start=0.0,
                       t_obs_end=d["tobs"]) for d in direct]
-    hg = [HetGroup(het, walkers, **kw)]
+    hg = [HetGroup(h, w, **kw) for h, w in hets]
     return UnevenBatch(dg, hg, precision=precision)
 
 
 def test_uneven_fp64_matches_per_group(golden, golden_data):
-    direct, het, walkers, kw = _problem(golden, golden_data)
-    batch = _batch(direct, het, walkers, kw, "fp64")
+    direct, hets, kw = _problem(golden, golden_data)
+    batch = _batch(direct, hets, kw, "fp64")
     out = [o.cpu().numpy() for o in batch.run()]
     shapes = [(t, c) for t in batch.autotuner.TILES for c in batch.autotuner.CTAS]
     assert batch.shape and all(sh in shapes for sh in batch.shape.values())
@@ -62,16 +68,33 @@ def test_uneven_fp64_matches_per_group(golden, golden_data):
         ref = d["like"].get_ll(d["params"], length=d["length"], modes=d["modes"], t_obs_start=0.0,
                                t_obs_end=d["tobs"])
         np.testing.assert_allclose(got, ref, rtol=1e-9, atol=1e-6)
-    het.precision = "fp64"
-    np.testing.assert_allclose(out[-1], het.get_ll(walkers, **kw), rtol=1e-12, atol=1e-8)
+    # the walkers inside the persistent launch == the single-problem heterodyne kernel
+    for (het, walkers), got in zip(hets, out[len(direct):]):
+        het.precision = "fp64"
+        np.testing.assert_allclose(got, het.get_ll(walkers, **kw), rtol=1e-12, atol=1e-8)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_uneven_heterodyned_only(golden, golden_data, precision):
+    """A batch of heterodyned problems alone (two sparse grids) in one launch equals each
+    problem's own fused evaluation in the same precision."""
+    from bbhx_b200.uneven import HetGroup, UnevenBatch
+
+    _, hets, kw = _problem(golden, golden_data)
+    batch = UnevenBatch([], [HetGroup(h, w, **kw) for h, w in hets], precision=precision,
+                        shape={precision: (4096, 3)})
+    out = [o.cpu().numpy() for o in batch.run()]
+    for (het, walkers), got in zip(hets, out):
+        het.precision = precision
+        np.testing.assert_allclose(got, het.get_ll(walkers, **kw), rtol=1e-12, atol=1e-8)
 
 
 def test_uneven_mixed_error_and_graph_replay(golden, golden_data):
-    direct, het, walkers, kw = _problem(golden, golden_data)
-    b64 = _batch(direct, het, walkers, kw, "fp64")
+    direct, hets, kw = _problem(golden, golden_data)
+    b64 = _batch(direct, hets, kw, "fp64")
     ref = [o.cpu().numpy() for o in b64.run()]
     hh = [g.h_h.real.cpu().numpy() for g in b64.direct]
-    bm = _batch(direct, het, walkers, kw, "mixed")
+    bm = _batch(direct, hets, kw, "mixed")
     out = [o.clone() for o in bm.capture()]
     for k, (a, r) in enumerate(zip(out, ref)):
         scale = hh[k] if k < len(hh) else np.abs(r)
@@ -83,7 +106,7 @@ def test_uneven_mixed_error_and_graph_replay(golden, golden_data):
     bm.set_params(1, newp)
     rep = [o.cpu().numpy().copy() for o in bm.replay()]
     direct[1]["params"] = newp
-    eager = _batch(direct, het, walkers, kw, "mixed")
+    eager = _batch(direct, hets, kw, "mixed")
     eager.shape = dict(bm.shape)
     ev = [o.cpu().numpy() for o in eager.run()]
     for a, b in zip(rep, ev):
