@@ -256,10 +256,11 @@ constexpr int HET_STRIP = 128;  // sparse frequencies whose residuals r are held
 struct HetArgs {
   cplx* d_h;
   cplx* h_h;
-  const ModeCoeffs* coeffs;  // [B, M]
-  const int* ells;           // [M]
-  const int* mms;            // [M]
-  const double* phi_ref;     // [B] each: the response-mode inputs
+  const ModeCoeffs* coeffs;    // [B, M]
+  const ResponseMode* rmodes;  // [B, M] (k_het_response_setup)
+  const int* ells;             // [M]
+  const int* mms;              // [M]
+  const double* phi_ref;       // [B] each: the response-mode inputs
   const double* inc;
   const double* lam;
   const double* beta;
@@ -375,9 +376,19 @@ __device__ __forceinline__ void het_bin(const HetArgs& A, int j, int ch, cplx cu
   him += B0.im * mag2 + 2.0 * B1.im * re01;
 }
 
+// Response-mode records of walkers [0, B) of A into A.rmodes (one thread per (walker, mode)),
+// set up once per evaluation outside the walker loop: inlined there, the set-up's code and
+// registers slow the per-point loop down.
+__device__ __forceinline__ void het_response_setup(const HetArgs& A, long long t) {
+  const int b = (int)(t / A.M), i = (int)(t % A.M);
+  ResponseMode r;
+  response_mode_setup(r, A.ells[i], A.mms[i], A.phi_ref[b], A.inc[b], A.lam[b], A.beta[b],
+                      A.psi[b]);
+  const_cast<ResponseMode*>(A.rmodes)[t] = r;
+}
+
 // Walker b of A by one warp, in the shared-memory slice `base` (HetSmemLayout(M, L, GH)):
-// records staged (PhenomHM copied, response modes set up by lanes < M), then the points and the
-// bin sums; lane 0 writes d_h[b], h_h[b] and flags a non-finite result in *nonfinite.  Bin j is
+// records staged (PhenomHM and response modes copied), then the points and the bin sums; lane 0 writes d_h[b], h_h[b] and flags a non-finite result in *nonfinite.  Bin j is
 // summed by lane (j - 1) mod 32 in increasing j, in both residual layouts.  GH (FP64 only): all
 // L residuals are kept and d lnL / d h is written to A.gh.
 template <bool MIXED, bool GH>
@@ -396,9 +407,10 @@ __device__ __forceinline__ void het_item(const HetArgs& A, int b, unsigned char*
     unsigned long long* dst = (unsigned long long*)sc;
     const int n = (int)(sizeof(ModeCoeffs) * A.M / 8);
     for (int i = lane; i < n; i += 32) dst[i] = src[i];
-    if (lane < A.M)
-      response_mode_setup(sr[lane], A.ells[lane], A.mms[lane], A.phi_ref[b], A.inc[b], A.lam[b],
-                          A.beta[b], A.psi[b]);
+    src = (const unsigned long long*)(A.rmodes + (size_t)b * A.M);
+    dst = (unsigned long long*)sr;
+    const int n2 = (int)(sizeof(ResponseMode) * A.M / 8);
+    for (int i = lane; i < n2; i += 32) dst[i] = src[i];
   }
   __syncwarp();
   if (MIXED) {

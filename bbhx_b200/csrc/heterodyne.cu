@@ -41,8 +41,15 @@ int take_nonfinite_heterodyne(cudaStream_t s, unsigned* any) {
 // One WARP per walker (het_item, het_item.cuh), each warp with its own slice of shared memory:
 // no block-wide barrier, so a warp never waits for another walker's slower points or for the
 // serial per-walker set-up of the others.
+__global__ void k_het_response_setup(HetArgs A) {
+  const long long n = (long long)A.B * A.M;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x)
+    het_response_setup(A, t);
+}
+
 template <bool MIXED, bool GH>
-__global__ void __launch_bounds__(HET_THREADS) k_het_fused(HetArgs A) {
+__global__ void __launch_bounds__(HET_THREADS, 4) k_het_fused(HetArgs A) {
   extern __shared__ __align__(16) unsigned char het_smem[];
   const int lane = threadIdx.x & 31;
   const int nwarps = blockDim.x >> 5;
@@ -70,21 +77,31 @@ inline int het_launch_shape(int M, int L, bool full_r, int* threads, size_t* sme
   return OK;
 }
 
+// Response-mode set-up into scratch, then the walkers; A.rmodes is set here.
 template <bool MIXED, bool GH>
-int launch_het(const HetArgs& A, cudaStream_t s) {
+int launch_het(HetArgs A, cudaStream_t s) {
   int threads = HET_THREADS;
   size_t smem = 0;
   int st = het_launch_shape(A.M, A.L, GH, &threads, &smem);
   if (st) return st;
+  ResponseMode* rm = nullptr;
+  BBHX_CHECK_CUDA(pool_alloc((void**)&rm, sizeof(ResponseMode) * (size_t)A.B * A.M, s));
+  A.rmodes = rm;
+  k_het_response_setup<<<grid_for((long long)A.B * A.M, 128), 128, 0, s>>>(A);
+  st = launch_status("k_het_response_setup");
   const long long wpc = threads / 32;
   const unsigned grid =
       (unsigned)std::min<long long>((A.B + wpc - 1) / wpc, (long long)sm_count() * 16);
-  st = cuda_status(cudaFuncSetAttribute(k_het_fused<MIXED, GH>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-                   "cudaFuncSetAttribute(k_het_fused)");
-  if (st) return st;
-  k_het_fused<MIXED, GH><<<grid, threads, smem, s>>>(A);
-  return launch_status("k_het_fused");
+  if (!st)
+    st = cuda_status(cudaFuncSetAttribute(k_het_fused<MIXED, GH>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                     "cudaFuncSetAttribute(k_het_fused)");
+  if (!st) {
+    k_het_fused<MIXED, GH><<<grid, threads, smem, s>>>(A);
+    st = launch_status("k_het_fused");
+  }
+  cudaFreeAsync(rm, s);
+  return st;
 }
 
 }  // namespace bbhx
@@ -109,6 +126,7 @@ HetArgs het_args(void* orbits, void* d_h, void* h_h, const void* coeffs, const i
   A.d_h = (cplx*)d_h;
   A.h_h = (cplx*)h_h;
   A.coeffs = (const ModeCoeffs*)coeffs;
+  A.rmodes = nullptr;
   A.ells = ells;
   A.mms = mms;
   A.phi_ref = phi_ref;

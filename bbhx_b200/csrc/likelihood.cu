@@ -1249,6 +1249,7 @@ __global__ void k_store_groups(MultiArgs M, MultiArgs* dst) {
 struct HetMulti {
   HetArgs g[FD_MAXGROUPS];
   long long woff[FD_MAXGROUPS + 1];  // walker offsets; woff[ngroups] = total walkers
+  long long roff[FD_MAXGROUPS + 1];  // (walker, mode) record offsets
   int ngroups;
 };
 
@@ -1267,6 +1268,16 @@ __device__ __forceinline__ int group_of(const long long* off, int n, long long q
     if (off[mid] <= q) lo = mid; else hi = mid;
   }
   return lo;
+}
+
+// Response-mode records of every walker of every heterodyned problem (thread per (walker,
+// mode) of the concatenated record range).
+__global__ void k_het_response_setup_multi(const HetMulti* __restrict__ HM, long long n) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int g = group_of(HM->roff, HM->ngroups, t);
+    het_response_setup(HM->g[g], t - HM->roff[g]);
+  }
 }
 
 // An uneven batch in ONE persistent launch: the walkers of every heterodyned problem (one
@@ -1610,7 +1621,7 @@ static int uneven_like(const bbhx_direct_group* groups, int num_groups,
   HetMulti HM;
   memset(&HM, 0, sizeof(HM));
   HM.ngroups = num_het;
-  long long walkers = 0;
+  long long walkers = 0, records = 0;
   size_t het_slot = 0;
   for (int g = 0; g < num_het; ++g) {
     const bbhx_hdyn_group& H = hgroups[g];
@@ -1622,10 +1633,13 @@ static int uneven_like(const bbhx_direct_group* groups, int num_groups,
                        H.consts, H.TDItag, H.rescaled, H.tdi2, H.num_modes, H.length,
                        H.num_bin_all);
     HM.woff[g] = walkers;
+    HM.roff[g] = records;
     walkers += H.num_bin_all;
+    records += (long long)H.num_bin_all * H.num_modes;
     het_slot = std::max(het_slot, align16(HetSmemLayout(H.num_modes, H.length, false).total));
   }
   HM.woff[num_het] = walkers;
+  HM.roff[num_het] = records;
   MultiArgs MA;
   memset(&MA, 0, sizeof(MA));
   MA.ngroups = num_groups;
@@ -1718,9 +1732,24 @@ static int uneven_like(const bbhx_direct_group* groups, int num_groups,
       k_store_groups<<<1, 256, 0, s>>>(MA, dMA);
       st = launch_status("k_store_groups");
     }
+    // response-mode records of all walkers (scratch), then the walker table
+    ResponseMode* rm = nullptr;
+    if (!st && records > 0) {
+      if (pool_alloc((void**)&rm, sizeof(ResponseMode) * records, s) != cudaSuccess) {
+        set_error("device allocation of the response records failed");
+        st = ERR_CUDA;
+      } else {
+        scratch.push_back(rm);
+        for (int g = 0; g < num_het; ++g) HM.g[g].rmodes = rm + HM.roff[g];
+      }
+    }
     if (!st) {
       k_store_het<<<1, 256, 0, s>>>(HM, dHM);
       st = launch_status("k_store_het");
+    }
+    if (!st && records > 0) {
+      k_het_response_setup_multi<<<grid_for(records, 128), 128, 0, s>>>(dHM, records);
+      st = launch_status("k_het_response_setup_multi");
     }
   }
   if (!st && items + walkers > 0) {
