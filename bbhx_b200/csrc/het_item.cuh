@@ -282,8 +282,8 @@ __host__ __device__ __forceinline__ size_t align16(size_t n) { return (n + 15) &
 
 // Shared memory of one warp (walker): ModeCoeffs[M] | ResponseMode[M] | AmpModeF[M] |
 // RespModeF[M] | residuals r, each region starting on a 16-byte boundary.  r holds
-// r = h / h0 of all L frequencies [3][L] when the adjoint is written (FULL_R), else one strip of
-// HET_STRIP frequencies plus the previous strip's last one [3][HET_STRIP + 1].
+// r = h / h0 of all L frequencies [3][L] (FULL), or one strip of HET_STRIP frequencies plus the
+// previous strip's last one [3][HET_STRIP + 1], which bounds the slice for any L.
 struct HetSmemLayout {
   size_t sr, sa, sf, rr, total;
   __host__ __device__ HetSmemLayout(int M, int L, bool full_r) {
@@ -295,26 +295,37 @@ struct HetSmemLayout {
   }
 };
 
-// h (three channels, conjugated mode sum) of walker b at sparse frequency f, as r = h / h0[j].
+// Typed views of one warp's slice (shared memory).
+struct HetSlice {
+  ModeCoeffs* sc;
+  ResponseMode* sr;
+  AmpModeF* sa;
+  RespModeF* sf;
+  cplx* rr;
+  __device__ __forceinline__ HetSlice(unsigned char* base, const HetSmemLayout& lay)
+      : sc((ModeCoeffs*)base), sr((ResponseMode*)(base + lay.sr)), sa((AmpModeF*)(base + lay.sa)),
+        sf((RespModeF*)(base + lay.sf)), rr((cplx*)(base + lay.rr)) {}
+};
+
+// r = h / h0 of walker b at sparse frequency index j (h: the conjugated mode sum in the three
+// channels), written to dst[0], dst[stride], dst[2 stride].
 template <bool MIXED>
-__device__ __forceinline__ void het_point(const HetArgs& A, const ModeCoeffs* sc,
-                                          const ResponseMode* sr, const AmpModeF* sa,
-                                          const RespModeF* sf, double tr, double ts, double te,
-                                          int j, cplx* r) {
+__device__ __forceinline__ void het_point(const HetArgs& A, const HetSlice& W, double tr,
+                                          double ts, double te, int j, cplx* dst, int stride) {
   const double f = A.freqs[j];
   double h[6] = {0, 0, 0, 0, 0, 0};
   for (int m = 0; m < A.M; ++m) {
     if (MIXED) {
-      const ModeCoeffs& c = sc[m];
+      const ModeCoeffs& c = W.sc[m];
       const double Mf = f * c.M_sec;
       double ph, tf;
       mode_phase_tf(c, Mf, &ph, &tf);  // FP64
       ph += f * (tr - A.t_init) * 2 * PI;
       tf += tr;
       if (!tf_gate(tf, ts, te)) continue;
-      const float ampf = c.phenomd_only ? phenomd_amp_f(sa[m], (float)Mf)
-                                        : mode_amp_f(sa[m], (float)Mf);
-      const TransferF T = response_point_mixed(sf[m], A.orb, f, tf, A.TDItag, A.rescaled, A.tdi2);
+      const float ampf = c.phenomd_only ? phenomd_amp_f(W.sa[m], (float)Mf)
+                                        : mode_amp_f(W.sa[m], (float)Mf);
+      const TransferF T = response_point_mixed(W.sf[m], A.orb, f, tf, A.TDItag, A.rescaled, A.tdi2);
       // phasor and channel products in FP64 (the scale factor stays FP64 as well)
       double sn, cs;
       sincos_cw(ph + T.phaseRdelay, &sn, &cs);
@@ -328,11 +339,11 @@ __device__ __forceinline__ void het_point(const HetArgs& A, const ModeCoeffs* sc
         h[2 * ch + 1] -= trr * api + tii * apr;
       }
     } else {
-      PointOut o = phm_eval_point(sc[m], f);
+      PointOut o = phm_eval_point(W.sc[m], f);
       o.phase += f * (tr - A.t_init) * 2 * PI;
       o.tf += tr;
       if (!tf_gate(o.tf, ts, te)) continue;
-      const Transfer T = response_point(sr[m], A.orb, f, o.tf, A.TDItag, A.rescaled, A.tdi2);
+      const Transfer T = response_point(W.sr[m], A.orb, f, o.tf, A.TDItag, A.rescaled, A.tdi2);
       const cplx ap = o.amp * expi(o.phase + T.phaseRdelay);
       const cplx Tc[3] = {T.L1, T.L2, T.L3};
 #pragma unroll
@@ -343,13 +354,12 @@ __device__ __forceinline__ void het_point(const HetArgs& A, const ModeCoeffs* sc
       }
     }
   }
-  // r = h / h0 per channel
 #pragma unroll
   for (int ch = 0; ch < 3; ++ch) {
     const cplx d = A.h0[(size_t)ch * A.L + j];
     const double den = d.re * d.re + d.im * d.im;
-    r[ch] = mk((h[2 * ch] * d.re + h[2 * ch + 1] * d.im) / den,
-               (h[2 * ch + 1] * d.re - h[2 * ch] * d.im) / den);
+    dst[ch * stride] = mk((h[2 * ch] * d.re + h[2 * ch + 1] * d.im) / den,
+                          (h[2 * ch + 1] * d.re - h[2 * ch] * d.im) / den);
   }
 }
 
@@ -387,47 +397,39 @@ __device__ __forceinline__ void het_response_setup(const HetArgs& A, long long t
   const_cast<ResponseMode*>(A.rmodes)[t] = r;
 }
 
-// Walker b of A by one warp, in the shared-memory slice `base` (HetSmemLayout(M, L, GH)):
-// records staged (PhenomHM and response modes copied), then the points and the bin sums; lane 0 writes d_h[b], h_h[b] and flags a non-finite result in *nonfinite.  Bin j is
-// summed by lane (j - 1) mod 32 in increasing j, in both residual layouts.  GH (FP64 only): all
-// L residuals are kept and d lnL / d h is written to A.gh.
-template <bool MIXED, bool GH>
-__device__ __forceinline__ void het_item(const HetArgs& A, int b, unsigned char* base, int lane,
+// Walker b of A by one warp in its slice W (HetSmemLayout(M, L, FULL)): records staged
+// (PhenomHM and response modes copied), then the points and the bin sums; lane 0 writes
+// d_h[b], h_h[b] and flags a non-finite result in *nonfinite.  Bin j is summed by lane
+// (j - 1) mod 32 in increasing j in both residual layouts, so both give the same sums.
+// GH (FP64, FULL): d lnL / d h is written to A.gh as well.
+template <bool MIXED, bool FULL, bool GH>
+__device__ __forceinline__ void het_item(const HetArgs& A, int b, const HetSlice& W, int lane,
                                          unsigned* nonfinite) {
   static_assert(!(MIXED && GH), "d lnL / d h is written by the FP64 form only");
-  const HetSmemLayout lay(A.M, A.L, GH);
-  ModeCoeffs* sc = (ModeCoeffs*)base;
-  ResponseMode* sr = (ResponseMode*)(base + lay.sr);
-  AmpModeF* sa = (AmpModeF*)(base + lay.sa);
-  RespModeF* sf = (RespModeF*)(base + lay.sf);
-  cplx* rr = (cplx*)(base + lay.rr);
+  static_assert(FULL || !GH, "the adjoint needs all residuals");
   __syncwarp();  // the previous walker's shared data is no longer in use
   {
     const unsigned long long* src = (const unsigned long long*)(A.coeffs + (size_t)b * A.M);
-    unsigned long long* dst = (unsigned long long*)sc;
+    unsigned long long* dst = (unsigned long long*)W.sc;
     const int n = (int)(sizeof(ModeCoeffs) * A.M / 8);
     for (int i = lane; i < n; i += 32) dst[i] = src[i];
     src = (const unsigned long long*)(A.rmodes + (size_t)b * A.M);
-    dst = (unsigned long long*)sr;
+    dst = (unsigned long long*)W.sr;
     const int n2 = (int)(sizeof(ResponseMode) * A.M / 8);
     for (int i = lane; i < n2; i += 32) dst[i] = src[i];
   }
   __syncwarp();
   if (MIXED) {
-    if (lane < A.M) build_amp_f(sa[lane], sc[lane]);
-    else if (lane >= 16 && lane < 16 + A.M) build_resp_f(sf[lane - 16], sr[lane - 16]);
+    if (lane < A.M) build_amp_f(W.sa[lane], W.sc[lane]);
+    else if (lane >= 16 && lane < 16 + A.M) build_resp_f(W.sf[lane - 16], W.sr[lane - 16]);
     __syncwarp();
   }
   const double tr = A.t_ref[b];
   const double ts = A.t_start[b], te = A.t_end[b];
+  cplx* rr = W.rr;
   double dre = 0, dim = 0, hre = 0, him = 0;
-  if (GH) {
-    for (int j = lane; j < A.L; j += 32) {
-      cplx r[3];
-      het_point<MIXED>(A, sc, sr, sa, sf, tr, ts, te, j, r);
-#pragma unroll
-      for (int ch = 0; ch < 3; ++ch) rr[ch * A.L + j] = r[ch];
-    }
+  if (FULL) {
+    for (int j = lane; j < A.L; j += 32) het_point<MIXED>(A, W, tr, ts, te, j, rr + j, A.L);
     __syncwarp();
     for (int j = 1 + lane; j < A.L; j += 32) {
 #pragma unroll
@@ -436,15 +438,11 @@ __device__ __forceinline__ void het_item(const HetArgs& A, int b, unsigned char*
     }
   } else {
     // strips of HET_STRIP frequencies; rr[ch][0] carries r of the previous strip's last one
-    constexpr int W = HET_STRIP + 1;
+    constexpr int SW = HET_STRIP + 1;
     for (int j0 = 0; j0 < A.L; j0 += HET_STRIP) {
       const int jn = min(HET_STRIP, A.L - j0);
-      for (int jj = lane; jj < jn; jj += 32) {
-        cplx r[3];
-        het_point<MIXED>(A, sc, sr, sa, sf, tr, ts, te, j0 + jj, r);
-#pragma unroll
-        for (int ch = 0; ch < 3; ++ch) rr[ch * W + 1 + jj] = r[ch];
-      }
+      for (int jj = lane; jj < jn; jj += 32)
+        het_point<MIXED>(A, W, tr, ts, te, j0 + jj, rr + 1 + jj, SW);
       __syncwarp();
       // bin j = j0 + jj (lane (j - 1) mod 32, as with all residuals held)
       for (int jj = (j0 + lane + 1) & 31; jj < jn; jj += 32) {
@@ -452,10 +450,10 @@ __device__ __forceinline__ void het_item(const HetArgs& A, int b, unsigned char*
         if (j < 1) continue;
 #pragma unroll
         for (int ch = 0; ch < 3; ++ch)
-          het_bin(A, j, ch, rr[ch * W + 1 + jj], rr[ch * W + jj], dre, dim, hre, him);
+          het_bin(A, j, ch, rr[ch * SW + 1 + jj], rr[ch * SW + jj], dre, dim, hre, him);
       }
       __syncwarp();
-      if (lane < 3) rr[lane * W] = rr[lane * W + jn];
+      if (lane < 3) rr[lane * SW] = rr[lane * SW + jn];
       __syncwarp();
     }
   }

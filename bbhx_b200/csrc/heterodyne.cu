@@ -38,9 +38,7 @@ int take_nonfinite_heterodyne(cudaStream_t s, unsigned* any) {
 }
 
 // ------------------------------------------------------------------ fused kernel
-// One WARP per walker (het_item, het_item.cuh), each warp with its own slice of shared memory:
-// no block-wide barrier, so a warp never waits for another walker's slower points or for the
-// serial per-walker set-up of the others.
+// Response-mode records of the walkers (thread per (walker, mode)).
 __global__ void k_het_response_setup(HetArgs A) {
   const long long n = (long long)A.B * A.M;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
@@ -48,15 +46,20 @@ __global__ void k_het_response_setup(HetArgs A) {
     het_response_setup(A, t);
 }
 
+// One WARP per walker (het_item, het_item.cuh), each warp with its own slice of shared memory:
+// no block-wide barrier, so a warp never waits for another walker's slower points or for the
+// serial per-walker set-up of the others.  All L residuals of the sparse grid are held in the
+// slice (the layout the adjoint needs; the strip layout of the uneven-batch kernel ran this
+// kernel ~20 % slower in the mixed form).
 template <bool MIXED, bool GH>
 __global__ void __launch_bounds__(HET_THREADS, 4) k_het_fused(HetArgs A) {
   extern __shared__ __align__(16) unsigned char het_smem[];
+  const HetSmemLayout lay(A.M, A.L, true);
   const int lane = threadIdx.x & 31;
   const int nwarps = blockDim.x >> 5;
-  unsigned char* base =
-      het_smem + (size_t)(threadIdx.x >> 5) * align16(HetSmemLayout(A.M, A.L, GH).total);
+  const HetSlice W(het_smem + (size_t)(threadIdx.x >> 5) * align16(lay.total), lay);
   for (int b = blockIdx.x * nwarps + (threadIdx.x >> 5); b < A.B; b += gridDim.x * nwarps)
-    het_item<MIXED, GH>(A, b, base, lane, &g_nonfinite_heterodyne);
+    het_item<MIXED, true, GH>(A, b, W, lane, &g_nonfinite_heterodyne);
 }
 
 // Warps (walkers) per CTA of k_het_fused and its dynamic shared memory: up to
@@ -82,7 +85,7 @@ template <bool MIXED, bool GH>
 int launch_het(HetArgs A, cudaStream_t s) {
   int threads = HET_THREADS;
   size_t smem = 0;
-  int st = het_launch_shape(A.M, A.L, GH, &threads, &smem);
+  int st = het_launch_shape(A.M, A.L, true, &threads, &smem);
   if (st) return st;
   ResponseMode* rm = nullptr;
   BBHX_CHECK_CUDA(pool_alloc((void**)&rm, sizeof(ResponseMode) * (size_t)A.B * A.M, s));

@@ -1318,8 +1318,10 @@ __global__ void __launch_bounds__(FD_WARPS * 32, (MIXED && !HET) ? 4 : 3)
         for (int i = lane; i < n8; i += 32) dst[i] = src[i];
         __syncwarp();
       }
-      het_item<MIXED, false>(hcur[warp], (int)(q - HM->woff[hg]), mine, lane,
-                             &g_nonfinite_likelihood);
+      const HetArgs& H = hcur[warp];
+      het_item<MIXED, false, false>(H, (int)(q - HM->woff[hg]),
+                                    HetSlice(mine, HetSmemLayout(H.M, H.L, false)), lane,
+                                    &g_nonfinite_likelihood);
     } else {
       const long long qd = q - nh;
       if (g < 0 || qd >= MA->off[g + 1] || qd < MA->off[g]) {

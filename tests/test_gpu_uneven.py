@@ -77,16 +77,19 @@ def test_uneven_fp64_matches_per_group(golden, golden_data):
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_uneven_heterodyned_only(golden, golden_data, precision):
     """A batch of heterodyned problems alone (two sparse grids) in one launch equals each
-    problem's own fused evaluation in the same precision."""
+    problem's own fused evaluation in the same precision: to 1e-12 in FP64; in the mixed form
+    the FP32 parts are compiled into two different kernels, so the two evaluations agree to the
+    mixed form's own accuracy (2e-6 relative, as mixed against FP64 elsewhere)."""
     from bbhx_b200.uneven import HetGroup, UnevenBatch
 
     _, hets, kw = _problem(golden, golden_data)
     batch = UnevenBatch([], [HetGroup(h, w, **kw) for h, w in hets], precision=precision,
                         shape={precision: (4096, 3)})
     out = [o.cpu().numpy() for o in batch.run()]
+    rtol = 1e-12 if precision == "fp64" else 2e-6
     for (het, walkers), got in zip(hets, out):
         het.precision = precision
-        np.testing.assert_allclose(got, het.get_ll(walkers, **kw), rtol=1e-12, atol=1e-8)
+        np.testing.assert_allclose(got, het.get_ll(walkers, **kw), rtol=rtol, atol=1e-8)
 
 
 def test_uneven_mixed_error_and_graph_replay(golden, golden_data):
