@@ -34,4 +34,8 @@ def __getattr__(name):
         from . import likelihood
 
         return getattr(likelihood, name)
+    if name == "workspace":
+        from .workspace import workspace
+
+        return workspace
     raise AttributeError(name)

@@ -1,4 +1,5 @@
 // Library-wide C-ABI helpers: error strings, version, stream sync, device pointer checks.
+#include <cstdint>
 #include <cstring>
 
 #include "capi_internal.cuh"
@@ -15,6 +16,9 @@ void set_error(const char* fmt, ...) {
 }
 
 const char* get_error() { return g_err; }
+
+static thread_local Arena g_arena;
+Arena& thread_arena() { return g_arena; }
 
 int sm_count() {
   static int cached[256] = {};
@@ -74,6 +78,26 @@ int bbhx_selftest_sincos(const double* x, double* out, int n, void* stream) {
 }
 
 const char* bbhx_last_error_string(void) { return bbhx::get_error(); }
+
+// Caller-provided workspace for the calling thread's scratch (see bbhx_b200.h).
+int bbhx_workspace_set(void* base, size_t bytes) {
+  bbhx::Arena& a = bbhx::thread_arena();
+  BBHX_REQUIRE(a.live == 0, "the current workspace is in use by %d scratch buffers", a.live);
+  if (base == nullptr) {
+    a = bbhx::Arena();
+    return bbhx::OK;
+  }
+  BBHX_REQUIRE(((uintptr_t)base & 255u) == 0, "workspace base must be 256-byte aligned");
+  BBHX_REQUIRE(bytes >= 256, "workspace must hold at least 256 bytes");
+  a.base = (char*)base;
+  a.size = bytes;
+  a.top = 0;
+  a.peak = 0;
+  a.live = 0;
+  return bbhx::OK;
+}
+
+size_t bbhx_workspace_peak(void) { return bbhx::thread_arena().peak; }
 
 int bbhx_version(void) { return 100; }
 

@@ -1,6 +1,7 @@
 // Host-side helpers shared by the C-ABI translation units: error capture and status codes.
 #pragma once
 
+#include <algorithm>
 #include <cstdarg>
 #include <cstdio>
 #include <initializer_list>
@@ -48,10 +49,64 @@ inline int launch_status(const char* kernel) {
 // cudaMallocAsync would re-map it.  Applied once per device to the device's default pool.
 int retain_pool_memory();
 
-// Stream-ordered scratch allocation used by the regular entry points.
+// Caller-provided workspace of the calling thread (bbhx_workspace_set): while one is set, the
+// entry points' scratch is carved from it, 256-byte aligned, by a bump pointer.  Released
+// pieces are reclaimed in stack order (the pieces above the highest live one), and the pointer
+// returns to the start when nothing is live (at the end of every entry point).
+struct Arena {
+  static constexpr int kDepth = 64;  // pieces tracked for stack-order reclamation
+  char* base = nullptr;
+  size_t size = 0, top = 0, peak = 0;
+  int live = 0, depth = 0;
+  size_t off[kDepth];
+  bool freed[kDepth];
+};
+Arena& thread_arena();
+
+// Scratch allocation used by the regular entry points: from the caller's workspace when one is
+// set, else stream-ordered from the device's default pool.
 inline cudaError_t pool_alloc(void** p, size_t bytes, cudaStream_t s) {
+  Arena& a = thread_arena();
+  if (a.base != nullptr) {
+    const size_t off = (a.top + 255) & ~(size_t)255;
+    a.peak = std::max(a.peak, off + bytes);
+    if (off + bytes > a.size) {
+      *p = nullptr;
+      return cudaErrorMemoryAllocation;
+    }
+    *p = a.base + off;
+    a.top = off + bytes;
+    ++a.live;
+    if (a.depth < Arena::kDepth) {
+      a.off[a.depth] = off;
+      a.freed[a.depth] = false;
+      ++a.depth;
+    }
+    return cudaSuccess;
+  }
   retain_pool_memory();
   return cudaMallocAsync(p, bytes, s);
+}
+
+// Releases scratch from pool_alloc (stream-ordered for pool memory).
+inline void pool_free(void* p, cudaStream_t s) {
+  if (p == nullptr) return;
+  Arena& a = thread_arena();
+  if (a.base != nullptr && (char*)p >= a.base && (char*)p < a.base + a.size) {
+    const size_t o = (size_t)((char*)p - a.base);
+    for (int i = a.depth - 1; i >= 0; --i)
+      if (a.off[i] == o && !a.freed[i]) {
+        a.freed[i] = true;
+        break;
+      }
+    while (a.depth > 0 && a.freed[a.depth - 1]) a.top = a.off[--a.depth];
+    if (--a.live == 0) {
+      a.top = 0;
+      a.depth = 0;
+    }
+    return;
+  }
+  cudaFreeAsync(p, s);
 }
 
 // Several stream-ordered allocations, all or none: on a failure the buffers already obtained
@@ -66,7 +121,7 @@ inline cudaError_t pool_alloc_all(cudaStream_t s,
   }
   if (e != cudaSuccess) {
     for (const auto& r : req) {
-      if (*r.first) cudaFreeAsync(*r.first, s);
+      pool_free(*r.first, s);
       *r.first = nullptr;
     }
   }

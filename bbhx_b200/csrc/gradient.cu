@@ -556,14 +556,14 @@ int bbhx_direct_like_grad(void* orbits, void* d_h, void* h_h, double* grad, cons
           wreg, TDItag, rescaled, tdi2, M, L, k0);
       st = launch_status("k_contract_direct");
     }
-    if (gh) cudaFreeAsync(gh, s);
-    if (off) cudaFreeAsync(off, s);
+    if (gh) pool_free(gh, s);
+    if (off) pool_free(off, s);
     b0 += nb;
   }
-  if (rD) cudaFreeAsync(rD, s);
-  if (cD) cudaFreeAsync(cD, s);
-  if (ybd) cudaFreeAsync(ybd, s);
-  if (start) cudaFreeAsync(start, s);
+  if (rD) pool_free(rD, s);
+  if (cD) pool_free(cD, s);
+  if (ybd) pool_free(ybd, s);
+  if (start) pool_free(start, s);
   return st;
 }
 

@@ -146,7 +146,7 @@ int bbhx_hdyn_constants(void* consts, double* ref, const double* f, const void* 
     k_hdyn_ref_sums<<<1, 32, 0, s>>>(partial, L - 1, ref);
     st = launch_status("k_hdyn_ref_sums");
   }
-  cudaFreeAsync(partial, s);
+  pool_free(partial, s);
   return st;
 }
 

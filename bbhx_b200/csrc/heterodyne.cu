@@ -103,7 +103,7 @@ int launch_het(HetArgs A, cudaStream_t s) {
     k_het_fused<MIXED, GH><<<grid, threads, smem, s>>>(A);
     st = launch_status("k_het_fused");
   }
-  cudaFreeAsync(rm, s);
+  pool_free(rm, s);
   return st;
 }
 
@@ -237,9 +237,9 @@ int bbhx_hdyn_grad(void* orbits, void* d_h, void* h_h, double* grad, const void*
       }
     }
   }
-  if (rD) cudaFreeAsync(rD, s);
-  if (cD) cudaFreeAsync(cD, s);
-  if (gh) cudaFreeAsync(gh, s);
+  if (rD) pool_free(rD, s);
+  if (cD) pool_free(cD, s);
+  if (gh) pool_free(gh, s);
   return st;
 }
 

@@ -1487,9 +1487,9 @@ int direct_fused_gh(cplx* gh, const long long* gh_off, double* d_h, double* h_h,
                                                             d_h + 2LL * b0, h_h + 2LL * b0);
     st = launch_status("k_fused_reduce");
   }
-  cudaFreeAsync(part, s);
-  cudaFreeAsync(segtab, s);
-  cudaFreeAsync(grid, s);
+  pool_free(part, s);
+  pool_free(segtab, s);
+  pool_free(grid, s);
   return st;
 }
 
@@ -1549,9 +1549,9 @@ int bbhx_direct_like(double* d_h, double* h_h, const double* data, const double*
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) st = cuda_status(e, "direct_like result copy");
   }
-  cudaFreeAsync(d_jobs, s);
-  cudaFreeAsync(d_part, s);
-  cudaFreeAsync(d_out, s);
+  pool_free(d_jobs, s);
+  pool_free(d_part, s);
+  pool_free(d_out, s);
   if (st) return st;
   bool finite = true;
   for (int b = 0; b < num_bin_all; ++b) {
@@ -1778,7 +1778,7 @@ static int uneven_like(const bbhx_direct_group* groups, int num_groups,
     k_fused_reduce_multi<<<grid_for(32LL * bins, 128), 128, 0, s>>>(dMA);
     st = launch_status("k_fused_reduce_multi");
   }
-  for (void* p : scratch) cudaFreeAsync(p, s);
+  for (void* p : scratch) pool_free(p, s);
   return st;
 }
 
@@ -1894,10 +1894,10 @@ int bbhx_direct_like_fused(double* d_h, double* h_h, const double* data_freqs, c
                                                               num_bin_all, d_h, h_h);
     st = launch_status("k_fused_reduce");
   }
-  cudaFreeAsync(sup, s);
-  cudaFreeAsync(part, s);
-  cudaFreeAsync(segtab, s);
-  cudaFreeAsync(grid, s);
+  pool_free(sup, s);
+  pool_free(part, s);
+  pool_free(segtab, s);
+  pool_free(grid, s);
   return st;
 }
 

@@ -354,7 +354,7 @@ int bbhx_waveform_amp_phase(double* waveform_out, const int* ells, const int* mm
                                                             length, num_bin_all, nullptr, 0.0);
     st = launch_status("k_phm_points");
   }
-  cudaFreeAsync(c, s);
+  pool_free(c, s);
   return st;
 }
 

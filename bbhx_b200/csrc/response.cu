@@ -180,7 +180,7 @@ int bbhx_LISA_response(void* orbits, double* response_out, const int* ells, cons
                                                        TDItag, rescaled, tdi2);
     st = launch_status("k_response_points");
   }
-  cudaFreeAsync(rm, s);
+  pool_free(rm, s);
   return st;
 }
 
@@ -209,7 +209,7 @@ int bbhx_waveform_response_fused(void* orbits, double* buf, const double* freqs,
         num_bin_all, t_ref, t_init, TDItag, rescaled, tdi2);
     st = launch_status("k_phm_response");
   }
-  cudaFreeAsync(rm, s);
+  pool_free(rm, s);
   return st;
 }
 

@@ -143,7 +143,7 @@ int bbhx_interpolate(const double* freqs, const double* y, double* B_, double* u
                                                       length, num_interp_params, S, use_smem,
                                                       scratch);
   int st = launch_status("k_spline");
-  if (scratch) cudaFreeAsync(scratch, s);
+  if (scratch) pool_free(scratch, s);
   return st;
 }
 

@@ -163,7 +163,7 @@ int bbhx_InterpTDI(const int64_t* template_ptrs, const double* data_freqs, const
   k_interp_tdi<<<dim3(gx, num_bin_all), threads, 0, s>>>(d_jobs, data_freqs, freqs, y, c1, c2, c3,
                                                          length, num_bin_all, num_modes);
   int st = launch_status("k_interp_tdi");
-  cudaFreeAsync(d_jobs, s);
+  pool_free(d_jobs, s);
   // the host job array must outlive the asynchronous copy
   cudaError_t e = cudaStreamSynchronize(s);
   if (!st && e != cudaSuccess) st = cuda_status(e, "InterpTDI sync");
@@ -214,7 +214,7 @@ int bbhx_fill_templates(void* out, const int64_t* template_ptrs, const int* star
       st = launch_status("k_fill_each");
     }
   }
-  cudaFreeAsync(d_jobs, s);
+  pool_free(d_jobs, s);
   // the host job array must outlive the asynchronous copy
   cudaError_t e = cudaStreamSynchronize(s);
   if (!st && e != cudaSuccess) st = cuda_status(e, "fill sync");

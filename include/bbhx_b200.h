@@ -30,6 +30,18 @@ extern "C" {
 
 /* ------------------------------------------------------------------ library */
 const char *bbhx_last_error_string(void);
+
+/* Caller-provided workspace: while one is set for the calling thread, every entry point takes
+   its scratch (segment tables, partial sums, per-(binary, mode) records, adjoint arrays, ...)
+   from [base, base + bytes) of device memory instead of the stream-ordered pool
+   (cudaMallocAsync), by a 256-byte aligned bump pointer that is rewound when each call
+   releases its scratch.  The workspace serves one stream at a time: calls on other streams must
+   not overlap with it.  base 256-byte aligned (null: back to the pool); refused (status 1)
+   while scratch is live.  A call that needs more than the workspace holds returns status 2;
+   bbhx_workspace_peak() is the largest extent the calling thread's calls have needed since the
+   workspace was set, including that failed request, so the caller can size it. */
+int bbhx_workspace_set(void *base, size_t bytes);
+size_t bbhx_workspace_peak(void);
 int bbhx_version(void);
 int bbhx_stream_synchronize(void *stream);
 /* synchronise the stream; return 4 if any likelihood output written since the previous call on
@@ -160,7 +172,8 @@ int bbhx_interpolate(const double *freqs, const double *y, double *B_, double *u
 
 /* ------------------------------------------------------------------ templates */
 /* replaces InterpTDI (src/bbhx/cutils/WaveformBuild.hh:6); template_ptrs, t_start, t_end,
- * inds_ptrs, inds_start, ind_lengths are [host] arrays (pointer arrays hold device addresses) */
+ * inds_ptrs, inds_start, ind_lengths are [host] arrays (pointer arrays hold device addresses);
+ * synchronises the stream once (the job table is copied from those host arrays) */
 int bbhx_InterpTDI(const int64_t *template_ptrs, const double *data_freqs, const double *freqs,
                    const double *y, const double *c1, const double *c2, const double *c3,
                    const double *t_start, const double *t_end, int length, int data_length,
@@ -170,7 +183,8 @@ int bbhx_InterpTDI(const int64_t *template_ptrs, const double *data_freqs, const
 /* fill=True placement of per-binary templates on the data grid (replaces the Python slice
  * additions of src/bbhx/waveformbuild.py:663-693; no C counterpart there); template_ptrs,
  * starts, lengths are [host] arrays (device addresses of [3, len] complex128 templates);
- * combine 0: out [B, 3, N], 1: out [3, N] summed in binary order; out zeroed by the caller */
+ * combine 0: out [B, 3, N], 1: out [3, N] summed in binary order; out zeroed by the caller;
+ * synchronises the stream once (the job table is copied from the host arrays) */
 int bbhx_fill_templates(void *out, const int64_t *template_ptrs, const int *starts,
                         const int *lengths, int num_bin_all, int data_length, int combine,
                         void *stream);
@@ -348,7 +362,8 @@ int bbhx_hdyn_grad(void *orbits, void *d_h, void *h_h, double *grad, const void 
    (bbhx_phenomhm_tf), both [B, M, L], and the L-frame observation limits t_obs_start_L,
    t_obs_end_L [s]; f_default or tf_default null holds the knots fixed.
    d_h, h_h: device complex128 [B], overwritten with <d|h>, <h|h> of the same evaluation (as
-   bbhx_direct_like_fused in FP64, so no separate likelihood call is needed). */
+   bbhx_direct_like_fused in FP64, so no separate likelihood call is needed).  Synchronises the
+   stream once: the binaries' support lengths are read on the host to batch the adjoint. */
 int bbhx_direct_like_grad(void *orbits, void *d_h, void *h_h, double *grad,
                           const double *params, const int *ells,
                           const int *mms, const double *qnm_table, int qnm_n, double dspin,

@@ -62,3 +62,20 @@ def test_backend_methods_mirror_the_reference_table():
     # host memory in a device slot is refused before anything reaches the library's kernels
     with pytest.raises(TypeError, match="device memory"):
         backend._device_addr(np.zeros(4), "f8", "x")
+
+
+def test_workspace_registration_rules():
+    """bbhx_workspace_set needs no GPU: it records the caller's buffer for the calling thread.
+    A 256-byte aligned base is taken, an unaligned one or a tiny size is refused (status 1), a
+    null base returns to the stream-ordered pool, and nothing has been needed yet (peak 0)."""
+    from bbhx_b200 import build_ext
+
+    build_ext.build()
+    lib = ctypes.CDLL(build_ext.OUT)
+    lib.bbhx_workspace_set.argtypes = [ctypes.c_void_p, ctypes.c_size_t]
+    lib.bbhx_workspace_peak.restype = ctypes.c_size_t
+    assert lib.bbhx_workspace_set(ctypes.c_void_p(1 << 20), 1 << 16) == 0
+    assert lib.bbhx_workspace_peak() == 0
+    assert lib.bbhx_workspace_set(ctypes.c_void_p((1 << 20) + 8), 1 << 16) == 1
+    assert lib.bbhx_workspace_set(ctypes.c_void_p(1 << 20), 16) == 1
+    assert lib.bbhx_workspace_set(ctypes.c_void_p(0), 0) == 0
