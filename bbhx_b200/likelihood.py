@@ -19,6 +19,18 @@ from .waveformbuild import PRECISIONS
 from .waveforms.phenomhm import raise_chi_flag
 
 
+def pack_lnl(d_h, h_h, d_d, out=None):
+    """lnL = -(d_d + Re h_h - 2 Re d_h) / 2 of complex [B] device sums, by the library's packing
+    kernel (bbhx_pack_lnl); ``out``: optional preallocated float64 [3 B] buffer (fixed address,
+    e.g. under CUDA graph capture).  Returns the lnL view [B]."""
+    B = d_h.numel()
+    if out is None:
+        out = torch().empty(3 * B, dtype=torch().float64, device=device())
+    _lib.call("bbhx_pack_lnl", _lib.dptr(out), _lib.dptr(d_h), _lib.dptr(h_h), float(d_d), B, 0,
+              _lib._VP(0), 0, _lib.stream())
+    return out[:B]
+
+
 class Likelihood:
     """Direct log-likelihood.  ``precision`` selects the arithmetic of the fused kernel:
     "fp64" (default, the parity form) or "mixed" (FP64 phase / t(f) / accumulations, FP32
@@ -122,11 +134,7 @@ class Likelihood:
         kw = {k: v for k, v in kw.items() if k in ("t_obs_start", "t_obs_end", "length", "modes")}
         d_h, h_h = self.waveform_gen.inner_products(rows, self.data_freqs, self.data_channels,
                                                     self.noise_factors, precision="fp64", **kw)
-        B = d_h.numel()
-        packed = torch().empty(3 * B, dtype=torch().float64, device=device())
-        _lib.call("bbhx_pack_lnl", _lib.dptr(packed), _lib.dptr(d_h), _lib.dptr(h_h),
-                  float(self.d_d), B, 0, _lib._VP(0), 0, _lib.stream())
-        return packed[:B]
+        return pack_lnl(d_h, h_h, self.d_d)
 
     def get_ll_and_grad(self, params, **waveform_kwargs):
         """lnL [B] and d lnL / d theta [B, 11] (device tensors); theta = (m1, m2, chi1z,
@@ -139,7 +147,7 @@ class Likelihood:
               if k in ("t_obs_start", "t_obs_end", "length", "modes")}
         d_h, h_h, grad = self.waveform_gen.direct_grad(P, self.data_freqs, self.data_channels,
                                                        self.noise_factors, **kw)
-        return -0.5 * (self.d_d + h_h.real - 2 * d_h.real), grad
+        return pack_lnl(d_h, h_h, self.d_d), grad
 
     def loglike_torch(self, params, **waveform_kwargs):
         """Differentiable lnL [B] tensor; the backward pass runs the gradient kernels."""
@@ -273,11 +281,7 @@ class HeterodynedLikelihood:
         d_h, h_h = self.template_gen.heterodyne_sums(rows, self.freqs, self._h0_flat,
                                                      self.data_constants, precision=precision,
                                                      flags=flags, **kw)
-        B = d_h.numel()
-        packed = torch().empty(3 * B, dtype=torch().float64, device=device())
-        _lib.call("bbhx_pack_lnl", _lib.dptr(packed), _lib.dptr(d_h), _lib.dptr(h_h),
-                  float(self.reference_d_d), B, 0, _lib._VP(0), 0, _lib.stream())
-        return packed[:B], (d_h, h_h)
+        return pack_lnl(d_h, h_h, self.reference_d_d), (d_h, h_h)
 
     def get_ll_and_grad(self, params, **waveform_kwargs):
         """lnL [B] and d lnL / d theta [B, 11] (device tensors) for walkers ``params``
@@ -291,8 +295,7 @@ class HeterodynedLikelihood:
         kw = {k: v for k, v in kw.items() if k in ("t_obs_start", "t_obs_end", "modes")}
         d_h, h_h, grad = self.template_gen.heterodyne_grad(P, self.freqs, self._h0_flat,
                                                            self.data_constants, **kw)
-        ll = -0.5 * (self.reference_d_d + h_h.real - 2 * d_h.real)
-        return ll, grad
+        return pack_lnl(d_h, h_h, self.reference_d_d), grad
 
     def loglike_torch(self, params, **waveform_kwargs):
         """Differentiable lnL: a [B] tensor whose backward pass runs the gradient kernels

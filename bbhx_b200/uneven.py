@@ -21,6 +21,7 @@ import itertools
 
 from . import _lib
 from .utils.arrays import device, torch
+from .likelihood import pack_lnl
 from .waveformbuild import PRECISIONS
 
 
@@ -79,6 +80,7 @@ class DirectGroup:
         self.M, self.L = M, L
         self.d_h = t.empty(B, dtype=t.complex128, device=device())
         self.h_h = t.empty(B, dtype=t.complex128, device=device())
+        self.packed = t.empty(3 * B, dtype=t.float64, device=device())
         self._keep = (buf, c1, c2, c3, x, ts, te)
         lk = self.like
         d32, n32 = lk.fp32_data() if precision == "mixed" else (None, None)
@@ -92,7 +94,7 @@ class DirectGroup:
                             _lib.dptr(n32).value if n32 is not None else None)
 
     def lnl(self):
-        return -0.5 * (self.like.d_d + self.h_h.real - 2 * self.d_h.real)
+        return pack_lnl(self.d_h, self.h_h, self.like.d_d, self.packed)
 
 
 class HetGroup:
@@ -115,12 +117,13 @@ class HetGroup:
                                               self.t_obs_start, self.t_obs_end, flags=self.flags)
         self._keep = a
         self.d_h, self.h_h = a["d_h"], a["h_h"]
+        self.packed = torch().empty(3 * self.size, dtype=torch().float64, device=device())
         fields = {k: (a[k] if isinstance(a[k], (int, float)) else _lib.dptr(a[k]).value)
                   for k in het.template_gen.HDYN_ARGS}
         return HdynGroupC(orbits=het.template_gen.response_gen.orbit_handle.ptr.value, **fields)
 
     def lnl(self):
-        return -0.5 * (self.het.reference_d_d + self.h_h.real - 2 * self.d_h.real)
+        return pack_lnl(self.d_h, self.h_h, self.het.reference_d_d, self.packed)
 
 
 class Autotuner:
