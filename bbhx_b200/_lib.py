@@ -61,6 +61,7 @@ _SIGS = {
     "bbhx_hdyn_grad": [_VP] * 9 + [_I, _D, _D] + [_VP] * 5 + [_I] * 7 + [_VP],
     "bbhx_direct_like_multi": [_VP, _I, _I, _I, _I, _VP],
     "bbhx_uneven_like": [_VP, _I, _VP, _I, _I, _I, _I, _VP],
+    "bbhx_uneven_batch": [_VP, _I, _VP, _I, _I, _I, _I, _VP],
     "bbhx_workspace_set": [_VP, ctypes.c_size_t],
     "bbhx_workspace_peak": [],
     "bbhx_direct_like_grad": [_VP] * 8 + [_I, _D, _D] + [_VP] * 3 + [_I] + [_VP] * 9 + [_D, _D] + [_I] * 7 + [_VP],

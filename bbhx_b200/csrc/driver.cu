@@ -10,6 +10,7 @@
 
 #include "capi_internal.cuh"
 #include "frames.cuh"
+#include "sparse_stages.cuh"
 
 namespace bbhx {
 
@@ -56,15 +57,14 @@ __global__ void k_step_front(double* __restrict__ out, double* __restrict__ t_st
                              const double* __restrict__ lam, const double* __restrict__ beta,
                              int B, int M, double tL_start, double tL_end, int* flags) {
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < B; b += gridDim.x * blockDim.x) {
-    const double a1 = m1[b], a2 = m2[b], x1 = chi1[b], x2 = chi2[b];
-    const bool sw = a1 < a2;
-    const double mm1 = sw ? a2 : a1, mm2 = sw ? a1 : a2;
-    out[0 * (long long)B + b] = mm1;
-    out[1 * (long long)B + b] = mm2;
-    out[2 * (long long)B + b] = sw ? x2 : x1;
-    out[3 * (long long)B + b] = sw ? x1 : x2;
-    out[4 * (long long)B + b] = mm1 * MSUN_SI;
-    out[5 * (long long)B + b] = mm2 * MSUN_SI;
+    const double x1 = chi1[b], x2 = chi2[b];
+    const FrontMasses fr = front_masses(m1[b], m2[b], x1, x2);
+    out[0 * (long long)B + b] = fr.m1;
+    out[1 * (long long)B + b] = fr.m2;
+    out[2 * (long long)B + b] = fr.chi1;
+    out[3 * (long long)B + b] = fr.chi2;
+    out[4 * (long long)B + b] = fr.m1_SI;
+    out[5 * (long long)B + b] = fr.m2_SI;
     if (flags != nullptr && fabs(x1) > 1.0) atomicOr(flags + 2, 1);  // chi1z out of range
     if (flags != nullptr && fabs(x2) > 1.0) atomicOr(flags + 2, 2);  // chi2z out of range
     if (t_start != nullptr) {

@@ -1605,7 +1605,7 @@ static_assert(sizeof(HetArgs) % 8 == 0 && sizeof(FusedArgs) % 8 == 0,
 // Direct and heterodyned problems in ONE persistent launch of k_uneven (direct groups only:
 // the same kernel with an empty walker range).  groups / hgroups: HOST arrays of descriptors
 // (device pointers inside).
-static int uneven_like(const bbhx_direct_group* groups, int num_groups,
+int uneven_like(const bbhx_direct_group* groups, int num_groups,
                        const bbhx_hdyn_group* hgroups, int num_het, int precision, int tile_bins,
                        int ctas_per_sm, cudaStream_t s) {
   BBHX_REQUIRE(num_groups >= 0 && num_groups <= FD_MAXGROUPS && (groups != nullptr || num_groups == 0),

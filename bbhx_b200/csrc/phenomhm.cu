@@ -9,6 +9,7 @@
 
 #include "capi_internal.cuh"
 #include "phenomhm_model.cuh"
+#include "sparse_stages.cuh"
 
 namespace bbhx {
 
@@ -21,30 +22,9 @@ __global__ void k_ringdown_hm(double* fring, double* fdamp, const double* m1, co
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
        t += (long long)gridDim.x * blockDim.x) {
     int b = (int)(t / M), i = (int)(t % M);
-    double fm, fs;
-    final_mass_spin(m1[b], m2[b], chi1[b], chi2[b], &fm, &fs);
-    cplx z = qnm_cw(fs, ells[i], mms[i]);
     long long o = (long long)b * out_stride + i;
-    fring[o] = (0.5 / PI) * z.re / fm;
-    fdamp[o] = (0.5 / PI) * z.im / fm;
+    ringdown_hm(m1[b], m2[b], chi1[b], chi2[b], ells[i], mms[i], &fring[o], &fdamp[o]);
   }
-}
-
-// PhenomD 22 ringdown/damping frequency from the tabulated QNM spline of the final spin
-// (PhenomHMWaveform.cu:1930-1993): index int((a + 1) / dspin), local cubic in (a - a_k).
-__device__ __forceinline__ void phenomd_qnm_lookup(double fs, double fm, const double* y_rd,
-                                                   const double* c1_rd, const double* c2_rd,
-                                                   const double* c3_rd, const double* y_dm,
-                                                   const double* c1_dm, const double* c2_dm,
-                                                   const double* c3_dm, double dspin,
-                                                   double* fr, double* fd) {
-  int ind = int((fs - (-1.0)) / dspin);
-  double x = fs - (dspin * ind + (-1.0));
-  double x2 = x * x, x3 = x2 * x;
-  double r = y_rd[ind] + c1_rd[ind] * x + c2_rd[ind] * x2 + c3_rd[ind] * x3;
-  double d = y_dm[ind] + c1_dm[ind] * x + c2_dm[ind] * x2 + c3_dm[ind] * x3;
-  *fr = r / fm;
-  *fd = d / fm;
 }
 
 __global__ void k_ringdown_d(double* fring, double* fdamp, const double* m1, const double* m2,
@@ -117,22 +97,7 @@ __global__ void k_phm_tf(double* tf_out, const double* freqs, const ModeCoeffs* 
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
        t += (long long)gridDim.x * blockDim.x) {
     long long bm = t / L;
-    const ModeCoeffs& c = coeffs[bm];
-    double Mf = freqs[t] * c.M_sec;
-    double Mfp;
-    if (c.phenomd_only)
-      Mfp = Mf;
-    else if (!(Mf > c.ph_fi))
-      Mfp = c.ph_ai * Mf;
-    else if (!(Mf > c.ph_fr))
-      Mfp = c.ph_am * Mf + c.ph_bm;
-    else
-      Mfp = c.ph_ar * Mf;
-    double tf;
-    if (c.phenomd_only)
-      tf = c.M_sec * phenomd_dphase(c.d, Mfp) / (2 * PI) - (c.t0 / (2. * PI) * c.M_sec);
-    else
-      tf = c.M_sec * (phenomd_dphase(c.d, Mfp) / (2. * PI)) - (c.t0 / (2. * PI) * c.M_sec);
+    const double tf = phm_tf_value(coeffs[bm], freqs[t]);
     tf_out[t] = tf + (t_ref ? t_ref[bm / M] : 0.0);
   }
 }
@@ -147,54 +112,12 @@ __global__ void k_tf_window(double* freqs_out, double* fminmax, const double* fr
                             const double* tf, const double* Tobs, int L, long long BM, int* err) {
   for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < BM;
        r += (long long)gridDim.x * blockDim.x) {
-    const double* f = freqs_in + r * L;
-    const double* x = tf + r * L;
-    double tmin = x[0], tmax = x[0], flo = f[0], fhi = f[0];
-    for (int i = 1; i < L; ++i) {
-      tmin = fmin(tmin, x[i]);
-      tmax = fmax(tmax, x[i]);
-      flo = fmin(flo, f[i]);
-      fhi = fmax(fhi, f[i]);
-    }
-    if (tmin < 0.0) {
-      int cnt = 0, seg = -1;
-      for (int i = 0; i < L - 1; ++i)
-        if ((0.0 < x[i + 1]) && (0.0 > x[i])) {
-          if (cnt == 0) seg = i;
-          ++cnt;
-        }
-      if (cnt != 1) {
-        atomicCAS(err, 0, 1);
-      } else {
-        double m = (f[seg + 1] - f[seg]) / (x[seg + 1] - x[seg]);
-        flo = m * (0.0 - x[seg]) + f[seg];
-      }
-    }
-    double To = Tobs[r];
-    if (tmax > To) {
-      int cnt = 0, seg = -1;
-      for (int i = 0; i < L - 1; ++i)
-        if ((To < x[i + 1]) && (To > x[i])) {
-          if (cnt == 0) seg = i;
-          ++cnt;
-        }
-      if (cnt != 1) {
-        atomicCAS(err, 0, 2);
-      } else {
-        double m = (f[seg + 1] - f[seg]) / (x[seg + 1] - x[seg]);
-        fhi = m * (To - x[seg]) + f[seg];
-      }
-    }
-    fminmax[2 * r] = flo;
-    fminmax[2 * r + 1] = fhi;
-    // numpy.logspace: y_k = k * step + start (two roundings), last y = stop, f = 10**y
-    double start = log10(flo), stop = log10(fhi);
-    double step = (stop - start) / (double)(L - 1);
+    const WindowEdges w = tf_window_edges(freqs_in + r * L, tf + r * L, L, Tobs[r]);
+    if (w.err) atomicCAS(err, 0, w.err);
+    fminmax[2 * r] = w.flo;
+    fminmax[2 * r + 1] = w.fhi;
     double* o = freqs_out + r * L;
-    for (int k = 0; k < L; ++k) {
-      double y = (k == L - 1) ? stop : __dadd_rn(__dmul_rn((double)k, step), start);
-      o[k] = pow(10.0, y);
-    }
+    for (int k = 0; k < L; ++k) o[k] = window_knot(k, L, w.flo, w.fhi);
   }
 }
 
@@ -202,17 +125,12 @@ __global__ void k_tf_window(double* freqs_out, double* fminmax, const double* fr
 __global__ void k_default_freqs(double* freqs, const double* m1, const double* m2, const int* mms,
                                 double mf_min, double mf_max, int M, int L, int B) {
   long long n = (long long)B * M * L;
-  double start = log10(mf_min), stop = log10(mf_max);
-  double step = (stop - start) / (double)(L - 1);
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
        t += (long long)gridDim.x * blockDim.x) {
     int k = (int)(t % L);
     int i = (int)((t / L) % M);
     int b = (int)(t / ((long long)L * M));
-    double y = (k == L - 1) ? stop : __dadd_rn(__dmul_rn((double)k, step), start);
-    double base = pow(10.0, y);
-    double Msec = (m1[b] + m2[b]) * MTSUN_SI;
-    freqs[t] = base / Msec * (double)mms[i] / 2;
+    freqs[t] = default_freq(k, L, mf_min, mf_max, m1[b], m2[b], mms[i]);
   }
 }
 

@@ -11,6 +11,7 @@
 #include "capi_internal.cuh"
 #include "phenomhm_model.cuh"
 #include "response_model.cuh"
+#include "sparse_stages.cuh"
 
 namespace bbhx {
 
@@ -61,21 +62,8 @@ __global__ void k_phm_response(double* buf, const double* freqs, const ModeCoeff
        t += (long long)gridDim.x * blockDim.x) {
     long long bm = t / L;
     int b = (int)(bm / M);
-    double f = freqs[t];
-    PointOut o = phm_eval_point(coeffs[bm], f);
-    double tr = t_ref[b];
-    o.phase += f * (tr - t_init) * 2 * PI;
-    o.tf += tr;
-    Transfer r = response_point(rmodes[bm], orb, f, o.tf, TDItag, rescaled, tdi2);
-    buf[t] = o.amp;
-    buf[n + t] = o.phase + r.phaseRdelay;
-    buf[2 * n + t] = o.tf;
-    buf[3 * n + t] = r.L1.re;
-    buf[4 * n + t] = r.L1.im;
-    buf[5 * n + t] = r.L2.re;
-    buf[6 * n + t] = r.L2.im;
-    buf[7 * n + t] = r.L3.re;
-    buf[8 * n + t] = r.L3.im;
+    phm_response_point(buf, n, t, freqs[t], coeffs[bm], rmodes[bm], orb, t_ref[b], t_init,
+                       TDItag, rescaled, tdi2);
   }
 }
 

@@ -1,0 +1,285 @@
+// Sparse-grid build of many direct-likelihood problems in one launch (uneven batches).
+//
+// Replaces, for every (binary, mode) row of every problem, the chain the single-problem path
+// runs as separate launches (the reference's phenomhm.py:270-614 + fastfdresponse.py:278-531 +
+// interpolate.py:77-211): mass ordering and SSB observation limits, ringdown frequencies,
+// PhenomHM record, default grid and its t(f), observation-window regrid, waveform + TDI
+// response at the new knots, orbit-coverage check and the not-a-knot spline of the nine
+// quantities.  One CTA owns one row: thread 0 sets up the row's records, the block evaluates the
+// grid points, thread 0 finds the window edges, the block evaluates the knots and solves the
+// spline in shared memory.  The steps are the same device functions as the separate kernels
+// (sparse_stages.cuh), so the outputs are the same numbers.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "capi_internal.cuh"
+#include "sparse_stages.cuh"
+
+namespace bbhx {
+
+constexpr int SB_MAXGROUPS = 64;
+constexpr int SB_THREADS = 256;
+constexpr size_t kBuildSmemMax = 200 * 1024;
+
+// One problem's build, in device memory (from bbhx_direct_source).
+struct BuildArgs {
+  const double* params;  // [12, B]
+  const int* ells;
+  const int* mms;
+  const double* qnm;  // [8, nq]
+  OrbitTables orb;
+  double dspin, mf_min, mf_max, t_init, tL_start, tL_end, orb_tmin, orb_tmax;
+  double *x, *y, *c1, *c2, *c3, *t_start, *t_end;
+  double* scratch;  // (4 + 9) L doubles per CTA when a row does not fit in shared memory
+  int* flags;
+  int nq, TDItag, rescaled, tdi2, run_phenomd, M, L, B;
+};
+
+struct BuildMulti {
+  BuildArgs g[SB_MAXGROUPS];
+  long long roff[SB_MAXGROUPS + 1];  // row offsets; roff[ngroups] = total rows
+  int ngroups;
+  int max_length;  // work-area stride of one CTA in `scratch`
+};
+
+__global__ void k_store_build(BuildMulti H, BuildMulti* dst) {
+  const int n = (int)(sizeof(BuildMulti) / sizeof(unsigned long long));
+  const unsigned long long* src = reinterpret_cast<const unsigned long long*>(&H);
+  unsigned long long* d = reinterpret_cast<unsigned long long*>(dst);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) d[i] = src[i];
+}
+
+__global__ void k_clear_build_flags(const BuildMulti* __restrict__ H) {
+  if (blockIdx.x < H->ngroups && threadIdx.x < 3) H->g[blockIdx.x].flags[threadIdx.x] = 0;
+}
+
+// row = (problem, binary, mode); rows of all problems, CTAs striding over them.
+__global__ void __launch_bounds__(SB_THREADS) k_sparse_build(const BuildMulti* __restrict__ H,
+                                                              int use_smem) {
+  extern __shared__ double sb_smem[];
+  __shared__ ModeCoeffs sc;
+  __shared__ ResponseMode sr;
+  __shared__ double s_val[4];  // m1, m2 (ordered, Msun), To, t_ref
+  __shared__ double s_edge[2];
+  const int tid = threadIdx.x;
+  const long long total = H->roff[H->ngroups];
+  for (long long row = blockIdx.x; row < total; row += gridDim.x) {
+    int lo = 0, hi = H->ngroups;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (H->roff[mid] <= row) lo = mid; else hi = mid;
+    }
+    const BuildArgs& A = H->g[lo];
+    const long long r = row - H->roff[lo];
+    const int b = (int)(r / A.M), m = (int)(r % A.M);
+    const int B = A.B, L = A.L;
+    const double* P = A.params;
+    const int ell = A.run_phenomd ? 2 : A.ells[m];
+    const int mm = A.run_phenomd ? 2 : A.mms[m];
+    double* work = use_smem ? sb_smem : A.scratch + (size_t)blockIdx.x * (4 + 9) * H->max_length;
+    __syncthreads();  // the previous row's records and work area are no longer read
+    if (tid == 0) {
+      // front end (k_step_front), ringdown frequencies, PhenomHM record (k_phm_setup)
+      const double x1 = P[2 * (size_t)B + b], x2 = P[3 * (size_t)B + b];
+      const FrontMasses fr = front_masses(P[0 * (size_t)B + b], P[1 * (size_t)B + b], x1, x2);
+      const double lam = P[8 * (size_t)B + b], beta = P[9 * (size_t)B + b];
+      const double ts = tssb_from_l(A.tL_start, lam, beta, 0.0);
+      const double te = tssb_from_l(A.tL_end, lam, beta, 0.0);
+      if (m == 0) {
+        A.t_start[b] = ts;
+        A.t_end[b] = te;
+        if (fabs(x1) > 1.0) atomicOr(A.flags + 2, 1);
+        if (fabs(x2) > 1.0) atomicOr(A.flags + 2, 2);
+      }
+      double rd22, dm22, rd, dm;
+      ringdown_d(fr.m1, fr.m2, fr.chi1, fr.chi2, A.qnm, A.nq, A.dspin, &rd22, &dm22);
+      if (A.run_phenomd) {
+        rd = rd22;
+        dm = dm22;
+      } else {
+        ringdown_hm(fr.m1, fr.m2, fr.chi1, fr.chi2, ell, mm, &rd, &dm);
+      }
+      phm_setup_mode(sc, fr.m1_SI, fr.m2_SI, fr.chi1, fr.chi2, P[4 * (size_t)B + b], ell, mm, rd,
+                     dm, rd22, dm22, A.run_phenomd);
+      s_val[0] = fr.m1;
+      s_val[1] = fr.m2;
+      s_val[2] = te - ts;
+      s_val[3] = P[11 * (size_t)B + b];
+    } else if (tid == 32) {  // response-mode record (k_response_setup), on another warp
+      response_mode_setup(sr, ell, mm, P[5 * (size_t)B + b], P[7 * (size_t)B + b],
+                          P[8 * (size_t)B + b], P[9 * (size_t)B + b], P[10 * (size_t)B + b]);
+    }
+    __syncthreads();
+    // default grid and its t(f) (k_default_freqs, k_phm_tf) in the work area
+    double* f0 = work;
+    double* tf0 = work + L;
+    const double tr = s_val[3];
+    for (int k = tid; k < L; k += blockDim.x) {
+      const double f = default_freq(k, L, A.mf_min, A.mf_max, s_val[0], s_val[1], mm);
+      f0[k] = f;
+      tf0[k] = phm_tf_value(sc, f) + tr;
+    }
+    __syncthreads();
+    if (tid == 0) {  // observation-window edges (k_tf_window)
+      const WindowEdges w = tf_window_edges(f0, tf0, L, s_val[2]);
+      if (w.err) atomicCAS(A.flags, 0, w.err);
+      s_edge[0] = w.flo;
+      s_edge[1] = w.fhi;
+    }
+    __syncthreads();
+    // knots, waveform + response (k_phm_response) and the orbit-coverage check (k_tf_range)
+    const long long n = (long long)B * A.M * L;
+    const long long ro = r * L;
+    bool bad = false;
+    for (int k = tid; k < L; k += blockDim.x) {
+      const double xk = window_knot(k, L, s_edge[0], s_edge[1]);
+      A.x[ro + k] = xk;
+      phm_response_point(A.y, n, ro + k, xk, sc, sr, A.orb, tr, A.t_init, A.TDItag, A.rescaled,
+                         A.tdi2);
+      const double tf = A.y[2 * n + ro + k];
+      bad = bad || (tf < A.orb_tmin) || (tf > A.orb_tmax);
+    }
+    if (__syncthreads_or(bad) && tid == 0) atomicOr(A.flags + 1, 1);
+    // not-a-knot spline of the nine quantities (k_spline), reading the row just written
+    spline_system(A.x + ro, A.y + ro, n, nullptr, A.c1 + ro, A.c2 + ro, A.c3 + ro, L, 9, work);
+  }
+}
+
+}  // namespace bbhx
+
+using namespace bbhx;
+
+namespace bbhx {
+int uneven_like(const bbhx_direct_group* groups, int num_groups, const bbhx_hdyn_group* hgroups,
+                int num_het, int precision, int tile_bins, int ctas_per_sm, cudaStream_t s);
+}
+
+extern "C" {
+
+int bbhx_uneven_batch(const bbhx_direct_source* direct, int num_direct,
+                      const bbhx_hdyn_group* het, int num_het, int precision, int tile_bins,
+                      int ctas_per_sm, void* stream) {
+  BBHX_REQUIRE(num_direct >= 0 && num_direct <= SB_MAXGROUPS &&
+                   (direct != nullptr || num_direct == 0),
+               "num_direct must be 0..%d", SB_MAXGROUPS);
+  cudaStream_t s = (cudaStream_t)stream;
+  BuildMulti H;
+  memset(&H, 0, sizeof(H));
+  H.ngroups = num_direct;
+  long long rows = 0;
+  int maxL = 3;
+  for (int g = 0; g < num_direct; ++g) {
+    const bbhx_direct_source& D = direct[g];
+    BBHX_REQUIRE(D.orbits && ((OrbitHandle*)D.orbits)->ready, "direct group %d: orbit information not added", g);
+    BBHX_REQUIRE(D.TDItag == 1 || D.TDItag == 2, "direct group %d: TDItag must be 1 or 2", g);
+    BBHX_REQUIRE(D.num_modes >= 1 && D.num_modes <= MAX_MODES && (!D.run_phenomd || D.num_modes == 1),
+                 "direct group %d: bad mode count %d", g, D.num_modes);
+    BBHX_REQUIRE(D.length >= 4 && D.num_bin_all >= 0 && D.qnm_n >= 2 && D.dspin > 0.0,
+                 "direct group %d: bad sizes", g);
+    BBHX_REQUIRE(D.x && D.y && D.c1 && D.c2 && D.c3 && D.t_start && D.t_end && D.flags && D.params,
+                 "direct group %d: missing buffer", g);
+    BuildArgs& A = H.g[g];
+    A.params = D.params;
+    A.ells = D.ells;
+    A.mms = D.mms;
+    A.qnm = D.qnm_table;
+    A.orb = ((OrbitHandle*)D.orbits)->tab;
+    A.dspin = D.dspin;
+    A.mf_min = D.mf_min;
+    A.mf_max = D.mf_max;
+    A.t_init = D.t_init;
+    A.tL_start = D.t_obs_start_L;
+    A.tL_end = D.t_obs_end_L;
+    A.orb_tmin = D.orbit_tmin;
+    A.orb_tmax = D.orbit_tmax;
+    A.x = D.x;
+    A.y = D.y;
+    A.c1 = D.c1;
+    A.c2 = D.c2;
+    A.c3 = D.c3;
+    A.t_start = D.t_start;
+    A.t_end = D.t_end;
+    A.flags = D.flags;
+    A.nq = D.qnm_n;
+    A.TDItag = D.TDItag;
+    A.rescaled = D.rescaled;
+    A.tdi2 = D.tdi2;
+    A.run_phenomd = D.run_phenomd;
+    A.M = D.num_modes;
+    A.L = D.length;
+    A.B = D.num_bin_all;
+    H.roff[g] = rows;
+    rows += (long long)D.num_bin_all * D.num_modes;
+    maxL = std::max(maxL, D.length);
+  }
+  H.roff[num_direct] = rows;
+  H.max_length = maxL;
+  int st = OK;
+  std::vector<void*> scratch;
+  if (num_direct > 0) {
+    const size_t smem = sizeof(double) * (size_t)(4 + 9) * maxL;
+    const bool use_smem = smem <= kBuildSmemMax;
+    const int nsm = sm_count();
+    const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>(rows, (long long)nsm * (use_smem ? 2 : 1)));
+    double* work = nullptr;
+    BuildMulti* dH = nullptr;
+    if (pool_alloc((void**)&dH, sizeof(BuildMulti), s) != cudaSuccess ||
+        (!use_smem && pool_alloc((void**)&work, sizeof(double) * grid * (size_t)(4 + 9) * maxL, s) != cudaSuccess)) {
+      set_error("device allocation for the sparse build failed");
+      st = ERR_CUDA;
+    }
+    if (dH) scratch.push_back(dH);
+    if (work) scratch.push_back(work);
+    if (!st) {
+      for (int g = 0; g < num_direct; ++g) H.g[g].scratch = work;
+      k_store_build<<<1, 256, 0, s>>>(H, dH);
+      st = launch_status("k_store_build");
+    }
+    if (!st) {
+      k_clear_build_flags<<<num_direct, 32, 0, s>>>(dH);
+      st = launch_status("k_clear_build_flags");
+    }
+    if (!st && rows > 0) {
+      if (use_smem)
+        st = cuda_status(cudaFuncSetAttribute(k_sparse_build,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)smem),
+                         "cudaFuncSetAttribute(k_sparse_build)");
+      if (!st) {
+        k_sparse_build<<<grid, SB_THREADS, use_smem ? smem : 0, s>>>(dH, use_smem ? 1 : 0);
+        st = launch_status("k_sparse_build");
+      }
+    }
+  }
+  if (!st) {
+    std::vector<bbhx_direct_group> groups(std::max(num_direct, 1));
+    for (int g = 0; g < num_direct; ++g) {
+      const bbhx_direct_source& D = direct[g];
+      bbhx_direct_group& G = groups[g];
+      G.data_freqs = D.data_freqs;
+      G.data = D.data;
+      G.noise = D.noise;
+      G.data_length = D.data_length;
+      G.x = D.x;
+      G.y = D.y;
+      G.c1 = D.c1;
+      G.c2 = D.c2;
+      G.c3 = D.c3;
+      G.t_start = D.t_start;
+      G.t_end = D.t_end;
+      G.num_modes = D.num_modes;
+      G.length = D.length;
+      G.num_bin_all = D.num_bin_all;
+      G.d_h = D.d_h;
+      G.h_h = D.h_h;
+      G.data32 = D.data32;
+      G.noise32 = D.noise32;
+    }
+    st = uneven_like(groups.data(), num_direct, het, num_het, precision, tile_bins, ctas_per_sm, s);
+  }
+  for (void* p : scratch) pool_free(p, s);
+  return st;
+}
+
+}  // extern "C"

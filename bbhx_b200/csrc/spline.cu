@@ -20,7 +20,7 @@
 // Entry L-1 of c1/c2/c3 (no segment) holds the last row's (upper, diagonal, lower)
 // coefficients, as the reference GPU path leaves them.
 #include "capi_internal.cuh"
-#include "tridiag.cuh"
+#include "sparse_stages.cuh"
 
 namespace bbhx {
 
@@ -31,78 +31,11 @@ __global__ void k_spline(const double* __restrict__ x, const double* __restrict_
                          double* slopes, double* c1, double* c2, double* c3, int L, int P,
                          long long S, bool use_smem, double* scratch) {
   extern __shared__ double smem[];
-  double* base = use_smem ? smem : scratch + (size_t)blockIdx.x * (4 + P) * L;
-  double* xs = base;
-  double* a = xs + L;
-  double* b = a + L;
-  double* c = b + L;
-  double* d = c + L;
+  double* work = use_smem ? smem : scratch + (size_t)blockIdx.x * (4 + P) * L;
   for (long long sys = blockIdx.x; sys < S; sys += gridDim.x) {
-    const double* xg = x + sys * L;
-    for (int i = threadIdx.x; i < L; i += blockDim.x) xs[i] = xg[i];
-    __syncthreads();
-    for (int i = threadIdx.x; i < L; i += blockDim.x) {
-      double dx1, dx2, dd;
-      int i0, i1, i2;
-      if (i == 0) {
-        i0 = 0; i1 = 1; i2 = 2;
-      } else if (i == L - 1) {
-        i0 = L - 3; i1 = L - 2; i2 = L - 1;
-      } else {
-        i0 = i - 1; i1 = i; i2 = i + 1;
-      }
-      dx1 = xs[i1] - xs[i0];
-      dx2 = xs[i2] - xs[i1];
-      dd = xs[i2] - xs[i0];
-      if (i == 0) {
-        a[i] = 0.0; b[i] = dx2; c[i] = dd;
-      } else if (i == L - 1) {
-        a[i] = dd; b[i] = dx1; c[i] = 0.0;
-      } else {
-        a[i] = dx2; b[i] = 2 * (dx1 + dx2); c[i] = dx1;
-      }
-      for (int p = 0; p < P; ++p) {
-        const double* yg = y + ((long long)p * S + sys) * L;
-        double y1 = yg[i1];
-        double m1 = (y1 - yg[i0]) / dx1;
-        double m2 = (yg[i2] - y1) / dx2;
-        double r;
-        if (i == 0)
-          r = ((dx1 + 2 * dd) * dx2 * m1 + dx1 * dx1 * m2) / dd;
-        else if (i == L - 1)
-          r = (dx2 * dx2 * m1 + (2 * dd + dx2) * dx1 * m2) / dd;
-        else
-          r = 3.0 * (dx2 * m1 + dx1 * m2);
-        d[(size_t)p * L + i] = r;
-      }
-    }
-    __syncthreads();
-    // keep the last row's matrix entries for the c1/c2/c3[L-1] convention
-    double last_a = a[L - 1], last_b = b[L - 1];
-    __syncthreads();
-    cr_solve(a, b, c, d, L, P, L);
-    for (int p = 0; p < P; ++p) {
-      const double* yg = y + ((long long)p * S + sys) * L;
-      long long o = ((long long)p * S + sys) * L;
-      const double* sp = d + (size_t)p * L;
-      for (int i = threadIdx.x; i < L; i += blockDim.x) {
-        double si = sp[i];
-        if (slopes) slopes[o + i] = si;
-        if (i < L - 1) {
-          double h = xs[i + 1] - xs[i];
-          double m = (yg[i + 1] - yg[i]) / h;
-          double t = (si + sp[i + 1] - 2 * m) / h;
-          c1[o + i] = si;
-          c2[o + i] = (m - si) / h - t;
-          c3[o + i] = t / h;
-        } else {
-          c1[o + i] = 0.0;
-          c2[o + i] = last_b;
-          c3[o + i] = last_a;
-        }
-      }
-    }
-    __syncthreads();
+    const long long o = sys * L;
+    spline_system(x + o, y + o, S * L, slopes ? slopes + o : nullptr, c1 + o, c2 + o, c3 + o, L,
+                  P, work);
   }
 }
 

@@ -21,6 +21,7 @@ import itertools
 
 from . import _lib
 from .utils.arrays import device, torch
+from .utils.constants import YRSID_SI
 from .likelihood import pack_lnl
 from .waveformbuild import PRECISIONS
 
@@ -52,6 +53,20 @@ class HdynGroupC(ctypes.Structure):
                 ("num_bin_all", ctypes.c_int)]
 
 
+class DirectSourceC(ctypes.Structure):
+    """Mirror of ``bbhx_direct_source`` (include/bbhx_b200.h)."""
+
+    _P, _D, _I = ctypes.c_void_p, ctypes.c_double, ctypes.c_int
+    _fields_ = [("orbits", _P), ("params", _P), ("ells", _P), ("mms", _P), ("qnm_table", _P),
+                ("qnm_n", _I), ("dspin", _D), ("mf_min", _D), ("mf_max", _D), ("t_init", _D),
+                ("t_obs_start_L", _D), ("t_obs_end_L", _D), ("orbit_tmin", _D),
+                ("orbit_tmax", _D), ("TDItag", _I), ("rescaled", _I), ("tdi2", _I),
+                ("run_phenomd", _I), ("num_modes", _I), ("length", _I), ("num_bin_all", _I),
+                ("x", _P), ("y", _P), ("c1", _P), ("c2", _P), ("c3", _P), ("t_start", _P),
+                ("t_end", _P), ("flags", _P), ("data_freqs", _P), ("data", _P), ("noise", _P),
+                ("data_length", _I), ("data32", _P), ("noise32", _P), ("d_h", _P), ("h_h", _P)]
+
+
 class DirectGroup:
     def __init__(self, like, params, length=1024, modes=None, t_obs_start=0.0, t_obs_end=1.0):
         t = torch()
@@ -65,33 +80,44 @@ class DirectGroup:
     def size(self):
         return self.params.shape[1]
 
-    def build(self, precision="fp64"):
-        """Sparse buffer + splines of this group (device; no host synchronisation)."""
+    def source(self, precision="fp64"):
+        """Descriptor of this group for bbhx_uneven_batch: its parameters and model settings,
+        and the device buffers the batch's sparse build and likelihood write (allocated here;
+        no host synchronisation)."""
+        from .waveforms.ringdownphenomd import dspin
+
         t = torch()
         wave = self.like.waveform_gen
-        rows = tuple(self.params[k] for k in range(12))
-        buf, ts, te = wave._sparse_buffer(rows, self.t_obs_start, self.t_obs_end, None, self.length,
-                                          self.modes, False, flags=self.flags)
-        B, M, L = wave.num_bin_all, wave.num_modes, wave.length
-        x = wave.amp_phase_gen.freqs
-        c1, c2, c3 = t.empty_like(buf), t.empty_like(buf), t.empty_like(buf)
-        _lib.call("bbhx_interpolate", _lib.dptr(x), _lib.dptr(buf), _lib._VP(0), _lib.dptr(c1),
-                  _lib.dptr(c2), _lib.dptr(c3), L, 9, M, B, _lib.stream())
+        ap, rg = wave.amp_phase_gen, wave.response_gen
+        ells, mms = ap.mode_tensors(self.modes)
+        B, M, L = self.size, int(ells.numel()), self.length
+        n = B * M * L
+        f64 = dict(dtype=t.float64, device=device())
+        x, y = t.empty(n, **f64), t.empty(9 * n, **f64)
+        c1, c2, c3 = t.empty(9 * n, **f64), t.empty(9 * n, **f64), t.empty(9 * n, **f64)
+        ts, te = t.empty(B, **f64), t.empty(B, **f64)
         self.M, self.L = M, L
         self.d_h = t.empty(B, dtype=t.complex128, device=device())
         self.h_h = t.empty(B, dtype=t.complex128, device=device())
-        self.packed = t.empty(3 * B, dtype=t.float64, device=device())
-        self._keep = (buf, c1, c2, c3, x, ts, te)
+        self.packed = t.empty(3 * B, **f64)
         lk = self.like
         d32, n32 = lk.fp32_data() if precision == "mixed" else (None, None)
-        return DirectGroupC(_lib.dptr(lk.data_freqs).value, _lib.dptr(lk.data_channels).value,
-                            _lib.dptr(lk.noise_factors).value, int(lk.data_freqs.numel()),
-                            _lib.dptr(x).value, _lib.dptr(buf).value, _lib.dptr(c1).value,
-                            _lib.dptr(c2).value, _lib.dptr(c3).value, _lib.dptr(ts).value,
-                            _lib.dptr(te).value, M, L, B, _lib.dptr(self.d_h).value,
-                            _lib.dptr(self.h_h).value,
-                            _lib.dptr(d32).value if d32 is not None else None,
-                            _lib.dptr(n32).value if n32 is not None else None)
+        tab = ap.qnm_table
+        self._keep = (x, y, c1, c2, c3, ts, te, ells, mms, tab)
+        p = lambda a: _lib.dptr(a).value if a is not None else None  # noqa: E731
+        return DirectSourceC(
+            orbits=rg.orbit_handle.ptr.value, params=p(self.params), ells=p(ells), mms=p(mms),
+            qnm_table=p(tab), qnm_n=int(tab.shape[1]), dspin=float(dspin),
+            mf_min=float(ap.mf_min), mf_max=float(ap.mf_max), t_init=float(ap.initial_t_val),
+            t_obs_start_L=float(self.t_obs_start * YRSID_SI),
+            t_obs_end_L=float(self.t_obs_end * YRSID_SI),
+            orbit_tmin=float(rg.orbits.t_base.min()), orbit_tmax=float(rg.orbits.t_base.max()),
+            TDItag=rg.TDItag_int, rescaled=int(rg.rescaled), tdi2=int(rg.tdi2),
+            run_phenomd=int(ap.run_phenomd), num_modes=M, length=L, num_bin_all=B, x=p(x),
+            y=p(y), c1=p(c1), c2=p(c2), c3=p(c3), t_start=p(ts), t_end=p(te),
+            flags=p(self.flags), data_freqs=p(lk.data_freqs), data=p(lk.data_channels),
+            noise=p(lk.noise_factors), data_length=int(lk.data_freqs.numel()), data32=p(d32),
+            noise32=p(n32), d_h=p(self.d_h), h_h=p(self.h_h))
 
     def lnl(self):
         return pack_lnl(self.d_h, self.h_h, self.like.d_d, self.packed)
@@ -202,19 +228,20 @@ class UnevenBatch:
         return out + [self.precision] * len(self.het)
 
     def _launch(self, descs, hdescs, precision, tile, ctas):
-        arr = (DirectGroupC * max(len(descs), 1))(*descs)
+        arr = (DirectSourceC * max(len(descs), 1))(*descs)
         harr = (HdynGroupC * max(len(hdescs), 1))(*hdescs)
-        _lib.call("bbhx_uneven_like", ctypes.cast(arr, ctypes.c_void_p), len(descs),
+        _lib.call("bbhx_uneven_batch", ctypes.cast(arr, ctypes.c_void_p), len(descs),
                   ctypes.cast(harr, ctypes.c_void_p), len(hdescs), PRECISIONS[precision],
                   int(tile), int(ctas), _lib.stream())
 
     def run(self):
         """All groups' lnL (list of device tensors, direct groups first).  The groups of each
-        precision class (direct and heterodyned) run in one persistent launch."""
+        precision class run as one call: one launch builds every direct group's sparse grids
+        and splines, one persistent launch evaluates every direct tile and heterodyned walker."""
         precs = self.group_precisions()
         classes = {}
         for g, pr in zip(self.direct, precs):
-            classes.setdefault(pr, ([], []))[0].append(g.build(pr))
+            classes.setdefault(pr, ([], []))[0].append(g.source(pr))
         for h, pr in zip(self.het, precs[len(self.direct):]):
             classes.setdefault(pr, ([], []))[1].append(h.build(pr))
         for pr, (descs, hdescs) in classes.items():

@@ -193,22 +193,8 @@ class PhenomHMAmpPhase:
         t = torch()
         pars = front if front is not None else step_front(m1, m2, chi1z, chi2z, flags=flags)[0]
         m1, m2, chi1z, chi2z, m1_SI, m2_SI = pars
-        if modes is not None:
-            key = tuple(tuple(md) for md in modes)
-            cache = self.__dict__.setdefault("_mode_tensors", {})
-            if key not in cache:  # device copies made once (no host copy inside graph capture)
-                self._sanity_check_modes([e for e, _ in modes], [m for _, m in modes])
-                cache[key] = (to_dev([ell for ell, mm in modes], t.int32),
-                              to_dev([mm for ell, mm in modes], t.int32))
-            ells, mms = cache[key]
-            self.modes = modes
-        else:
-            self.modes = self.allowable_modes
-            ells, mms = self.ells_default, self.mms_default
-        if self.run_phenomd:
-            ells = to_dev([2], t.int32)
-            mms = to_dev([2], t.int32)
-            self.modes = self.allowable_modes
+        ells, mms = self.mode_tensors(modes)
+        self.modes = modes if (modes is not None and not self.run_phenomd) else self.allowable_modes
         self.ells, self.mms = ells, mms
         num_modes = len(ells)
         num_bin_all = len(m1)
@@ -233,6 +219,25 @@ class PhenomHMAmpPhase:
                   _lib.dptr(distance), _lib.dptr(self.fringdown), _lib.dptr(self.fdamp), num_modes,
                   num_bin_all, int(self.run_phenomd), _lib.stream())
         self._m1, self._m2 = m1, m2
+
+    def mode_tensors(self, modes):
+        """Device (ells, mms) int32 tensors of a mode list (None: all allowable modes; (2, 2)
+        only for PhenomD), made once per list so that no host copy happens inside a CUDA graph
+        capture."""
+        t = torch()
+        cache = self.__dict__.setdefault("_mode_tensors", {})
+        key = None
+        if modes is not None:
+            key = tuple(tuple(md) for md in modes)
+            if key not in cache:
+                self._sanity_check_modes([e for e, _ in modes], [m for _, m in modes])
+                cache[key] = (to_dev([ell for ell, mm in modes], t.int32),
+                              to_dev([mm for ell, mm in modes], t.int32))
+        if self.run_phenomd:
+            if "phenomd" not in cache:
+                cache["phenomd"] = (to_dev([2], t.int32), to_dev([2], t.int32))
+            return cache["phenomd"]
+        return cache[key] if key is not None else (self.ells_default, self.mms_default)
 
     def _evaluate(self):
         _lib.call("bbhx_phenomhm_points", _lib.dptr(self.waveform_carrier), _lib.dptr(self._freqs),

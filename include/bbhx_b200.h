@@ -297,6 +297,36 @@ typedef struct {
   int TDItag, rescaled, tdi2, num_modes, length, num_bin_all;
 } bbhx_hdyn_group;
 
+/* One direct-likelihood problem of an uneven batch given by its binaries' parameters (the
+   sparse grids and splines are built inside bbhx_uneven_batch): params [12, B] device
+   (m1, m2 [Msun], chi1z, chi2z, distance [m], phi_ref, f_ref, inc, lam, beta, psi, t_ref [s]);
+   ells, mms [M] device; the PhenomD ringdown table [8, qnm_n] (y, c1, c2, c3 of the ringdown
+   and of the damping spline over the final spin, step dspin); mf_min, mf_max the default
+   grid's geometric-frequency bounds; t_init the phase reference time; the L-frame
+   observation limits [s]; the orbit table's time coverage [s].  Outputs of the build (device):
+   x [B, M, L] knots, y, c1, c2, c3 [9, B, M, L], t_start, t_end [B] and flags [3] (window
+   search 1 lower / 2 upper, orbit coverage, |chi| > 1 bits 1 / 2: the flags of
+   bbhx_step_front, bbhx_tf_window_regrid and bbhx_tf_range_check).  The data stream and the
+   likelihood outputs as in bbhx_direct_group. */
+typedef struct {
+  void *orbits;
+  const double *params;
+  const int *ells, *mms;
+  const double *qnm_table;
+  int qnm_n;
+  double dspin, mf_min, mf_max, t_init, t_obs_start_L, t_obs_end_L, orbit_tmin, orbit_tmax;
+  int TDItag, rescaled, tdi2, run_phenomd, num_modes, length, num_bin_all;
+  double *x, *y, *c1, *c2, *c3, *t_start, *t_end;
+  int *flags;
+  const double *data_freqs;
+  const void *data;
+  const double *noise;
+  int data_length;
+  const void *data32;
+  const float *noise32;
+  void *d_h, *h_h;
+} bbhx_direct_source;
+
 /* Direct and heterodyned problems with uneven grid lengths, mode sets, observation spans and
    sparse grids in ONE persistent launch: the walkers of every heterodyned problem and the
    (data tile, binary) items of every direct problem form one work range that the warps stride
@@ -306,6 +336,13 @@ typedef struct {
    free of host synchronisation (graph-capturable). */
 int bbhx_uneven_like(const bbhx_direct_group *direct, int num_direct, const bbhx_hdyn_group *het,
                      int num_het, int precision, int tile_bins, int ctas_per_sm, void *stream);
+
+/* A whole uneven batch from parameters: the sparse grids and splines of every direct problem
+   in ONE launch (one CTA per (binary, mode) row: records, default grid and t(f), window regrid,
+   waveform + response, coverage check, spline), then bbhx_uneven_like.  No reference
+   counterpart; stream-ordered and graph-capturable. */
+int bbhx_uneven_batch(const bbhx_direct_source *direct, int num_direct, const bbhx_hdyn_group *het,
+                      int num_het, int precision, int tile_bins, int ctas_per_sm, void *stream);
 
 /* fused interpolate + mode sum + noise weighting + <d|h>, <h|h> reduction; no templates are
  * stored (equivalent to InterpTDI followed by direct_like, waveformbuild.py:641-660 +

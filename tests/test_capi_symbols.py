@@ -79,3 +79,36 @@ def test_workspace_registration_rules():
     assert lib.bbhx_workspace_set(ctypes.c_void_p((1 << 20) + 8), 1 << 16) == 1
     assert lib.bbhx_workspace_set(ctypes.c_void_p(1 << 20), 16) == 1
     assert lib.bbhx_workspace_set(ctypes.c_void_p(0), 0) == 0
+
+
+def test_descriptor_layouts_match_the_header(tmp_path):
+    """The ctypes mirrors of the C descriptor structs (bbhx_b200.uneven) have the header's
+    sizes and field offsets (checked with the host C compiler on the header itself)."""
+    import shutil
+    import subprocess
+
+    import pytest
+
+    from bbhx_b200.uneven import DirectGroupC, DirectSourceC, HdynGroupC
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no host C compiler")
+    mirrors = {"bbhx_direct_group": DirectGroupC, "bbhx_hdyn_group": HdynGroupC,
+               "bbhx_direct_source": DirectSourceC}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "bbhx_b200.h"', "int main(void) {"]
+    for cname, py in mirrors.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'  printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", os.path.join(REPO, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {tuple(ln.split()[:2]): int(ln.split()[2]) for ln in out if ln.strip()}
+    for cname, py in mirrors.items():
+        assert got[(cname, "size")] == ctypes.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)

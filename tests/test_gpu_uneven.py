@@ -1,6 +1,7 @@
 """Uneven batch: direct groups with different data streams (observation spans), grid lengths and
-mode sets, and heterodyned groups with different sparse grids, evaluated in one persistent
-launch, autotuned, captured in a CUDA graph.
+mode sets, and heterodyned groups with different sparse grids: the direct groups' sparse grids
+and splines built in one launch from their parameters, then every direct tile and heterodyned
+walker evaluated in one persistent launch, autotuned, captured in a CUDA graph.
 
 Checks: FP64 batch == per-group Likelihood.get_ll to 1e-9 relative (same arithmetic, different
 summation order of the tiles); mixed batch vs FP64 |dlnL| <= 2e-6 <h|h>; graph replay with new
@@ -145,3 +146,30 @@ def test_uneven_mixed_routes_coarse_grids_to_fp64():
             assert np.all(err <= 1e-2), err
         else:
             assert np.all(err <= 2e-6 * np.maximum(hh, 1.0)), err
+
+
+def test_prebuilt_spline_entry_point_matches_the_batch(golden, golden_data):
+    """bbhx_direct_like_multi fed the sparse grids and splines that bbhx_uneven_batch built in
+    its fused build launch gives the batch's own direct lnL (FP64)."""
+    import ctypes
+
+    from bbhx_b200 import _lib
+    from bbhx_b200.uneven import DirectGroupC
+
+    direct, _, kw = _problem(golden, golden_data)
+    batch = _batch(direct, [], kw, "fp64")
+    batch.shape = {"fp64": (4096, 3)}
+    out = [o.cpu().numpy().copy() for o in batch.run()]
+    descs = []
+    for g in batch.direct:
+        x, y, c1, c2, c3, ts, te = g._keep[:7]
+        lk = g.like
+        p = lambda a: _lib.dptr(a).value  # noqa: E731
+        descs.append(DirectGroupC(p(lk.data_freqs), p(lk.data_channels), p(lk.noise_factors),
+                                  int(lk.data_freqs.numel()), p(x), p(y), p(c1), p(c2), p(c3),
+                                  p(ts), p(te), g.M, g.L, g.size, p(g.d_h), p(g.h_h), None, None))
+    arr = (DirectGroupC * len(descs))(*descs)
+    _lib.call("bbhx_direct_like_multi", ctypes.cast(arr, ctypes.c_void_p), len(descs), 0, 4096, 3,
+              _lib.stream())
+    for g, ref in zip(batch.direct, out):
+        np.testing.assert_allclose(g.lnl().cpu().numpy(), ref, rtol=1e-12, atol=1e-9)
