@@ -154,9 +154,11 @@ __global__ void k_hdyn(cplx* d_h, cplx* h_h, const cplx* __restrict__ r,
 // ---------------------------------------------------------------------------- fused direct
 // Support of each binary on the data grid (waveformbuild.py:136-177): [start, start+len) with
 // start = searchsorted(f, min x, 'right'), end = searchsorted(f, max x, 'right').
-__global__ void k_support(const double* __restrict__ x, int M, int L, int B,
-                          const double* __restrict__ data_freqs, int N, int* start, int* len) {
-  int b = blockIdx.x;
+// Support [start, start + len) on the data grid of binary b (whole block): the data bins in
+// [min x, max x] of its knots over all modes (searchsorted right of both ends).
+__device__ __forceinline__ void support_of(const double* __restrict__ x, int M, int L, int b,
+                                           const double* __restrict__ data_freqs, int N,
+                                           int* start, int* len) {
   double lo = 1e300, hi = -1e300;
   for (int t = threadIdx.x; t < M * L; t += blockDim.x) {
     double v = x[(long long)b * M * L + t];
@@ -195,6 +197,12 @@ __global__ void k_support(const double* __restrict__ x, int M, int L, int B,
     start[b] = s;
     len[b] = a - s;
   }
+  __syncthreads();
+}
+
+__global__ void k_support(const double* __restrict__ x, int M, int L, int B,
+                          const double* __restrict__ data_freqs, int N, int* start, int* len) {
+  support_of(x, M, L, blockIdx.x, data_freqs, N, start, len);
 }
 
 constexpr int FD_WARPS = 4;
@@ -257,7 +265,10 @@ struct GridInfo {
   unsigned pad;
 };
 
-__global__ void k_grid_detect(const double* __restrict__ f, int N, GridInfo* g) {
+// Uniform-grid check of f[0..N) by block bx of nb: every bin against the three candidate
+// spacings; block 0 also records k0 and the candidates.
+__device__ __forceinline__ void grid_detect_part(const double* __restrict__ f, int N, GridInfo* g,
+                                                 long long bx, long long nb) {
   unsigned ok = 0;
   double k0 = 0.0, cand[3] = {0.0, 0.0, 0.0};
   if (N >= 2) {
@@ -270,8 +281,7 @@ __global__ void k_grid_detect(const double* __restrict__ f, int N, GridInfo* g) 
     cand[1] = nextafter(dc, 0.0);
     cand[2] = nextafter(dc, 1e300);
     ok = (f0 > 0.0 && dfa > 0.0 && k0 >= 1.0 && kN < 4.0e15) ? 7u : 0u;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; ok && i < N;
-         i += (long long)gridDim.x * blockDim.x) {
+    for (long long i = bx * blockDim.x + threadIdx.x; ok && i < N; i += nb * blockDim.x) {
       const double kd = k0 + (double)i;
       const double fi = f[i];
 #pragma unroll
@@ -281,12 +291,16 @@ __global__ void k_grid_detect(const double* __restrict__ f, int N, GridInfo* g) 
   }
   ok = __reduce_and_sync(0xffffffffu, ok);
   if ((threadIdx.x & 31) == 0) atomicAnd(&g->ok, ok);
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (bx == 0 && threadIdx.x == 0) {
     g->k0 = k0;
     g->df[0] = cand[0];
     g->df[1] = cand[1];
     g->df[2] = cand[2];
   }
+}
+
+__global__ void k_grid_detect(const double* __restrict__ f, int N, GridInfo* g) {
+  grid_detect_part(f, N, g, blockIdx.x, gridDim.x);
 }
 
 // Launch the grid detection into g (device) on stream s.
@@ -300,39 +314,41 @@ inline int detect_grid(const double* f, int N, GridInfo* g, cudaStream_t s) {
 // Segment table: for every (tile, binary, mode) the spline segments holding the first and the
 // last data bin of the binary's support inside the tile (searchsorted(side='right') - 1 of
 // their frequencies), or (1, 0) when the tile misses the support.  One thread per entry.
+__device__ __forceinline__ int2 tile_segment_entry(long long t, const double* __restrict__ x,
+                                                   const double* __restrict__ data_freqs,
+                                                   const int* sup_start, const int* sup_len,
+                                                   int B, int M, int L, int tile_bins) {
+  const int m = (int)(t % M);
+  const long long tb = t / M;
+  const int b = (int)(tb % B);
+  const int tile = (int)(tb / B);
+  const int s0 = sup_start[b], s1 = s0 + sup_len[b];
+  const int i0 = max(tile * tile_bins, s0), i1 = min((tile + 1) * tile_bins, s1) - 1;
+  if (i0 > i1) return make_int2(1, 0);
+  const double* xr = x + ((long long)b * M + m) * L;
+  const double f0 = data_freqs[i0], f1 = data_freqs[i1];
+  int lo = 0, hi = L;  // count of knots <= f0
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (xr[mid] <= f0) lo = mid + 1; else hi = mid;
+  }
+  const int ka = lo - 1;
+  hi = L;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (xr[mid] <= f1) lo = mid + 1; else hi = mid;
+  }
+  return make_int2(ka, lo - 1);
+}
+
 __global__ void k_tile_segments(int2* tab, const double* __restrict__ x,
                                 const double* __restrict__ data_freqs, const int* sup_start,
                                 const int* sup_len, int B, int M, int L, int ntiles, int tile_bins) {
   const long long n = (long long)ntiles * B * M;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
-       t += (long long)gridDim.x * blockDim.x) {
-    const int m = (int)(t % M);
-    const long long tb = t / M;
-    const int b = (int)(tb % B);
-    const int tile = (int)(tb / B);
-    const int s0 = sup_start[b], s1 = s0 + sup_len[b];
-    const int i0 = max(tile * tile_bins, s0), i1 = min((tile + 1) * tile_bins, s1) - 1;
-    if (i0 > i1) {
-      tab[t] = make_int2(1, 0);
-      continue;
-    }
-    const double* xr = x + ((long long)b * M + m) * L;
-    const double f0 = data_freqs[i0], f1 = data_freqs[i1];
-    int lo = 0, hi = L;  // count of knots <= f0
-    while (lo < hi) {
-      int mid = (lo + hi) >> 1;
-      if (xr[mid] <= f0) lo = mid + 1; else hi = mid;
-    }
-    const int ka = lo - 1;
-    hi = L;
-    while (lo < hi) {
-      int mid = (lo + hi) >> 1;
-      if (xr[mid] <= f1) lo = mid + 1; else hi = mid;
-    }
-    tab[t] = make_int2(ka, lo - 1);
-  }
+       t += (long long)gridDim.x * blockDim.x)
+    tab[t] = tile_segment_entry(t, x, data_freqs, sup_start, sup_len, B, M, L, tile_bins);
 }
-
 
 // Cubic coefficients of one spline segment held by a lane: phase and t(f) always in FP64,
 // amplitude and the six transfer components in R (FP32 when mixed).
@@ -1234,6 +1250,7 @@ struct MultiArgs {
   FusedArgs g[FD_MAXGROUPS];
   long long off[FD_MAXGROUPS + 1];   // item offsets; off[ngroups] = total items
   long long boff[FD_MAXGROUPS + 1];  // binary offsets; boff[ngroups] = total binaries
+  long long soff[FD_MAXGROUPS + 1];  // segment-table entry offsets (ntiles B M per group)
   int ngroups;
 };
 
@@ -1605,6 +1622,34 @@ static_assert(sizeof(HetArgs) % 8 == 0 && sizeof(FusedArgs) % 8 == 0,
 // Direct and heterodyned problems in ONE persistent launch of k_uneven (direct groups only:
 // the same kernel with an empty walker range).  groups / hgroups: HOST arrays of descriptors
 // (device pointers inside).
+// The per-problem set-up of an uneven batch as one launch each over all problems: supports
+// (block per (problem, binary)), uniform-grid checks (blockIdx.y = problem) and segment tables
+// (thread per entry of the concatenated tables).
+__global__ void k_support_multi(const MultiArgs* __restrict__ MA) {
+  const long long gb = blockIdx.x;
+  const int g = group_of(MA->boff, MA->ngroups, gb);
+  const FusedArgs& A = MA->g[g];
+  support_of(A.x, A.M, A.L, (int)(gb - MA->boff[g]), A.data_freqs, A.N,
+             const_cast<int*>(A.sup_start), const_cast<int*>(A.sup_len));
+}
+
+__global__ void k_grid_detect_multi(const MultiArgs* __restrict__ MA) {
+  const FusedArgs& A = MA->g[blockIdx.y];
+  if (A.B == 0 || A.grid == nullptr) return;
+  grid_detect_part(A.data_freqs, A.N, const_cast<GridInfo*>(A.grid), blockIdx.x, gridDim.x);
+}
+
+__global__ void k_tile_segments_multi(const MultiArgs* __restrict__ MA) {
+  const long long n = MA->soff[MA->ngroups];
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int g = group_of(MA->soff, MA->ngroups, t);
+    const FusedArgs& A = MA->g[g];
+    const_cast<int2*>(A.segtab)[t - MA->soff[g]] = tile_segment_entry(
+        t - MA->soff[g], A.x, A.data_freqs, A.sup_start, A.sup_len, A.B, A.M, A.L, A.tile);
+  }
+}
+
 int uneven_like(const bbhx_direct_group* groups, int num_groups,
                        const bbhx_hdyn_group* hgroups, int num_het, int precision, int tile_bins,
                        int ctas_per_sm, cudaStream_t s) {
@@ -1647,7 +1692,7 @@ int uneven_like(const bbhx_direct_group* groups, int num_groups,
   MA.ngroups = num_groups;
   std::vector<void*> scratch;
   int st = OK;
-  long long items = 0, bins = 0;
+  long long items = 0, bins = 0, entries = 0;
   for (int g = 0; g < num_groups && !st; ++g) {
     const bbhx_direct_group& G = groups[g];
     if (G.num_bin_all < 0 || G.length < 2 || G.num_modes < 1 || G.num_modes > FD_MAXM ||
@@ -1684,42 +1729,47 @@ int uneven_like(const bbhx_direct_group* groups, int num_groups,
     A.grid = nullptr;
     MA.off[g] = items;
     MA.boff[g] = bins;
+    MA.soff[g] = entries;
     const long long nit = (long long)A.ntiles * A.B;
     items += nit;
     bins += A.B;
     if (A.B == 0) continue;
+    entries += nit * A.M;
     int* sup = nullptr;
     double* part = nullptr;
     int2* segtab = nullptr;
-    GridInfo* grid = nullptr;
     if (pool_alloc((void**)&sup, sizeof(int) * 2 * A.B, s) != cudaSuccess ||
         pool_alloc((void**)&part, sizeof(double) * 3 * nit, s) != cudaSuccess ||
-        pool_alloc((void**)&segtab, sizeof(int2) * nit * A.M, s) != cudaSuccess ||
-        pool_alloc((void**)&grid, sizeof(GridInfo), s) != cudaSuccess) {
+        pool_alloc((void**)&segtab, sizeof(int2) * nit * A.M, s) != cudaSuccess) {
       set_error("device allocation for group %d failed", g);
       st = ERR_CUDA;
     }
     if (sup) scratch.push_back(sup);
     if (part) scratch.push_back(part);
     if (segtab) scratch.push_back(segtab);
-    if (grid) scratch.push_back(grid);
     if (st) break;
     A.sup_start = sup;
     A.sup_len = sup + A.B;
     A.partials = part;
     A.segtab = segtab;
-    A.grid = grid;
-    k_support<<<A.B, 128, 0, s>>>(A.x, A.M, A.L, A.B, A.data_freqs, A.N, sup, sup + A.B);
-    st = launch_status("k_support");
-    if (!st) st = detect_grid(A.data_freqs, A.N, grid, s);
-    if (!st) {
-      k_tile_segments<<<grid_for(nit * A.M, 256, sm_count() * 64), 256, 0, s>>>(
-          segtab, A.x, A.data_freqs, sup, sup + A.B, A.B, A.M, A.L, A.ntiles, tile_bins);
-      st = launch_status("k_tile_segments");
-    }
   }
   MA.off[num_groups] = items;
   MA.boff[num_groups] = bins;
+  MA.soff[num_groups] = entries;
+  // uniform-grid records of all problems in one array (one initialisation)
+  GridInfo* grids = nullptr;
+  if (!st && num_groups > 0) {
+    if (pool_alloc((void**)&grids, sizeof(GridInfo) * num_groups, s) != cudaSuccess) {
+      set_error("device allocation of the grid records failed");
+      st = ERR_CUDA;
+    } else {
+      scratch.push_back(grids);
+      for (int g = 0; g < num_groups; ++g)
+        if (MA.g[g].B > 0) MA.g[g].grid = grids + g;
+      st = cuda_status(cudaMemsetAsync(grids, 0xff, sizeof(GridInfo) * num_groups, s),
+                       "grid record init");
+    }
+  }
   MultiArgs* dMA = nullptr;
   HetMulti* dHM = nullptr;
   if (!st) {
@@ -1733,6 +1783,19 @@ int uneven_like(const bbhx_direct_group* groups, int num_groups,
     if (!st) {
       k_store_groups<<<1, 256, 0, s>>>(MA, dMA);
       st = launch_status("k_store_groups");
+    }
+    if (!st && bins > 0) {
+      k_support_multi<<<(unsigned)bins, 128, 0, s>>>(dMA);
+      st = launch_status("k_support_multi");
+    }
+    if (!st && bins > 0) {
+      k_grid_detect_multi<<<dim3(std::max(1, sm_count() * 8 / std::max(1, num_groups)),
+                                 num_groups), 256, 0, s>>>(dMA);
+      st = launch_status("k_grid_detect_multi");
+    }
+    if (!st && entries > 0) {
+      k_tile_segments_multi<<<grid_for(entries, 256, sm_count() * 64), 256, 0, s>>>(dMA);
+      st = launch_status("k_tile_segments_multi");
     }
     // response-mode records of all walkers (scratch), then the walker table
     ResponseMode* rm = nullptr;
