@@ -5,9 +5,9 @@
 // interpolate.py:77-211): mass ordering and SSB observation limits, ringdown frequencies,
 // PhenomHM record, default grid and its t(f), observation-window regrid, waveform + TDI
 // response at the new knots, orbit-coverage check and the not-a-knot spline of the nine
-// quantities.  One CTA owns one row: thread 0 sets up the row's records, the block evaluates the
-// grid points, thread 0 finds the window edges, the block evaluates the knots and solves the
-// spline in shared memory.  The steps are the same device functions as the separate kernels
+// quantities.  A first launch sets up every row's records (thread per row); then one CTA owns
+// one row: it stages the row's records, evaluates the default grid, finds the window edges by
+// block reductions, evaluates the knots and solves the spline in shared memory.  The steps are the same device functions as the separate kernels
 // (sparse_stages.cuh), so the outputs are the same numbers.
 #include <algorithm>
 #include <cstring>
@@ -50,93 +50,200 @@ __global__ void k_store_build(BuildMulti H, BuildMulti* dst) {
   for (int i = threadIdx.x; i < n; i += blockDim.x) d[i] = src[i];
 }
 
+// Per-row set-up, made by k_row_records (thread per row) and staged into the row's CTA.
+struct RowRec {
+  ModeCoeffs c;    // PhenomHM record (k_phm_setup)
+  ResponseMode r;  // response-mode record (k_response_setup)
+  double m1, m2;   // ordered masses [Msun] (the default grid's total mass)
+  double To;       // SSB observation span (the regrid's upper edge)
+  double t_ref;
+};
+static_assert(sizeof(RowRec) % 8 == 0, "row records are staged in 8-byte words");
+
+__device__ __forceinline__ int build_group(const BuildMulti* H, long long row) {
+  int lo = 0, hi = H->ngroups;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (H->roff[mid] <= row) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+// Thread per (problem, binary, mode) row: front end (k_step_front: mass ordering, SSB
+// observation limits, |chi| checks), ringdown frequencies (k_ringdown_hm / k_ringdown_d), the
+// PhenomHM record (k_phm_setup) and the response-mode record.
+__global__ void k_row_records(const BuildMulti* __restrict__ H, RowRec* recs) {
+  const long long total = H->roff[H->ngroups];
+  for (long long row = blockIdx.x * (long long)blockDim.x + threadIdx.x; row < total;
+       row += (long long)gridDim.x * blockDim.x) {
+    const int g = build_group(H, row);
+    const BuildArgs& A = H->g[g];
+    const long long r = row - H->roff[g];
+    const int b = (int)(r / A.M), m = (int)(r % A.M);
+    const int B = A.B;
+    const double* P = A.params;
+    const int ell = A.run_phenomd ? 2 : A.ells[m];
+    const int mm = A.run_phenomd ? 2 : A.mms[m];
+    const double x1 = P[2 * (size_t)B + b], x2 = P[3 * (size_t)B + b];
+    const FrontMasses fr = front_masses(P[0 * (size_t)B + b], P[1 * (size_t)B + b], x1, x2);
+    const double lam = P[8 * (size_t)B + b], beta = P[9 * (size_t)B + b];
+    const double ts = tssb_from_l(A.tL_start, lam, beta, 0.0);
+    const double te = tssb_from_l(A.tL_end, lam, beta, 0.0);
+    if (m == 0) {
+      A.t_start[b] = ts;
+      A.t_end[b] = te;
+      if (fabs(x1) > 1.0) atomicOr(A.flags + 2, 1);
+      if (fabs(x2) > 1.0) atomicOr(A.flags + 2, 2);
+    }
+    double rd22, dm22, rd, dm;
+    ringdown_d(fr.m1, fr.m2, fr.chi1, fr.chi2, A.qnm, A.nq, A.dspin, &rd22, &dm22);
+    if (A.run_phenomd) {
+      rd = rd22;
+      dm = dm22;
+    } else {
+      ringdown_hm(fr.m1, fr.m2, fr.chi1, fr.chi2, ell, mm, &rd, &dm);
+    }
+    RowRec& R = recs[row];
+    ModeCoeffs c;
+    phm_setup_mode(c, fr.m1_SI, fr.m2_SI, fr.chi1, fr.chi2, P[4 * (size_t)B + b], ell, mm, rd, dm,
+                   rd22, dm22, A.run_phenomd);
+    R.c = c;
+    ResponseMode rm;
+    response_mode_setup(rm, ell, mm, P[5 * (size_t)B + b], P[7 * (size_t)B + b], lam, beta,
+                        P[10 * (size_t)B + b]);
+    R.r = rm;
+    R.m1 = fr.m1;
+    R.m2 = fr.m2;
+    R.To = te - ts;
+    R.t_ref = P[11 * (size_t)B + b];
+  }
+}
+
+// Window edges of one row by the whole block: the same minima, maxima and crossing counts as
+// tf_window_edges (sparse_stages.cuh) formed by block reductions, then the same formulas.
+__device__ inline WindowEdges tf_window_edges_block(const double* f, const double* x, int L,
+                                                    double To) {
+  __shared__ double r_d[4][32];
+  __shared__ int r_i[4][32];
+  __shared__ WindowEdges out;
+  double tmin = x[0], tmax = x[0], flo = f[0], fhi = f[0];
+  int c0 = 0, c1 = 0, s0 = L, s1 = L;
+  for (int i = threadIdx.x; i < L; i += blockDim.x) {
+    tmin = fmin(tmin, x[i]);
+    tmax = fmax(tmax, x[i]);
+    flo = fmin(flo, f[i]);
+    fhi = fmax(fhi, f[i]);
+    if (i < L - 1) {
+      if ((0.0 < x[i + 1]) && (0.0 > x[i])) {
+        ++c0;
+        s0 = min(s0, i);
+      }
+      if ((To < x[i + 1]) && (To > x[i])) {
+        ++c1;
+        s1 = min(s1, i);
+      }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    tmin = fmin(tmin, __shfl_xor_sync(0xffffffffu, tmin, o));
+    tmax = fmax(tmax, __shfl_xor_sync(0xffffffffu, tmax, o));
+    flo = fmin(flo, __shfl_xor_sync(0xffffffffu, flo, o));
+    fhi = fmax(fhi, __shfl_xor_sync(0xffffffffu, fhi, o));
+    c0 += __shfl_xor_sync(0xffffffffu, c0, o);
+    c1 += __shfl_xor_sync(0xffffffffu, c1, o);
+    s0 = min(s0, __shfl_xor_sync(0xffffffffu, s0, o));
+    s1 = min(s1, __shfl_xor_sync(0xffffffffu, s1, o));
+  }
+  const int w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    r_d[0][w] = tmin; r_d[1][w] = tmax; r_d[2][w] = flo; r_d[3][w] = fhi;
+    r_i[0][w] = c0; r_i[1][w] = c1; r_i[2][w] = s0; r_i[3][w] = s1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < nw; ++k) {
+      tmin = fmin(tmin, r_d[0][k]);
+      tmax = fmax(tmax, r_d[1][k]);
+      flo = fmin(flo, r_d[2][k]);
+      fhi = fmax(fhi, r_d[3][k]);
+      c0 += r_i[0][k];
+      c1 += r_i[1][k];
+      s0 = min(s0, r_i[2][k]);
+      s1 = min(s1, r_i[3][k]);
+    }
+    WindowEdges e;
+    e.err = 0;
+    e.flo = flo;
+    e.fhi = fhi;
+    if (tmin < 0.0) {
+      if (c0 != 1) {
+        e.err = 1;
+      } else {
+        double m = (f[s0 + 1] - f[s0]) / (x[s0 + 1] - x[s0]);
+        e.flo = m * (0.0 - x[s0]) + f[s0];
+      }
+    }
+    if (tmax > To) {
+      if (c1 != 1) {
+        if (e.err == 0) e.err = 2;
+      } else {
+        double m = (f[s1 + 1] - f[s1]) / (x[s1 + 1] - x[s1]);
+        e.fhi = m * (To - x[s1]) + f[s1];
+      }
+    }
+    out = e;
+  }
+  __syncthreads();
+  return out;
+}
+
 __global__ void k_clear_build_flags(const BuildMulti* __restrict__ H) {
   if (blockIdx.x < H->ngroups && threadIdx.x < 3) H->g[blockIdx.x].flags[threadIdx.x] = 0;
 }
 
-// row = (problem, binary, mode); rows of all problems, CTAs striding over them.
+// row = (problem, binary, mode); rows of all problems, CTAs striding over them.  The row's
+// records come from k_row_records.
 __global__ void __launch_bounds__(SB_THREADS) k_sparse_build(const BuildMulti* __restrict__ H,
+                                                              const RowRec* __restrict__ recs,
                                                               int use_smem) {
   extern __shared__ double sb_smem[];
-  __shared__ ModeCoeffs sc;
-  __shared__ ResponseMode sr;
-  __shared__ double s_val[4];  // m1, m2 (ordered, Msun), To, t_ref
-  __shared__ double s_edge[2];
+  __shared__ RowRec R;
   const int tid = threadIdx.x;
   const long long total = H->roff[H->ngroups];
   for (long long row = blockIdx.x; row < total; row += gridDim.x) {
-    int lo = 0, hi = H->ngroups;
-    while (hi - lo > 1) {
-      const int mid = (lo + hi) >> 1;
-      if (H->roff[mid] <= row) lo = mid; else hi = mid;
-    }
-    const BuildArgs& A = H->g[lo];
-    const long long r = row - H->roff[lo];
-    const int b = (int)(r / A.M), m = (int)(r % A.M);
+    const int g = build_group(H, row);
+    const BuildArgs& A = H->g[g];
+    const long long r = row - H->roff[g];
     const int B = A.B, L = A.L;
-    const double* P = A.params;
-    const int ell = A.run_phenomd ? 2 : A.ells[m];
-    const int mm = A.run_phenomd ? 2 : A.mms[m];
+    const int mm = A.run_phenomd ? 2 : A.mms[(int)(r % A.M)];
     double* work = use_smem ? sb_smem : A.scratch + (size_t)blockIdx.x * (4 + 9) * H->max_length;
     __syncthreads();  // the previous row's records and work area are no longer read
-    if (tid == 0) {
-      // front end (k_step_front), ringdown frequencies, PhenomHM record (k_phm_setup)
-      const double x1 = P[2 * (size_t)B + b], x2 = P[3 * (size_t)B + b];
-      const FrontMasses fr = front_masses(P[0 * (size_t)B + b], P[1 * (size_t)B + b], x1, x2);
-      const double lam = P[8 * (size_t)B + b], beta = P[9 * (size_t)B + b];
-      const double ts = tssb_from_l(A.tL_start, lam, beta, 0.0);
-      const double te = tssb_from_l(A.tL_end, lam, beta, 0.0);
-      if (m == 0) {
-        A.t_start[b] = ts;
-        A.t_end[b] = te;
-        if (fabs(x1) > 1.0) atomicOr(A.flags + 2, 1);
-        if (fabs(x2) > 1.0) atomicOr(A.flags + 2, 2);
-      }
-      double rd22, dm22, rd, dm;
-      ringdown_d(fr.m1, fr.m2, fr.chi1, fr.chi2, A.qnm, A.nq, A.dspin, &rd22, &dm22);
-      if (A.run_phenomd) {
-        rd = rd22;
-        dm = dm22;
-      } else {
-        ringdown_hm(fr.m1, fr.m2, fr.chi1, fr.chi2, ell, mm, &rd, &dm);
-      }
-      phm_setup_mode(sc, fr.m1_SI, fr.m2_SI, fr.chi1, fr.chi2, P[4 * (size_t)B + b], ell, mm, rd,
-                     dm, rd22, dm22, A.run_phenomd);
-      s_val[0] = fr.m1;
-      s_val[1] = fr.m2;
-      s_val[2] = te - ts;
-      s_val[3] = P[11 * (size_t)B + b];
-    } else if (tid == 32) {  // response-mode record (k_response_setup), on another warp
-      response_mode_setup(sr, ell, mm, P[5 * (size_t)B + b], P[7 * (size_t)B + b],
-                          P[8 * (size_t)B + b], P[9 * (size_t)B + b], P[10 * (size_t)B + b]);
+    {
+      const unsigned long long* src = reinterpret_cast<const unsigned long long*>(recs + row);
+      unsigned long long* dst = reinterpret_cast<unsigned long long*>(&R);
+      for (int i = tid; i < (int)(sizeof(RowRec) / 8); i += blockDim.x) dst[i] = src[i];
     }
     __syncthreads();
     // default grid and its t(f) (k_default_freqs, k_phm_tf) in the work area
     double* f0 = work;
     double* tf0 = work + L;
-    const double tr = s_val[3];
     for (int k = tid; k < L; k += blockDim.x) {
-      const double f = default_freq(k, L, A.mf_min, A.mf_max, s_val[0], s_val[1], mm);
+      const double f = default_freq(k, L, A.mf_min, A.mf_max, R.m1, R.m2, mm);
       f0[k] = f;
-      tf0[k] = phm_tf_value(sc, f) + tr;
+      tf0[k] = phm_tf_value(R.c, f) + R.t_ref;
     }
     __syncthreads();
-    if (tid == 0) {  // observation-window edges (k_tf_window)
-      const WindowEdges w = tf_window_edges(f0, tf0, L, s_val[2]);
-      if (w.err) atomicCAS(A.flags, 0, w.err);
-      s_edge[0] = w.flo;
-      s_edge[1] = w.fhi;
-    }
-    __syncthreads();
+    const WindowEdges w = tf_window_edges_block(f0, tf0, L, R.To);  // (k_tf_window)
+    if (tid == 0 && w.err) atomicCAS(A.flags, 0, w.err);
     // knots, waveform + response (k_phm_response) and the orbit-coverage check (k_tf_range)
     const long long n = (long long)B * A.M * L;
     const long long ro = r * L;
     bool bad = false;
     for (int k = tid; k < L; k += blockDim.x) {
-      const double xk = window_knot(k, L, s_edge[0], s_edge[1]);
+      const double xk = window_knot(k, L, w.flo, w.fhi);
       A.x[ro + k] = xk;
-      phm_response_point(A.y, n, ro + k, xk, sc, sr, A.orb, tr, A.t_init, A.TDItag, A.rescaled,
-                         A.tdi2);
+      phm_response_point(A.y, n, ro + k, xk, R.c, R.r, A.orb, R.t_ref, A.t_init, A.TDItag,
+                         A.rescaled, A.tdi2);
       const double tf = A.y[2 * n + ro + k];
       bad = bad || (tf < A.orb_tmin) || (tf > A.orb_tmax);
     }
@@ -224,12 +331,15 @@ int bbhx_uneven_batch(const bbhx_direct_source* direct, int num_direct,
     const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>(rows, (long long)nsm * (use_smem ? 2 : 1)));
     double* work = nullptr;
     BuildMulti* dH = nullptr;
+    RowRec* recs = nullptr;
     if (pool_alloc((void**)&dH, sizeof(BuildMulti), s) != cudaSuccess ||
+        pool_alloc((void**)&recs, sizeof(RowRec) * (size_t)std::max(rows, 1ll), s) != cudaSuccess ||
         (!use_smem && pool_alloc((void**)&work, sizeof(double) * grid * (size_t)(4 + 9) * maxL, s) != cudaSuccess)) {
       set_error("device allocation for the sparse build failed");
       st = ERR_CUDA;
     }
     if (dH) scratch.push_back(dH);
+    if (recs) scratch.push_back(recs);
     if (work) scratch.push_back(work);
     if (!st) {
       for (int g = 0; g < num_direct; ++g) H.g[g].scratch = work;
@@ -247,7 +357,11 @@ int bbhx_uneven_batch(const bbhx_direct_source* direct, int num_direct,
                                               (int)smem),
                          "cudaFuncSetAttribute(k_sparse_build)");
       if (!st) {
-        k_sparse_build<<<grid, SB_THREADS, use_smem ? smem : 0, s>>>(dH, use_smem ? 1 : 0);
+        k_row_records<<<grid_for(rows, 64), 64, 0, s>>>(dH, recs);
+        st = launch_status("k_row_records");
+      }
+      if (!st) {
+        k_sparse_build<<<grid, SB_THREADS, use_smem ? smem : 0, s>>>(dH, recs, use_smem ? 1 : 0);
         st = launch_status("k_sparse_build");
       }
     }
