@@ -50,7 +50,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--batch", type=int, default=1024)
-    ap.add_argument("--no-extra", action="store_true", help="skip the heterodyned metric")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip every metric after the headline (spline, heterodyned, gradients, uneven)")
+    ap.add_argument("--no-het", action="store_true", help="skip the heterodyned metric")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--het-batch", type=int, default=65536)
     ap.add_argument("--grad-batch", type=int, default=4096)
@@ -349,7 +351,8 @@ def gpu_arm(args):
     # reports the headline direct lnL only (every rank's own batch, no collective)
     if not args.no_extra and world == 1:
         extra.update(spline_metric(timing, B, wave.num_modes))
-        extra.update(het_metric(args, wave, like, f, params))
+        if not args.no_het:
+            extra.update(het_metric(args, wave, like, f, params))
         if not args.no_grad:
             extra.update(grad_metric(args))
         if not args.no_uneven:
