@@ -173,3 +173,27 @@ def test_prebuilt_spline_entry_point_matches_the_batch(golden, golden_data):
               _lib.stream())
     for g, ref in zip(batch.direct, out):
         np.testing.assert_allclose(g.lnl().cpu().numpy(), ref, rtol=1e-12, atol=1e-9)
+
+
+def test_builder_covers_phenomd_xyz_and_rescaled_groups(golden, golden_data):
+    """The fused sparse build handles every waveform / response switch of the single-problem
+    path: a PhenomD-only group (the tabulated 22 ringdown, one mode), an XYZ group and a
+    rescaled-AET group, each equal to its own Likelihood.get_ll (FP64)."""
+    from bbhx_b200 import BBHWaveformFD, EqualArmlengthOrbits, Likelihood
+    from bbhx_b200.uneven import DirectGroup, UnevenBatch
+
+    f, data, psd, tobs = golden_data["f"], golden_data["data"], golden_data["psd"], golden_data["tobs"]
+    P = golden["params"]
+    waves = [BBHWaveformFD(amp_phase_kwargs=dict(run_phenomd=True),
+                           response_kwargs=dict(orbits=EqualArmlengthOrbits(), TDItag="AET", tdi2=True)),
+             BBHWaveformFD(response_kwargs=dict(orbits=EqualArmlengthOrbits(), TDItag="XYZ")),
+             BBHWaveformFD(response_kwargs=dict(orbits=EqualArmlengthOrbits(), TDItag="AET",
+                                                rescaled=True))]
+    likes = [Likelihood(w, f, data, psd) for w in waves]
+    groups = [DirectGroup(lk, P, length=512, t_obs_start=0.0, t_obs_end=tobs) for lk in likes]
+    batch = UnevenBatch(groups, precision="fp64", shape={"fp64": (4096, 3)})
+    out = [o.cpu().numpy() for o in batch.run()]
+    for lk, got in zip(likes, out):
+        ref = lk.get_ll(P, length=512, t_obs_start=0.0, t_obs_end=tobs)
+        np.testing.assert_allclose(got, ref, rtol=1e-9, atol=1e-6)
+    assert all(int(fl.abs().sum().item()) == 0 for fl in batch.flags())
