@@ -218,10 +218,11 @@ class HeterodynedLikelihood:
         template_gen_kwargs["compress"] = True
         template_gen_kwargs["direct"] = True
         fd = to_np(self.f_dense)
-        minF = fd.min() * 0.999999999999
-        maxF = fd.max() * 1.000000000001
-        if minF == 0.0:
-            minF = 1e-6
+        # a probe grid just wider than the data, then narrowed (likelihood.py:424-462)
+        f_lo = fd.min() * 0.999999999999
+        f_hi = fd.max() * 1.000000000001
+        if f_lo == 0.0:
+            f_lo = 1e-6
         reference_gen_kwargs["squeeze"] = True
         reference_gen_kwargs["compress"] = True
         reference_gen_kwargs["fill"] = True
@@ -229,13 +230,13 @@ class HeterodynedLikelihood:
             reference_gen_kwargs["direct"] = False
             if "length" not in reference_gen_kwargs:
                 reference_gen_kwargs["length"] = 8096
-        freqs = np.logspace(np.log10(minF), np.log10(maxF), self.length_f_het)
+        probe = np.logspace(np.log10(f_lo), np.log10(f_hi), self.length_f_het)
         p = [np.atleast_1d(v) for v in reference_template_params]
         h0 = self.template_gen(*p, freqs=self.f_dense, **reference_gen_kwargs)[0]
-        h0_temp = self.template_gen(*p, freqs=freqs, **template_gen_kwargs)[0]
-        keep = to_np(~(h0_temp.abs() == 0.0))
-        freqs_keep = freqs[keep]
-        freqs = np.logspace(np.log10(freqs_keep[0]), np.log10(freqs_keep[-1]), self.length_f_het)
+        # the sparse grid spans the probe points where the reference template is non-zero
+        nonzero = to_np(self.template_gen(*p, freqs=probe, **template_gen_kwargs)[0].abs() != 0.0)
+        band = probe[nonzero]
+        freqs = np.logspace(np.log10(band[0]), np.log10(band[-1]), self.length_f_het)
         self.h0_sparse = self.template_gen(*p, freqs=freqs, **template_gen_kwargs)[None, :, :]
         self._h0_flat = self.h0_sparse[0].contiguous()
         # the band the reference keeps, (f >= freqs[0]) & (f <= freqs[-1]), is a contiguous run
