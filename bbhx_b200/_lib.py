@@ -26,6 +26,7 @@ _SIGS = {
     "bbhx_mode_coeffs_bytes": [],
     "bbhx_response_mode_bytes": [],
     "bbhx_selftest_sincos": [_VP, _VP, _I, _VP],
+    "bbhx_selftest_recurrence": [_VP, _D, _D, _D, _I, _I, _VP, _VP],
     "bbhx_count_point_ops": [_VP] * 5 + [_I, _VP, _I, _VP, _I, _D, _I, _I, _I, _VP],
     "bbhx_get_phenomhm_ringdown_frequencies": [_VP] * 8 + [_I, _I, _VP],
     "bbhx_get_phenomd_ringdown_frequencies": [_VP] * 6 + [_I] + [_VP] * 8 + [_D, _VP],

@@ -486,9 +486,10 @@ struct alignas(16) WarpStage {
 // per-bin phase cubic, range reduction and polynomial sine / cosine.  The state is re-anchored
 // (rot_anchor) at the first chunk of a segment and every kRecChunks chunks; the anchor phase is
 // evaluated at the bin's exact frequency k df (error-free product) with a compensated final sum,
-// so it carries ~1e-12 rad instead of the ~ulp(phi) ~ 1e-9 rad of a plain FP64 evaluation, and
-// the products add < 1e-12 rad over the kRecChunks * FD_K steps between anchors.
-constexpr int kRecChunks = 16;  // chunks (of FD_K steps per lane) between anchors
+// so it carries < 1e-13 rad instead of the ~ulp(phi) ~ 1e-10 - 1e-9 rad of a plain FP64
+// evaluation, and the products add ~2e-11 rad over the kRecChunks * FD_K = 128 steps between
+// anchors (bounded by the self-test against 50-digit phases: k_selftest_recurrence).
+constexpr int kRecChunks = 32;  // chunks (of FD_K steps per lane) between anchors
 
 struct Rot {
   double er, ei, rr, ri, qr, qi, pr, pi;
@@ -603,6 +604,25 @@ __device__ __forceinline__ void accumulate_chunk_rec(const WarpStage<R>& S, int 
       a[2 * ch + 1] = fma(-tr[j], api[j], a[2 * ch + 1]);
       a[2 * ch + 1] = fma(-ti[j], apr[j], a[2 * ch + 1]);
     }
+  }
+}
+
+// Self-test of the phase recurrence (no reference counterpart): thread l anchors at grid bin
+// k0 + l of the phase cubic pc = (y, c1, c2, c3) about knot xk (rot_anchor, step h = 32 df) and
+// advances `steps` times as the fused kernel does; out[2 (l steps + j) + {0, 1}] =
+// (cos, sin) of the phase at bin k0 + l + 32 j.
+__global__ void k_selftest_recurrence(const double* pc, double xk, double k0, double df, int lanes,
+                                      int steps, double* out) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= lanes) return;
+  Rot z;
+  rot_anchor(z, pc, xk, k0 + (double)l, df, 32.0 * df);
+  for (int j = 0; j < steps; ++j) {
+    out[2 * ((size_t)l * steps + j)] = z.er;
+    out[2 * ((size_t)l * steps + j) + 1] = z.ei;
+    cmul_inplace(z.er, z.ei, z.rr, z.ri);
+    cmul_inplace(z.rr, z.ri, z.qr, z.qi);
+    cmul_inplace(z.qr, z.qi, z.pr, z.pi);
   }
 }
 
@@ -1594,6 +1614,15 @@ int bbhx_hdyn(double* d_h, double* h_h, const double* residuals, const double* c
       (cplx*)d_h, (cplx*)h_h, (const cplx*)residuals, (const cplx*)constants, freqs, num_bin_all,
       length, n_channels);
   return launch_status("k_hdyn");
+}
+
+// Phase-recurrence self-test (k_selftest_recurrence); pc [4] and out [2 lanes steps] device.
+int bbhx_selftest_recurrence(const double* pc, double xk, double k0, double df, int lanes,
+                             int steps, double* out, void* stream) {
+  BBHX_REQUIRE(lanes >= 1 && lanes <= 1024 && steps >= 1 && steps <= 4096, "bad sizes");
+  k_selftest_recurrence<<<(lanes + 127) / 128, 128, 0, (cudaStream_t)stream>>>(pc, xk, k0, df,
+                                                                              lanes, steps, out);
+  return launch_status("k_selftest_recurrence");
 }
 
 // Support [start, start+len) of each binary on the data grid (device int arrays).

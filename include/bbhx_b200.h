@@ -54,6 +54,11 @@ size_t bbhx_response_mode_bytes(void);
 /* self-test (no reference counterpart): out[4i..4i+3] = sin, cos of x[i] from the hot-loop
  * Cody-Waite + Taylor routine and from CUDA's sincos */
 int bbhx_selftest_sincos(const double *x, double *out, int n, void *stream);
+/* self-test (no reference counterpart) of the fused kernel's phase recurrence: thread l anchors
+ * at grid bin k0 + l of the phase cubic pc [4] (y, c1, c2, c3 about knot xk; grid f = k df) and
+ * steps `steps` times by 32 bins; out [2 lanes steps] = (cos, sin) per (lane, step), device */
+int bbhx_selftest_recurrence(const double *pc, double xk, double k0, double df, int lanes,
+                             int steps, double *out, void *stream);
 /* diagnostic (no reference counterpart): algorithmic operation tallies of the FP64 heterodyne
  * point chain (PhenomHM amp / phase / t(f), TDI transfer, phasor, channel products) summed over
  * num_modes x length points, set-up excluded; out [12] device = add/sub, mul, div, compare,

@@ -25,3 +25,40 @@ def test_hot_loop_sincos_matches_cuda():
     small = np.abs(x) < 10
     assert np.max(np.abs(o[small, 0] - np.sin(x[small]))) < 4e-16
     assert np.max(np.abs(o[small, 1] - np.cos(x[small]))) < 4e-16
+
+
+def test_phase_recurrence_drift_is_bounded():
+    """The fused FP64 kernel's phase recurrence -- its own anchor and complex rotations, run by
+    bbhx_selftest_recurrence -- against the exact phase of the cubic at the exact grid
+    frequencies (mpmath, 50 digits), for phase cubics like a 1-yr stream's segments at 5e-2
+    and 1e-3 Hz: the anchor is within 1e-12 and 128 steps of 32 bins (the kernel re-anchors
+    every 128) stay within 4e-11, against ~2e-10 for a plain FP64 evaluation of a 1e6 rad phase."""
+    import math
+
+    import mpmath
+    import torch
+
+    from bbhx_b200 import _lib
+
+    mpmath.mp.dps = 50
+    df = 1.0 / 31558149.763545603
+    lanes, steps = 32, 128
+    tp = 2 * math.pi
+    for k0, pc in [(1_500_000, (1.234567e6, tp * 2.0e7, tp * 3.0e9, tp * 1.0e11)),
+                   (31_000, (2.0e5, tp * 3.0e7, tp * 4.0e10, tp * 5.0e13))]:
+        xk = (k0 - 37) * df
+        pcd = torch.tensor(pc, dtype=torch.float64, device="cuda")
+        out = torch.empty(2 * lanes * steps, dtype=torch.float64, device="cuda")
+        _lib.call("bbhx_selftest_recurrence", _lib.dptr(pcd), float(xk), float(k0), float(df),
+                  lanes, steps, _lib.dptr(out), _lib.stream())
+        e = out.cpu().numpy().reshape(lanes, steps, 2)
+        y, c1, c2, c3 = (mpmath.mpf(v) for v in pc)
+        err = np.zeros((lanes, steps))
+        for lane in range(lanes):
+            for j in range(steps):
+                u = mpmath.mpf(k0 + lane + 32 * j) * mpmath.mpf(df) - mpmath.mpf(xk)
+                ph = y + c1 * u + c2 * u ** 2 + c3 * u ** 3
+                err[lane, j] = math.hypot(e[lane, j, 0] - float(mpmath.cos(ph)),
+                                          e[lane, j, 1] - float(mpmath.sin(ph)))
+        assert err[:, 0].max() < 1e-12, err[:, 0].max()
+        assert err.max() < 4e-11, err.max()
