@@ -32,22 +32,42 @@ struct BuildArgs {
   double dspin, mf_min, mf_max, t_init, tL_start, tL_end, orb_tmin, orb_tmax;
   double *x, *y, *c1, *c2, *c3, *t_start, *t_end;
   double* scratch;  // (4 + 9) L doubles per CTA when a row does not fit in shared memory
+  ModeCoeffs* coeffs_out;  // heterodyned problems: the walkers' PhenomHM records (no build)
   int* flags;
   int nq, TDItag, rescaled, tdi2, run_phenomd, M, L, B;
 };
 
 struct BuildMulti {
-  BuildArgs g[SB_MAXGROUPS];
-  long long roff[SB_MAXGROUPS + 1];  // row offsets; roff[ngroups] = total rows
-  int ngroups;
+  BuildArgs g[2 * SB_MAXGROUPS];  // direct problems, then heterodyned ones
+  long long roff[2 * SB_MAXGROUPS + 1];  // row offsets; roff[ngroups] = total rows
+  int ngroups;     // direct + heterodyned problems
+  int ndirect;     // the first ndirect are built; the rest only get records
   int max_length;  // work-area stride of one CTA in `scratch`
 };
 
-__global__ void k_store_build(BuildMulti H, BuildMulti* dst) {
-  const int n = (int)(sizeof(BuildMulti) / sizeof(unsigned long long));
-  const unsigned long long* src = reinterpret_cast<const unsigned long long*>(&H);
-  unsigned long long* d = reinterpret_cast<unsigned long long*>(dst);
-  for (int i = threadIdx.x; i < n; i += blockDim.x) d[i] = src[i];
+// A host struct copied to device memory through kernel parameters, 24 KB per launch (no host
+// copy is involved, so the copy is part of a captured graph like any launch).
+struct WordChunk {
+  unsigned long long w[3072];
+};
+__global__ void k_store_words(WordChunk c, unsigned long long* dst, int n) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = c.w[i];
+}
+static_assert(sizeof(BuildMulti) % 8 == 0, "the build table is stored in 8-byte words");
+
+int store_struct(const void* host, size_t bytes, void* dev, cudaStream_t s) {
+  const unsigned long long* src = static_cast<const unsigned long long*>(host);
+  unsigned long long* dst = static_cast<unsigned long long*>(dev);
+  const size_t n = bytes / 8;
+  for (size_t o = 0; o < n; o += 3072) {
+    WordChunk c;
+    const int m = (int)std::min<size_t>(3072, n - o);
+    memcpy(c.w, src + o, 8 * (size_t)m);
+    k_store_words<<<1, 256, 0, s>>>(c, dst + o, m);
+    const int st = launch_status("k_store_words");
+    if (st) return st;
+  }
+  return OK;
 }
 
 // Per-row set-up, made by k_row_records (thread per row) and staged into the row's CTA.
@@ -103,10 +123,14 @@ __global__ void k_row_records(const BuildMulti* __restrict__ H, RowRec* recs) {
     } else {
       ringdown_hm(fr.m1, fr.m2, fr.chi1, fr.chi2, ell, mm, &rd, &dm);
     }
-    RowRec& R = recs[row];
     ModeCoeffs c;
     phm_setup_mode(c, fr.m1_SI, fr.m2_SI, fr.chi1, fr.chi2, P[4 * (size_t)B + b], ell, mm, rd, dm,
                    rd22, dm22, A.run_phenomd);
+    if (A.coeffs_out != nullptr) {  // heterodyned walker: its record is all that is needed
+      A.coeffs_out[r] = c;
+      continue;
+    }
+    RowRec& R = recs[row];
     R.c = c;
     ResponseMode rm;
     response_mode_setup(rm, ell, mm, P[5 * (size_t)B + b], P[7 * (size_t)B + b], lam, beta,
@@ -209,7 +233,7 @@ __global__ void __launch_bounds__(SB_THREADS) k_sparse_build(const BuildMulti* _
   extern __shared__ double sb_smem[];
   __shared__ RowRec R;
   const int tid = threadIdx.x;
-  const long long total = H->roff[H->ngroups];
+  const long long total = H->roff[H->ndirect];
   for (long long row = blockIdx.x; row < total; row += gridDim.x) {
     const int g = build_group(H, row);
     const BuildArgs& A = H->g[g];
@@ -265,11 +289,13 @@ int uneven_like(const bbhx_direct_group* groups, int num_groups, const bbhx_hdyn
 extern "C" {
 
 int bbhx_uneven_batch(const bbhx_direct_source* direct, int num_direct,
-                      const bbhx_hdyn_group* het, int num_het, int precision, int tile_bins,
+                      const bbhx_hdyn_source* het, int num_het, int precision, int tile_bins,
                       int ctas_per_sm, void* stream) {
   BBHX_REQUIRE(num_direct >= 0 && num_direct <= SB_MAXGROUPS &&
                    (direct != nullptr || num_direct == 0),
                "num_direct must be 0..%d", SB_MAXGROUPS);
+  BBHX_REQUIRE(num_het >= 0 && num_het <= SB_MAXGROUPS && (het != nullptr || num_het == 0),
+               "num_het must be 0..%d", SB_MAXGROUPS);
   cudaStream_t s = (cudaStream_t)stream;
   BuildMulti H;
   memset(&H, 0, sizeof(H));
@@ -320,20 +346,54 @@ int bbhx_uneven_batch(const bbhx_direct_source* direct, int num_direct,
     rows += (long long)D.num_bin_all * D.num_modes;
     maxL = std::max(maxL, D.length);
   }
-  H.roff[num_direct] = rows;
+  const long long rows_direct = rows;
+  // heterodyned problems: records and observation limits only
+  for (int h = 0; h < num_het; ++h) {
+    const bbhx_hdyn_source& S = het[h];
+    const bbhx_hdyn_group& G = S.group;
+    BBHX_REQUIRE(G.num_modes >= 1 && G.num_modes <= MAX_MODES && (!S.run_phenomd || G.num_modes == 1),
+                 "heterodyned group %d: bad mode count %d", h, G.num_modes);
+    BBHX_REQUIRE(G.num_bin_all >= 0 && S.qnm_n >= 2 && S.dspin > 0.0,
+                 "heterodyned group %d: bad sizes", h);
+    BBHX_REQUIRE(S.params && G.coeffs && G.t_start && G.t_end && S.flags && G.ells && G.mms,
+                 "heterodyned group %d: missing buffer", h);
+    BuildArgs& A = H.g[num_direct + h];
+    A.params = S.params;
+    A.ells = G.ells;
+    A.mms = G.mms;
+    A.qnm = S.qnm_table;
+    A.dspin = S.dspin;
+    A.tL_start = S.t_obs_start_L;
+    A.tL_end = S.t_obs_end_L;
+    A.t_start = const_cast<double*>(G.t_start);
+    A.t_end = const_cast<double*>(G.t_end);
+    A.coeffs_out = (ModeCoeffs*)const_cast<void*>(G.coeffs);
+    A.flags = S.flags;
+    A.nq = S.qnm_n;
+    A.run_phenomd = S.run_phenomd;
+    A.M = G.num_modes;
+    A.L = G.length;
+    A.B = G.num_bin_all;
+    H.roff[num_direct + h] = rows;
+    rows += (long long)G.num_bin_all * G.num_modes;
+  }
+  H.ngroups = num_direct + num_het;
+  H.ndirect = num_direct;
+  H.roff[H.ngroups] = rows;
   H.max_length = maxL;
   int st = OK;
   std::vector<void*> scratch;
-  if (num_direct > 0) {
+  if (H.ngroups > 0) {
     const size_t smem = sizeof(double) * (size_t)(4 + 9) * maxL;
     const bool use_smem = smem <= kBuildSmemMax;
     const int nsm = sm_count();
-    const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>(rows, (long long)nsm * (use_smem ? 2 : 1)));
+    const unsigned grid = (unsigned)std::max<long long>(
+        1, std::min<long long>(rows_direct, (long long)nsm * (use_smem ? 2 : 1)));
     double* work = nullptr;
     BuildMulti* dH = nullptr;
     RowRec* recs = nullptr;
     if (pool_alloc((void**)&dH, sizeof(BuildMulti), s) != cudaSuccess ||
-        pool_alloc((void**)&recs, sizeof(RowRec) * (size_t)std::max(rows, 1ll), s) != cudaSuccess ||
+        pool_alloc((void**)&recs, sizeof(RowRec) * (size_t)std::max(rows_direct, 1ll), s) != cudaSuccess ||
         (!use_smem && pool_alloc((void**)&work, sizeof(double) * grid * (size_t)(4 + 9) * maxL, s) != cudaSuccess)) {
       set_error("device allocation for the sparse build failed");
       st = ERR_CUDA;
@@ -343,23 +403,22 @@ int bbhx_uneven_batch(const bbhx_direct_source* direct, int num_direct,
     if (work) scratch.push_back(work);
     if (!st) {
       for (int g = 0; g < num_direct; ++g) H.g[g].scratch = work;
-      k_store_build<<<1, 256, 0, s>>>(H, dH);
-      st = launch_status("k_store_build");
+      st = store_struct(&H, sizeof(H), dH, s);
     }
     if (!st) {
-      k_clear_build_flags<<<num_direct, 32, 0, s>>>(dH);
+      k_clear_build_flags<<<H.ngroups, 32, 0, s>>>(dH);
       st = launch_status("k_clear_build_flags");
     }
     if (!st && rows > 0) {
+      k_row_records<<<grid_for(rows, 64), 64, 0, s>>>(dH, recs);
+      st = launch_status("k_row_records");
+    }
+    if (!st && rows_direct > 0) {
       if (use_smem)
         st = cuda_status(cudaFuncSetAttribute(k_sparse_build,
                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               (int)smem),
                          "cudaFuncSetAttribute(k_sparse_build)");
-      if (!st) {
-        k_row_records<<<grid_for(rows, 64), 64, 0, s>>>(dH, recs);
-        st = launch_status("k_row_records");
-      }
       if (!st) {
         k_sparse_build<<<grid, SB_THREADS, use_smem ? smem : 0, s>>>(dH, recs, use_smem ? 1 : 0);
         st = launch_status("k_sparse_build");
@@ -390,7 +449,10 @@ int bbhx_uneven_batch(const bbhx_direct_source* direct, int num_direct,
       G.data32 = D.data32;
       G.noise32 = D.noise32;
     }
-    st = uneven_like(groups.data(), num_direct, het, num_het, precision, tile_bins, ctas_per_sm, s);
+    std::vector<bbhx_hdyn_group> hgroups(std::max(num_het, 1));
+    for (int h = 0; h < num_het; ++h) hgroups[h] = het[h].group;
+    st = uneven_like(groups.data(), num_direct, hgroups.data(), num_het, precision, tile_bins,
+                     ctas_per_sm, s);
   }
   for (void* p : scratch) pool_free(p, s);
   return st;

@@ -53,6 +53,15 @@ class HdynGroupC(ctypes.Structure):
                 ("num_bin_all", ctypes.c_int)]
 
 
+class HdynSourceC(ctypes.Structure):
+    """Mirror of ``bbhx_hdyn_source`` (include/bbhx_b200.h)."""
+
+    _fields_ = [("group", HdynGroupC), ("params", ctypes.c_void_p), ("qnm_table", ctypes.c_void_p),
+                ("qnm_n", ctypes.c_int), ("dspin", ctypes.c_double),
+                ("t_obs_start_L", ctypes.c_double), ("t_obs_end_L", ctypes.c_double),
+                ("run_phenomd", ctypes.c_int), ("flags", ctypes.c_void_p)]
+
+
 class DirectSourceC(ctypes.Structure):
     """Mirror of ``bbhx_direct_source`` (include/bbhx_b200.h)."""
 
@@ -135,18 +144,41 @@ class HetGroup:
     def size(self):
         return self.params.shape[1]
 
-    def build(self, precision="fp64"):
-        """Per-walker records and outputs of this group (device; no host synchronisation)."""
+    def source(self, precision="fp64"):
+        """Descriptor of this group for bbhx_uneven_batch: the walkers' parameters and the
+        device buffers the batch fills (PhenomHM records, observation limits, sums); no host
+        synchronisation."""
+        from .waveforms.ringdownphenomd import dspin
+
+        t = torch()
         het = self.het
-        rows = tuple(self.params[k] for k in range(12))
-        a = het.template_gen.heterodyne_setup(rows, het.freqs, het._h0_flat, het.data_constants,
-                                              self.t_obs_start, self.t_obs_end, flags=self.flags)
-        self._keep = a
-        self.d_h, self.h_h = a["d_h"], a["h_h"]
-        self.packed = torch().empty(3 * self.size, dtype=torch().float64, device=device())
-        fields = {k: (a[k] if isinstance(a[k], (int, float)) else _lib.dptr(a[k]).value)
-                  for k in het.template_gen.HDYN_ARGS}
-        return HdynGroupC(orbits=het.template_gen.response_gen.orbit_handle.ptr.value, **fields)
+        gen = het.template_gen
+        ap, rg = gen.amp_phase_gen, gen.response_gen
+        ells, mms = ap.mode_tensors(None)
+        B, M, L = self.size, int(ells.numel()), int(het.freqs.numel())
+        f64 = dict(dtype=t.float64, device=device())
+        nbytes = int(_lib.lib().bbhx_mode_coeffs_bytes())
+        coeffs = t.empty(B * M * nbytes, dtype=t.uint8, device=device())
+        ts, te = t.empty(B, **f64), t.empty(B, **f64)
+        self.d_h = t.empty(B, dtype=t.complex128, device=device())
+        self.h_h = t.empty(B, dtype=t.complex128, device=device())
+        self.packed = t.empty(3 * B, **f64)
+        tab = ap.qnm_table
+        self._keep = (coeffs, ts, te, ells, mms, tab)
+        p = lambda a: _lib.dptr(a).value  # noqa: E731
+        row = lambda k: self.params.data_ptr() + 8 * k * B  # noqa: E731
+        group = HdynGroupC(
+            orbits=rg.orbit_handle.ptr.value, d_h=p(self.d_h), h_h=p(self.h_h), coeffs=p(coeffs),
+            ells=p(ells), mms=p(mms), phi_ref=row(5), inc=row(7), lam=row(8), beta=row(9),
+            psi=row(10), t_ref=row(11), t_init=float(ap.initial_t_val), t_start=p(ts), t_end=p(te),
+            freqs=p(het.freqs), h0=p(het._h0_flat), consts=p(het.data_constants),
+            TDItag=rg.TDItag_int, rescaled=int(rg.rescaled), tdi2=int(rg.tdi2), num_modes=M,
+            length=L, num_bin_all=B)
+        return HdynSourceC(group=group, params=p(self.params), qnm_table=p(tab),
+                           qnm_n=int(tab.shape[1]), dspin=float(dspin),
+                           t_obs_start_L=float(self.t_obs_start * YRSID_SI),
+                           t_obs_end_L=float(self.t_obs_end * YRSID_SI),
+                           run_phenomd=int(ap.run_phenomd), flags=p(self.flags))
 
     def lnl(self):
         return pack_lnl(self.d_h, self.h_h, self.het.reference_d_d, self.packed)
@@ -168,7 +200,8 @@ class Autotuner:
         return (precision, len(descs), sum(d.num_bin_all for d in descs),
                 max((d.data_length for d in descs), default=0),
                 max((d.length for d in descs), default=0), len(hdescs),
-                sum(h.num_bin_all for h in hdescs), max((h.length for h in hdescs), default=0))
+                sum(h.group.num_bin_all for h in hdescs),
+                max((h.group.length for h in hdescs), default=0))
 
     def best(self, descs, hdescs, precision, launch):
         key = self.signature(descs, hdescs, precision)
@@ -229,7 +262,7 @@ class UnevenBatch:
 
     def _launch(self, descs, hdescs, precision, tile, ctas):
         arr = (DirectSourceC * max(len(descs), 1))(*descs)
-        harr = (HdynGroupC * max(len(hdescs), 1))(*hdescs)
+        harr = (HdynSourceC * max(len(hdescs), 1))(*hdescs)
         _lib.call("bbhx_uneven_batch", ctypes.cast(arr, ctypes.c_void_p), len(descs),
                   ctypes.cast(harr, ctypes.c_void_p), len(hdescs), PRECISIONS[precision],
                   int(tile), int(ctas), _lib.stream())
@@ -243,7 +276,7 @@ class UnevenBatch:
         for g, pr in zip(self.direct, precs):
             classes.setdefault(pr, ([], []))[0].append(g.source(pr))
         for h, pr in zip(self.het, precs[len(self.direct):]):
-            classes.setdefault(pr, ([], []))[1].append(h.build(pr))
+            classes.setdefault(pr, ([], []))[1].append(h.source(pr))
         for pr, (descs, hdescs) in classes.items():
             if pr not in self.shape:
                 self.shape[pr] = self.autotuner.best(

@@ -342,12 +342,30 @@ typedef struct {
 int bbhx_uneven_like(const bbhx_direct_group *direct, int num_direct, const bbhx_hdyn_group *het,
                      int num_het, int precision, int tile_bins, int ctas_per_sm, void *stream);
 
+/* One heterodyned problem of an uneven batch given by its walkers' parameters: `group` as for
+   bbhx_uneven_like, except that group.coeffs ([B, M] PhenomHM records, sized
+   bbhx_mode_coeffs_bytes() each), group.t_start and group.t_end are device buffers the batch
+   fills from params [12, B] (group.phi_ref .. t_ref may point at params' rows) with the
+   PhenomD ringdown table, the L-frame observation limits [s] and run_phenomd as in
+   bbhx_direct_source; flags [3] receives the |chi| > 1 bits at flags[2] (cleared first). */
+typedef struct bbhx_hdyn_source {
+  bbhx_hdyn_group group;
+  const double *params;
+  const double *qnm_table;
+  int qnm_n;
+  double dspin, t_obs_start_L, t_obs_end_L;
+  int run_phenomd;
+  int *flags;
+} bbhx_hdyn_source;
+
 /* A whole uneven batch from parameters: the sparse grids and splines of every direct problem
    in ONE launch (one CTA per (binary, mode) row: records, default grid and t(f), window regrid,
-   waveform + response, coverage check, spline), then bbhx_uneven_like.  No reference
-   counterpart; stream-ordered and graph-capturable. */
-int bbhx_uneven_batch(const bbhx_direct_source *direct, int num_direct, const bbhx_hdyn_group *het,
-                      int num_het, int precision, int tile_bins, int ctas_per_sm, void *stream);
+   waveform + response, coverage check, spline) -- the same launch that sets up the records
+   also makes the heterodyned walkers' PhenomHM records and observation limits -- then
+   bbhx_uneven_like.  No reference counterpart; stream-ordered and graph-capturable. */
+int bbhx_uneven_batch(const bbhx_direct_source *direct, int num_direct,
+                      const struct bbhx_hdyn_source *het, int num_het, int precision,
+                      int tile_bins, int ctas_per_sm, void *stream);
 
 /* fused interpolate + mode sum + noise weighting + <d|h>, <h|h> reduction; no templates are
  * stored (equivalent to InterpTDI followed by direct_like, waveformbuild.py:641-660 +

@@ -89,13 +89,13 @@ def test_descriptor_layouts_match_the_header(tmp_path):
 
     import pytest
 
-    from bbhx_b200.uneven import DirectGroupC, DirectSourceC, HdynGroupC
+    from bbhx_b200.uneven import DirectGroupC, DirectSourceC, HdynGroupC, HdynSourceC
 
     cc = shutil.which("gcc") or shutil.which("cc")
     if cc is None:
         pytest.skip("no host C compiler")
     mirrors = {"bbhx_direct_group": DirectGroupC, "bbhx_hdyn_group": HdynGroupC,
-               "bbhx_direct_source": DirectSourceC}
+               "bbhx_direct_source": DirectSourceC, "bbhx_hdyn_source": HdynSourceC}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "bbhx_b200.h"', "int main(void) {"]
     for cname, py in mirrors.items():
         lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')

@@ -143,7 +143,10 @@ def test_uneven_mixed_routes_coarse_grids_to_fp64():
         hh = like.h_h.real.cpu().numpy()
         err = np.abs(got - ref)
         if g["length"] == 256:
-            assert np.all(err <= 1e-2), err
+            # FP64 on both sides; the phase recurrences re-anchor at different bins, and a
+            # recurrence phase error (<= 4e-11 rad, the drift self-test) moves the modes'
+            # cross terms of h_h by up to that fraction
+            assert np.all(err <= 1e-6 + 4e-11 * hh), (err, hh)
         else:
             assert np.all(err <= 2e-6 * np.maximum(hh, 1.0)), err
 
