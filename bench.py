@@ -41,6 +41,10 @@ SEED_PARAMS = 1234
 SEED_NOISE = 99
 HBM_BYTES_PER_PAIR = 72.0  # 3 x complex128 weighted data + 3 x float64 noise weights
 MIXED_BYTES_PER_PAIR = 36.0  # 3 x complex64 + 3 x float32: the FP32 copies the mixed form reads
+# FP64 instructions per (pair, mode) the direct algorithm cannot do without: 7 cubics (amplitude,
+# 3 complex transfer functions) x 3 FMAs, 3 complex products of the phase recurrence x 4, the
+# amplitude times e^{i phi} 2, and the 3 channels' complex multiply-accumulates x 4
+FP64_INSTR_PER_PAIR_MODE = 7 * 3 + 3 * 4 + 2 + 3 * 4
 
 
 def parse():
@@ -410,7 +414,8 @@ def gpu_arm(args):
                      "traffic": (tpp * pairs if tpp is not None else None),
                      "kernel": "k_direct_fused<FP64> (bbhx_direct_like_fused, precision 0)",
                      "kernel_ms": statistics.mean(fused_ms),
-                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback"},
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback",
+                     "fp64_floor": fp64_floor(pairs, wave.num_modes, fused_avg_s, peak)},
         "gpu_launches": 12 * args.steps,
         "clocks": clocks,
     }
@@ -546,6 +551,18 @@ def het_metric(args, wave, like, f, params):
 FP64_LANE_OPS_PER_S = 148 * 64 * 1.965e9  # B200: 64 FP64 lanes per SM (nominal, 1965 MHz)
 OPC_NAMES = ("add_sub", "mul", "div", "compare", "sqrt", "cbrt", "log", "exp", "pow", "atan",
              "sin_cos", "other")
+
+
+def fp64_floor(pairs, modes, kernel_s, hbm_peak_gbs):
+    """The FP64 pipe's bound on the direct kernel: FP64_INSTR_PER_PAIR_MODE instructions for every
+    (pair, mode) (pairs x modes is an upper bound: every mode counted over the union support) at
+    the nominal FP64 lane rate give the shortest possible kernel time, and the HBM-roofline
+    fraction the kernel would reach there."""
+    floor_s = FP64_INSTR_PER_PAIR_MODE * pairs * modes / FP64_LANE_OPS_PER_S
+    return {"fp64_instr_per_pair_mode": FP64_INSTR_PER_PAIR_MODE, "floor_ms": floor_s * 1e3,
+            "kernel_over_floor": kernel_s / floor_s,
+            "hbm_frac_at_floor": HBM_BYTES_PER_PAIR * pairs / floor_s / 1e9 / hbm_peak_gbs,
+            "lane_rate": "nominal 148 SMs x 64 FP64 lanes x 1965 MHz"}
 
 
 def het_roofline(het, wave, center, evals_per_s):
