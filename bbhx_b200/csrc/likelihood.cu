@@ -251,6 +251,9 @@ struct FusedArgs {
   const long long* gh_off;
   // uniform-grid record of data_freqs (k_grid_detect) enabling the phase recurrence, or null
   const struct GridInfo* grid;
+  // work-queue counter, zero at launch: warps claim (tile, binary) items from it in increasing
+  // order (claim_item)
+  unsigned long long* next;
 };
 
 // Data grid of the form f_i = fl((k0 + i) df): numpy's k * df and rfftfreq grids, the form
@@ -1243,6 +1246,16 @@ constexpr size_t fused_smem_bytes() {
   return FD_WARPS * (sizeof(WarpStage<R>) + (MIXED ? 0 : sizeof(RecStage)));
 }
 
+// The calling warp's next work item from the launch's queue counter.  Items are handed out in
+// increasing order, so the warps in flight stay on neighbouring items (the same data tile for
+// different binaries); a warp that finishes a cheap item takes the next one at once, so the
+// resident warps stay busy until the queue drains however unequal the items are.
+__device__ __forceinline__ long long claim_item(unsigned long long* next, int lane) {
+  unsigned long long q = 0;
+  if (lane == 0) q = atomicAdd(next, 1ull);
+  return (long long)__shfl_sync(0xffffffffu, q, 0);
+}
+
 template <bool MIXED, bool GH = false>
 __global__ void __launch_bounds__(FD_WARPS * 32, MIXED ? 4 : 3) k_direct_fused(FusedArgs A) {
   static_assert(!(MIXED && GH), "d lnL / d h is written by the FP64 form only");
@@ -1255,9 +1268,8 @@ __global__ void __launch_bounds__(FD_WARPS * 32, MIXED ? 4 : 3) k_direct_fused(F
   RecStage* RS = REC ? reinterpret_cast<RecStage*>(smem_raw + FD_WARPS * sizeof(WarpStage<R>)) + warp
                      : nullptr;
   const long long nitems = (long long)A.ntiles * A.B;
-  const long long gw = (long long)blockIdx.x * FD_WARPS + warp;
-  const long long nw = (long long)gridDim.x * FD_WARPS;
-  for (long long q = gw; q < nitems; q += nw) fused_item<MIXED, R, GH, REC>(A, q, S, RS, lane);
+  for (long long q = claim_item(A.next, lane); q < nitems; q = claim_item(A.next, lane))
+    fused_item<MIXED, R, GH, REC>(A, q, S, RS, lane);
 }
 
 // Several independent problems (groups: own data stream, grid length L, mode count M,
@@ -1328,7 +1340,8 @@ __global__ void k_het_response_setup_multi(const HetMulti* __restrict__ HM, long
 // (168 registers, 3 CTAs per SM), which the FP32 heterodyne models need without spilling.
 template <bool MIXED, bool HET>
 __global__ void __launch_bounds__(FD_WARPS * 32, (MIXED && !HET) ? 4 : 3)
-    k_uneven(const MultiArgs* __restrict__ MA, const HetMulti* __restrict__ HM, int slot) {
+    k_uneven(const MultiArgs* __restrict__ MA, const HetMulti* __restrict__ HM, int slot,
+             unsigned long long* next) {
   using R = typename std::conditional<MIXED, float, double>::type;
   constexpr bool REC = !MIXED;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1341,10 +1354,8 @@ __global__ void __launch_bounds__(FD_WARPS * 32, (MIXED && !HET) ? 4 : 3)
   RecStage* RS = REC ? reinterpret_cast<RecStage*>(mine + sizeof(WarpStage<R>)) : nullptr;
   const long long nh = HM->woff[HM->ngroups];
   const long long total = nh + MA->off[MA->ngroups];
-  const long long gw = (long long)blockIdx.x * FD_WARPS + warp;
-  const long long nw = (long long)gridDim.x * FD_WARPS;
   int g = -1, hg = -1;
-  for (long long q = gw; q < total; q += nw) {
+  for (long long q = claim_item(next, lane); q < total; q = claim_item(next, lane)) {
     if (HET && q < nh) {
       if (hg < 0 || q >= HM->woff[hg + 1] || q < HM->woff[hg]) {
         hg = group_of(HM->woff, HM->ngroups, q);
@@ -1457,6 +1468,22 @@ namespace bbhx {
 // FP64 fused kernel (gradient chain, gradient.cu): gh packed by the batch-local support
 // offsets gh_off; start / len the support of all B_all binaries (bbhx_template_support);
 // d_h, h_h (complex [B_all], may be null) receive the batch's <d|h>, <h|h>.
+// Grid of a queue-driven fused kernel: the CTAs (FD_WARPS warps, `smem` bytes of dynamic shared
+// memory, its attribute already set) that are resident on the whole GPU at once, fewer when the
+// items are fewer.  Every warp then claims items until the queue drains, with no second wave.
+template <typename K>
+unsigned resident_grid(K kernel, size_t smem, long long nitems) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, FD_WARPS * 32, smem) !=
+          cudaSuccess ||
+      per_sm < 1) {
+    (void)cudaGetLastError();
+    per_sm = 1;
+  }
+  const long long want = (nitems + FD_WARPS - 1) / FD_WARPS;
+  return (unsigned)std::max<long long>(1, std::min<long long>(want, (long long)per_sm * sm_count()));
+}
+
 int direct_fused_gh(cplx* gh, const long long* gh_off, double* d_h, double* h_h,
                     const int* start, const int* len, const double* data_freqs,
                     const double* data, const double* noise, int N, const double* x,
@@ -1470,9 +1497,11 @@ int direct_fused_gh(cplx* gh, const long long* gh_off, double* d_h, double* h_h,
   double* part = nullptr;
   int2* segtab = nullptr;
   GridInfo* grid = nullptr;
+  unsigned long long* next = nullptr;
   BBHX_CHECK_CUDA(pool_alloc_all(s, {{(void**)&part, sizeof(double) * 3 * nitems},
                                      {(void**)&segtab, sizeof(int2) * nitems * M},
-                                     {(void**)&grid, sizeof(GridInfo)}}));
+                                     {(void**)&grid, sizeof(GridInfo)},
+                                     {(void**)&next, sizeof(unsigned long long)}}));
   k_tile_segments<<<grid_for(nitems * M, 256, sm_count() * 64), 256, 0, s>>>(
       segtab, x + row0, data_freqs, start + b0, len + b0, nb, M, L, ntiles, FD_TILE);
   int st = launch_status("k_tile_segments");
@@ -1507,14 +1536,15 @@ int direct_fused_gh(cplx* gh, const long long* gh_off, double* d_h, double* h_h,
     A.gh = gh;
     A.gh_off = gh_off;
     A.grid = grid;
-    const long long g = (nitems + FD_WARPS - 1) / FD_WARPS;
-    const long long cap = 16LL * sm_count();
-    const unsigned grid = (unsigned)(g < cap ? g : cap);
+    A.next = next;
     const size_t sm = fused_smem_bytes<false>();
     st = cuda_status(cudaFuncSetAttribute(k_direct_fused<false, true>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm),
                      "cudaFuncSetAttribute(k_direct_fused)");
+    if (!st)
+      st = cuda_status(cudaMemsetAsync(next, 0, sizeof(unsigned long long), s), "work-queue counter");
     if (!st) {
+      const unsigned grid = resident_grid(k_direct_fused<false, true>, sm, nitems);
       k_direct_fused<false, true><<<grid, FD_WARPS * 32, sm, s>>>(A);
       st = launch_status("k_direct_fused (d lnL / d h)");
     }
@@ -1527,6 +1557,7 @@ int direct_fused_gh(cplx* gh, const long long* gh_off, double* d_h, double* h_h,
   pool_free(part, s);
   pool_free(segtab, s);
   pool_free(grid, s);
+  pool_free(next, s);
   return st;
 }
 
@@ -1853,16 +1884,25 @@ int uneven_like(const bbhx_direct_group* groups, int num_groups,
     const size_t dslot = (precision == 1 ? fused_smem_bytes<true>() : fused_smem_bytes<false>()) / FD_WARPS;
     const size_t slot = align16(std::max(dslot, het_slot));
     const size_t sm = slot * FD_WARPS;
+    unsigned long long* next = nullptr;
+    if (pool_alloc((void**)&next, sizeof(unsigned long long), s) != cudaSuccess) {
+      set_error("device allocation of the work-queue counter failed");
+      st = ERR_CUDA;
+    } else {
+      scratch.push_back(next);
+      st = cuda_status(cudaMemsetAsync(next, 0, sizeof(unsigned long long), s),
+                       "work-queue counter");
+    }
     auto launch = [&](auto kernel) {
       int r = cuda_status(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                (int)sm),
                           "cudaFuncSetAttribute(k_uneven)");
-      if (!r) kernel<<<grid, FD_WARPS * 32, sm, s>>>(dMA, dHM, (int)slot);
+      if (!r) kernel<<<grid, FD_WARPS * 32, sm, s>>>(dMA, dHM, (int)slot, next);
       return r;
     };
-    if (precision == 1)
+    if (!st && precision == 1)
       st = walkers > 0 ? launch(k_uneven<true, true>) : launch(k_uneven<true, false>);
-    else
+    else if (!st)
       st = walkers > 0 ? launch(k_uneven<false, true>) : launch(k_uneven<false, false>);
     if (!st) st = launch_status("k_uneven");
   }
@@ -1918,10 +1958,12 @@ int bbhx_direct_like_fused(double* d_h, double* h_h, const double* data_freqs, c
   double* part = nullptr;
   int2* segtab = nullptr;
   GridInfo* grid = nullptr;
+  unsigned long long* next = nullptr;
   BBHX_CHECK_CUDA(pool_alloc_all(s, {{(void**)&sup, sizeof(int) * 2 * num_bin_all},
                                      {(void**)&part, sizeof(double) * 3 * nitems},
                                      {(void**)&segtab, sizeof(int2) * nitems * num_modes},
-                                     {(void**)&grid, sizeof(GridInfo)}}));
+                                     {(void**)&grid, sizeof(GridInfo)},
+                                     {(void**)&next, sizeof(unsigned long long)}}));
   k_support<<<num_bin_all, 128, 0, s>>>(x, num_modes, length, num_bin_all, data_freqs, data_length,
                                         sup, sup + num_bin_all);
   int st = launch_status("k_support");
@@ -1962,23 +2004,21 @@ int bbhx_direct_like_fused(double* d_h, double* h_h, const double* data_freqs, c
     A.gh = nullptr;
     A.gh_off = nullptr;
     A.grid = grid;
-    const long long warps_needed = (nitems + 0);
-    long long g = (warps_needed + FD_WARPS - 1) / FD_WARPS;
-    const long long cap = 16LL * sm_count();
-    unsigned grid = (unsigned)(g < cap ? g : cap);
-    if (precision == 1) {
-      const size_t sm = fused_smem_bytes<true>();
-      st = cuda_status(cudaFuncSetAttribute(k_direct_fused<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)sm),
-                       "cudaFuncSetAttribute(k_direct_fused<true>)");
-      if (!st) k_direct_fused<true><<<grid, FD_WARPS * 32, sm, s>>>(A);
-    } else {
-      const size_t sm = fused_smem_bytes<false>();
-      st = cuda_status(cudaFuncSetAttribute(k_direct_fused<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)sm),
-                       "cudaFuncSetAttribute(k_direct_fused<false>)");
-      if (!st) k_direct_fused<false><<<grid, FD_WARPS * 32, sm, s>>>(A);
-    }
+    A.next = next;
+    st = cuda_status(cudaMemsetAsync(next, 0, sizeof(unsigned long long), s), "work-queue counter");
+    auto launch = [&](auto kernel, size_t sm, const char* what) {
+      int r = cuda_status(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)sm),
+                          what);
+      if (!r) kernel<<<resident_grid(kernel, sm, nitems), FD_WARPS * 32, sm, s>>>(A);
+      return r;
+    };
+    if (!st)
+      st = (precision == 1)
+               ? launch(k_direct_fused<true>, fused_smem_bytes<true>(),
+                        "cudaFuncSetAttribute(k_direct_fused<true>)")
+               : launch(k_direct_fused<false>, fused_smem_bytes<false>(),
+                        "cudaFuncSetAttribute(k_direct_fused<false>)");
     if (!st) st = launch_status("k_direct_fused");
   }
   if (!st) {
@@ -1990,6 +2030,7 @@ int bbhx_direct_like_fused(double* d_h, double* h_h, const double* data_freqs, c
   pool_free(part, s);
   pool_free(segtab, s);
   pool_free(grid, s);
+  pool_free(next, s);
   return st;
 }
 
