@@ -39,6 +39,16 @@ enum Status : int {
   ERR_TOO_LARGE = 6,
 };
 
+// The calling warp's next work item from a launch's queue counter (zero at launch).  Items are
+// handed out in increasing order, so the warps in flight stay on neighbouring items; a warp that
+// finishes a cheap item takes the next one at once, so the resident warps stay busy until the
+// queue drains however unequal the items are.  Every lane of the warp must call it.
+__device__ __forceinline__ long long claim_item(unsigned long long* next, int lane) {
+  unsigned long long q = 0;
+  if (lane == 0) q = atomicAdd(next, 1ull);
+  return (long long)__shfl_sync(0xffffffffu, q, 0);
+}
+
 // Set *word when any of the values is NaN or infinite (the sum is non-finite then).
 __device__ __forceinline__ void note_nonfinite(unsigned* word, double a, double b, double c,
                                                double d) {

@@ -102,7 +102,7 @@ __global__ void __launch_bounds__(ADJ_THREADS)
 k_adj_coeffs(double* ybd, double* cb1, double* cb2, double* cb3, const cplx* gh,
              const long long* off, const int* start, const int* len, SplineRefs S,
              const double* data_freqs, int N, const double* t_start, const double* t_end, int b0,
-             int nb) {
+             int nb, unsigned long long* next) {
   __shared__ double sa[ADJ_THREADS / 32][32][12];  // per bin: a_0..a_7, 1, u, u^2, u^3
   __shared__ double scw[ADJ_THREADS / 32][36];      // the segment's (y, c1, c2, c3) x 9
   const int lane = threadIdx.x & 31;
@@ -111,8 +111,7 @@ k_adj_coeffs(double* ybd, double* cb1, double* cb2, double* cb3, const cplx* gh,
   const int mp = lane >> 2, mk = lane & 3;
   const long long nseg = (long long)S.L - 1;
   const long long total = (long long)nb * S.M * nseg;
-  for (long long wid = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; wid < total;
-       wid += ((long long)gridDim.x * blockDim.x) >> 5) {
+  for (long long wid = claim_item(next, lane); wid < total; wid = claim_item(next, lane)) {
     const int bl = (int)(wid / (S.M * nseg));
     const int m = (int)((wid / nseg) % S.M);
     const int s = (int)(wid % nseg);
@@ -474,7 +473,8 @@ int bbhx_direct_like_grad(void* orbits, void* d_h, void* h_h, double* grad, cons
   const int chunk = std::min(B, kDirectGradChunk);
   if (!st) {
     const size_t nscratch = nall * 5 + (size_t)B * M * L + (size_t)chunk * M * 2 * GRAD_CHUNK;
-    if (pool_alloc((void**)&ybd, sizeof(double) * nscratch, s) != cudaSuccess ||
+    // + one 8-byte word after the arrays: the work-queue counter of k_adj_coeffs
+    if (pool_alloc((void**)&ybd, sizeof(double) * (nscratch + 1), s) != cudaSuccess ||
         pool_alloc((void**)&cD, sizeof(ModeCoeffsT<GD>) * (size_t)chunk * M, s) != cudaSuccess ||
         pool_alloc((void**)&rD, sizeof(ResponseModeT<GD>) * (size_t)chunk * M, s) != cudaSuccess) {
       set_error("device allocation of the gradient scratch failed");
@@ -528,10 +528,27 @@ int bbhx_direct_like_grad(void* orbits, void* d_h, void* h_h, double* grad, cons
                            t_end, M, L, B, b0, nb, s);
     if (!st) {
       const long long warps = (long long)nb * M * (L - 1);
-      const unsigned grid = (unsigned)std::min<long long>((warps + 7) / 8, (long long)nsm * 64);
-      k_adj_coeffs<<<grid, ADJ_THREADS, 0, s>>>(ybd, cb, cb + nall, cb + 2 * nall, gh, off, start, len, S,
-                                        data_freqs, data_length, t_start, t_end, b0, nb);
-      st = launch_status("k_adj_coeffs");
+      unsigned long long* next = reinterpret_cast<unsigned long long*>(
+          ybd + nall * 5 + (size_t)B * M * L + (size_t)chunk * M * 2 * GRAD_CHUNK);
+      st = cuda_status(cudaMemsetAsync(next, 0, sizeof(unsigned long long), s),
+                       "work-queue counter");
+      // resident CTAs only: every warp claims segments until the queue drains (a segment holds
+      // from zero to ~10^4 data bins)
+      int per_sm = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adj_coeffs, ADJ_THREADS, 0) !=
+              cudaSuccess ||
+          per_sm < 1) {
+        (void)cudaGetLastError();
+        per_sm = 1;
+      }
+      const unsigned grid =
+          (unsigned)std::min<long long>((warps + 7) / 8, (long long)nsm * per_sm);
+      if (!st) {
+        k_adj_coeffs<<<grid, ADJ_THREADS, 0, s>>>(ybd, cb, cb + nall, cb + 2 * nall, gh, off,
+                                                  start, len, S, data_freqs, data_length, t_start,
+                                                  t_end, b0, nb, next);
+        st = launch_status("k_adj_coeffs");
+      }
     }
     if (!st) {
       k_spline_adj<<<(unsigned)std::min(nb * M, nsm * 4), 256, smem, s>>>(

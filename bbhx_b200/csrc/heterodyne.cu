@@ -52,14 +52,13 @@ __global__ void k_het_response_setup(HetArgs A) {
 // slice (the layout the adjoint needs; the strip layout of the uneven-batch kernel ran this
 // kernel ~20 % slower in the mixed form).
 template <bool MIXED, bool GH>
-__global__ void __launch_bounds__(HET_THREADS, 4) k_het_fused(HetArgs A) {
+__global__ void __launch_bounds__(HET_THREADS, 4) k_het_fused(HetArgs A, unsigned long long* next) {
   extern __shared__ __align__(16) unsigned char het_smem[];
   const HetSmemLayout lay(A.M, A.L, true);
   const int lane = threadIdx.x & 31;
-  const int nwarps = blockDim.x >> 5;
   const HetSlice W(het_smem + (size_t)(threadIdx.x >> 5) * align16(lay.total), lay);
-  for (int b = blockIdx.x * nwarps + (threadIdx.x >> 5); b < A.B; b += gridDim.x * nwarps)
-    het_item<MIXED, true, GH>(A, b, W, lane, &g_nonfinite_heterodyne);
+  for (long long b = claim_item(next, lane); b < A.B; b = claim_item(next, lane))
+    het_item<MIXED, true, GH>(A, (int)b, W, lane, &g_nonfinite_heterodyne);
 }
 
 // Warps (walkers) per CTA of k_het_fused and its dynamic shared memory: up to
@@ -88,22 +87,35 @@ int launch_het(HetArgs A, cudaStream_t s) {
   int st = het_launch_shape(A.M, A.L, true, &threads, &smem);
   if (st) return st;
   ResponseMode* rm = nullptr;
-  BBHX_CHECK_CUDA(pool_alloc((void**)&rm, sizeof(ResponseMode) * (size_t)A.B * A.M, s));
+  unsigned long long* next = nullptr;
+  BBHX_CHECK_CUDA(pool_alloc_all(s, {{(void**)&rm, sizeof(ResponseMode) * (size_t)A.B * A.M},
+                                     {(void**)&next, sizeof(unsigned long long)}}));
   A.rmodes = rm;
   k_het_response_setup<<<grid_for((long long)A.B * A.M, 128), 128, 0, s>>>(A);
   st = launch_status("k_het_response_setup");
-  const long long wpc = threads / 32;
-  const unsigned grid =
-      (unsigned)std::min<long long>((A.B + wpc - 1) / wpc, (long long)sm_count() * 16);
   if (!st)
     st = cuda_status(cudaFuncSetAttribute(k_het_fused<MIXED, GH>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                      "cudaFuncSetAttribute(k_het_fused)");
+  if (!st)
+    st = cuda_status(cudaMemsetAsync(next, 0, sizeof(unsigned long long), s), "work-queue counter");
   if (!st) {
-    k_het_fused<MIXED, GH><<<grid, threads, smem, s>>>(A);
+    // resident CTAs only: every warp claims walkers until the queue drains
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_het_fused<MIXED, GH>, threads,
+                                                      smem) != cudaSuccess ||
+        per_sm < 1) {
+      (void)cudaGetLastError();
+      per_sm = 1;
+    }
+    const long long wpc = threads / 32;
+    const unsigned grid =
+        (unsigned)std::min<long long>((A.B + wpc - 1) / wpc, (long long)sm_count() * per_sm);
+    k_het_fused<MIXED, GH><<<grid, threads, smem, s>>>(A, next);
     st = launch_status("k_het_fused");
   }
   pool_free(rm, s);
+  pool_free(next, s);
   return st;
 }
 

@@ -1246,16 +1246,6 @@ constexpr size_t fused_smem_bytes() {
   return FD_WARPS * (sizeof(WarpStage<R>) + (MIXED ? 0 : sizeof(RecStage)));
 }
 
-// The calling warp's next work item from the launch's queue counter.  Items are handed out in
-// increasing order, so the warps in flight stay on neighbouring items (the same data tile for
-// different binaries); a warp that finishes a cheap item takes the next one at once, so the
-// resident warps stay busy until the queue drains however unequal the items are.
-__device__ __forceinline__ long long claim_item(unsigned long long* next, int lane) {
-  unsigned long long q = 0;
-  if (lane == 0) q = atomicAdd(next, 1ull);
-  return (long long)__shfl_sync(0xffffffffu, q, 0);
-}
-
 template <bool MIXED, bool GH = false>
 __global__ void __launch_bounds__(FD_WARPS * 32, MIXED ? 4 : 3) k_direct_fused(FusedArgs A) {
   static_assert(!(MIXED && GH), "d lnL / d h is written by the FP64 form only");

@@ -225,23 +225,32 @@ __global__ void k_clear_build_flags(const BuildMulti* __restrict__ H) {
   if (blockIdx.x < H->ngroups && threadIdx.x < 3) H->g[blockIdx.x].flags[threadIdx.x] = 0;
 }
 
-// row = (problem, binary, mode); rows of all problems, CTAs striding over them.  The row's
-// records come from k_row_records.
+// row = (problem, binary, mode); rows of all problems, CTAs claiming them from a queue.  The
+// row's records come from k_row_records.
 __global__ void __launch_bounds__(SB_THREADS) k_sparse_build(const BuildMulti* __restrict__ H,
                                                               const RowRec* __restrict__ recs,
-                                                              int use_smem) {
+                                                              int use_smem,
+                                                              unsigned long long* next) {
   extern __shared__ double sb_smem[];
   __shared__ RowRec R;
+  __shared__ long long claimed;
   const int tid = threadIdx.x;
   const long long total = H->roff[H->ndirect];
-  for (long long row = blockIdx.x; row < total; row += gridDim.x) {
+  // rows are claimed from the launch's queue counter (rows of long sparse grids cost several
+  // times those of short ones, so a static row stride leaves CTAs idle)
+  for (;;) {
+    // every thread is done with the previous claim, its records and its work area
+    __syncthreads();
+    if (tid == 0) claimed = (long long)atomicAdd(next, 1ull);
+    __syncthreads();
+    const long long row = claimed;
+    if (row >= total) break;
     const int g = build_group(H, row);
     const BuildArgs& A = H->g[g];
     const long long r = row - H->roff[g];
     const int B = A.B, L = A.L;
     const int mm = A.run_phenomd ? 2 : A.mms[(int)(r % A.M)];
     double* work = use_smem ? sb_smem : A.scratch + (size_t)blockIdx.x * (4 + 9) * H->max_length;
-    __syncthreads();  // the previous row's records and work area are no longer read
     {
       const unsigned long long* src = reinterpret_cast<const unsigned long long*>(recs + row);
       unsigned long long* dst = reinterpret_cast<unsigned long long*>(&R);
@@ -387,20 +396,27 @@ int bbhx_uneven_batch(const bbhx_direct_source* direct, int num_direct,
     const size_t smem = sizeof(double) * (size_t)(4 + 9) * maxL;
     const bool use_smem = smem <= kBuildSmemMax;
     const int nsm = sm_count();
+    // two CTAs of SB_THREADS per SM (the register limit at 128 registers a thread)
     const unsigned grid = (unsigned)std::max<long long>(
-        1, std::min<long long>(rows_direct, (long long)nsm * (use_smem ? 2 : 1)));
+        1, std::min<long long>(rows_direct, (long long)nsm * 2));
     double* work = nullptr;
     BuildMulti* dH = nullptr;
     RowRec* recs = nullptr;
+    unsigned long long* next = nullptr;
     if (pool_alloc((void**)&dH, sizeof(BuildMulti), s) != cudaSuccess ||
         pool_alloc((void**)&recs, sizeof(RowRec) * (size_t)std::max(rows_direct, 1ll), s) != cudaSuccess ||
+        pool_alloc((void**)&next, sizeof(unsigned long long), s) != cudaSuccess ||
         (!use_smem && pool_alloc((void**)&work, sizeof(double) * grid * (size_t)(4 + 9) * maxL, s) != cudaSuccess)) {
       set_error("device allocation for the sparse build failed");
       st = ERR_CUDA;
     }
     if (dH) scratch.push_back(dH);
     if (recs) scratch.push_back(recs);
+    if (next) scratch.push_back(next);
     if (work) scratch.push_back(work);
+    if (!st)
+      st = cuda_status(cudaMemsetAsync(next, 0, sizeof(unsigned long long), s),
+                       "work-queue counter");
     if (!st) {
       for (int g = 0; g < num_direct; ++g) H.g[g].scratch = work;
       st = store_struct(&H, sizeof(H), dH, s);
@@ -420,7 +436,8 @@ int bbhx_uneven_batch(const bbhx_direct_source* direct, int num_direct,
                                               (int)smem),
                          "cudaFuncSetAttribute(k_sparse_build)");
       if (!st) {
-        k_sparse_build<<<grid, SB_THREADS, use_smem ? smem : 0, s>>>(dH, recs, use_smem ? 1 : 0);
+        k_sparse_build<<<grid, SB_THREADS, use_smem ? smem : 0, s>>>(dH, recs, use_smem ? 1 : 0,
+                                                                     next);
         st = launch_status("k_sparse_build");
       }
     }
