@@ -334,8 +334,8 @@ typedef struct {
 
 /* Direct and heterodyned problems with uneven grid lengths, mode sets, observation spans and
    sparse grids in ONE persistent launch: the walkers of every heterodyned problem and the
-   (data tile, binary) items of every direct problem form one work range that the warps stride
-   through (no reference counterpart).  direct / het: HOST arrays of at most 64 descriptors
+   (data tile, binary) items of every direct problem form one work range from which the warps
+   claim items through a queue counter (no reference counterpart).  direct / het: HOST arrays of at most 64 descriptors
    each (either may be empty); precision, tile_bins and ctas_per_sm as for
    bbhx_direct_like_multi (the heterodyned walkers use the same precision).  Stream-ordered,
    free of host synchronisation (graph-capturable). */
