@@ -182,9 +182,14 @@ __device__ __forceinline__ void phm_response_point(double* buf, long long n, lon
 // block: matrix once, P right-hand sides through one cyclic reduction in `work`
 // ((4 + P) L doubles: x, a, b, c, d[P][L]); slopes (optional) and c1, c2, c3 written in y's
 // layout.  Entry L-1 of c1 / c2 / c3 holds the last row's (0, diagonal, lower) entries.
-__device__ inline void spline_system(const double* xg, const double* y, long long pstride,
-                                     double* slopes, double* c1, double* c2, double* c3, int L,
-                                     int P, double* work) {
+// PT > 0 fixes P at compile time: a row's 3 PT (right-hand sides) and 2 PT (coefficients)
+// global loads are then issued together into registers instead of one quantity at a time.
+template <int PT>
+__device__ inline void spline_system_t(const double* xg, const double* y, long long pstride,
+                                       double* slopes, double* c1, double* c2, double* c3, int L,
+                                       int Pr, double* work) {
+  const int P = PT > 0 ? PT : Pr;
+  constexpr int NV = PT > 0 ? PT : 1;
   double* xs = work;
   double* a = xs + L;
   double* b = a + L;
@@ -193,7 +198,6 @@ __device__ inline void spline_system(const double* xg, const double* y, long lon
   for (int i = threadIdx.x; i < L; i += blockDim.x) xs[i] = xg[i];
   __syncthreads();
   for (int i = threadIdx.x; i < L; i += blockDim.x) {
-    double dx1, dx2, dd;
     int i0, i1, i2;
     if (i == 0) {
       i0 = 0; i1 = 1; i2 = 2;
@@ -202,9 +206,9 @@ __device__ inline void spline_system(const double* xg, const double* y, long lon
     } else {
       i0 = i - 1; i1 = i; i2 = i + 1;
     }
-    dx1 = xs[i1] - xs[i0];
-    dx2 = xs[i2] - xs[i1];
-    dd = xs[i2] - xs[i0];
+    const double dx1 = xs[i1] - xs[i0];
+    const double dx2 = xs[i2] - xs[i1];
+    const double dd = xs[i2] - xs[i0];
     if (i == 0) {
       a[i] = 0.0; b[i] = dx2; c[i] = dd;
     } else if (i == L - 1) {
@@ -212,48 +216,78 @@ __device__ inline void spline_system(const double* xg, const double* y, long lon
     } else {
       a[i] = dx2; b[i] = 2 * (dx1 + dx2); c[i] = dx1;
     }
-    for (int p = 0; p < P; ++p) {
-      const double* yg = y + (long long)p * pstride;
-      double y1 = yg[i1];
-      double m1 = (y1 - yg[i0]) / dx1;
-      double m2 = (yg[i2] - y1) / dx2;
-      double r;
-      if (i == 0)
-        r = ((dx1 + 2 * dd) * dx2 * m1 + dx1 * dx1 * m2) / dd;
-      else if (i == L - 1)
-        r = (dx2 * dx2 * m1 + (2 * dd + dx2) * dx1 * m2) / dd;
-      else
-        r = 3.0 * (dx2 * m1 + dx1 * m2);
-      d[(size_t)p * L + i] = r;
-    }
-  }
-  __syncthreads();
-  // keep the last row's matrix entries for the c1/c2/c3[L-1] convention
-  double last_a = a[L - 1], last_b = b[L - 1];
-  __syncthreads();
-  cr_solve(a, b, c, d, L, P, L);
-  for (int p = 0; p < P; ++p) {
-    const double* yg = y + (long long)p * pstride;
-    const long long o = (long long)p * pstride;
-    const double* sp = d + (size_t)p * L;
-    for (int i = threadIdx.x; i < L; i += blockDim.x) {
-      double si = sp[i];
-      if (slopes) slopes[o + i] = si;
-      if (i < L - 1) {
-        double h = xs[i + 1] - xs[i];
-        double m = (yg[i + 1] - yg[i]) / h;
-        double t = (si + sp[i + 1] - 2 * m) / h;
-        c1[o + i] = si;
-        c2[o + i] = (m - si) / h - t;
-        c3[o + i] = t / h;
-      } else {
-        c1[o + i] = 0.0;
-        c2[o + i] = last_b;
-        c3[o + i] = last_a;
+    for (int p0 = 0; p0 < P; p0 += NV) {
+      double v0[NV], v1[NV], v2[NV];
+#pragma unroll
+      for (int q = 0; q < NV; ++q) {
+        const double* yg = y + (long long)(p0 + q) * pstride;
+        v0[q] = yg[i0];
+        v1[q] = yg[i1];
+        v2[q] = yg[i2];
+      }
+#pragma unroll
+      for (int q = 0; q < NV; ++q) {
+        const double m1 = (v1[q] - v0[q]) / dx1;
+        const double m2 = (v2[q] - v1[q]) / dx2;
+        double r;
+        if (i == 0)
+          r = ((dx1 + 2 * dd) * dx2 * m1 + dx1 * dx1 * m2) / dd;
+        else if (i == L - 1)
+          r = (dx2 * dx2 * m1 + (2 * dd + dx2) * dx1 * m2) / dd;
+        else
+          r = 3.0 * (dx2 * m1 + dx1 * m2);
+        d[(size_t)(p0 + q) * L + i] = r;
       }
     }
   }
   __syncthreads();
+  // keep the last row's matrix entries for the c1/c2/c3[L-1] convention
+  const double last_a = a[L - 1], last_b = b[L - 1];
+  __syncthreads();
+  cr_solve(a, b, c, d, L, P, L);
+  for (int i = threadIdx.x; i < L; i += blockDim.x) {
+    const bool seg = i < L - 1;
+    const double h = seg ? xs[i + 1] - xs[i] : 1.0;
+    for (int p0 = 0; p0 < P; p0 += NV) {
+      double ylo[NV], yhi[NV];
+#pragma unroll
+      for (int q = 0; q < NV; ++q) {
+        const double* yg = y + (long long)(p0 + q) * pstride;
+        ylo[q] = yg[i];
+        yhi[q] = seg ? yg[i + 1] : 0.0;
+      }
+#pragma unroll
+      for (int q = 0; q < NV; ++q) {
+        const long long o = (long long)(p0 + q) * pstride;
+        const double* sp = d + (size_t)(p0 + q) * L;
+        const double si = sp[i];
+        if (slopes) slopes[o + i] = si;
+        if (seg) {
+          const double m = (yhi[q] - ylo[q]) / h;
+          const double t = (si + sp[i + 1] - 2 * m) / h;
+          c1[o + i] = si;
+          c2[o + i] = (m - si) / h - t;
+          c3[o + i] = t / h;
+        } else {
+          c1[o + i] = 0.0;
+          c2[o + i] = last_b;
+          c3[o + i] = last_a;
+        }
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// The interpolants of the sparse buffer are nine quantities (amplitude, phase, t(f) and six
+// transfer components); other counts take the generic path.
+__device__ inline void spline_system(const double* xg, const double* y, long long pstride,
+                                     double* slopes, double* c1, double* c2, double* c3, int L,
+                                     int P, double* work) {
+  if (P == 9)
+    spline_system_t<9>(xg, y, pstride, slopes, c1, c2, c3, L, P, work);
+  else
+    spline_system_t<0>(xg, y, pstride, slopes, c1, c2, c3, L, P, work);
 }
 
 }  // namespace bbhx
