@@ -858,13 +858,15 @@ __device__ __forceinline__ void stage_segments(const FusedArgs& A, WarpStage<R>&
   }
 }
 
-// One WARP item = (data tile of FD_TILE bins, binary).  Items are enumerated tile-major, so the
-// warps in flight work on the same data tile for different binaries and share it through L2.
+// One WARP item = (data tile of FD_TILE bins, binary).  Items are enumerated tile-major and
+// claimed in increasing order (claim_item), so the warps in flight work on the same data tile
+// for different binaries and share it through L2.
 // The warp stages the tile's segments of every mode (from the segment table) into its slice of
 // shared memory, then walks the tile in FD_TILE / FD_WARP_BINS chunks of 128 bins (lane l owns
 // bins chunk + l + 32 j, j < FD_K) and keeps the <d|h>, <h|h> partial sums in registers; no
-// block-wide barrier is involved.  Tiles whose modes span more than NSEG segments (only the
-// lowest frequencies) take a per-lane walk over global memory instead.
+// block-wide barrier is involved.  Modes whose tile spans more than NSEG segments (low
+// frequencies) are staged a window of NSEG segments at a time from a forward cursor in the FP64
+// form, and walked per lane over global memory in the mixed form.
 // MIXED: phase, t(f), the phase reduction and all accumulations in FP64; amplitude, transfer
 // functions, sin/cos of the reduced phase and the mode sum (the template) in FP32; the per-bin
 // products with data and weights in FP64 when the FP32 copies of data and weights are given
