@@ -5,6 +5,7 @@
 //   waveform_amp_phase.
 // Layout of the waveform buffer (phenomhm.py:201-249): flat [nparams, B, M, L] with
 // slot 0 = amplitude, 1 = phase, 2 = t(f); freqs flat [B, M, L].
+#include <algorithm>
 #include <mutex>
 
 #include "capi_internal.cuh"
@@ -108,16 +109,19 @@ __global__ void k_phm_tf(double* tf_out, const double* freqs, const ModeCoeffs* 
 //   freqs_in/tf: [BM, L]; Tobs [BM]; writes freqs_out [BM, L] and fminmax [BM, 2].
 // err[0] is set to 1 (lower edge) or 2 (upper edge) when a row that needs clipping does not
 // have exactly one crossing (the reference raises ValueError there).
+// One CTA per row: the edges by block reductions (the same results as the sequential scan),
+// then the row's knots by all threads.
 __global__ void k_tf_window(double* freqs_out, double* fminmax, const double* freqs_in,
                             const double* tf, const double* Tobs, int L, long long BM, int* err) {
-  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < BM;
-       r += (long long)gridDim.x * blockDim.x) {
-    const WindowEdges w = tf_window_edges(freqs_in + r * L, tf + r * L, L, Tobs[r]);
-    if (w.err) atomicCAS(err, 0, w.err);
-    fminmax[2 * r] = w.flo;
-    fminmax[2 * r + 1] = w.fhi;
+  for (long long r = blockIdx.x; r < BM; r += gridDim.x) {
+    const WindowEdges w = tf_window_edges_block(freqs_in + r * L, tf + r * L, L, Tobs[r]);
+    if (threadIdx.x == 0) {
+      if (w.err) atomicCAS(err, 0, w.err);
+      fminmax[2 * r] = w.flo;
+      fminmax[2 * r + 1] = w.fhi;
+    }
     double* o = freqs_out + r * L;
-    for (int k = 0; k < L; ++k) o[k] = window_knot(k, L, w.flo, w.fhi);
+    for (int k = threadIdx.x; k < L; k += blockDim.x) o[k] = window_knot(k, L, w.flo, w.fhi);
   }
 }
 
@@ -380,8 +384,9 @@ int bbhx_tf_window_regrid(double* freqs_out, double* fminmax, const double* freq
                           int* err_dev, void* stream) {
   BBHX_REQUIRE(length >= 2, "length must be >= 2");
   if (num_rows == 0) return OK;
-  k_tf_window<<<grid_for(num_rows, 128), 128, 0, (cudaStream_t)stream>>>(
-      freqs_out, fminmax, freqs_in, tf, Tobs, length, num_rows, err_dev);
+  const unsigned grid = (unsigned)std::min<long long>(num_rows, (long long)sm_count() * 16);
+  k_tf_window<<<grid, 128, 0, (cudaStream_t)stream>>>(freqs_out, fminmax, freqs_in, tf, Tobs,
+                                                      length, num_rows, err_dev);
   return launch_status("k_tf_window");
 }
 

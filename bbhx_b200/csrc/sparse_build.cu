@@ -143,84 +143,6 @@ __global__ void k_row_records(const BuildMulti* __restrict__ H, RowRec* recs) {
   }
 }
 
-// Window edges of one row by the whole block: the same minima, maxima and crossing counts as
-// tf_window_edges (sparse_stages.cuh) formed by block reductions, then the same formulas.
-__device__ inline WindowEdges tf_window_edges_block(const double* f, const double* x, int L,
-                                                    double To) {
-  __shared__ double r_d[4][32];
-  __shared__ int r_i[4][32];
-  __shared__ WindowEdges out;
-  double tmin = x[0], tmax = x[0], flo = f[0], fhi = f[0];
-  int c0 = 0, c1 = 0, s0 = L, s1 = L;
-  for (int i = threadIdx.x; i < L; i += blockDim.x) {
-    tmin = fmin(tmin, x[i]);
-    tmax = fmax(tmax, x[i]);
-    flo = fmin(flo, f[i]);
-    fhi = fmax(fhi, f[i]);
-    if (i < L - 1) {
-      if ((0.0 < x[i + 1]) && (0.0 > x[i])) {
-        ++c0;
-        s0 = min(s0, i);
-      }
-      if ((To < x[i + 1]) && (To > x[i])) {
-        ++c1;
-        s1 = min(s1, i);
-      }
-    }
-  }
-  for (int o = 16; o > 0; o >>= 1) {
-    tmin = fmin(tmin, __shfl_xor_sync(0xffffffffu, tmin, o));
-    tmax = fmax(tmax, __shfl_xor_sync(0xffffffffu, tmax, o));
-    flo = fmin(flo, __shfl_xor_sync(0xffffffffu, flo, o));
-    fhi = fmax(fhi, __shfl_xor_sync(0xffffffffu, fhi, o));
-    c0 += __shfl_xor_sync(0xffffffffu, c0, o);
-    c1 += __shfl_xor_sync(0xffffffffu, c1, o);
-    s0 = min(s0, __shfl_xor_sync(0xffffffffu, s0, o));
-    s1 = min(s1, __shfl_xor_sync(0xffffffffu, s1, o));
-  }
-  const int w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-  if ((threadIdx.x & 31) == 0) {
-    r_d[0][w] = tmin; r_d[1][w] = tmax; r_d[2][w] = flo; r_d[3][w] = fhi;
-    r_i[0][w] = c0; r_i[1][w] = c1; r_i[2][w] = s0; r_i[3][w] = s1;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int k = 1; k < nw; ++k) {
-      tmin = fmin(tmin, r_d[0][k]);
-      tmax = fmax(tmax, r_d[1][k]);
-      flo = fmin(flo, r_d[2][k]);
-      fhi = fmax(fhi, r_d[3][k]);
-      c0 += r_i[0][k];
-      c1 += r_i[1][k];
-      s0 = min(s0, r_i[2][k]);
-      s1 = min(s1, r_i[3][k]);
-    }
-    WindowEdges e;
-    e.err = 0;
-    e.flo = flo;
-    e.fhi = fhi;
-    if (tmin < 0.0) {
-      if (c0 != 1) {
-        e.err = 1;
-      } else {
-        double m = (f[s0 + 1] - f[s0]) / (x[s0 + 1] - x[s0]);
-        e.flo = m * (0.0 - x[s0]) + f[s0];
-      }
-    }
-    if (tmax > To) {
-      if (c1 != 1) {
-        if (e.err == 0) e.err = 2;
-      } else {
-        double m = (f[s1 + 1] - f[s1]) / (x[s1 + 1] - x[s1]);
-        e.fhi = m * (To - x[s1]) + f[s1];
-      }
-    }
-    out = e;
-  }
-  __syncthreads();
-  return out;
-}
-
 __global__ void k_clear_build_flags(const BuildMulti* __restrict__ H) {
   if (blockIdx.x < H->ngroups && threadIdx.x < 3) H->g[blockIdx.x].flags[threadIdx.x] = 0;
 }

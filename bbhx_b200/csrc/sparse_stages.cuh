@@ -103,47 +103,83 @@ struct WindowEdges {
   double flo, fhi;
   int err;
 };
-__device__ inline WindowEdges tf_window_edges(const double* f, const double* x, int L, double To) {
-  WindowEdges w;
-  w.err = 0;
-  double tmin = x[0], tmax = x[0];
-  w.flo = f[0];
-  w.fhi = f[0];
-  for (int i = 1; i < L; ++i) {
+// The edges of one row by the whole block: the minima and maxima of t(f) and f, and the number
+// and first index of the intervals whose t(f) crosses 0 and To, by block reductions (exact, so
+// independent of the block size), then the crossing formulas of phenomhm.py:520-606.
+__device__ inline WindowEdges tf_window_edges_block(const double* f, const double* x, int L,
+                                                    double To) {
+  __shared__ double r_d[4][32];
+  __shared__ int r_i[4][32];
+  __shared__ WindowEdges out;
+  double tmin = x[0], tmax = x[0], flo = f[0], fhi = f[0];
+  int c0 = 0, c1 = 0, s0 = L, s1 = L;
+  for (int i = threadIdx.x; i < L; i += blockDim.x) {
     tmin = fmin(tmin, x[i]);
     tmax = fmax(tmax, x[i]);
-    w.flo = fmin(w.flo, f[i]);
-    w.fhi = fmax(w.fhi, f[i]);
-  }
-  if (tmin < 0.0) {
-    int cnt = 0, seg = -1;
-    for (int i = 0; i < L - 1; ++i)
+    flo = fmin(flo, f[i]);
+    fhi = fmax(fhi, f[i]);
+    if (i < L - 1) {
       if ((0.0 < x[i + 1]) && (0.0 > x[i])) {
-        if (cnt == 0) seg = i;
-        ++cnt;
+        ++c0;
+        s0 = min(s0, i);
       }
-    if (cnt != 1) {
-      w.err = 1;
-    } else {
-      double m = (f[seg + 1] - f[seg]) / (x[seg + 1] - x[seg]);
-      w.flo = m * (0.0 - x[seg]) + f[seg];
-    }
-  }
-  if (tmax > To) {
-    int cnt = 0, seg = -1;
-    for (int i = 0; i < L - 1; ++i)
       if ((To < x[i + 1]) && (To > x[i])) {
-        if (cnt == 0) seg = i;
-        ++cnt;
+        ++c1;
+        s1 = min(s1, i);
       }
-    if (cnt != 1) {
-      if (w.err == 0) w.err = 2;
-    } else {
-      double m = (f[seg + 1] - f[seg]) / (x[seg + 1] - x[seg]);
-      w.fhi = m * (To - x[seg]) + f[seg];
     }
   }
-  return w;
+  for (int o = 16; o > 0; o >>= 1) {
+    tmin = fmin(tmin, __shfl_xor_sync(0xffffffffu, tmin, o));
+    tmax = fmax(tmax, __shfl_xor_sync(0xffffffffu, tmax, o));
+    flo = fmin(flo, __shfl_xor_sync(0xffffffffu, flo, o));
+    fhi = fmax(fhi, __shfl_xor_sync(0xffffffffu, fhi, o));
+    c0 += __shfl_xor_sync(0xffffffffu, c0, o);
+    c1 += __shfl_xor_sync(0xffffffffu, c1, o);
+    s0 = min(s0, __shfl_xor_sync(0xffffffffu, s0, o));
+    s1 = min(s1, __shfl_xor_sync(0xffffffffu, s1, o));
+  }
+  const int w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    r_d[0][w] = tmin; r_d[1][w] = tmax; r_d[2][w] = flo; r_d[3][w] = fhi;
+    r_i[0][w] = c0; r_i[1][w] = c1; r_i[2][w] = s0; r_i[3][w] = s1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < nw; ++k) {
+      tmin = fmin(tmin, r_d[0][k]);
+      tmax = fmax(tmax, r_d[1][k]);
+      flo = fmin(flo, r_d[2][k]);
+      fhi = fmax(fhi, r_d[3][k]);
+      c0 += r_i[0][k];
+      c1 += r_i[1][k];
+      s0 = min(s0, r_i[2][k]);
+      s1 = min(s1, r_i[3][k]);
+    }
+    WindowEdges e;
+    e.err = 0;
+    e.flo = flo;
+    e.fhi = fhi;
+    if (tmin < 0.0) {
+      if (c0 != 1) {
+        e.err = 1;
+      } else {
+        double m = (f[s0 + 1] - f[s0]) / (x[s0 + 1] - x[s0]);
+        e.flo = m * (0.0 - x[s0]) + f[s0];
+      }
+    }
+    if (tmax > To) {
+      if (c1 != 1) {
+        if (e.err == 0) e.err = 2;
+      } else {
+        double m = (f[s1 + 1] - f[s1]) / (x[s1 + 1] - x[s1]);
+        e.fhi = m * (To - x[s1]) + f[s1];
+      }
+    }
+    out = e;
+  }
+  __syncthreads();
+  return out;
 }
 
 // Knot k of the regridded row (phenomhm.py:608-610, numpy.logspace: y_k = k * step + start
