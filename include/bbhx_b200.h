@@ -335,8 +335,9 @@ typedef struct {
 /* Direct and heterodyned problems with uneven grid lengths, mode sets, observation spans and
    sparse grids in ONE persistent launch: the walkers of every heterodyned problem and the
    (data tile, binary) items of every direct problem form one work range from which the warps
-   claim items through a queue counter (no reference counterpart).  direct / het: HOST arrays of at most 64 descriptors
-   each (either may be empty); precision, tile_bins and ctas_per_sm as for
+   claim items through a queue counter (no reference counterpart).  direct / het: HOST arrays
+   of at most 64 descriptors each (either may be empty); precision, tile_bins and ctas_per_sm
+   as for
    bbhx_direct_like_multi (the heterodyned walkers use the same precision).  Stream-ordered,
    free of host synchronisation (graph-capturable). */
 int bbhx_uneven_like(const bbhx_direct_group *direct, int num_direct, const bbhx_hdyn_group *het,
@@ -358,11 +359,12 @@ typedef struct bbhx_hdyn_source {
   int *flags;
 } bbhx_hdyn_source;
 
-/* A whole uneven batch from parameters: the sparse grids and splines of every direct problem
-   in ONE launch (one CTA per (binary, mode) row: records, default grid and t(f), window regrid,
-   waveform + response, coverage check, spline) -- the same launch that sets up the records
-   also makes the heterodyned walkers' PhenomHM records and observation limits -- then
-   bbhx_uneven_like.  No reference counterpart; stream-ordered and graph-capturable. */
+/* A whole uneven batch from parameters: one launch makes the records of every row (direct
+   rows: PhenomHM and response-mode records and observation limits; heterodyned walkers:
+   PhenomHM records and observation limits), one launch builds the sparse grids and splines of
+   every direct problem (one CTA per (binary, mode) row: default grid and t(f), window regrid,
+   waveform + response, coverage check, spline), then bbhx_uneven_like.  No reference
+   counterpart; stream-ordered and graph-capturable. */
 int bbhx_uneven_batch(const bbhx_direct_source *direct, int num_direct,
                       const struct bbhx_hdyn_source *het, int num_het, int precision,
                       int tile_bins, int ctas_per_sm, void *stream);
