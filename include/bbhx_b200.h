@@ -337,9 +337,8 @@ typedef struct {
    (data tile, binary) items of every direct problem form one work range from which the warps
    claim items through a queue counter (no reference counterpart).  direct / het: HOST arrays
    of at most 64 descriptors each (either may be empty); precision, tile_bins and ctas_per_sm
-   as for
-   bbhx_direct_like_multi (the heterodyned walkers use the same precision).  Stream-ordered,
-   free of host synchronisation (graph-capturable). */
+   as for bbhx_direct_like_multi (the heterodyned walkers use the same precision).
+   Stream-ordered, free of host synchronisation (graph-capturable). */
 int bbhx_uneven_like(const bbhx_direct_group *direct, int num_direct, const bbhx_hdyn_group *het,
                      int num_het, int precision, int tile_bins, int ctas_per_sm, void *stream);
 
