@@ -94,19 +94,34 @@ struct SplineRefs {
 // 2. Warp per (local binary, mode, segment s < L-1): sums over the segment's data bins of
 // a_p, a_p u, a_p u^2, a_p u^3 with a_p = d lnL / d q_p (p = amp, phase, 6 transfers), into
 // ybd (d lnL / d y directly) and cb1..cb3 (d lnL / d c1..c3), all [9, B, M, L].
-// The warp takes 32 bins at a time: lane j evaluates bin j's eight a_p and the powers of u
-// into shared memory, then lane l owns the sum of (p, k) = (l / 4, l % 4) and adds the 32
-// bins' a_p u^k, so each lane keeps one accumulator instead of 32.
-constexpr int ADJ_THREADS = 256;
-__global__ void __launch_bounds__(ADJ_THREADS)
+// Each lane walks its own bins of the segment (k0 + lane, + 32, ...) and keeps the 32 moment
+// sums of those bins in registers; at the end of the segment one transposing reduction across
+// the warp (31 shuffles) leaves the total of moment l = (p, k) = (l / 4, l % 4) in lane l.
+constexpr int ADJ_THREADS = 128;
+
+// m[0..31] of every lane -> lane l returns the warp total of m[l] (recursive halving: at the
+// step of width w a lane keeps the half of its w values whose index bit matches its lane bit).
+__device__ __forceinline__ double warp_transpose_sum32(double (&m)[32], int lane) {
+#pragma unroll
+  for (int w = 16; w >= 1; w >>= 1) {
+    const bool upper = (lane & w) != 0;
+#pragma unroll
+    for (int i = 0; i < w; ++i) {
+      const double send = upper ? m[i] : m[i + w];
+      const double keep = upper ? m[i + w] : m[i];
+      m[i] = keep + __shfl_xor_sync(0xffffffffu, send, w);
+    }
+  }
+  return m[0];
+}
+
+__global__ void __launch_bounds__(ADJ_THREADS, 3)
 k_adj_coeffs(double* ybd, double* cb1, double* cb2, double* cb3, const cplx* gh,
              const long long* off, const int* start, const int* len, SplineRefs S,
              const double* data_freqs, int N, const double* t_start, const double* t_end, int b0,
              int nb, unsigned long long* next) {
-  __shared__ double sa[ADJ_THREADS / 32][32][12];  // per bin: a_0..a_7, 1, u, u^2, u^3
-  __shared__ double scw[ADJ_THREADS / 32][36];      // the segment's (y, c1, c2, c3) x 9
+  __shared__ double scw[ADJ_THREADS / 32][36];  // the segment's (y, c1, c2, c3) x 9
   const int lane = threadIdx.x & 31;
-  double (*w)[12] = sa[threadIdx.x >> 5];
   double* cw = scw[threadIdx.x >> 5];
   const int mp = lane >> 2, mk = lane & 3;
   const long long nseg = (long long)S.L - 1;
@@ -123,7 +138,6 @@ k_adj_coeffs(double* ybd, double* cb1, double* cb2, double* cb3, const cplx* gh,
     int k1 = lower_bound_guess(data_freqs, N, xs[s + 1]);
     k0 = max(k0, st);
     k1 = min(k1, st + n);
-    double acc = 0.0;
     const double ts = t_start[b], te = t_end[b];
     __syncwarp();  // the previous item's coefficients are no longer read
     for (int i = lane; i < 36; i += 32) {
@@ -131,46 +145,44 @@ k_adj_coeffs(double* ybd, double* cb1, double* cb2, double* cb3, const cplx* gh,
       cw[i] = src[(size_t)(i >> 2) * S.n + row * S.L + s];
     }
     __syncwarp();
-    for (int base = k0; base < k1; base += 32) {
-      const int k = base + lane;
+    double mom[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) mom[i] = 0.0;
+    const double xk = xs[s];
+    for (int k = k0 + lane; k < k1; k += 32) {
+      const double u = data_freqs[k] - xk;
+      double q[9];
+#pragma unroll
+      for (int p = 0; p < 9; ++p)
+        q[p] = cw[4 * p] + u * (cw[4 * p + 1] + u * (cw[4 * p + 2] + u * cw[4 * p + 3]));
+      if (!tf_gate(q[2], ts, te)) continue;
+      const cplx* g = gh + (off[bl] + (k - st)) * 3;
+      double sn, cs;
+      sincos_cw(q[1], &sn, &cs);
+      const double er = cs, ei = sn;                  // e^{i phase}
+      const double aer = q[0] * er, aei = q[0] * ei;  // A e^{i phase}
       double a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-      double u = 0.0;
-      if (k < k1) {
-        u = data_freqs[k] - xs[s];
-        double q[9];
 #pragma unroll
-        for (int p = 0; p < 9; ++p)
-          q[p] = cw[4 * p] + u * (cw[4 * p + 1] + u * (cw[4 * p + 2] + u * cw[4 * p + 3]));
-        if (tf_gate(q[2], ts, te)) {
-          const cplx* g = gh + (off[bl] + (k - st)) * 3;
-          double sn, cs;
-          sincos_cw(q[1], &sn, &cs);
-          const double er = cs, ei = sn;                  // e^{i phase}
-          const double aer = q[0] * er, aei = q[0] * ei;  // A e^{i phase}
-#pragma unroll
-          for (int ch = 0; ch < 3; ++ch) {
-            const cplx u_ = g[ch];
-            const double tr = q[3 + 2 * ch], ti = q[4 + 2 * ch];
-            // dL = Re(u dW), W = T A e^{i phase}
-            const double wr = tr * aer - ti * aei, wi = tr * aei + ti * aer;
-            a[0] += u_.re * (tr * er - ti * ei) - u_.im * (tr * ei + ti * er);
-            a[1] += -(u_.re * wi + u_.im * wr);
-            a[2 + 2 * ch] = u_.re * aer - u_.im * aei;
-            a[3 + 2 * ch] = -(u_.re * aei + u_.im * aer);
-          }
-        }
+      for (int ch = 0; ch < 3; ++ch) {
+        const cplx u_ = g[ch];
+        const double tr = q[3 + 2 * ch], ti = q[4 + 2 * ch];
+        // dL = Re(u dW), W = T A e^{i phase}
+        const double wr = tr * aer - ti * aei, wi = tr * aei + ti * aer;
+        a[0] += u_.re * (tr * er - ti * ei) - u_.im * (tr * ei + ti * er);
+        a[1] += -(u_.re * wi + u_.im * wr);
+        a[2 + 2 * ch] = u_.re * aer - u_.im * aei;
+        a[3 + 2 * ch] = -(u_.re * aei + u_.im * aer);
       }
+      const double u2 = u * u, u3 = u2 * u;
 #pragma unroll
-      for (int p = 0; p < 8; ++p) w[lane][p] = a[p];
-      w[lane][8] = 1.0;
-      w[lane][9] = u;
-      w[lane][10] = u * u;
-      w[lane][11] = u * u * u;
-      __syncwarp();
-      const int cnt = min(32, k1 - base);
-      for (int j = 0; j < cnt; ++j) acc = fma(w[j][mp], w[j][8 + mk], acc);
-      __syncwarp();
+      for (int p = 0; p < 8; ++p) {
+        mom[4 * p] += a[p];
+        mom[4 * p + 1] = fma(a[p], u, mom[4 * p + 1]);
+        mom[4 * p + 2] = fma(a[p], u2, mom[4 * p + 2]);
+        mom[4 * p + 3] = fma(a[p], u3, mom[4 * p + 3]);
+      }
     }
+    const double acc = warp_transpose_sum32(mom, lane);
     const int slot = (mp == 0) ? 0 : (mp == 1 ? 1 : mp + 1);  // skip t(f), slot 2
     const size_t i = (size_t)slot * S.n + row * S.L + s;
     double* dst = (mk == 0) ? ybd : (mk == 1) ? cb1 : (mk == 2) ? cb2 : cb3;
