@@ -45,6 +45,11 @@ MIXED_BYTES_PER_PAIR = 36.0  # 3 x complex64 + 3 x float32: the FP32 copies the 
 # 3 complex transfer functions) x 3 FMAs, 3 complex products of the phase recurrence x 4, the
 # amplitude times e^{i phi} 2, and the 3 channels' complex multiply-accumulates x 4
 FP64_INSTR_PER_PAIR_MODE = 7 * 3 + 3 * 4 + 2 + 3 * 4
+# the library's kernels in one direct step (ncu launch list): k_clear_flags, k_step_front,
+# k_ringdown_hm, k_ringdown_d, k_phm_setup, k_default_freqs, k_phm_tf, k_tf_window,
+# k_response_setup, k_phm_response, k_tf_range, k_spline, k_support, k_grid_detect,
+# k_tile_segments, k_direct_fused, k_fused_reduce, k_pack_lnl
+LAUNCHES_PER_STEP = 18
 
 
 def parse():
@@ -257,6 +262,8 @@ def gpu_arm(args):
     from bbhx_b200 import build_ext
 
     build_ext.build()
+    from bbhx_b200.likelihood import pack_lnl
+
     B = args.batch
     wave, like, params, f = build_problem(B, shard_seed(rank))
     dev_params = tuple(torch.as_tensor(params[k], device="cuda") for k in range(12))
@@ -269,7 +276,7 @@ def gpu_arm(args):
                                        precision=precision,
                                        data32=like.fp32_data() if precision == "mixed" else None,
                                        **kw)
-        return -0.5 * (like.d_d + h_h - 2 * d_h).real
+        return pack_lnl(d_h, h_h, like.d_d)
 
     def barrier():
         if world > 1:
@@ -416,7 +423,7 @@ def gpu_arm(args):
                      "kernel_ms": statistics.mean(fused_ms),
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback",
                      "fp64_floor": fp64_floor(pairs, wave.num_modes, fused_avg_s, peak)},
-        "gpu_launches": 12 * args.steps,
+        "gpu_launches": LAUNCHES_PER_STEP * args.steps,
         "clocks": clocks,
     }
     res.update(extra)
