@@ -555,7 +555,16 @@ def het_metric(args, wave, like, f, params):
         "finite": bool(np.all(np.isfinite(ll64)) and np.all(np.isfinite(llmx)))}}
 
 
-FP64_LANE_OPS_PER_S = 148 * 64 * 1.965e9  # B200: 64 FP64 lanes per SM (nominal, 1965 MHz)
+def fp64_lane_rate():
+    """FP64 lane operations per second: the device's SMs x 64 FP64 lanes (B200) x the nominal
+    1965 MHz SM clock."""
+    import torch
+
+    try:
+        sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    except Exception:
+        sms = 148
+    return sms * 64 * 1.965e9
 OPC_NAMES = ("add_sub", "mul", "div", "compare", "sqrt", "cbrt", "log", "exp", "pow", "atan",
              "sin_cos", "other")
 
@@ -565,19 +574,19 @@ def fp64_floor(pairs, modes, kernel_s, hbm_peak_gbs):
     (pair, mode) (pairs x modes is an upper bound: every mode counted over the union support) at
     the nominal FP64 lane rate give the shortest possible kernel time, and the HBM-roofline
     fraction the kernel would reach there."""
-    floor_s = FP64_INSTR_PER_PAIR_MODE * pairs * modes / FP64_LANE_OPS_PER_S
+    floor_s = FP64_INSTR_PER_PAIR_MODE * pairs * modes / fp64_lane_rate()
     return {"fp64_instr_per_pair_mode": FP64_INSTR_PER_PAIR_MODE, "floor_ms": floor_s * 1e3,
             "kernel_over_floor": kernel_s / floor_s,
             "hbm_frac_at_floor": HBM_BYTES_PER_PAIR * pairs / floor_s / 1e9 / hbm_peak_gbs,
-            "lane_rate": "nominal 148 SMs x 64 FP64 lanes x 1965 MHz"}
+            "lane_rate": "the device's SMs x 64 FP64 lanes x 1965 MHz (nominal clock)"}
 
 
 def het_roofline(het, wave, center, evals_per_s):
     """FP64 roofline of the heterodyned form: the algorithmic operations of one (walker, mode,
     frequency) point, tallied by running the templated FP64 model on an op-counting scalar
     (bbhx_count_point_ops; the per-binary set-up and the per-bin relative-binning arithmetic
-    are excluded), times the points per second, against the nominal FP64 lane rate (148 SMs x
-    64 lanes x 1965 MHz; no measured FP64 peak exists for this pool)."""
+    are excluded), times the points per second, against the nominal FP64 lane rate (the
+    device's SMs x 64 lanes x 1965 MHz; the measured peaks hold no FP64 figure)."""
     import torch
 
     from bbhx_b200 import _lib
@@ -600,10 +609,10 @@ def het_roofline(het, wave, center, evals_per_s):
     points_per_s = evals_per_s * M * L
     return {"ops_per_point": per_point, "arith_ops_per_point": arith,
             "elementary_calls_per_point": special, "points_per_s": points_per_s,
-            "arith_ops_per_s": arith * points_per_s, "peak_lane_ops_per_s": FP64_LANE_OPS_PER_S,
-            "frac_arith": arith * points_per_s / FP64_LANE_OPS_PER_S,
+            "arith_ops_per_s": arith * points_per_s, "peak_lane_ops_per_s": fp64_lane_rate(),
+            "frac_arith": arith * points_per_s / fp64_lane_rate(),
             "form": "FP64 fused kernel (k_het_fused<FP64>)",
-            "peak_source": "nominal (148 SMs x 64 FP64 lanes x 1965 MHz); cross-check: ncu FP64 pipe % in profiles/"}
+            "peak_source": "nominal (the device's SMs x 64 FP64 lanes x 1965 MHz); cross-check: ncu FP64 pipe % in profiles/"}
 
 
 def grad_metric(args):
