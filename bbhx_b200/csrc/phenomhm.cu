@@ -45,25 +45,41 @@ __global__ void k_ringdown_d(double* fring, double* fdamp, const double* m1, con
 }
 
 // ------------------------------------------------------------------ per-mode setup
-__global__ void k_phm_setup(ModeCoeffs* coeffs, const int* ells, const int* mms,
-                            const double* m1_SI, const double* m2_SI, const double* chi1,
-                            const double* chi2, const double* dist, const double* Mf_RD_lm,
-                            const double* Mf_DM_lm, int M, int B, int run_phenomd) {
-  long long n = (long long)B * M;
-  int add = run_phenomd ? 0 : 1;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
-       t += (long long)gridDim.x * blockDim.x) {
-    int b = (int)(t / M), i = (int)(t % M);
-    const double* rd = Mf_RD_lm + (long long)b * (M + add);
-    const double* dm = Mf_DM_lm + (long long)b * (M + add);
-    double rd22 = run_phenomd ? rd[0] : rd[M];
-    double dm22 = run_phenomd ? dm[0] : dm[M];
-    int ell = run_phenomd ? 2 : ells[i];
-    int mm = run_phenomd ? 2 : mms[i];
-    ModeCoeffs c;
-    phm_setup_mode(c, m1_SI[b], m2_SI[b], chi1[b], chi2[b], dist[b], ell, mm, rd[i], dm[i], rd22,
-                   dm22, run_phenomd);
-    coeffs[t] = c;
+// The records of a block's threads are staged in shared memory and written out as one
+// contiguous run with 16-byte stores: written straight from each thread, the 848-byte records
+// at an 848-byte stride made every warp store touch 32 cache lines.
+constexpr int kSetupThreads = 32;
+static_assert(sizeof(ModeCoeffs) % 16 == 0, "records are copied in 16-byte words");
+__global__ void __launch_bounds__(kSetupThreads)
+    k_phm_setup(ModeCoeffs* coeffs, const int* ells, const int* mms, const double* m1_SI,
+                const double* m2_SI, const double* chi1, const double* chi2, const double* dist,
+                const double* Mf_RD_lm, const double* Mf_DM_lm, int M, int B, int run_phenomd) {
+  __shared__ __align__(16) ModeCoeffs stage[kSetupThreads];
+  const long long n = (long long)B * M;
+  const int add = run_phenomd ? 0 : 1;
+  for (long long base = (long long)blockIdx.x * kSetupThreads; base < n;
+       base += (long long)gridDim.x * kSetupThreads) {
+    const long long t = base + threadIdx.x;
+    if (t < n) {
+      const int b = (int)(t / M), i = (int)(t % M);
+      const double* rd = Mf_RD_lm + (long long)b * (M + add);
+      const double* dm = Mf_DM_lm + (long long)b * (M + add);
+      const double rd22 = run_phenomd ? rd[0] : rd[M];
+      const double dm22 = run_phenomd ? dm[0] : dm[M];
+      const int ell = run_phenomd ? 2 : ells[i];
+      const int mm = run_phenomd ? 2 : mms[i];
+      ModeCoeffs c;
+      phm_setup_mode(c, m1_SI[b], m2_SI[b], chi1[b], chi2[b], dist[b], ell, mm, rd[i], dm[i],
+                     rd22, dm22, run_phenomd);
+      stage[threadIdx.x] = c;
+    }
+    __syncthreads();
+    const int cnt = (int)min((long long)kSetupThreads, n - base);
+    const int words = cnt * (int)(sizeof(ModeCoeffs) / 16);
+    const uint4* src = reinterpret_cast<const uint4*>(stage);
+    uint4* dst = reinterpret_cast<uint4*>(coeffs + base);
+    for (int w = threadIdx.x; w < words; w += kSetupThreads) dst[w] = src[w];
+    __syncthreads();
   }
 }
 
@@ -266,9 +282,9 @@ int bbhx_waveform_amp_phase(double* waveform_out, const int* ells, const int* mm
   ModeCoeffs* c = nullptr;
   int st = alloc_coeffs(&c, nbm, s);
   if (st) return st;
-  k_phm_setup<<<grid_for(nbm, 128), 128, 0, s>>>(c, ells, mms, m1_SI, m2_SI, chi1z, chi2z,
-                                                  distance, Mf_RD_lm, Mf_DM_lm, num_modes,
-                                                  num_bin_all, run_phenomd);
+  k_phm_setup<<<grid_for(nbm, kSetupThreads), kSetupThreads, 0, s>>>(
+      c, ells, mms, m1_SI, m2_SI, chi1z, chi2z, distance, Mf_RD_lm, Mf_DM_lm, num_modes,
+      num_bin_all, run_phenomd);
   st = launch_status("k_phm_setup");
   if (!st) {
     long long n = nbm * length;
@@ -319,9 +335,9 @@ int bbhx_waveform_amp_phase_noalloc(double* waveform_out, const int* ells, const
   int st = noalloc_records(&c);
   if (st) return st;
   cudaStream_t s = (cudaStream_t)stream;
-  k_phm_setup<<<grid_for(nbm, 128), 128, 0, s>>>(c, ells, mms, m1_SI, m2_SI, chi1z, chi2z,
-                                                  distance, Mf_RD_lm, Mf_DM_lm, num_modes,
-                                                  num_bin_all, run_phenomd);
+  k_phm_setup<<<grid_for(nbm, kSetupThreads), kSetupThreads, 0, s>>>(
+      c, ells, mms, m1_SI, m2_SI, chi1z, chi2z, distance, Mf_RD_lm, Mf_DM_lm, num_modes,
+      num_bin_all, run_phenomd);
   st = launch_status("k_phm_setup");
   if (st) return st;
   long long n = nbm * length;
@@ -338,8 +354,9 @@ int bbhx_phenomhm_setup(void* coeffs, const int* ells, const int* mms, const dou
                         int num_modes, int num_bin_all, int run_phenomd, void* stream) {
   BBHX_REQUIRE(num_modes > 0 && num_modes <= MAX_MODES, "num_modes must be 1..6");
   if (num_bin_all == 0) return OK;
+  BBHX_REQUIRE(((uintptr_t)coeffs & 15) == 0, "coeffs must be 16-byte aligned");
   long long nbm = (long long)num_bin_all * num_modes;
-  k_phm_setup<<<grid_for(nbm, 128), 128, 0, (cudaStream_t)stream>>>(
+  k_phm_setup<<<grid_for(nbm, kSetupThreads), kSetupThreads, 0, (cudaStream_t)stream>>>(
       (ModeCoeffs*)coeffs, ells, mms, m1_SI, m2_SI, chi1z, chi2z, distance, Mf_RD_lm, Mf_DM_lm,
       num_modes, num_bin_all, run_phenomd);
   return launch_status("k_phm_setup");

@@ -121,9 +121,9 @@ int bbhx_waveform_amp_phase_noalloc(double *waveform_out, const int *ells, const
                                     int length, int num_bin_all, const double *Mf_RD_lm,
                                     const double *Mf_DM_lm, int run_phenomd, void *stream);
 
-/* split form of waveform_amp_phase: per-(binary, mode) records (B*M * bbhx_mode_coeffs_bytes()),
- * then per-frequency evaluation with the t_ref shift of phenomhm.py:485-507 fused (t_ref may
- * be NULL), or t(f) alone */
+/* split form of waveform_amp_phase: per-(binary, mode) records (B*M * bbhx_mode_coeffs_bytes(),
+ * coeffs 16-byte aligned, else status 1), then per-frequency evaluation with the t_ref shift
+ * of phenomhm.py:485-507 fused (t_ref may be NULL), or t(f) alone */
 int bbhx_phenomhm_setup(void *coeffs, const int *ells, const int *mms, const double *m1_SI,
                         const double *m2_SI, const double *chi1z, const double *chi2z,
                         const double *distance, const double *Mf_RD_lm, const double *Mf_DM_lm,
@@ -279,8 +279,8 @@ typedef struct {
 
 /* Several direct-likelihood problems (uneven grid lengths, mode sets and observation spans) in
    ONE persistent launch of the fused kernel; no reference counterpart.  groups is a HOST array
-   of num_groups <= 64 descriptors; tile_bins (multiple of 128, at most 4096) and ctas_per_sm are the launch
-   shape (chosen by bbhx_b200.uneven.Autotuner).  Stream-ordered and free of host
+   of num_groups <= 64 descriptors; tile_bins (multiple of 128, at most 4096) and ctas_per_sm
+   are the launch shape (chosen by bbhx_b200.uneven.Autotuner).  Stream-ordered and free of host
    synchronisation, so it can be captured in a CUDA graph. */
 int bbhx_direct_like_multi(const bbhx_direct_group *groups, int num_groups, int precision,
                            int tile_bins, int ctas_per_sm, void *stream);
