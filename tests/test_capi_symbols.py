@@ -112,3 +112,19 @@ def test_descriptor_layouts_match_the_header(tmp_path):
         assert got[(cname, "size")] == ctypes.sizeof(py), cname
         for fname, _ in py._fields_:
             assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
+
+
+def test_misaligned_record_buffer_is_refused():
+    """bbhx_phenomhm_setup writes its records with 16-byte stores: a buffer that is not 16-byte
+    aligned is refused with status 1 before anything is launched (no GPU needed)."""
+    from bbhx_b200 import build_ext
+
+    build_ext.build()
+    lib = ctypes.CDLL(build_ext.OUT)
+    f = lib.bbhx_phenomhm_setup
+    f.argtypes = [ctypes.c_void_p] * 10 + [ctypes.c_int] * 3 + [ctypes.c_void_p]
+    f.restype = ctypes.c_int
+    args = [None] * 9 + [6, 1, 0, None]
+    assert f(ctypes.c_void_p((1 << 20) + 8), *args) == 1
+    lib.bbhx_last_error_string.restype = ctypes.c_char_p
+    assert b"aligned" in lib.bbhx_last_error_string()
