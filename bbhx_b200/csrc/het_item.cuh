@@ -389,12 +389,15 @@ __device__ __forceinline__ void het_bin(const HetArgs& A, int j, int ch, cplx cu
 // Response-mode records of walkers [0, B) of A into A.rmodes (one thread per (walker, mode)),
 // set up once per evaluation outside the walker loop: inlined there, the set-up's code and
 // registers slow the per-point loop down.
-__device__ __forceinline__ void het_response_setup(const HetArgs& A, long long t) {
+__device__ __forceinline__ ResponseMode het_response_record(const HetArgs& A, long long t) {
   const int b = (int)(t / A.M), i = (int)(t % A.M);
   ResponseMode r;
   response_mode_setup(r, A.ells[i], A.mms[i], A.phi_ref[b], A.inc[b], A.lam[b], A.beta[b],
                       A.psi[b]);
-  const_cast<ResponseMode*>(A.rmodes)[t] = r;
+  return r;
+}
+__device__ __forceinline__ void het_response_setup(const HetArgs& A, long long t) {
+  const_cast<ResponseMode*>(A.rmodes)[t] = het_response_record(A, t);
 }
 
 // Walker b of A by one warp in its slice W (HetSmemLayout(M, L, FULL)): records staged

@@ -38,12 +38,26 @@ int take_nonfinite_heterodyne(cudaStream_t s, unsigned* any) {
 }
 
 // ------------------------------------------------------------------ fused kernel
-// Response-mode records of the walkers (thread per (walker, mode)).
-__global__ void k_het_response_setup(HetArgs A) {
+// Response-mode records of the walkers (thread per (walker, mode)), staged in shared memory
+// per block of 32 and written out as one contiguous run of 8-byte words (each thread's 168-byte
+// record stored directly made every warp store touch ~40 cache lines).
+constexpr int kRespSetupThreads = 32;
+__global__ void __launch_bounds__(kRespSetupThreads) k_het_response_setup(HetArgs A) {
+  __shared__ ResponseMode stage[kRespSetupThreads];
   const long long n = (long long)A.B * A.M;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
-       t += (long long)gridDim.x * blockDim.x)
-    het_response_setup(A, t);
+  for (long long base = (long long)blockIdx.x * kRespSetupThreads; base < n;
+       base += (long long)gridDim.x * kRespSetupThreads) {
+    const long long t = base + threadIdx.x;
+    if (t < n) stage[threadIdx.x] = het_response_record(A, t);
+    __syncwarp();
+    const int cnt = (int)min((long long)kRespSetupThreads, n - base);
+    const int words = cnt * (int)(sizeof(ResponseMode) / 8);
+    const unsigned long long* src = reinterpret_cast<const unsigned long long*>(stage);
+    unsigned long long* dst =
+        reinterpret_cast<unsigned long long*>(const_cast<ResponseMode*>(A.rmodes) + base);
+    for (int w = threadIdx.x; w < words; w += kRespSetupThreads) dst[w] = src[w];
+    __syncwarp();
+  }
 }
 
 // One WARP per walker (het_item, het_item.cuh), each warp with its own slice of shared memory:
@@ -91,7 +105,8 @@ int launch_het(HetArgs A, cudaStream_t s) {
   BBHX_CHECK_CUDA(pool_alloc_all(s, {{(void**)&rm, sizeof(ResponseMode) * (size_t)A.B * A.M},
                                      {(void**)&next, sizeof(unsigned long long)}}));
   A.rmodes = rm;
-  k_het_response_setup<<<grid_for((long long)A.B * A.M, 128), 128, 0, s>>>(A);
+  k_het_response_setup<<<grid_for((long long)A.B * A.M, kRespSetupThreads), kRespSetupThreads,
+                         0, s>>>(A);
   st = launch_status("k_het_response_setup");
   if (!st)
     st = cuda_status(cudaFuncSetAttribute(k_het_fused<MIXED, GH>,

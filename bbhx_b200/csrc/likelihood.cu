@@ -487,12 +487,15 @@ struct alignas(16) WarpStage {
 // with R = e^{i Delta}, Q = e^{i Delta^2}, P = e^{i Delta^3} the first, second and (constant)
 // third differences of the phase cubic.  Three FP64 complex products per bin replace the
 // per-bin phase cubic, range reduction and polynomial sine / cosine.  The state is re-anchored
-// (rot_anchor) at the first chunk of a segment and every kRecChunks chunks; the anchor phase is
+// (rot_anchor) at a mode's first chunk of a work item and wherever the chunk's segment changes;
+// an item holds at most kRecChunks chunks, so no lane runs more than kRecChunks * FD_K steps
+// from its anchor.  The anchor phase is
 // evaluated at the bin's exact frequency k df (error-free product) with a compensated final sum,
 // so it carries < 1e-13 rad instead of the ~ulp(phi) ~ 1e-10 - 1e-9 rad of a plain FP64
 // evaluation, and the products add ~2e-11 rad over the kRecChunks * FD_K = 128 steps between
 // anchors (bounded by the self-test against 50-digit phases: k_selftest_recurrence).
-constexpr int kRecChunks = 32;  // chunks (of FD_K steps per lane) between anchors
+constexpr int kRecChunks = 32;  // chunks (of FD_K steps per lane) between anchors, at most
+static_assert(FD_MAXCHUNK <= kRecChunks, "a work item must not run the recurrence longer");
 
 struct Rot {
   double er, ei, rr, ri, qr, qi, pr, pi;
@@ -682,13 +685,12 @@ __device__ __forceinline__ void accumulate_bin_src(const Src& src, double f, dou
 }
 
 // Per-warp recurrence state: E, R, Q of every (mode, lane), P per mode and, per mode, the chunk
-// and segment the saved state belongs to and the chunks left before the next anchor.
+// and segment the saved state belongs to.
 struct alignas(16) RecStage {
   double2 st[FD_MAXM][3][32];  // E, R, Q of every lane
   double2 P[FD_MAXM];          // e^{i Delta^3}: the same for every lane of a segment
   int next_chunk[FD_MAXM];
   int seg[FD_MAXM];
-  int left[FD_MAXM];
 };
 
 // G bins of one lane that lie in the same spline segment: the same arithmetic as
@@ -799,15 +801,14 @@ __device__ __forceinline__ void load_seg(SegCoef<R>& cf, const WarpStage<R>& S, 
 
 // One (chunk, mode) on the phase recurrence: staged segment kl (global segment kg of the mode's
 // grid) holds every support bin of the chunk.  The saved state is continued when this mode's
-// previous chunk was the one before, in the same segment, and fewer than kRecChunks chunks
-// ago; otherwise it is re-anchored at this lane's first bin.
+// previous chunk of the item was the one before, in the same segment; otherwise it is
+// re-anchored at this lane's first bin.
 template <typename R>
 __device__ __forceinline__ void rec_chunk_mode(const WarpStage<R>& S, RecStage* RS, int m, int kl,
                                                int kg, int gate, int ck, int c0, int lane,
                                                const double* fbin, double ts, double te,
                                                R (*acc)[6], double gk0, double gdf, double hstep) {
-  const int nc = RS->next_chunk[m], sg = RS->seg[m], left = RS->left[m];
-  const bool cont = (nc == ck) && (sg == kg) && (left > 0);
+  const bool cont = (RS->next_chunk[m] == ck) && (RS->seg[m] == kg);
   Rot z;
   if (cont) {
     const double2 e = RS->st[m][0][lane], r = RS->st[m][1][lane];
@@ -829,7 +830,6 @@ __device__ __forceinline__ void rec_chunk_mode(const WarpStage<R>& S, RecStage* 
   if (lane == 0) {
     RS->next_chunk[m] = ck + 1;
     RS->seg[m] = kg;
-    RS->left[m] = cont ? left - 1 : kRecChunks - 1;
     RS->P[m] = pnew;  // every lane's P of the segment is bitwise the same
   }
   __syncwarp();
@@ -1323,7 +1323,7 @@ __global__ void k_het_response_setup_multi(const HetMulti* __restrict__ HM, long
 
 // An uneven batch in ONE persistent launch: the walkers of every heterodyned problem (one
 // warp item each, het_item) followed by the (tile, binary) items of every direct problem
-// (fused_item), enumerated as one range that the warps stride through.  Each warp owns a
+// (fused_item), enumerated as one range from which the warps claim items (claim_item).  Each warp owns a
 // shared-memory slot of `slot` bytes that holds either a direct item's staged segments (and
 // recurrence state) or a walker's records and residual strip; the problem's argument block is
 // copied to shared memory when the warp moves to another problem.  HET = false compiles the
